@@ -1,0 +1,403 @@
+"""Benchmark of the phase2 state-vector hot path on B200.
+
+Metric: Pauli-rotation x amplitudes per second (and HBM GB/s) at 30 qubits,
+FP32 state with FP64 arithmetic ("FP32-batched": fused passes) against the
+plain FP64 path (one rotation per pass), on the qDRIFT workload: 30 qubits,
+100,000 Jordan-Wigner-like terms (seeded synthetic, phase2_b200.workloads),
+4096 draws per sample, step_size 1e-3.
+
+A step is one qDRIFT sample through the library's C-ABI driver
+(qdrift_simul): state prep, 4096 rotations, overlap.  ``value`` is timed
+with CUDA events recorded on the register's own stream; ``e2e`` is the same
+steps timed around the host call (host-side sampling and planning, record
+upload, overlap download included).  The 8 GiB state is larger than L2, so
+no L2 flush is needed between steps.
+
+Multi-GPU (torchrun): each rank runs independent qDRIFT samples of its own
+seed on its own GPU (replicas, weak scaling); no data-path collective.
+Timing is the max over ranks.
+
+``--impl reference`` times the reference's own CPU path (oracle/_ref,
+qreg_paulirot compiled from the reference sources) on the host cores.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = ("Pauli-rot·amplitudes/s and HBM GB/s at 30 qb: FP32-batched "
+          "vs FP64 plain")
+UNIT = "rot·amp/s"
+
+
+def _peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.is_file():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+class Clocks:
+    """Samples nvidia-smi every 200 ms while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,"
+         "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev: int):
+        self.dev = dev
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def _max_over_ranks(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(ws: int) -> None:
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---- the GPU arm -------------------------------------------------------
+
+
+def _qdrift_obj(p2, cfg, prec, fusion, seed):
+    """Build a one-sample qDRIFT driver through the C-ABI."""
+    from phase2_b200 import _ffi
+    L = p2.lib()
+    p2.set_precision(prec)
+    hm, md = p2._hamil(cfg["nqb"], cfg["terms"]), p2._muldet(cfg["dets"])
+    obj = _ffi.Qdrift()
+    dt = _ffi.QdriftData(1, cfg["depth"], cfg["step_size"], seed)
+    if L.qdrift_init(C.byref(obj), C.byref(dt), hm, _ffi.STPREP_MULTIDET,
+                     C.cast(C.pointer(md), C.c_void_p), None) != 0:
+        raise RuntimeError("qdrift_init failed")
+    L.qreg_set_fusion(C.byref(obj.ct.reg), *fusion)
+    return obj
+
+
+def _run_steps(p2, obj, steps: int, timing: bool):
+    """Run `steps` samples; return (device_ms, wall_s, stats delta, z)."""
+    import torch
+    L = p2.lib()
+    reg = C.byref(obj.ct.reg)
+    L.qreg_set_timing(reg, int(timing))
+    stream = torch.cuda.ExternalStream(L.qreg_stream(reg))
+    L.qreg_reset_stats(reg)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    w0 = time.perf_counter()
+    ev0.record(stream)
+    zs = []
+    for _ in range(steps):
+        if L.qdrift_simul(C.byref(obj)) != 0:
+            raise RuntimeError("qdrift_simul failed")
+        zs.append(complex(obj.ct.vals.z[0], obj.ct.vals.z[1]))
+    ev1.record(stream)
+    ev1.synchronize()
+    wall = time.perf_counter() - w0
+    st = _ffi_stats(p2, obj)
+    return ev0.elapsed_time(ev1), wall, st, zs
+
+
+def _ffi_stats(p2, obj):
+    from phase2_b200 import _ffi
+    st = _ffi.Stats()
+    p2.lib().qreg_get_stats(C.byref(obj.ct.reg), C.byref(st))
+    return {k: getattr(st, k) for k, _ in _ffi.Stats._fields_}
+
+
+def _traffic_per_launch():
+    p = ROOT / "profiles" / "k_pass_traffic.json"
+    if p.is_file():
+        try:
+            return json.loads(p.read_text()).get("bytes_per_launch_30q_fp32")
+        except (ValueError, KeyError):
+            return None
+    return None
+
+
+def _cpu_baseline(nrot: int = 8, reps: int = 2, max_qb: int = 25) -> dict:
+    """Reference CPU qreg_paulirot on R processes x one 2^(30-log2 R) slab.
+
+    R is the largest power of two <= the host's cores (at most 128); each
+    process holds one rank's share of the 30-qubit state (capped at
+    2^max_qb amplitudes to bound the sample to tens of seconds)."""
+    exe = ROOT / "oracle" / "_ref" / "ref_bench"
+    if not exe.is_file():
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                "sample": "oracle/_ref/ref_bench not built"}
+    cores = os.cpu_count() or 1
+    R = 1 << int(math.log2(max(1, min(cores, 128))))
+    qb = min(max(16, 30 - int(math.log2(R))), max_qb)
+    procs = [subprocess.Popen([str(exe), str(qb), str(nrot), str(reps)],
+                              stdout=subprocess.PIPE,
+                              stderr=subprocess.DEVNULL, text=True)
+             for _ in range(R)]
+    rates = []
+    for p in procs:
+        out, _ = p.communicate(timeout=600)
+        try:
+            rates.append(float(out.split()[-1]))
+        except (IndexError, ValueError):
+            pass
+    total = sum(rates)
+    return {"value": total, "unit": UNIT, "cores": len(rates),
+            "kind": "reference",
+            "sample": (f"{len(rates)} processes x reference qreg_paulirot "
+                       f"(CPU backend, 1 rank each) on a {qb}-qubit slab, "
+                       f"{nrot} JW-like rotations, min of {reps}; each process "
+                       f"is one rank's share of the 30-qubit state; the "
+                       f"partner exchange is omitted (upper bound)")}
+
+
+def gpu_arm(args) -> None:
+    ws, rank, local = _dist()
+    import torch
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(
+            seconds=300))
+    import phase2_b200 as p2
+    from phase2_b200 import workloads
+    p2.world_ensure()
+    cfg = workloads.qdrift30(nqb=args.nqb, depth=args.depth)
+    nqb, depth = cfg["nqb"], cfg["depth"]
+    namp = 1 << nqb
+    seed = cfg["seed"] + 1000003 * rank
+
+    # headline: FP32 state, fused passes
+    obj = _qdrift_obj(p2, cfg, p2.PREC_FP32, (5, 0), seed)
+    try:
+        _run_steps(p2, obj, args.warmup, timing=False)
+        _barrier(ws)
+        torch.cuda.synchronize()
+        with Clocks(local) as clk:
+            dev_ms, wall, st, zs = _run_steps(p2, obj, args.steps,
+                                              timing=False)
+        _barrier(ws)
+        # per-launch kernel timing in a separate, untimed step
+        _, _, st_t, _ = _run_steps(p2, obj, 1, timing=True)
+    finally:
+        p2.lib().qdrift_free(C.byref(obj))
+    dev_ms = _max_over_ranks(dev_ms, ws)
+    wall = _max_over_ranks(wall, ws)
+    rot_amp = args.steps * depth * namp
+    value = ws * rot_amp / (dev_ms / 1e3)
+    e2e_value = ws * rot_amp / wall
+
+    # comparison arms on a bounded number of rotations (same sample shape)
+    cmp_depth = max(64, min(depth, args.cmp_depth))
+    cmp_cfg = dict(cfg, depth=cmp_depth)
+    arms = {}
+    for name, prec, fusion in (("fp64_plain", p2.PREC_FP64, (1, 1)),
+                               ("fp64_fused", p2.PREC_FP64, (5, 0)),
+                               ("fp32_plain", p2.PREC_FP32, (1, 1))):
+        if args.quick and name != "fp64_plain":
+            continue
+        o = _qdrift_obj(p2, cmp_cfg, prec, fusion, seed + 7)
+        try:
+            _run_steps(p2, o, 1, timing=False)
+            ms, _, s, _ = _run_steps(p2, o, 1, timing=True)
+        finally:
+            p2.lib().qdrift_free(C.byref(o))
+        ms = _max_over_ranks(ms, ws)
+        elem = 16 if prec == p2.PREC_FP64 else 8
+        arms[name] = {
+            "value": ws * cmp_depth * namp / (ms / 1e3), "unit": UNIT,
+            "rotations": cmp_depth,
+            "passes": s["passes"],
+            "kernel_gbs": (s["passes"] * 2 * namp * elem / 1e9) /
+            (s["pass_ms"] / 1e3) if s["pass_ms"] else None}
+    p2.set_precision(p2.PREC_FP64)
+
+    peaks = _peaks()
+    passes_per_step = st["passes"] / args.steps
+    launch_ms = st_t["pass_ms"] / max(1, st_t["timed_passes"])
+    bytes_per_launch = 2 * namp * 8
+    achieved = bytes_per_launch / (launch_ms / 1e3) / 1e9
+    hbm_gbs_step = passes_per_step * bytes_per_launch / (
+        dev_ms / args.steps / 1e3) / 1e9
+    cpu = _cpu_baseline() if (rank == 0 and ws == 1 and not args.quick) \
+        else None
+    if rank != 0:
+        return
+    clocks = clk.summary()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "storage": "complex64 state (f32), f64 rotation arithmetic",
+        "data": "synthetic (seeded JW-like Hamiltonian, no dataset)",
+        "config": {
+            "workload": (f"qdrift {nqb} qubits, {len(cfg['terms'])} JW "
+                         f"terms, {depth} draws per sample, FP32 state, "
+                         f"fused passes"),
+            "nqb": nqb, "terms": len(cfg["terms"]), "depth": depth,
+            "step": "one qDRIFT sample: prepst + rotations + overlap",
+            "l2": f"inputs larger than L2 ({namp * 8 / 2**30:.0f} GiB state)",
+            "parallelism": f"replicas x{ws} (independent samples)"},
+        "hbm_gbs": hbm_gbs_step,
+        "passes_per_step": passes_per_step,
+        "rotations_per_pass": depth / passes_per_step,
+        "roofline": {"bound": "hbm", "achieved": achieved,
+                     "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"],
+                     "peak_source": peaks["source"],
+                     "kernel": "k_pass<M,float2,false>",
+                     "bytes_per_launch": bytes_per_launch,
+                     "launch_ms": launch_ms,
+                     "traffic": _traffic_per_launch()},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": UNIT,
+                "h2d_bytes_per_step": st["h2d_bytes"] / args.steps,
+                "d2h_bytes_per_step": st["d2h_bytes"] / args.steps},
+        "gpu_launches": st["launches"],
+        "clocks": clocks,
+        "comparison": arms,
+        "fp32_fused_vs_fp64_plain": (value / arms["fp64_plain"]["value"]
+                                     if arms.get("fp64_plain") else None),
+        "overlaps": [[z.real, z.imag] for z in zs[:2]],
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---- the reference arm -------------------------------------------------
+
+
+def reference_arm(args) -> None:
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return
+    exe = ROOT / "oracle" / "_ref" / "ref_bench"
+    if not exe.is_file():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/ref_bench was not built (reference "
+                          "sources absent at build time)"}), flush=True)
+        return
+    for _ in range(args.warmup):
+        _cpu_baseline(nrot=1, reps=1)
+    vals = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        vals.append(_cpu_baseline(nrot=4, reps=1))
+    elapsed = time.perf_counter() - t0
+    v = statistics.median(x["value"] for x in vals)
+    cb = dict(vals[0], value=v)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * elapsed / max(1, args.steps),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": (f"qdrift {args.nqb} qubits rotation sweep "
+                                "(reference CPU qreg_paulirot)"),
+                   "nqb": args.nqb},
+        "cpu_baseline": cb,
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nqb", type=int, default=30)
+    ap.add_argument("--depth", type=int, default=4096)
+    ap.add_argument("--cmp-depth", type=int, default=512)
+    ap.add_argument("--quick", action="store_true",
+                    help="skip the CPU baseline and secondary arms")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,175 @@
+#ifndef PHASE2_B200_H
+#define PHASE2_B200_H
+
+/*
+ * Extensions of this B200 library beyond the phase2 C surface.  None of
+ * these has a counterpart in Quantum-for-Life/phase2; code written against
+ * the reference headers never needs them.  They select the state precision,
+ * the fusion policy and the term order, expose bulk state access, device
+ * reductions and counters, and the planner used by qreg_paulirot.
+ */
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "phase2/circ.h"
+#include "phase2/qreg.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- precision ---------------------------------------------------------- */
+
+/* FP64: complex128 state, rotations bit-identical to the reference CPU
+ * path.  FP32: complex64 state (half the HBM bytes per sweep); cos/sin,
+ * the rotation arithmetic inside a pass, norms and overlaps stay FP64, and
+ * each amplitude is rounded to FP32 once per pass. */
+enum phase2_prec {
+	PHASE2_PREC_FP64 = 0,
+	PHASE2_PREC_FP32 = 1,
+};
+
+/* Process default used by qreg_init (hence circ_init and the drivers).
+ * Initial value: FP64, or the PHASE2_PRECISION environment variable
+ * ("fp32"/"fp64") read at world_init.  Returns 0 or -1. */
+int phase2_set_precision(int prec);
+int phase2_get_precision(void);
+
+/* qreg_init at an explicit precision. */
+int qreg_init_prec(struct qreg *reg, uint32_t nqb, int prec);
+int qreg_precision(const struct qreg *reg);
+
+/* ---- fusion policy ------------------------------------------------------ */
+
+/* A pass streams the state once and applies a run of consecutive rotations
+ * whose flip masks span a space of dimension <= max_span (each thread owns
+ * whole cosets of that space in registers).  max_span in [1,5];
+ * max_rots caps rotations per pass (1 = one rotation per pass, the unfused
+ * "plain" path; 0 = no cap beyond the per-pass limit).  Defaults 5 and 0.
+ * The process default applies to registers created afterwards. */
+int phase2_set_fusion(int max_span, int max_rots);
+int qreg_set_fusion(struct qreg *reg, int max_span, int max_rots);
+
+/* ---- term order --------------------------------------------------------- */
+
+/* Order used by trott_init / trott2_init and the deterministic part of
+ * cmpsit_init.  LEX (default) is the reference's lexicographic sort and
+ * keeps results identical to it; GIVEN keeps the caller's order; FLIP
+ * sorts by flip mask (stable), which groups terms that fuse into one pass
+ * but changes the product formula. */
+enum phase2_order {
+	PHASE2_ORDER_LEX = 0,
+	PHASE2_ORDER_GIVEN = 1,
+	PHASE2_ORDER_FLIP = 2,
+};
+int phase2_set_term_order(int order);
+int phase2_get_term_order(void);
+
+/* Stable sort by (flip mask, phase mask). */
+void circ_hamil_sort_flip(struct circ_hamil *hm);
+
+/* ---- execution control and bulk access ---------------------------------- */
+
+/* Launch all queued rotations (asynchronously).  0 or -1. */
+int qreg_flush(struct qreg *reg);
+
+/* Flush and wait for the register's stream.  0, or -1 if a CUDA error was
+ * raised on it. */
+int qreg_synchronize(struct qreg *reg);
+
+/* Batched amplitude access (one launch and one copy each way). */
+int qreg_getamps(struct qreg *reg, const uint64_t *idx, _Complex double *z,
+	size_t n);
+int qreg_setamps(struct qreg *reg, const uint64_t *idx,
+	const _Complex double *z, size_t n);
+
+/* Whole state as interleaved FP64 re/im (2 * namp doubles). */
+int qreg_get_state(struct qreg *reg, double *out);
+int qreg_set_state(struct qreg *reg, const double *in);
+
+/* sum |a_i|^2 in FP64 on the device: warp-shuffle tree per block, blocks
+ * combined with compensated (Neumaier) summation.  0 or -1. */
+int qreg_norm2(struct qreg *reg, double *out);
+
+/* <trial|psi> for a dense FP64 trial state given in host memory
+ * (2 * namp doubles), reduced on the device like qreg_norm2. */
+int qreg_inner_dense(struct qreg *reg, const double *trial, double out[2]);
+
+/* ---- counters ----------------------------------------------------------- */
+
+struct phase2_stats {
+	uint64_t rotations; /* rotations executed */
+	uint64_t passes;    /* state sweeps (pass kernels) */
+	uint64_t launches;  /* kernels launched by this library */
+	uint64_t bytes;     /* algorithmic HBM bytes: 2 * namp * elem per pass */
+	uint64_t timed_passes;
+	double pass_ms;     /* device time of timed pass launches (CUDA events) */
+	uint64_t h2d_bytes; /* host-to-device bytes copied for this register */
+	uint64_t d2h_bytes; /* device-to-host bytes copied for this register */
+};
+
+int qreg_get_stats(const struct qreg *reg, struct phase2_stats *st);
+void qreg_reset_stats(struct qreg *reg);
+
+/* Record CUDA events around each flush's pass launches on the register's
+ * stream and accumulate their elapsed time into pass_ms. */
+int qreg_set_timing(struct qreg *reg, int on);
+
+/* The cudaStream_t (as void *) on which all work of this register runs,
+ * for callers that record CUDA events around library calls. */
+void *qreg_stream(const struct qreg *reg);
+
+/* ---- planner (host) ----------------------------------------------------- */
+
+/* One rotation exp(i phi P) with P = (flip, phase). */
+struct phase2_rot_in {
+	uint64_t flip, phase;
+	double phi;
+};
+
+/* Pass descriptor as executed by the device.  Slot u of a thread with
+ * representative x (x has zeros at the pivot bits) is amplitude
+ * x ^ (xor of basis[k] over the set bits k of u). */
+#define PHASE2_MAX_SPAN 5
+struct phase2_pass {
+	uint32_t span;     /* M: slots per thread = 2^M */
+	uint32_t nrot;     /* rotations in this pass */
+	uint32_t rot_off;  /* first rotation record */
+	uint8_t piv[PHASE2_MAX_SPAN]; /* pivot bits, ascending */
+	uint8_t pad[3];
+	uint64_t basis[PHASE2_MAX_SPAN];
+};
+
+/* Rotation record in slot coordinates: the partner of slot u is u ^ U; the
+ * sign bit of slot u for a thread with representative x is
+ * bit u of smask XOR parity(x & z); odd = 1 multiplies the partner by i. */
+struct phase2_rot_rec {
+	uint64_t z;
+	double c, s;
+	uint32_t smask;
+	uint16_t U;
+	uint8_t odd;
+	uint8_t pad;
+};
+
+/* Plan n rotations for an nqb-qubit register.  Writes at most n passes and
+ * n records; returns the number of passes, or -1. */
+long phase2_plan(uint32_t nqb, const struct phase2_rot_in *rots, size_t n,
+	int max_span, int max_rots, struct phase2_pass *passes,
+	struct phase2_rot_rec *recs);
+
+/* ---- misc --------------------------------------------------------------- */
+
+const char *phase2_version(void);
+
+/* sizeof of public structs, for FFI layout checks: 0 qreg, 1 circ, 2 trott,
+ * 3 trott2, 4 qdrift, 5 cmpsit, 6 circ_hamil_term, 7 phase2_pass,
+ * 8 phase2_rot_rec, 9 phase2_stats; 0 for unknown ids. */
+size_t phase2_sizeof(int which);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PHASE2_B200_H */

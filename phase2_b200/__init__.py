@@ -1,0 +1,338 @@
+"""B200-native phase2 state-vector hot path (Python side).
+
+``run`` is the drop-in for the phase2 Python entry point
+(python/phase2/__init__.py:71-124 of Quantum-for-Life/phase2): same
+arguments, same return type, same ``ValueError`` on bad input.  It calls
+``phase2_run`` in this package's ``libphase2.so`` (sm_100a kernels).
+
+The other helpers drive the library's C surface (register, circuit
+drivers, planner) for tests and benchmarks.  All computation happens in
+libphase2.so on the GPU; nothing here computes amplitudes.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _ffi
+from ._ffi import lib
+
+__all__ = ["run", "world_ensure", "Register", "Terms", "Dets", "trott",
+           "trott2", "qdrift", "cmpsit", "plan", "set_precision",
+           "set_fusion", "set_term_order", "PREC_FP64", "PREC_FP32"]
+
+PREC_FP64 = _ffi.PREC_FP64
+PREC_FP32 = _ffi.PREC_FP32
+_WORLD_SEED = 0x2B200C0DE5EED001
+
+
+def world_ensure() -> None:
+    """Initialise the library world (CUDA device) once; raise if no GPU."""
+    L = lib()
+    if L.world_info(None) == _ffi.WORLD_READY:
+        return
+    if L.world_init(None, None, _WORLD_SEED) != _ffi.WORLD_READY:
+        raise RuntimeError("phase2 world_init failed (no usable CUDA "
+                           "device?)")
+
+
+def run(paulis: list[str], coeffs: list[float], delta: float,
+        psi: str) -> complex:
+    """<psi| prod_k exp(i*delta*coeffs[k]*P_k) |psi>, as phase2.run."""
+    nterms = len(paulis)
+    if nterms != len(coeffs):
+        raise ValueError(f"len(paulis)={nterms} != len(coeffs)="
+                         f"{len(coeffs)}")
+    L = lib()
+    c_paulis = (C.c_char_p * max(nterms, 1))(
+        *(s.encode("ascii") for s in paulis))
+    c_coeffs = (C.c_double * max(nterms, 1))(*coeffs)
+    out_re, out_im = C.c_double(0.0), C.c_double(0.0)
+    rc = L.phase2_run(c_paulis, c_coeffs, C.c_size_t(nterms),
+                      C.c_double(delta), psi.encode("ascii"),
+                      C.byref(out_re), C.byref(out_im))
+    if rc == -1:
+        raise ValueError("phase2_run returned -1: invalid input")
+    return complex(out_re.value, out_im.value)
+
+
+def set_precision(prec: int) -> None:
+    if lib().phase2_set_precision(prec) != 0:
+        raise ValueError(f"bad precision {prec}")
+
+
+def set_fusion(max_span: int, max_rots: int = 0) -> None:
+    if lib().phase2_set_fusion(max_span, max_rots) != 0:
+        raise ValueError("bad fusion setting")
+
+
+def set_term_order(order: int) -> None:
+    if lib().phase2_set_term_order(order) != 0:
+        raise ValueError("bad term order")
+
+
+# ---- inputs ------------------------------------------------------------
+
+
+@dataclass
+class Terms:
+    """Hamiltonian terms: flip/phase masks (uint64) and real coefficients."""
+    flip: np.ndarray
+    phase: np.ndarray
+    cf: np.ndarray
+
+    def __len__(self) -> int:
+        return len(self.cf)
+
+    def records(self) -> np.ndarray:
+        """24-byte records laid out as struct circ_hamil_term."""
+        rec = np.zeros(len(self), dtype=[("cf", "<f8"), ("flip", "<u8"),
+                                         ("phase", "<u8")])
+        rec["cf"], rec["flip"], rec["phase"] = self.cf, self.flip, self.phase
+        return rec
+
+
+@dataclass
+class Dets:
+    """Initial state sum_d cf_d |idx_d>."""
+    idx: np.ndarray
+    cf: np.ndarray  # complex128
+
+    def __len__(self) -> int:
+        return len(self.idx)
+
+
+def _hamil(nqb: int, terms: Terms) -> _ffi.CircHamil:
+    L = lib()
+    hm = _ffi.CircHamil()
+    if L.circ_hamil_init(C.byref(hm), nqb, len(terms)) != 0:
+        raise MemoryError("circ_hamil_init")
+    rec = terms.records()
+    if len(terms):
+        C.memmove(hm.terms, rec.ctypes.data, rec.nbytes)
+    return hm
+
+
+def _muldet(dets: Dets) -> _ffi.CircMuldet:
+    L = lib()
+    md = _ffi.CircMuldet()
+    if L.circ_muldet_init(C.byref(md), len(dets)) != 0:
+        raise MemoryError("circ_muldet_init")
+    rec = np.zeros(len(dets), dtype=[("idx", "<u8"), ("cf", "<c16")])
+    rec["idx"], rec["cf"] = dets.idx, dets.cf
+    if len(dets):
+        C.memmove(md.dets, rec.ctypes.data, rec.nbytes)
+    return md
+
+
+def _values(v: _ffi.CircValues) -> np.ndarray:
+    n = int(v.len)
+    arr = np.ctypeslib.as_array(v.z, shape=(2 * n,)) if n else np.zeros(0)
+    return arr.view(np.complex128).copy()
+
+
+# ---- register ----------------------------------------------------------
+
+
+class Register:
+    """A device-resident register (struct qreg) of nqb qubits."""
+
+    def __init__(self, nqb: int, prec: int | None = None):
+        world_ensure()
+        self._L = lib()
+        self.reg = _ffi.Qreg()
+        if prec is None:
+            rc = self._L.qreg_init(C.byref(self.reg), nqb)
+        else:
+            rc = self._L.qreg_init_prec(C.byref(self.reg), nqb, prec)
+        if rc != 0:
+            raise RuntimeError(f"qreg_init({nqb}) failed")
+        self.nqb = nqb
+
+    def close(self) -> None:
+        if self.reg.backend:
+            self._L.qreg_free(C.byref(self.reg))
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def precision(self) -> int:
+        return self._L.qreg_precision(C.byref(self.reg))
+
+    def set_state(self, amp: np.ndarray) -> None:
+        a = np.ascontiguousarray(amp, dtype=np.complex128)
+        if self._L.qreg_set_state(C.byref(self.reg),
+                                  a.ctypes.data_as(C.POINTER(C.c_double))):
+            raise RuntimeError("qreg_set_state failed")
+
+    def get_state(self) -> np.ndarray:
+        out = np.empty(1 << self.nqb, dtype=np.complex128)
+        if self._L.qreg_get_state(C.byref(self.reg),
+                                  out.ctypes.data_as(C.POINTER(C.c_double))):
+            raise RuntimeError("qreg_get_state failed")
+        return out
+
+    def zero(self) -> None:
+        self._L.qreg_zero(C.byref(self.reg))
+
+    def paulirot(self, flip, phase, phi, batch: int = 1024) -> None:
+        """qreg_paulirot with code_hi = identity, `batch` terms per call."""
+        flip = np.ascontiguousarray(flip, dtype=np.uint64)
+        phase = np.ascontiguousarray(phase, dtype=np.uint64)
+        phi = np.ascontiguousarray(phi, dtype=np.float64)
+        codes = np.empty((len(phi), 2), dtype=np.uint64)
+        codes[:, 0], codes[:, 1] = flip, phase
+        hi = _ffi.Paulis()
+        for k in range(0, len(phi), batch):
+            m = min(batch, len(phi) - k)
+            self._L.qreg_paulirot(
+                C.byref(self.reg), hi,
+                codes[k:].ctypes.data_as(C.POINTER(_ffi.Paulis)),
+                phi[k:].ctypes.data_as(C.POINTER(C.c_double)), m)
+
+    def getamps(self, idx) -> np.ndarray:
+        idx = np.ascontiguousarray(idx, dtype=np.uint64)
+        out = np.empty(len(idx), dtype=np.complex128)
+        if self._L.qreg_getamps(C.byref(self.reg),
+                                idx.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                out.ctypes.data_as(C.POINTER(C.c_double)),
+                                len(idx)):
+            raise RuntimeError("qreg_getamps failed")
+        return out
+
+    def setamps(self, idx, z) -> None:
+        idx = np.ascontiguousarray(idx, dtype=np.uint64)
+        z = np.ascontiguousarray(z, dtype=np.complex128)
+        if self._L.qreg_setamps(C.byref(self.reg),
+                                idx.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                z.ctypes.data_as(C.POINTER(C.c_double)),
+                                len(idx)):
+            raise RuntimeError("qreg_setamps failed")
+
+    def set_fusion(self, max_span: int, max_rots: int = 0) -> None:
+        if self._L.qreg_set_fusion(C.byref(self.reg), max_span, max_rots):
+            raise ValueError("qreg_set_fusion failed")
+
+    def synchronize(self) -> None:
+        if self._L.qreg_synchronize(C.byref(self.reg)):
+            raise RuntimeError("qreg_synchronize reported a CUDA error")
+
+    def norm2(self) -> float:
+        v = C.c_double()
+        if self._L.qreg_norm2(C.byref(self.reg), C.byref(v)):
+            raise RuntimeError("qreg_norm2 failed")
+        return v.value
+
+    def inner_dense(self, trial: np.ndarray) -> complex:
+        t = np.ascontiguousarray(trial, dtype=np.complex128)
+        out = (C.c_double * 2)()
+        if self._L.qreg_inner_dense(C.byref(self.reg),
+                                    t.ctypes.data_as(C.POINTER(C.c_double)),
+                                    out):
+            raise RuntimeError("qreg_inner_dense failed")
+        return complex(out[0], out[1])
+
+    def set_timing(self, on: bool) -> None:
+        self._L.qreg_set_timing(C.byref(self.reg), int(on))
+
+    def stats(self) -> dict:
+        st = _ffi.Stats()
+        self._L.qreg_get_stats(C.byref(self.reg), C.byref(st))
+        return {k: getattr(st, k) for k, _ in _ffi.Stats._fields_}
+
+    def reset_stats(self) -> None:
+        self._L.qreg_reset_stats(C.byref(self.reg))
+
+
+# ---- drivers -----------------------------------------------------------
+
+
+def _run_driver(kind: str, nqb: int, terms: Terms, dets: Dets, **kw):
+    world_ensure()
+    L = lib()
+    hm, md = _hamil(nqb, terms), _muldet(dets)
+    if kind in ("trott", "trott2"):
+        obj = (_ffi.Trott if kind == "trott" else _ffi.Trott2)()
+        dt = _ffi.TrottData(kw["steps"], kw["delta"])
+    elif kind == "qdrift":
+        obj = _ffi.Qdrift()
+        dt = _ffi.QdriftData(kw["samples"], kw["depth"], kw["step_size"],
+                             kw["seed"])
+    else:
+        obj = _ffi.Cmpsit()
+        dt = _ffi.CmpsitData(kw["samples"], kw["steps"], kw["length"],
+                             kw["depth"], kw["angle_det"], kw["angle_rand"],
+                             kw["seed"])
+    init = getattr(L, f"{kind}_init")
+    if init(C.byref(obj), C.byref(dt), hm, _ffi.STPREP_MULTIDET,
+            C.cast(C.pointer(md), C.c_void_p), None) != 0:
+        raise RuntimeError(f"{kind}_init failed")
+    try:
+        if kw.get("fusion") is not None:
+            span, rots = kw["fusion"]
+            L.qreg_set_fusion(C.byref(obj.ct.reg), span, rots)
+        if kw.get("timing"):
+            L.qreg_set_timing(C.byref(obj.ct.reg), 1)
+        if getattr(L, f"{kind}_simul")(C.byref(obj)) != 0:
+            raise RuntimeError(f"{kind}_simul failed")
+        vals = _values(obj.ct.vals)
+        st = _ffi.Stats()
+        L.qreg_get_stats(C.byref(obj.ct.reg), C.byref(st))
+        stats = {k: getattr(st, k) for k, _ in _ffi.Stats._fields_}
+    finally:
+        getattr(L, f"{kind}_free")(C.byref(obj))
+    return (vals, stats) if kw.get("with_stats") else vals
+
+
+def trott(nqb, terms, dets, steps, delta, **kw):
+    return _run_driver("trott", nqb, terms, dets, steps=steps, delta=delta,
+                       **kw)
+
+
+def trott2(nqb, terms, dets, steps, delta, **kw):
+    return _run_driver("trott2", nqb, terms, dets, steps=steps, delta=delta,
+                       **kw)
+
+
+def qdrift(nqb, terms, dets, samples, depth, step_size, seed, **kw):
+    return _run_driver("qdrift", nqb, terms, dets, samples=samples,
+                       depth=depth, step_size=step_size, seed=seed, **kw)
+
+
+def cmpsit(nqb, terms, dets, samples, steps, length, depth, angle_det,
+           angle_rand, seed, **kw):
+    return _run_driver("cmpsit", nqb, terms, dets, samples=samples,
+                       steps=steps, length=length, depth=depth,
+                       angle_det=angle_det, angle_rand=angle_rand, seed=seed,
+                       **kw)
+
+
+# ---- planner (host only) -----------------------------------------------
+
+
+def plan(nqb: int, flip, phase, phi, max_span: int = 5, max_rots: int = 0):
+    """Run the host planner; returns (passes, records) as lists of dicts."""
+    L = lib()
+    n = len(phi)
+    rin = (_ffi.RotIn * max(n, 1))()
+    for k in range(n):
+        rin[k].flip, rin[k].phase, rin[k].phi = int(flip[k]), int(phase[k]), \
+            float(phi[k])
+    passes = (_ffi.Pass * max(n, 1))()
+    recs = (_ffi.RotRec * max(n, 1))()
+    np_ = L.phase2_plan(nqb, rin, n, max_span, max_rots, passes, recs)
+    if np_ < 0:
+        raise ValueError("phase2_plan failed")
+    out_p = [{"span": p.span, "nrot": p.nrot, "rot_off": p.rot_off,
+              "piv": list(p.piv)[:p.span], "basis": list(p.basis)[:p.span]}
+             for p in passes[:np_]]
+    out_r = [{"z": r.z, "c": r.c, "s": r.s, "smask": r.smask, "U": r.U,
+              "odd": r.odd} for r in recs[:n]]
+    return out_p, out_r

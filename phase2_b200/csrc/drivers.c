@@ -1,0 +1,348 @@
+/*
+ * drivers.c -- trott, trott2, qdrift and cmpsit (include/circ/ headers).  Same
+ * step loops as circ/trott.c, circ/trott2.c, circ/qdrift.c and
+ * circ/cmpsit.c of Quantum-for-Life/phase2:
+ *
+ *   trott   per step: circ_step(delta), measure            (trott.c:44-65)
+ *   trott2  per step: circ_step(delta/2), circ_step_reverse(delta/2),
+ *           measure                                        (trott2.c:44-74)
+ *   qdrift  per sample: prepst, depth draws from the |c| CDF with
+ *           cf = sign(c), circ_step(asin(step_size)), measure
+ *                                                          (qdrift.c:95-134)
+ *   cmpsit  split by |c| (top `length` lex-sorted, rest sampled); per
+ *           sample: prepst, per step a forward half of one sample and a
+ *           reverse half of a fresh one at omega 0.5; measure
+ *                                                          (cmpsit.c:65-235)
+ *
+ * Sampling uses the same generator, CDF and sign rule, so draws are
+ * identical to the reference for equal seeds.  The deterministic term
+ * order follows phase2_get_term_order() (lexicographic by default).
+ */
+#include <complex.h>
+#include <float.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define LOG_SUBSYS "circ"
+#include "log.h"
+
+#include "circ/cmpsit.h"
+#include "circ/qdrift.h"
+#include "circ/trott.h"
+#include "circ/trott2.h"
+#include "phase2_b200.h"
+
+#include "p2_host.h"
+
+/* |a| < DBL_EPSILON -> 0, else -1 or +1 (circ/internal.h:26-32). */
+static double sign_dz(double a)
+{
+	const double f = fabs(a);
+	if (f < DBL_EPSILON)
+		return 0.0;
+	return a < f ? -1.0 : 1.0;
+}
+
+static void order_terms(struct circ_hamil *hm)
+{
+	switch (p2_cfg.order) {
+	case PHASE2_ORDER_LEX:
+		circ_hamil_sort_lex(hm);
+		break;
+	case PHASE2_ORDER_FLIP:
+		circ_hamil_sort_flip(hm);
+		break;
+	default:
+		break;
+	}
+}
+
+static int emit(struct phase2_step_writer *sw, size_t i, _Complex double z)
+{
+	return (sw && sw->write(sw->ctx, i, z) < 0) ? -1 : 0;
+}
+
+/* ---- trott -------------------------------------------------------------- */
+
+int trott_init(struct trott *tt, const struct trott_data *dt,
+	struct circ_hamil hm, enum stprep_kind sp_kind, const void *sp_data,
+	struct phase2_step_writer *sw)
+{
+	if (circ_init(&tt->ct, hm, sp_kind, sp_data, dt->steps) < 0) {
+		log_error("trott_init: circ_init failed");
+		return -1;
+	}
+	tt->dt = *dt;
+	tt->sw = sw;
+	order_terms(&tt->ct.hm);
+	return 0;
+}
+
+void trott_free(struct trott *tt)
+{
+	circ_free(&tt->ct);
+}
+
+int trott_simul(struct trott *tt)
+{
+	struct circ *ct = &tt->ct;
+	struct circ_values *vals = &ct->vals;
+	if (circ_prepst(ct) < 0)
+		return -1;
+	for (size_t i = 0; i < vals->len; i++) {
+		if (circ_step(ct, &ct->hm, tt->dt.delta) < 0) {
+			log_error("trott_simul: step %zu failed", i);
+			return -1;
+		}
+		vals->z[i] = circ_measure(ct);
+		if (p2_qreg_error(&ct->reg) < 0 || emit(tt->sw, i, vals->z[i]) < 0) {
+			log_error("trott_simul: step %zu output failed", i);
+			return -1;
+		}
+	}
+	return 0;
+}
+
+/* ---- trott2 ------------------------------------------------------------- */
+
+int trott2_init(struct trott2 *t2, const struct trott2_data *dt,
+	struct circ_hamil hm, enum stprep_kind sp_kind, const void *sp_data,
+	struct phase2_step_writer *sw)
+{
+	if (circ_init(&t2->ct, hm, sp_kind, sp_data, dt->steps) < 0) {
+		log_error("trott2_init: circ_init failed");
+		return -1;
+	}
+	t2->dt = *dt;
+	t2->sw = sw;
+	order_terms(&t2->ct.hm);
+	return 0;
+}
+
+void trott2_free(struct trott2 *t2)
+{
+	circ_free(&t2->ct);
+}
+
+int trott2_simul(struct trott2 *t2)
+{
+	struct circ *ct = &t2->ct;
+	struct circ_values *vals = &ct->vals;
+	const double half = t2->dt.delta / 2.0;
+	if (circ_prepst(ct) < 0)
+		return -1;
+	for (size_t i = 0; i < vals->len; i++) {
+		if (circ_step(ct, &ct->hm, half) < 0 ||
+			circ_step_reverse(ct, &ct->hm, half) < 0) {
+			log_error("trott2_simul: step %zu failed", i);
+			return -1;
+		}
+		vals->z[i] = circ_measure(ct);
+		if (p2_qreg_error(&ct->reg) < 0 || emit(t2->sw, i, vals->z[i]) < 0) {
+			log_error("trott2_simul: step %zu output failed", i);
+			return -1;
+		}
+	}
+	return 0;
+}
+
+/* ---- qdrift ------------------------------------------------------------- */
+
+/* Default seed, replaced by the last non-zero seed seen (circ/qdrift.c:30,
+ * 72-75). */
+static uint64_t QDRIFT_SEED = UINT64_C(0xeccd9dcc749fcdca);
+
+int qdrift_init(struct qdrift *qd, const struct qdrift_data *dt,
+	struct circ_hamil hm, enum stprep_kind sp_kind, const void *sp_data,
+	struct phase2_step_writer *sw)
+{
+	memset(&qd->ranct, 0, sizeof qd->ranct);
+	if (circ_init(&qd->ct, hm, sp_kind, sp_data, dt->samples) < 0)
+		return -1;
+	qd->dt = *dt;
+	qd->sw = sw;
+	if (prob_cdf_init(&qd->ranct.cdf, qd->ct.hm.len) < 0 ||
+		circ_hamil_init(&qd->ranct.hm_ran, qd->ct.hm.qb, dt->depth) <
+			0) {
+		prob_cdf_free(&qd->ranct.cdf);
+		circ_free(&qd->ct);
+		return -1;
+	}
+	prob_cdf_from_array_strided(&qd->ranct.cdf, &qd->ct.hm.terms[0].cf,
+		sizeof qd->ct.hm.terms[0], NULL);
+	if (qd->dt.seed != 0)
+		QDRIFT_SEED = qd->dt.seed;
+	else
+		qd->dt.seed = QDRIFT_SEED;
+	xoshiro256ss_init(&qd->rng, qd->dt.seed);
+	return 0;
+}
+
+void qdrift_free(struct qdrift *qd)
+{
+	circ_hamil_free(&qd->ranct.hm_ran);
+	prob_cdf_free(&qd->ranct.cdf);
+	circ_free(&qd->ct);
+}
+
+static void qdrift_draw(struct qdrift *qd)
+{
+	struct circ_hamil *ran = &qd->ranct.hm_ran;
+	for (size_t i = 0; i < ran->len; i++) {
+		const double x = xoshiro256ss_dbl01(&qd->rng);
+		const size_t k = prob_cdf_inverse(&qd->ranct.cdf, x);
+		ran->terms[i].cf = sign_dz(qd->ct.hm.terms[k].cf);
+		ran->terms[i].op = qd->ct.hm.terms[k].op;
+	}
+}
+
+int qdrift_simul(struct qdrift *qd)
+{
+	struct circ *ct = &qd->ct;
+	struct circ_values *vals = &ct->vals;
+	const double omega = asin(qd->dt.step_size);
+	for (size_t i = 0; i < vals->len; i++) {
+		if (circ_prepst(ct) < 0)
+			return -1;
+		qdrift_draw(qd);
+		if (circ_step(ct, &qd->ranct.hm_ran, omega) < 0) {
+			log_error("qdrift_simul: sample %zu failed", i);
+			return -1;
+		}
+		vals->z[i] = circ_measure(ct);
+		if (p2_qreg_error(&ct->reg) < 0 || emit(qd->sw, i, vals->z[i]) < 0) {
+			log_error("qdrift_simul: sample %zu output failed", i);
+			return -1;
+		}
+	}
+	return 0;
+}
+
+/* ---- cmpsit ------------------------------------------------------------- */
+
+static uint64_t CMPSIT_SEED = UINT64_C(0xafb424901446f21f);
+
+static int cmp_abscf_desc(const void *a, const void *b)
+{
+	const double x = fabs(((const struct circ_hamil_term *)a)->cf);
+	const double y = fabs(((const struct circ_hamil_term *)b)->cf);
+	return x > y ? -1 : (x < y ? 1 : 0);
+}
+
+static int cmpsit_split(struct cmpsit_ranct *rc, const struct circ_hamil *hm,
+	const struct cmpsit_data *dt)
+{
+	if (dt->length > hm->len)
+		return -1;
+	struct circ_hamil tmp;
+	if (circ_hamil_init(&tmp, hm->qb, hm->len) < 0)
+		return -1;
+	memcpy(tmp.terms, hm->terms, sizeof *tmp.terms * hm->len);
+	qsort(tmp.terms, tmp.len, sizeof *tmp.terms, cmp_abscf_desc);
+	const size_t nran = hm->len - dt->length;
+	if (circ_hamil_init(&rc->hm_det, hm->qb, dt->length) < 0)
+		goto fail_tmp;
+	memcpy(rc->hm_det.terms, tmp.terms, sizeof *tmp.terms * dt->length);
+	order_terms(&rc->hm_det);
+	if (circ_hamil_init(&rc->hm_ran, hm->qb, nran) < 0)
+		goto fail_det;
+	memcpy(rc->hm_ran.terms, tmp.terms + dt->length,
+		sizeof *tmp.terms * nran);
+	if (prob_cdf_init(&rc->cdf, nran) < 0)
+		goto fail_ran;
+	prob_cdf_from_array_strided(&rc->cdf, &rc->hm_ran.terms[0].cf,
+		sizeof rc->hm_ran.terms[0], &rc->lambda_r);
+	rc->depth = dt->depth;
+	rc->angle_rand = dt->angle_rand;
+	circ_hamil_free(&tmp);
+	return 0;
+fail_ran:
+	circ_hamil_free(&rc->hm_ran);
+fail_det:
+	circ_hamil_free(&rc->hm_det);
+fail_tmp:
+	circ_hamil_free(&tmp);
+	return -1;
+}
+
+int cmpsit_init(struct cmpsit *cp, const struct cmpsit_data *dt,
+	struct circ_hamil hm, enum stprep_kind sp_kind, const void *sp_data,
+	struct phase2_step_writer *sw)
+{
+	memset(&cp->ranct, 0, sizeof cp->ranct);
+	if (circ_init(&cp->ct, hm, sp_kind, sp_data, dt->samples) < 0)
+		return -1;
+	cp->dt = *dt;
+	cp->sw = sw;
+	if (cmpsit_split(&cp->ranct, &cp->ct.hm, dt) < 0) {
+		circ_free(&cp->ct);
+		return -1;
+	}
+	if (cp->dt.seed != 0)
+		CMPSIT_SEED = cp->dt.seed;
+	else
+		cp->dt.seed = CMPSIT_SEED;
+	xoshiro256ss_init(&cp->rng, cp->dt.seed);
+	return 0;
+}
+
+void cmpsit_free(struct cmpsit *cp)
+{
+	circ_hamil_free(&cp->ranct.hm_smpl);
+	circ_hamil_free(&cp->ranct.hm_ran);
+	circ_hamil_free(&cp->ranct.hm_det);
+	prob_cdf_free(&cp->ranct.cdf);
+	circ_free(&cp->ct);
+}
+
+/* One composite sample: deterministic head at angle_det * c, then `depth`
+ * draws at sign(c) * angle_rand (circ/cmpsit.c:151-177). */
+static int cmpsit_sample(struct cmpsit *cp)
+{
+	struct cmpsit_ranct *rc = &cp->ranct;
+	const size_t len = cp->dt.length + rc->depth;
+	if (!rc->hm_smpl.terms || rc->hm_smpl.len != len) {
+		circ_hamil_free(&rc->hm_smpl);
+		if (circ_hamil_init(&rc->hm_smpl, cp->ct.hm.qb, len) < 0)
+			return -1;
+	}
+	for (size_t i = 0; i < cp->dt.length; i++) {
+		rc->hm_smpl.terms[i].op = rc->hm_det.terms[i].op;
+		rc->hm_smpl.terms[i].cf = rc->hm_det.terms[i].cf * cp->dt.angle_det;
+	}
+	const double tau = rc->angle_rand;
+	for (size_t i = cp->dt.length; i < len; i++) {
+		const double x = xoshiro256ss_dbl01(&cp->rng);
+		const size_t k = prob_cdf_inverse(&rc->cdf, x);
+		rc->hm_smpl.terms[i].op = rc->hm_ran.terms[k].op;
+		rc->hm_smpl.terms[i].cf = sign_dz(rc->hm_ran.terms[k].cf) * tau;
+	}
+	return 0;
+}
+
+int cmpsit_simul(struct cmpsit *cp)
+{
+	struct circ *ct = &cp->ct;
+	struct circ_values *vals = &ct->vals;
+	for (size_t i = 0; i < vals->len; i++) {
+		if (circ_prepst(ct) < 0)
+			return -1;
+		for (size_t s = 0; s < cp->dt.steps; s++) {
+			if (cmpsit_sample(cp) < 0 ||
+				circ_step(ct, &cp->ranct.hm_smpl, 0.5) < 0)
+				return -1;
+			if (cmpsit_sample(cp) < 0 ||
+				circ_step_reverse(ct, &cp->ranct.hm_smpl, 0.5) <
+					0)
+				return -1;
+		}
+		vals->z[i] = circ_measure(ct);
+		if (p2_qreg_error(&ct->reg) < 0 || emit(cp->sw, i, vals->z[i]) < 0) {
+			log_error("cmpsit_simul: sample %zu output failed", i);
+			return -1;
+		}
+	}
+	return 0;
+}

@@ -1,0 +1,898 @@
+/*
+ * engine.cu -- device side of libphase2.so for sm_100a (B200).
+ *
+ * The state vector is one flat array of 2^n complex amplitudes in HBM,
+ * complex128 (double2) or complex64 (float2), updated in place.
+ *
+ * Hot kernel: k_pass<M, Storage, EXACT>.  One launch = one HBM sweep that
+ * applies a planned run of rotations (plan.c).  Each thread owns whole
+ * cosets x + span(basis[0..M-1]): it loads the 2^M amplitudes of a coset
+ * into FP64 registers, applies every rotation of the run in order (partners
+ * of a rotation are always inside the coset), and writes them back.  Warp
+ * lanes take consecutive representatives x, so for each slot the warp
+ * touches one contiguous 256 B (FP32) or 512 B (FP64) segment: coalesced,
+ * one read and one write of every amplitude per pass, no shared-memory
+ * staging of amplitudes.  It is a streaming pair sweep on CUDA cores; there
+ * is no contraction for the tensor cores to do.
+ *
+ * EXACT (FP64 storage): products and sums are rounded separately with
+ * __dmul_rn/__dadd_rn, never fused, so every amplitude is bit-identical to
+ * the reference CPU update a_i <- c a_i + i conj(s z) a_j
+ * (phase2/qreg_qreg.c:149-160).  FP32 storage computes in FP64 with FMA and
+ * rounds to FP32 once per pass.
+ *
+ * Other kernels: gather/scatter of a few amplitudes (overlap, state prep),
+ * and a two-stage FP64 sum of squares / inner product (warp-shuffle tree
+ * per block, then one block combining the per-block partials with
+ * Neumaier compensated summation).
+ */
+#include <cuda_runtime.h>
+
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define LOG_SUBSYS "engine"
+#include "log.h"
+
+#include "p2_internal.h"
+
+#define P2_TPB 128
+#define P2_RED_TPB 256
+
+struct p2_dev {
+	uint32_t nqb;
+	int prec;
+	size_t elem;
+	uint64_t namp;
+	void *state;
+	cudaStream_t stream;
+	int sm_count;
+
+	struct phase2_rot_rec *d_recs;
+	size_t d_recs_cap;
+	struct phase2_rot_rec *h_recs[2];
+	size_t h_recs_cap[2];
+	cudaEvent_t h_ev[2];
+	int h_ev_live[2];
+	int ring;
+
+	uint64_t *d_idx;
+	double *d_val;
+	uint64_t *h_idx;
+	double *h_val;
+	size_t io_cap;
+
+	double *d_part;
+	size_t part_cap;
+
+	int timing;
+	cudaEvent_t t0, t1;
+
+	uint64_t rotations, passes, launches, timed_passes;
+	uint64_t h2d_bytes, d2h_bytes;
+	double pass_ms;
+};
+
+#define CUDA_OK(call, what)                                                    \
+	do {                                                                   \
+		cudaError_t e_ = (call);                                       \
+		if (e_ != cudaSuccess) {                                       \
+			log_error("%s: %s", (what), cudaGetErrorString(e_));  \
+			return -1;                                             \
+		}                                                              \
+	} while (0)
+
+/* ---- arithmetic --------------------------------------------------------- */
+
+template <bool EXACT>
+__device__ __forceinline__ double p2_mul(double a, double b)
+{
+	if constexpr (EXACT)
+		return __dmul_rn(a, b);
+	else
+		return a * b;
+}
+
+/* c*x + t: two roundings (EXACT) or one (FMA). */
+template <bool EXACT>
+__device__ __forceinline__ double p2_cxt(double c, double x, double t)
+{
+	if constexpr (EXACT)
+		return __dadd_rn(__dmul_rn(c, x), t);
+	else
+		return fma(c, x, t);
+}
+
+__host__ __device__ constexpr int p2_hibit(int v)
+{
+	return v <= 1 ? 0 : 1 + p2_hibit(v >> 1);
+}
+
+/* One rotation on the 2^M slots of a coset.  sm bit u = sign of slot u. */
+template <int M, int U, int ODD, bool EXACT>
+__device__ __forceinline__ void p2_rot(double (&re)[1 << M],
+	double (&im)[1 << M], double c, double s, uint32_t sm)
+{
+	if constexpr (U == 0) {
+#pragma unroll
+		for (int u = 0; u < (1 << M); ++u) {
+			const double su = (sm >> u & 1u) ? -s : s;
+			double tr, ti;
+			if constexpr (ODD) {
+				tr = p2_mul<EXACT>(-su, im[u]);
+				ti = p2_mul<EXACT>(su, re[u]);
+			} else {
+				tr = p2_mul<EXACT>(su, re[u]);
+				ti = p2_mul<EXACT>(su, im[u]);
+			}
+			re[u] = p2_cxt<EXACT>(c, re[u], tr);
+			im[u] = p2_cxt<EXACT>(c, im[u], ti);
+		}
+	} else {
+		constexpr int H = p2_hibit(U);
+#pragma unroll
+		for (int u = 0; u < (1 << M); ++u) {
+			if (u >> H & 1)
+				continue;
+			const int w = u ^ U;
+			const double su = (sm >> u & 1u) ? -s : s;
+			const double sw = (sm >> w & 1u) ? -s : s;
+			double tur, tui, twr, twi;
+			if constexpr (ODD) {
+				tur = p2_mul<EXACT>(-su, im[w]);
+				tui = p2_mul<EXACT>(su, re[w]);
+				twr = p2_mul<EXACT>(-sw, im[u]);
+				twi = p2_mul<EXACT>(sw, re[u]);
+			} else {
+				tur = p2_mul<EXACT>(su, re[w]);
+				tui = p2_mul<EXACT>(su, im[w]);
+				twr = p2_mul<EXACT>(sw, re[u]);
+				twi = p2_mul<EXACT>(sw, im[u]);
+			}
+			const double nur = p2_cxt<EXACT>(c, re[u], tur);
+			const double nui = p2_cxt<EXACT>(c, im[u], tui);
+			const double nwr = p2_cxt<EXACT>(c, re[w], twr);
+			const double nwi = p2_cxt<EXACT>(c, im[w], twi);
+			re[u] = nur;
+			im[u] = nui;
+			re[w] = nwr;
+			im[w] = nwi;
+		}
+	}
+}
+
+#define P2_CASE(K)                                                             \
+	case K:                                                                \
+		if constexpr ((K) < (2 << M))                                  \
+			p2_rot<M, ((K) >> 1), ((K)&1), EXACT>(re, im, c, s,    \
+				sm);                                           \
+		break;
+
+/* key = U << 1 | odd; a jump table over the (U, odd) variants. */
+template <int M, bool EXACT>
+__device__ __forceinline__ void p2_apply(uint32_t key, double (&re)[1 << M],
+	double (&im)[1 << M], double c, double s, uint32_t sm)
+{
+	switch (key) {
+		P2_CASE(0) P2_CASE(1) P2_CASE(2) P2_CASE(3) P2_CASE(4)
+		P2_CASE(5) P2_CASE(6) P2_CASE(7) P2_CASE(8) P2_CASE(9)
+		P2_CASE(10) P2_CASE(11) P2_CASE(12) P2_CASE(13) P2_CASE(14)
+		P2_CASE(15) P2_CASE(16) P2_CASE(17) P2_CASE(18) P2_CASE(19)
+		P2_CASE(20) P2_CASE(21) P2_CASE(22) P2_CASE(23) P2_CASE(24)
+		P2_CASE(25) P2_CASE(26) P2_CASE(27) P2_CASE(28) P2_CASE(29)
+		P2_CASE(30) P2_CASE(31) P2_CASE(32) P2_CASE(33) P2_CASE(34)
+		P2_CASE(35) P2_CASE(36) P2_CASE(37) P2_CASE(38) P2_CASE(39)
+		P2_CASE(40) P2_CASE(41) P2_CASE(42) P2_CASE(43) P2_CASE(44)
+		P2_CASE(45) P2_CASE(46) P2_CASE(47) P2_CASE(48) P2_CASE(49)
+		P2_CASE(50) P2_CASE(51) P2_CASE(52) P2_CASE(53) P2_CASE(54)
+		P2_CASE(55) P2_CASE(56) P2_CASE(57) P2_CASE(58) P2_CASE(59)
+		P2_CASE(60) P2_CASE(61) P2_CASE(62) P2_CASE(63)
+	default:
+		break;
+	}
+}
+#undef P2_CASE
+
+/* ---- storage ------------------------------------------------------------ */
+
+__device__ __forceinline__ void p2_ld(const double2 *st, uint64_t g,
+	double &re, double &im)
+{
+	const double2 v = st[g];
+	re = v.x;
+	im = v.y;
+}
+
+__device__ __forceinline__ void p2_ld(const float2 *st, uint64_t g,
+	double &re, double &im)
+{
+	const float2 v = st[g];
+	re = (double)v.x;
+	im = (double)v.y;
+}
+
+__device__ __forceinline__ void p2_st(double2 *st, uint64_t g, double re,
+	double im)
+{
+	st[g] = make_double2(re, im);
+}
+
+__device__ __forceinline__ void p2_st(float2 *st, uint64_t g, double re,
+	double im)
+{
+	st[g] = make_float2(__double2float_rn(re), __double2float_rn(im));
+}
+
+template <int M>
+__device__ __forceinline__ uint64_t p2_slot_off(int u, const uint64_t *basis)
+{
+	uint64_t off = 0;
+#pragma unroll
+	for (int k = 0; k < M; ++k)
+		if (u >> k & 1)
+			off ^= basis[k];
+	return off;
+}
+
+/* ---- the pass kernel ---------------------------------------------------- */
+
+template <int M, typename ST, bool EXACT>
+__global__ void __launch_bounds__(P2_TPB) k_pass(ST *__restrict__ st,
+	uint64_t nrep, struct phase2_pass p,
+	const struct phase2_rot_rec *__restrict__ recs)
+{
+	__shared__ struct phase2_rot_rec srec[P2_MAX_ROTS_PER_PASS];
+	for (uint32_t r = threadIdx.x; r < p.nrot; r += blockDim.x)
+		srec[r] = recs[p.rot_off + r];
+	__syncthreads();
+
+	const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+	for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+		t < nrep; t += stride) {
+		/* representative: zeros inserted at the pivots (ascending) */
+		uint64_t x = t;
+#pragma unroll
+		for (int k = 0; k < M; ++k) {
+			const uint32_t q = p.piv[k];
+			x = ((x >> q) << (q + 1)) | (x & ((UINT64_C(1) << q) - 1));
+		}
+		double re[1 << M], im[1 << M];
+#pragma unroll
+		for (int u = 0; u < (1 << M); ++u)
+			p2_ld(st, x ^ p2_slot_off<M>(u, p.basis), re[u], im[u]);
+
+		for (uint32_t r = 0; r < p.nrot; ++r) {
+			const uint64_t z = srec[r].z;
+			const uint32_t px = (uint32_t)(__popcll(x & z) & 1);
+			const uint32_t sm = srec[r].smask ^ (0u - px);
+			const uint32_t key =
+				((uint32_t)srec[r].U << 1) | srec[r].odd;
+			p2_apply<M, EXACT>(key, re, im, srec[r].c, srec[r].s, sm);
+		}
+
+#pragma unroll
+		for (int u = 0; u < (1 << M); ++u)
+			p2_st(st, x ^ p2_slot_off<M>(u, p.basis), re[u], im[u]);
+	}
+}
+
+/* ---- small kernels ------------------------------------------------------ */
+
+template <typename ST>
+__global__ void k_gather(const ST *__restrict__ st,
+	const uint64_t *__restrict__ idx, double *__restrict__ out, size_t n)
+{
+	const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n) {
+		double re, im;
+		p2_ld(st, idx[i], re, im);
+		out[2 * i] = re;
+		out[2 * i + 1] = im;
+	}
+}
+
+/* Later entries win on duplicate indices: one thread writes them all in
+ * order (n is small: determinants of a state-prep payload). */
+template <typename ST>
+__global__ void k_scatter(ST *__restrict__ st, const uint64_t *__restrict__ idx,
+	const double *__restrict__ val, size_t n)
+{
+	if (blockIdx.x == 0 && threadIdx.x == 0)
+		for (size_t i = 0; i < n; ++i)
+			p2_st(st, idx[i], val[2 * i], val[2 * i + 1]);
+}
+
+template <typename ST>
+__global__ void k_widen(const ST *__restrict__ st, double2 *__restrict__ out,
+	uint64_t n)
+{
+	const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+	for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+		i < n; i += stride) {
+		double re, im;
+		p2_ld(st, i, re, im);
+		out[i] = make_double2(re, im);
+	}
+}
+
+template <typename ST>
+__global__ void k_narrow(ST *__restrict__ st, const double2 *__restrict__ in,
+	uint64_t n)
+{
+	const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+	for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+		i < n; i += stride)
+		p2_st(st, i, in[i].x, in[i].y);
+}
+
+/* Neumaier: s + c carries the running sum and its rounding error. */
+__device__ __forceinline__ void p2_neumaier(double &s, double &c, double v)
+{
+	const double t = s + v;
+	if (fabs(s) >= fabs(v))
+		c += (s - t) + v;
+	else
+		c += (v - t) + s;
+	s = t;
+}
+
+__device__ __forceinline__ double p2_warp_sum(double v)
+{
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1)
+		v += __shfl_xor_sync(0xffffffffu, v, o);
+	return v;
+}
+
+/* Stage 1: per-block sums of |a|^2 (trial == NULL) or of conj(trial) * a,
+ * written to part[2*block + {0,1}].  Each thread accumulates its strided
+ * elements with compensation, then a warp-shuffle tree and one pass over
+ * the warp totals in shared memory. */
+template <typename ST>
+__global__ void __launch_bounds__(P2_RED_TPB) k_reduce_partial(
+	const ST *__restrict__ st, const double2 *__restrict__ trial, uint64_t n,
+	double *__restrict__ part)
+{
+	double sr = 0.0, cr = 0.0, si = 0.0, ci = 0.0;
+	const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+	for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+		i < n; i += stride) {
+		double re, im;
+		p2_ld(st, i, re, im);
+		if (trial) {
+			const double2 t = trial[i];
+			p2_neumaier(sr, cr, t.x * re + t.y * im);
+			p2_neumaier(si, ci, t.x * im - t.y * re);
+		} else {
+			p2_neumaier(sr, cr, re * re + im * im);
+		}
+	}
+	double vr = p2_warp_sum(sr + cr), vi = p2_warp_sum(si + ci);
+	__shared__ double wr[P2_RED_TPB / 32], wi[P2_RED_TPB / 32];
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	if (lane == 0) {
+		wr[warp] = vr;
+		wi[warp] = vi;
+	}
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double s0 = 0.0, c0 = 0.0, s1 = 0.0, c1 = 0.0;
+		for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+			p2_neumaier(s0, c0, wr[w]);
+			p2_neumaier(s1, c1, wi[w]);
+		}
+		part[2 * blockIdx.x] = s0 + c0;
+		part[2 * blockIdx.x + 1] = s1 + c1;
+	}
+}
+
+/* Stage 2: one block combines nblk partials (compensated). */
+__global__ void __launch_bounds__(P2_RED_TPB) k_reduce_final(
+	const double *__restrict__ part, uint32_t nblk, double *__restrict__ out)
+{
+	double sr = 0.0, cr = 0.0, si = 0.0, ci = 0.0;
+	for (uint32_t b = threadIdx.x; b < nblk; b += blockDim.x) {
+		p2_neumaier(sr, cr, part[2 * b]);
+		p2_neumaier(si, ci, part[2 * b + 1]);
+	}
+	__shared__ double a0[P2_RED_TPB], a1[P2_RED_TPB];
+	a0[threadIdx.x] = sr + cr;
+	a1[threadIdx.x] = si + ci;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double s0 = 0.0, c0 = 0.0, s1 = 0.0, c1 = 0.0;
+		for (int t = 0; t < (int)blockDim.x; ++t) {
+			p2_neumaier(s0, c0, a0[t]);
+			p2_neumaier(s1, c1, a1[t]);
+		}
+		out[0] = s0 + c0;
+		out[1] = s1 + c1;
+	}
+}
+
+/* ---- host side ---------------------------------------------------------- */
+
+extern "C" int p2d_device_init(int dev, int *count)
+{
+	int n = 0;
+	const cudaError_t e = cudaGetDeviceCount(&n);
+	if (count)
+		*count = e == cudaSuccess ? n : 0;
+	if (e != cudaSuccess || n == 0) {
+		log_error("no CUDA device: %s",
+			e == cudaSuccess ? "device count is 0"
+					 : cudaGetErrorString(e));
+		return -1;
+	}
+	if (dev < 0 || dev >= n) {
+		log_error("CUDA device %d out of range (count %d)", dev, n);
+		return -1;
+	}
+	CUDA_OK(cudaSetDevice(dev), "cudaSetDevice");
+	CUDA_OK(cudaFree(0), "CUDA context init");
+	return 0;
+}
+
+static int io_reserve(struct p2_dev *d, size_t n)
+{
+	if (n <= d->io_cap)
+		return 0;
+	size_t cap = d->io_cap ? d->io_cap : 64;
+	while (cap < n)
+		cap *= 2;
+	CUDA_OK(cudaStreamSynchronize(d->stream), "sync before io growth");
+	cudaFree(d->d_idx);
+	cudaFree(d->d_val);
+	cudaFreeHost(d->h_idx);
+	cudaFreeHost(d->h_val);
+	d->d_idx = NULL;
+	d->d_val = NULL;
+	d->h_idx = NULL;
+	d->h_val = NULL;
+	d->io_cap = 0;
+	CUDA_OK(cudaMalloc((void **)&d->d_idx, cap * sizeof(uint64_t)),
+		"alloc idx");
+	CUDA_OK(cudaMalloc((void **)&d->d_val, cap * 2 * sizeof(double)),
+		"alloc val");
+	CUDA_OK(cudaMallocHost((void **)&d->h_idx, cap * sizeof(uint64_t)),
+		"alloc pinned idx");
+	CUDA_OK(cudaMallocHost((void **)&d->h_val, cap * 2 * sizeof(double)),
+		"alloc pinned val");
+	d->io_cap = cap;
+	return 0;
+}
+
+extern "C" struct p2_dev *p2d_create(uint32_t nqb, int prec)
+{
+	if (nqb == 0 || nqb > 40) {
+		log_error("p2d_create: nqb=%u out of range", nqb);
+		return NULL;
+	}
+	if (prec != PHASE2_PREC_FP64 && prec != PHASE2_PREC_FP32) {
+		log_error("p2d_create: unknown precision %d", prec);
+		return NULL;
+	}
+	struct p2_dev *d = (struct p2_dev *)calloc(1, sizeof *d);
+	if (!d)
+		return NULL;
+	d->nqb = nqb;
+	d->prec = prec;
+	d->elem = prec == PHASE2_PREC_FP64 ? sizeof(double2) : sizeof(float2);
+	d->namp = UINT64_C(1) << nqb;
+	const size_t bytes = d->namp * d->elem;
+
+	int dev = 0;
+	cudaGetDevice(&dev);
+	cudaDeviceGetAttribute(&d->sm_count, cudaDevAttrMultiProcessorCount,
+		dev);
+	if (d->sm_count <= 0)
+		d->sm_count = 148;
+
+	size_t free_b = 0, total_b = 0;
+	if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess &&
+		bytes > free_b) {
+		log_error("p2d_create: state of %zu bytes exceeds free device"
+			  " memory (%zu bytes)",
+			bytes, free_b);
+		free(d);
+		return NULL;
+	}
+	if (cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) !=
+		cudaSuccess)
+		goto fail;
+	if (cudaMalloc(&d->state, bytes) != cudaSuccess) {
+		log_error("p2d_create: cudaMalloc(%zu) failed", bytes);
+		goto fail;
+	}
+	for (int k = 0; k < 2; k++)
+		if (cudaEventCreateWithFlags(&d->h_ev[k],
+			    cudaEventDisableTiming) != cudaSuccess)
+			goto fail;
+	if (cudaEventCreate(&d->t0) != cudaSuccess ||
+		cudaEventCreate(&d->t1) != cudaSuccess)
+		goto fail;
+	if (cudaMemsetAsync(d->state, 0, bytes, d->stream) != cudaSuccess)
+		goto fail;
+	return d;
+fail:
+	log_error("p2d_create: %s", cudaGetErrorString(cudaGetLastError()));
+	p2d_destroy(d);
+	return NULL;
+}
+
+extern "C" void p2d_destroy(struct p2_dev *d)
+{
+	if (!d)
+		return;
+	if (d->stream)
+		cudaStreamSynchronize(d->stream);
+	cudaFree(d->state);
+	cudaFree(d->d_recs);
+	for (int k = 0; k < 2; k++) {
+		cudaFreeHost(d->h_recs[k]);
+		if (d->h_ev[k])
+			cudaEventDestroy(d->h_ev[k]);
+	}
+	cudaFree(d->d_idx);
+	cudaFree(d->d_val);
+	cudaFreeHost(d->h_idx);
+	cudaFreeHost(d->h_val);
+	cudaFree(d->d_part);
+	if (d->t0)
+		cudaEventDestroy(d->t0);
+	if (d->t1)
+		cudaEventDestroy(d->t1);
+	if (d->stream)
+		cudaStreamDestroy(d->stream);
+	free(d);
+}
+
+extern "C" int p2d_zero(struct p2_dev *d)
+{
+	CUDA_OK(cudaMemsetAsync(d->state, 0, d->namp * d->elem, d->stream),
+		"zero state");
+	return 0;
+}
+
+static int check_idx(const struct p2_dev *d, const uint64_t *idx, size_t n)
+{
+	for (size_t i = 0; i < n; i++)
+		if (idx[i] >= d->namp) {
+			log_error("amplitude index %llu out of range (namp %llu)",
+				(unsigned long long)idx[i],
+				(unsigned long long)d->namp);
+			return -1;
+		}
+	return 0;
+}
+
+extern "C" int p2d_set(struct p2_dev *d, const uint64_t *idx, const double *z,
+	size_t n)
+{
+	if (n == 0)
+		return 0;
+	if (check_idx(d, idx, n) < 0 || io_reserve(d, n) < 0)
+		return -1;
+	CUDA_OK(cudaStreamSynchronize(d->stream), "sync before set");
+	memcpy(d->h_idx, idx, n * sizeof *idx);
+	memcpy(d->h_val, z, n * 2 * sizeof(double));
+	CUDA_OK(cudaMemcpyAsync(d->d_idx, d->h_idx, n * sizeof *idx,
+			cudaMemcpyHostToDevice, d->stream),
+		"upload idx");
+	CUDA_OK(cudaMemcpyAsync(d->d_val, d->h_val, n * 2 * sizeof(double),
+			cudaMemcpyHostToDevice, d->stream),
+		"upload val");
+	d->h2d_bytes += n * (sizeof(uint64_t) + 2 * sizeof(double));
+	if (d->prec == PHASE2_PREC_FP64)
+		k_scatter<<<1, 32, 0, d->stream>>>((double2 *)d->state, d->d_idx,
+			d->d_val, n);
+	else
+		k_scatter<<<1, 32, 0, d->stream>>>((float2 *)d->state, d->d_idx,
+			d->d_val, n);
+	d->launches++;
+	CUDA_OK(cudaGetLastError(), "scatter launch");
+	CUDA_OK(cudaStreamSynchronize(d->stream), "scatter");
+	return 0;
+}
+
+extern "C" int p2d_get(struct p2_dev *d, const uint64_t *idx, double *z,
+	size_t n)
+{
+	if (n == 0)
+		return 0;
+	if (check_idx(d, idx, n) < 0 || io_reserve(d, n) < 0)
+		return -1;
+	CUDA_OK(cudaStreamSynchronize(d->stream), "sync before get");
+	memcpy(d->h_idx, idx, n * sizeof *idx);
+	CUDA_OK(cudaMemcpyAsync(d->d_idx, d->h_idx, n * sizeof *idx,
+			cudaMemcpyHostToDevice, d->stream),
+		"upload idx");
+	const unsigned blocks = (unsigned)((n + 127) / 128);
+	if (d->prec == PHASE2_PREC_FP64)
+		k_gather<<<blocks, 128, 0, d->stream>>>(
+			(const double2 *)d->state, d->d_idx, d->d_val, n);
+	else
+		k_gather<<<blocks, 128, 0, d->stream>>>(
+			(const float2 *)d->state, d->d_idx, d->d_val, n);
+	d->launches++;
+	CUDA_OK(cudaGetLastError(), "gather launch");
+	CUDA_OK(cudaMemcpyAsync(d->h_val, d->d_val, n * 2 * sizeof(double),
+			cudaMemcpyDeviceToHost, d->stream),
+		"download val");
+	d->h2d_bytes += n * sizeof(uint64_t);
+	d->d2h_bytes += n * 2 * sizeof(double);
+	CUDA_OK(cudaStreamSynchronize(d->stream), "gather");
+	memcpy(z, d->h_val, n * 2 * sizeof(double));
+	return 0;
+}
+
+static unsigned grid_for(const struct p2_dev *d, uint64_t work, unsigned tpb,
+	unsigned per_sm)
+{
+	uint64_t b = (work + tpb - 1) / tpb;
+	const uint64_t cap = (uint64_t)d->sm_count * per_sm;
+	if (b > cap)
+		b = cap;
+	return b ? (unsigned)b : 1u;
+}
+
+extern "C" int p2d_get_state(struct p2_dev *d, double *out)
+{
+	const size_t bytes = d->namp * sizeof(double2);
+	if (d->prec == PHASE2_PREC_FP64) {
+		CUDA_OK(cudaMemcpyAsync(out, d->state, bytes,
+				cudaMemcpyDeviceToHost, d->stream),
+			"download state");
+		CUDA_OK(cudaStreamSynchronize(d->stream), "download state");
+		return 0;
+	}
+	double2 *tmp = NULL;
+	CUDA_OK(cudaMalloc((void **)&tmp, bytes), "alloc widen buffer");
+	k_widen<<<grid_for(d, d->namp, 256, 16), 256, 0, d->stream>>>(
+		(const float2 *)d->state, tmp, d->namp);
+	d->launches++;
+	cudaError_t e = cudaMemcpyAsync(out, tmp, bytes,
+		cudaMemcpyDeviceToHost, d->stream);
+	if (e == cudaSuccess)
+		e = cudaStreamSynchronize(d->stream);
+	cudaFree(tmp);
+	CUDA_OK(e, "download widened state");
+	return 0;
+}
+
+extern "C" int p2d_set_state(struct p2_dev *d, const double *in)
+{
+	const size_t bytes = d->namp * sizeof(double2);
+	CUDA_OK(cudaStreamSynchronize(d->stream), "sync before set_state");
+	if (d->prec == PHASE2_PREC_FP64) {
+		CUDA_OK(cudaMemcpyAsync(d->state, in, bytes,
+				cudaMemcpyHostToDevice, d->stream),
+			"upload state");
+		CUDA_OK(cudaStreamSynchronize(d->stream), "upload state");
+		return 0;
+	}
+	double2 *tmp = NULL;
+	CUDA_OK(cudaMalloc((void **)&tmp, bytes), "alloc narrow buffer");
+	cudaError_t e = cudaMemcpyAsync(tmp, in, bytes, cudaMemcpyHostToDevice,
+		d->stream);
+	if (e == cudaSuccess) {
+		k_narrow<<<grid_for(d, d->namp, 256, 16), 256, 0, d->stream>>>(
+			(float2 *)d->state, tmp, d->namp);
+		d->launches++;
+		e = cudaStreamSynchronize(d->stream);
+	}
+	cudaFree(tmp);
+	CUDA_OK(e, "upload narrowed state");
+	return 0;
+}
+
+template <int M, typename ST, bool EXACT>
+static void launch_pass_t(struct p2_dev *d, const struct phase2_pass &p,
+	const struct phase2_rot_rec *recs)
+{
+	const uint64_t nrep = d->namp >> M;
+	const unsigned grid = grid_for(d, nrep, P2_TPB, 16);
+	k_pass<M, ST, EXACT><<<grid, P2_TPB, 0, d->stream>>>(
+		(ST *)d->state, nrep, p, recs);
+}
+
+template <typename ST, bool EXACT>
+static int launch_pass(struct p2_dev *d, const struct phase2_pass &p,
+	const struct phase2_rot_rec *recs)
+{
+	switch (p.span) {
+	case 0:
+		launch_pass_t<0, ST, EXACT>(d, p, recs);
+		break;
+	case 1:
+		launch_pass_t<1, ST, EXACT>(d, p, recs);
+		break;
+	case 2:
+		launch_pass_t<2, ST, EXACT>(d, p, recs);
+		break;
+	case 3:
+		launch_pass_t<3, ST, EXACT>(d, p, recs);
+		break;
+	case 4:
+		launch_pass_t<4, ST, EXACT>(d, p, recs);
+		break;
+	case 5:
+		launch_pass_t<5, ST, EXACT>(d, p, recs);
+		break;
+	default:
+		log_error("pass span %u unsupported", p.span);
+		return -1;
+	}
+	return 0;
+}
+
+static int recs_reserve(struct p2_dev *d, size_t n)
+{
+	if (n > d->d_recs_cap) {
+		size_t cap = d->d_recs_cap ? d->d_recs_cap : 1024;
+		while (cap < n)
+			cap *= 2;
+		CUDA_OK(cudaStreamSynchronize(d->stream), "sync before growth");
+		cudaFree(d->d_recs);
+		d->d_recs = NULL;
+		d->d_recs_cap = 0;
+		CUDA_OK(cudaMalloc((void **)&d->d_recs,
+				cap * sizeof(struct phase2_rot_rec)),
+			"alloc rotation records");
+		d->d_recs_cap = cap;
+	}
+	const int k = d->ring;
+	if (d->h_ev_live[k]) {
+		CUDA_OK(cudaEventSynchronize(d->h_ev[k]), "staging reuse");
+		d->h_ev_live[k] = 0;
+	}
+	if (n > d->h_recs_cap[k]) {
+		size_t cap = d->h_recs_cap[k] ? d->h_recs_cap[k] : 1024;
+		while (cap < n)
+			cap *= 2;
+		cudaFreeHost(d->h_recs[k]);
+		d->h_recs[k] = NULL;
+		d->h_recs_cap[k] = 0;
+		CUDA_OK(cudaMallocHost((void **)&d->h_recs[k],
+				cap * sizeof(struct phase2_rot_rec)),
+			"alloc pinned records");
+		d->h_recs_cap[k] = cap;
+	}
+	return 0;
+}
+
+extern "C" int p2d_run(struct p2_dev *d, const struct phase2_pass *passes,
+	size_t npass, const struct phase2_rot_rec *recs, size_t nrec)
+{
+	if (npass == 0)
+		return 0;
+	if (recs_reserve(d, nrec) < 0)
+		return -1;
+	const int k = d->ring;
+	memcpy(d->h_recs[k], recs, nrec * sizeof *recs);
+	CUDA_OK(cudaMemcpyAsync(d->d_recs, d->h_recs[k], nrec * sizeof *recs,
+			cudaMemcpyHostToDevice, d->stream),
+		"upload rotation records");
+	CUDA_OK(cudaEventRecord(d->h_ev[k], d->stream), "record staging");
+	d->h2d_bytes += nrec * sizeof *recs;
+	d->h_ev_live[k] = 1;
+	d->ring ^= 1;
+
+	if (d->timing)
+		CUDA_OK(cudaEventRecord(d->t0, d->stream), "timing start");
+	for (size_t i = 0; i < npass; i++) {
+		const int rc = d->prec == PHASE2_PREC_FP64
+			? launch_pass<double2, true>(d, passes[i], d->d_recs)
+			: launch_pass<float2, false>(d, passes[i], d->d_recs);
+		if (rc < 0)
+			return -1;
+	}
+	CUDA_OK(cudaGetLastError(), "pass launch");
+	d->passes += npass;
+	d->launches += npass;
+	d->rotations += nrec;
+	if (d->timing) {
+		CUDA_OK(cudaEventRecord(d->t1, d->stream), "timing stop");
+		CUDA_OK(cudaEventSynchronize(d->t1), "timing wait");
+		float ms = 0.0f;
+		CUDA_OK(cudaEventElapsedTime(&ms, d->t0, d->t1), "elapsed");
+		d->pass_ms += ms;
+		d->timed_passes += npass;
+	}
+	return 0;
+}
+
+static int reduce(struct p2_dev *d, const double2 *trial, double out[2])
+{
+	const unsigned blocks = grid_for(d, d->namp, P2_RED_TPB, 4);
+	if (d->part_cap < 2 * (size_t)blocks + 2) {
+		CUDA_OK(cudaStreamSynchronize(d->stream), "sync before partials");
+		cudaFree(d->d_part);
+		d->d_part = NULL;
+		d->part_cap = 0;
+		CUDA_OK(cudaMalloc((void **)&d->d_part,
+				(2 * (size_t)blocks + 2) * sizeof(double)),
+			"alloc partials");
+		d->part_cap = 2 * (size_t)blocks + 2;
+	}
+	if (d->prec == PHASE2_PREC_FP64)
+		k_reduce_partial<<<blocks, P2_RED_TPB, 0, d->stream>>>(
+			(const double2 *)d->state, trial, d->namp, d->d_part);
+	else
+		k_reduce_partial<<<blocks, P2_RED_TPB, 0, d->stream>>>(
+			(const float2 *)d->state, trial, d->namp, d->d_part);
+	k_reduce_final<<<1, P2_RED_TPB, 0, d->stream>>>(d->d_part, blocks,
+		d->d_part + 2 * (size_t)blocks);
+	d->launches += 2;
+	CUDA_OK(cudaGetLastError(), "reduce launch");
+	double h[2];
+	CUDA_OK(cudaMemcpyAsync(h, d->d_part + 2 * (size_t)blocks, sizeof h,
+			cudaMemcpyDeviceToHost, d->stream),
+		"download reduction");
+	CUDA_OK(cudaStreamSynchronize(d->stream), "reduce");
+	out[0] = h[0];
+	out[1] = h[1];
+	return 0;
+}
+
+extern "C" int p2d_norm2(struct p2_dev *d, double *out)
+{
+	double v[2];
+	if (reduce(d, NULL, v) < 0)
+		return -1;
+	*out = v[0];
+	return 0;
+}
+
+extern "C" int p2d_inner_dense(struct p2_dev *d, const double *trial,
+	double out[2])
+{
+	double2 *t = NULL;
+	const size_t bytes = d->namp * sizeof(double2);
+	CUDA_OK(cudaMalloc((void **)&t, bytes), "alloc trial");
+	cudaError_t e = cudaMemcpyAsync(t, trial, bytes, cudaMemcpyHostToDevice,
+		d->stream);
+	int rc = e == cudaSuccess ? reduce(d, t, out) : -1;
+	cudaStreamSynchronize(d->stream);
+	cudaFree(t);
+	if (e != cudaSuccess)
+		log_error("upload trial: %s", cudaGetErrorString(e));
+	return rc;
+}
+
+extern "C" int p2d_sync(struct p2_dev *d)
+{
+	CUDA_OK(cudaStreamSynchronize(d->stream), "stream sync");
+	CUDA_OK(cudaGetLastError(), "pending error");
+	return 0;
+}
+
+extern "C" void p2d_stats(const struct p2_dev *d, struct phase2_stats *st)
+{
+	st->rotations = d->rotations;
+	st->passes = d->passes;
+	st->launches = d->launches;
+	st->bytes = d->passes * 2 * d->namp * d->elem;
+	st->timed_passes = d->timed_passes;
+	st->pass_ms = d->pass_ms;
+	st->h2d_bytes = d->h2d_bytes;
+	st->d2h_bytes = d->d2h_bytes;
+}
+
+extern "C" void p2d_stats_reset(struct p2_dev *d)
+{
+	d->rotations = d->passes = d->launches = d->timed_passes = 0;
+	d->h2d_bytes = d->d2h_bytes = 0;
+	d->pass_ms = 0.0;
+}
+
+extern "C" void p2d_set_timing(struct p2_dev *d, int on)
+{
+	d->timing = on != 0;
+}
+
+extern "C" void *p2d_stream(const struct p2_dev *d)
+{
+	return (void *)d->stream;
+}

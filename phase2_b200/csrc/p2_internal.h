@@ -1,0 +1,68 @@
+/*
+ * p2_internal.h -- interfaces private to libphase2.so: the planner and the
+ * device engine (engine.cu).  Plain C types only; engine.cu implements the
+ * p2d_* functions with extern "C" linkage.
+ */
+#ifndef P2_INTERNAL_H
+#define P2_INTERNAL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "phase2_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Rotation records held in shared memory per pass. */
+#define P2_MAX_ROTS_PER_PASS 256
+/* Passes are padded to at least this many basis vectors (2^3 amplitudes
+ * per thread) to keep enough loads in flight. */
+#define P2_DEFAULT_PAD_SPAN 3
+/* Queued rotations that trigger an automatic flush. */
+#define P2_QUEUE_FLUSH 8192
+
+long p2_plan(uint32_t nqb, const struct phase2_rot_in *rots, size_t n,
+	int max_span, int max_rots, int pad_span, struct phase2_pass *passes,
+	struct phase2_rot_rec *recs);
+
+/* ---- device engine ------------------------------------------------------ */
+
+struct p2_dev;
+
+/* Select and initialise CUDA device `dev`; 0 or -1.  Sets *count to the
+ * number of visible devices when non-NULL. */
+int p2d_device_init(int dev, int *count);
+
+/* Register state of 2^nqb amplitudes at precision prec (enum phase2_prec),
+ * with its own non-blocking stream.  NULL on failure (logged). */
+struct p2_dev *p2d_create(uint32_t nqb, int prec);
+void p2d_destroy(struct p2_dev *d);
+
+int p2d_zero(struct p2_dev *d);
+int p2d_set(struct p2_dev *d, const uint64_t *idx, const double *z, size_t n);
+int p2d_get(struct p2_dev *d, const uint64_t *idx, double *z, size_t n);
+int p2d_get_state(struct p2_dev *d, double *out);
+int p2d_set_state(struct p2_dev *d, const double *in);
+
+/* Upload `nrec` records and launch `npass` passes on the stream. */
+int p2d_run(struct p2_dev *d, const struct phase2_pass *passes, size_t npass,
+	const struct phase2_rot_rec *recs, size_t nrec);
+
+int p2d_norm2(struct p2_dev *d, double *out);
+int p2d_inner_dense(struct p2_dev *d, const double *trial, double out[2]);
+
+/* Wait for the stream; -1 if any CUDA error is pending. */
+int p2d_sync(struct p2_dev *d);
+
+void p2d_stats(const struct p2_dev *d, struct phase2_stats *st);
+void p2d_stats_reset(struct p2_dev *d);
+void p2d_set_timing(struct p2_dev *d, int on);
+void *p2d_stream(const struct p2_dev *d);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* P2_INTERNAL_H */

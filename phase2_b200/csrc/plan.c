@@ -1,0 +1,223 @@
+/*
+ * plan.c -- group an ordered list of Pauli rotations into state sweeps
+ * ("passes") for the coset kernel in engine.cu.
+ *
+ * A rotation exp(i phi P) with flip mask f pairs amplitude g with g ^ f.
+ * For a run of consecutive rotations whose flip masks lie in a GF(2) space
+ * S = span(b_0 .. b_{M-1}), every coset x + S is closed under all of them.
+ * The kernel gives each thread whole cosets: it loads the 2^M amplitudes
+ * x ^ off(u), off(u) = xor of b_k over the bits k of u, applies the run in
+ * registers in the original order, and stores them back.  Per amplitude the
+ * arithmetic is exactly the reference's one-rotation-at-a-time update
+ * (phase2/qreg_qreg.c:149-160), so grouping never reorders work and the
+ * FP64 result is unchanged; only the number of HBM sweeps drops.
+ *
+ * The planner is greedy and order preserving: it appends rotations to the
+ * current pass while the span dimension stays <= max_span (diagonal terms,
+ * f = 0, always fit) and starts a new pass otherwise.  Representatives x
+ * are the indices with zero bits at the pivots of a reduced echelon form
+ * of S; because the basis restricted to the pivot columns is invertible,
+ * (x, u) -> x ^ off(u) enumerates every amplitude exactly once.
+ *
+ * Each rotation is stored in slot coordinates:
+ *   U      coefficient vector of f in the basis (partner of slot u is u^U);
+ *   odd    (1 - popcount(f & z)) & 1 -- the partner is multiplied by i;
+ *   smask  bit u = parity(u & W) ^ (((1 - popcount(f & z)) & 3) >> 1),
+ *          W bit k = parity(b_k & z);
+ * and the thread adds parity(x & z).  Then slot u is updated as
+ *   a_u <- c a_u + (-1)^sigma_u s (odd ? i : 1) a_{u^U},
+ * which equals a_g <- c a_g + i s conj(z_g) a_{g^f} with z_g = i^r(g),
+ * r(g) = popcount(f & z) + 2 popcount(g & z)  (include/phase2/paulis.h:137-144).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include "phase2_b200.h"
+
+#include "p2_internal.h"
+
+struct echelon {
+	int rows;
+	uint64_t v[PHASE2_MAX_SPAN];     /* reduced rows, pivots descending */
+	uint32_t combo[PHASE2_MAX_SPAN]; /* row = xor of basis[k], k in combo */
+	int piv[PHASE2_MAX_SPAN];
+};
+
+static inline int top_bit(uint64_t v)
+{
+	return 63 - __builtin_clzll(v);
+}
+
+/* Reduce v by the rows; returns the remainder, *combo = rows used. */
+static uint64_t ech_reduce(const struct echelon *e, uint64_t v,
+	uint32_t *combo)
+{
+	uint32_t c = 0;
+	for (int r = 0; r < e->rows; r++)
+		if (v >> e->piv[r] & 1) {
+			v ^= e->v[r];
+			c ^= e->combo[r];
+		}
+	*combo = c;
+	return v;
+}
+
+/* Insert a non-zero remainder v (combination `combo`) keeping pivots in
+ * descending order. */
+static void ech_insert(struct echelon *e, uint64_t v, uint32_t combo)
+{
+	const int p = top_bit(v);
+	int at = e->rows;
+	while (at > 0 && e->piv[at - 1] < p) {
+		e->v[at] = e->v[at - 1];
+		e->combo[at] = e->combo[at - 1];
+		e->piv[at] = e->piv[at - 1];
+		at--;
+	}
+	e->v[at] = v;
+	e->combo[at] = combo;
+	e->piv[at] = p;
+	e->rows++;
+}
+
+struct pass_builder {
+	struct echelon ech;
+	uint64_t basis[PHASE2_MAX_SPAN];
+	int m;
+	/* rotations of the open pass (indices into the caller's arrays) */
+	size_t first_rec;
+	uint32_t nrot;
+};
+
+static void builder_reset(struct pass_builder *b, size_t first_rec)
+{
+	memset(b, 0, sizeof *b);
+	b->first_rec = first_rec;
+}
+
+/* Add basis vector f (not in the span); returns its slot bit. */
+static uint32_t builder_add(struct pass_builder *b, uint64_t f)
+{
+	uint32_t combo;
+	const uint64_t v = ech_reduce(&b->ech, f, &combo);
+	const int k = b->m++;
+	b->basis[k] = f;
+	ech_insert(&b->ech, v, combo ^ (UINT32_C(1) << k));
+	return UINT32_C(1) << k;
+}
+
+static inline int parity64(uint64_t v)
+{
+	return __builtin_popcountll(v) & 1;
+}
+
+/* Close the open pass: pad the basis with unit vectors (more amplitudes per
+ * thread, contiguous along low qubits), fix pivots, fill slot masks. */
+static void builder_close(struct pass_builder *b, uint32_t nqb, int pad_to,
+	const struct phase2_rot_in *rots, struct phase2_pass *pass,
+	struct phase2_rot_rec *recs)
+{
+	for (uint32_t q = 0; b->m < pad_to && q < nqb; q++) {
+		uint32_t combo;
+		if (ech_reduce(&b->ech, UINT64_C(1) << q, &combo) != 0)
+			(void)builder_add(b, UINT64_C(1) << q);
+	}
+	memset(pass, 0, sizeof *pass);
+	pass->span = (uint32_t)b->m;
+	pass->nrot = b->nrot;
+	pass->rot_off = (uint32_t)b->first_rec;
+	/* pivots ascending (the echelon keeps them descending) */
+	for (int k = 0; k < b->m; k++) {
+		pass->piv[k] = (uint8_t)b->ech.piv[b->m - 1 - k];
+		pass->basis[k] = b->basis[k];
+	}
+	const uint32_t nslot = UINT32_C(1) << b->m;
+	for (uint32_t r = 0; r < b->nrot; r++) {
+		struct phase2_rot_rec *rec = &recs[b->first_rec + r];
+		const struct phase2_rot_in *in = &rots[b->first_rec + r];
+		uint32_t W = 0;
+		for (int k = 0; k < b->m; k++)
+			W |= (uint32_t)parity64(b->basis[k] & in->phase) << k;
+		const int kbase =
+			(1 - __builtin_popcountll(in->flip & in->phase)) & 3;
+		uint32_t smask = 0;
+		for (uint32_t u = 0; u < nslot; u++)
+			smask |= (uint32_t)((__builtin_popcount(u & W) & 1) ^
+					(kbase >> 1))
+				<< u;
+		rec->smask = smask;
+		rec->odd = (uint8_t)(kbase & 1);
+	}
+}
+
+long phase2_plan(uint32_t nqb, const struct phase2_rot_in *rots, size_t n,
+	int max_span, int max_rots, struct phase2_pass *passes,
+	struct phase2_rot_rec *recs)
+{
+	return p2_plan(nqb, rots, n, max_span, max_rots, P2_DEFAULT_PAD_SPAN,
+		passes, recs);
+}
+
+/* Records are emitted in input order: recs[i] describes rots[i]. */
+long p2_plan(uint32_t nqb, const struct phase2_rot_in *rots, size_t n,
+	int max_span, int max_rots, int pad_span, struct phase2_pass *passes,
+	struct phase2_rot_rec *recs)
+{
+	if (nqb == 0 || nqb > QREG_MAX_WIDTH)
+		return -1;
+	if (max_span < 1)
+		max_span = 1;
+	if (max_span > PHASE2_MAX_SPAN)
+		max_span = PHASE2_MAX_SPAN;
+	if ((uint32_t)max_span > nqb)
+		max_span = (int)nqb;
+	if (pad_span > max_span)
+		pad_span = max_span;
+	if (pad_span < 0)
+		pad_span = 0;
+	const uint32_t cap = (max_rots > 0 && max_rots < P2_MAX_ROTS_PER_PASS)
+		? (uint32_t)max_rots
+		: P2_MAX_ROTS_PER_PASS;
+
+	long npass = 0;
+	struct pass_builder b;
+	builder_reset(&b, 0);
+	for (size_t i = 0; i < n; i++) {
+		const uint64_t f = rots[i].flip;
+		uint32_t U = 0;
+		int fits = b.nrot < cap;
+		if (fits && f != 0) {
+			uint32_t combo;
+			const uint64_t v = ech_reduce(&b.ech, f, &combo);
+			if (v == 0)
+				U = combo;
+			else if (b.m < max_span)
+				U = 0xffffffffu; /* new basis vector */
+			else
+				fits = 0;
+		}
+		if (!fits) {
+			builder_close(&b, nqb, pad_span, rots, &passes[npass],
+				recs);
+			npass++;
+			builder_reset(&b, i);
+			if (f != 0)
+				U = 0xffffffffu;
+		}
+		if (U == 0xffffffffu)
+			U = builder_add(&b, f);
+		struct phase2_rot_rec *rec = &recs[i];
+		rec->z = rots[i].phase;
+		rec->c = cos(rots[i].phi);
+		rec->s = sin(rots[i].phi);
+		rec->U = (uint16_t)U;
+		rec->pad = 0;
+		b.nrot++;
+	}
+	if (b.nrot > 0) {
+		builder_close(&b, nqb, pad_span, rots, &passes[npass], recs);
+		npass++;
+	}
+	return npass;
+}

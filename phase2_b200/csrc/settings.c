@@ -1,0 +1,74 @@
+/*
+ * settings.c -- process-wide defaults of the B200 extensions
+ * (include/phase2_b200.h): precision, fusion policy and term order.
+ */
+#include <stdlib.h>
+#include <string.h>
+
+#define LOG_SUBSYS "cfg"
+#include "log.h"
+
+#include "phase2_b200.h"
+
+#include "p2_host.h"
+
+struct p2_settings p2_cfg = {
+	.prec = PHASE2_PREC_FP64,
+	.max_span = PHASE2_MAX_SPAN,
+	.max_rots = 0,
+	.order = PHASE2_ORDER_LEX,
+};
+
+void p2_settings_from_env(void)
+{
+	const char *p = getenv("PHASE2_PRECISION");
+	if (p && *p) {
+		if (!strcmp(p, "fp32") || !strcmp(p, "FP32"))
+			p2_cfg.prec = PHASE2_PREC_FP32;
+		else if (!strcmp(p, "fp64") || !strcmp(p, "FP64"))
+			p2_cfg.prec = PHASE2_PREC_FP64;
+		else
+			log_warn("PHASE2_PRECISION=%s not understood", p);
+	}
+}
+
+int phase2_set_precision(int prec)
+{
+	if (prec != PHASE2_PREC_FP64 && prec != PHASE2_PREC_FP32)
+		return -1;
+	p2_cfg.prec = prec;
+	return 0;
+}
+
+int phase2_get_precision(void)
+{
+	return p2_cfg.prec;
+}
+
+int phase2_set_fusion(int max_span, int max_rots)
+{
+	if (max_span < 1 || max_span > PHASE2_MAX_SPAN || max_rots < 0)
+		return -1;
+	p2_cfg.max_span = max_span;
+	p2_cfg.max_rots = max_rots;
+	return 0;
+}
+
+int phase2_set_term_order(int order)
+{
+	if (order != PHASE2_ORDER_LEX && order != PHASE2_ORDER_GIVEN &&
+		order != PHASE2_ORDER_FLIP)
+		return -1;
+	p2_cfg.order = order;
+	return 0;
+}
+
+int phase2_get_term_order(void)
+{
+	return p2_cfg.order;
+}
+
+const char *phase2_version(void)
+{
+	return "phase2-b200 0.1.0 (sm_100a)";
+}

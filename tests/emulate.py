@@ -1,0 +1,59 @@
+"""numpy execution of planned passes (TEST INFRASTRUCTURE).
+
+Applies the pass descriptors and rotation records produced by
+phase2_plan exactly as the device kernel interprets them: each
+representative x (zeros at the pivots) owns the slots x ^ off(u), and
+rotation r updates slot u as
+    a_u <- c a_u + (-1)^sigma_u s (odd ? i : 1) a_{u ^ U},
+    sigma_u = bit u of (smask ^ -parity(x & z)).
+Products and sums are rounded separately (numpy never fuses), as the
+FP64 kernel does with __dmul_rn/__dadd_rn, so results must match the
+oracle bit for bit.
+"""
+
+import numpy as np
+
+
+def _parity(v: np.ndarray) -> np.ndarray:
+    v = v.copy()
+    for sh in (32, 16, 8, 4, 2, 1):
+        v ^= v >> np.uint64(sh)
+    return (v & np.uint64(1)).astype(np.int64)
+
+
+def emulate(amp: np.ndarray, nqb: int, passes, recs) -> np.ndarray:
+    a = np.array(amp, dtype=np.complex128)
+    re, im = a.real.copy(), a.imag.copy()
+    for p in passes:
+        M = p["span"]
+        x = np.arange(1 << (nqb - M), dtype=np.uint64)
+        for q in p["piv"]:
+            q = np.uint64(q)
+            low = x & ((np.uint64(1) << q) - np.uint64(1))
+            x = ((x >> q) << (q + np.uint64(1))) | low
+        offs = []
+        for u in range(1 << M):
+            o = 0
+            for k in range(M):
+                if u >> k & 1:
+                    o ^= int(p["basis"][k])
+            offs.append(o)
+        idx = x[:, None] ^ np.array(offs, dtype=np.uint64)[None, :]
+        R, I = re[idx], im[idx]
+        for r in recs[p["rot_off"]:p["rot_off"] + p["nrot"]]:
+            px = _parity(x & np.uint64(r["z"]))
+            sm = (np.int64(r["smask"]) ^ (-px)) & 0xFFFFFFFF
+            c, s, U, odd = r["c"], r["s"], r["U"], r["odd"]
+            nR, nI = R.copy(), I.copy()
+            for u in range(1 << M):
+                w = u ^ U
+                su = np.where((sm >> u) & 1, -s, s)
+                if odd:
+                    tr, ti = (-su) * I[:, w], su * R[:, w]
+                else:
+                    tr, ti = su * R[:, w], su * I[:, w]
+                nR[:, u] = c * R[:, u] + tr
+                nI[:, u] = c * I[:, u] + ti
+            R, I = nR, nI
+        re[idx], im[idx] = R, I
+    return re + 1j * im

@@ -1,0 +1,256 @@
+"""Host-side checks of libphase2.so that need no GPU.
+
+* the library loads and exports every function declared in include/;
+* ctypes struct layouts equal the C ones;
+* Pauli algebra, xoshiro256**, CDF sampling and the batch cache reproduce
+  the reference's golden vectors exactly;
+* the pass planner: its descriptors, executed by a numpy emulation of the
+  device kernel (tests/emulate.py), reproduce the oracle bit for bit.
+"""
+
+import ctypes as C
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from phase2_b200 import _ffi, plan, workloads
+from phase2_b200._ffi import lib
+
+from conftest import ROOT
+from emulate import emulate
+
+
+def _declared_functions() -> set[str]:
+    names = set()
+    for h in sorted((ROOT / "include").rglob("*.h")):
+        src = h.read_text()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        src = re.sub(r"^\s*#.*?(?<!\\)$", "", src, flags=re.M)
+        # drop static inline definitions (header-only helpers)
+        src = re.sub(r"static\s+inline[^{;]*\{.*?\n\}", "", src, flags=re.S)
+        for m in re.finditer(
+                r"([A-Za-z_][A-Za-z0-9_]*)\s*\(([^;{}()]|\([^;{}()]*\))*\)"
+                r"\s*(__attribute__\s*\(\(.*?\)\))?\s*;", src, flags=re.S):
+            name = m.group(1)
+            if name not in ("__attribute__", "format", "sizeof"):
+                names.add(name)
+    return names
+
+
+def test_library_loads():
+    L = lib()
+    assert b"sm_100a" in L.phase2_version()
+
+
+def test_exports_every_declared_function():
+    declared = _declared_functions()
+    assert "qreg_paulirot" in declared and "phase2_run" in declared
+    assert len(declared) > 80
+    out = subprocess.run(["nm", "-D", "--defined-only", str(_ffi.LIB_PATH)],
+                         capture_output=True, text=True, check=True).stdout
+    exported = {ln.split()[-1] for ln in out.splitlines() if " T " in ln}
+    missing = sorted(declared - exported)
+    assert not missing, missing
+    # internals stay hidden
+    assert not any(s.startswith(("p2d_", "p2_")) for s in exported)
+
+
+def test_struct_layouts():
+    for k, (py, c) in _ffi.check_layout().items():
+        assert py == c, (k, py, c)
+
+
+def _paulis(f, p):
+    return _ffi.Paulis((C.c_uint64 * 2)(f, p))
+
+
+def test_paulis_effect_and_cmp(golden):
+    L = lib()
+    for e in golden["paulis_effect"]:
+        z = (C.c_double * 2)(1.0, 0.0)
+        j = L.paulis_effect(_paulis(e["flip"], e["phase"]), e["i"], z)
+        assert j == e["j"]
+        assert (z[0] + 0.0, z[1] + 0.0) == (e["z"][0] + 0.0,
+                                            e["z"][1] + 0.0)
+    for c in golden["paulis_cmp"]:
+        a, b = c["a"], c["b"]
+        assert L.paulis_cmp(_paulis(*a), _paulis(*b)) == c["cmp"]
+
+
+def test_paulis_get_set_split():
+    L = lib()
+    p = L.paulis_new()
+    for q, op in ((0, 1), (1, 2), (2, 3), (63, 2), (40, 1)):
+        L.paulis_set(C.byref(p), op, q)
+        assert L.paulis_get(p, q) == op
+    L.paulis_set(C.byref(p), 0, 1)
+    assert L.paulis_get(p, 1) == 0
+    L.paulis_set(C.byref(p), 7, 2)  # unknown op: unchanged
+    assert L.paulis_get(p, 2) == 3
+    lo, hi = _ffi.Paulis(), _ffi.Paulis()
+    L.paulis_split(p, 3, 38, C.byref(lo), C.byref(hi))
+    assert lo.pak[0] == p.pak[0] & 7 and lo.pak[1] == p.pak[1] & 7
+    assert hi.pak[0] == p.pak[0] & ((1 << 41) - 8)
+    q = _ffi.Paulis((C.c_uint64 * 2)(p.pak[0], p.pak[1]))
+    L.paulis_shr(C.byref(q), 5)
+    L.paulis_shl(C.byref(q), 5)
+    assert q.pak[0] == p.pak[0] & ~31 & (2**64 - 1)
+
+
+def test_xoshiro(golden):
+    L = lib()
+    for case in golden["xoshiro"]:
+        st = _ffi.Xoshiro()
+        L.xoshiro256ss_init(C.byref(st), case["seed"])
+        got = [L.xoshiro256ss_next(C.byref(st)) for _ in range(32)]
+        assert got == case["next"]
+
+
+def test_prob(golden):
+    L = lib()
+    assert L.prob_cdf_init(C.byref(_ffi.ProbCdf()), 0) == -1
+    for c in golden["prob"]:
+        w = (C.c_double * len(c["w"]))(*c["w"])
+        cdf = _ffi.ProbCdf()
+        assert L.prob_cdf_init(C.byref(cdf), len(c["w"])) == 0
+        lam = C.c_double(-1)
+        rc = L.prob_cdf_from_array_strided(C.byref(cdf), w, 8, C.byref(lam))
+        assert rc == c["rc"]
+        if rc == 0:
+            assert lam.value == c["lambda"]
+            assert [cdf.y[k] for k in range(cdf.len)] == c["y"]
+            for q, want in zip(c["q"], c["inv"]):
+                assert L.prob_cdf_inverse(C.byref(cdf), q) == want
+        L.prob_cdf_free(C.byref(cdf))
+        assert cdf.len == 0 and not cdf.y
+        L.prob_cdf_free(C.byref(cdf))  # idempotent
+
+
+def test_cache_capacity_and_flush():
+    """Batch semantics of test/t-circ_cache.c: 1024 terms, hi-code split."""
+    L = lib()
+    c = L.circ_cache_init(0, 20)
+    for k in range(1024):
+        assert L.circ_cache_insert(c, _paulis(k & 0xFFFFF, 0), 0.1) == 0
+    assert L.circ_cache_len(c) == 1024
+    assert L.circ_cache_insert(c, _paulis(1, 0), 0.1) == -1
+    L.circ_cache_free(c)
+    c = L.circ_cache_init(2, 4)
+    assert L.circ_cache_insert(c, _paulis(0b010000, 0), 0.1) == 0
+    assert L.circ_cache_insert(c, _paulis(0b010001, 0), 0.1) == 0
+    assert L.circ_cache_insert(c, _paulis(0b100001, 0), 0.1) == -1
+    L.circ_cache_free(c)
+
+
+def _hamil(nqb, t):
+    L = lib()
+    hm = _ffi.CircHamil()
+    assert L.circ_hamil_init(C.byref(hm), nqb, len(t)) == 0
+    rec = t.records()
+    C.memmove(hm.terms, rec.ctypes.data, rec.nbytes)
+    return hm
+
+
+def _terms_of(hm):
+    n = hm.len
+    buf = np.ctypeslib.as_array(C.cast(hm.terms, C.POINTER(C.c_uint8)),
+                                shape=(24 * n,))
+    return np.frombuffer(buf.tobytes(), dtype=[("cf", "<f8"),
+                                               ("flip", "<u8"),
+                                               ("phase", "<u8")])
+
+
+def test_sort_lex_matches_oracle(oracle_lib):
+    L = lib()
+    t = workloads.random_terms(20, 500, seed=3)
+    # duplicate operators with different coefficients exercise ties
+    t.flip[::7], t.phase[::7] = t.flip[0], t.phase[0]
+    hm = _hamil(20, t)
+    L.circ_hamil_sort_lex(C.byref(hm))
+    got = _terms_of(hm)
+    want = oracle_lib.sort_lex(t.flip, t.phase, t.cf)
+    assert got.tobytes() == want.tobytes()
+    L.circ_hamil_free(C.byref(hm))
+
+
+def test_sort_flip_is_stable():
+    L = lib()
+    t = workloads.jw_terms(12, 400, seed=9)
+    hm = _hamil(12, t)
+    L.circ_hamil_sort_flip(C.byref(hm))
+    got = _terms_of(hm)
+    want = workloads.sort_by_flip(t)
+    assert np.array_equal(got["flip"], want.flip)
+    assert np.array_equal(got["phase"], want.phase)
+    assert np.array_equal(got["cf"], want.cf)
+    L.circ_hamil_free(C.byref(hm))
+
+
+def _rand_rotations(rng, n, k, diag_frac=0.2):
+    t = workloads.random_terms(n, k, seed=int(rng.integers(1 << 30)))
+    mask = rng.random(k) < diag_frac
+    t.flip[mask] = 0
+    phi = rng.uniform(-np.pi, np.pi, k)
+    return t.flip, t.phase, phi
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 8, 11])
+@pytest.mark.parametrize("span,max_rots", [(1, 1), (2, 0), (3, 0), (5, 0),
+                                           (5, 1), (4, 3)])
+def test_planner_emulation_bit_exact(n, span, max_rots, oracle_lib):
+    rng = np.random.Generator(np.random.PCG64(n * 100 + span * 10 + max_rots))
+    flip, phase, phi = _rand_rotations(rng, n, 60)
+    amp = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+    passes, recs = plan(n, flip, phase, phi, span, max_rots)
+    assert sum(p["nrot"] for p in passes) == 60
+    for p in passes:
+        assert p["span"] <= max(span, min(3, n))
+        if max_rots:
+            assert p["nrot"] <= max_rots
+    got = emulate(amp, n, passes, recs)
+    want = oracle_lib.rotate(amp, n, flip, phase, phi)
+    assert np.array_equal(got, want)
+
+
+def test_planner_fuses_jw_runs():
+    t = workloads.jw_terms(20, 2000, seed=4)
+    phi = np.full(len(t), 0.01)
+    passes, _ = plan(20, t.flip, t.phase, phi, 5, 0)
+    # 8 strings share each excitation's flip mask: runs fuse
+    assert len(passes) < len(t) / 8
+    one, _ = plan(20, t.flip, t.phase, phi, 5, 1)
+    assert len(one) == len(t)
+
+
+def test_planner_rejects_bad_width():
+    L = lib()
+    rin = (_ffi.RotIn * 1)()
+    assert L.phase2_plan(0, rin, 1, 5, 0, (_ffi.Pass * 1)(),
+                         (_ffi.RotRec * 1)()) == -1
+
+
+def test_settings_validate():
+    L = lib()
+    assert L.phase2_set_precision(7) == -1
+    assert L.phase2_set_fusion(0, 0) == -1
+    assert L.phase2_set_fusion(6, 0) == -1
+    assert L.phase2_set_term_order(9) == -1
+    assert L.phase2_set_term_order(2) == 0
+    assert L.phase2_get_term_order() == 2
+    assert L.phase2_set_term_order(0) == 0
+
+
+def test_phase2_run_rejects_without_touching_device():
+    """Inputs rejected before the world starts (psi NULL or bad length)."""
+    L = lib()
+    re_, im_ = C.c_double(), C.c_double()
+    arr = (C.c_char_p * 1)(b"Z0")
+    cf = (C.c_double * 1)(1.0)
+    assert L.phase2_run(arr, cf, 1, 0.1, None, C.byref(re_),
+                        C.byref(im_)) == -1
+    assert L.phase2_run(arr, cf, 1, 0.1, b"", C.byref(re_),
+                        C.byref(im_)) == -1
+    assert L.phase2_run(arr, cf, 1, 0.1, b"0" * 31, C.byref(re_),
+                        C.byref(im_)) == -1

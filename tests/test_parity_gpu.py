@@ -1,0 +1,374 @@
+"""GPU parity of libphase2.so against the oracle (the parity tests proper).
+
+Everything here runs the sm_100a kernels through the C-ABI and compares
+with the CPU restatement (oracle/liboracle.so), the reference's golden
+vectors (tests/golden/) or, for registers too wide for a dense CPU state,
+an exact sparse restatement (tests/sparse.py).
+
+Tolerances:
+  FP64 state  -- bit-identical (np.array_equal) to the oracle; the bar the
+                 path is held to is 1e-12 relative per overlap, which
+                 bit-identity implies.
+  FP32 state  -- 1e-5 absolute per amplitude / overlap for short runs
+                 (one FP32 rounding per pass, FP64 arithmetic inside).
+"""
+
+import math
+
+import numpy as np
+import pytest
+
+import phase2_b200 as p2
+from phase2_b200 import Dets, Register, Terms, workloads
+
+from conftest import GOLDEN
+from sparse import rotate as sparse_rotate
+
+pytestmark = pytest.mark.gpu
+
+FP32_TOL = 1e-5
+
+
+def _cz(v):
+    return complex(v[0], v[1])
+
+
+def _rand_state(rng, n):
+    a = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+    return a / np.linalg.norm(a)
+
+
+def _rand_rots(rng, n, k, diag_frac=0.2):
+    t = workloads.random_terms(n, k, seed=int(rng.integers(1 << 30)))
+    t.flip[rng.random(k) < diag_frac] = 0
+    return t.flip, t.phase, rng.uniform(-math.pi, math.pi, k)
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _world():
+    p2.world_ensure()
+    p2.set_precision(p2.PREC_FP64)
+    p2.set_fusion(5, 0)
+    yield
+
+
+# ---- register level ----------------------------------------------------
+
+
+def test_paulirot_golden_fixture():
+    f = np.load(GOLDEN / "paulirot.npz")
+    with Register(9, p2.PREC_FP64) as r:
+        r.set_state(f["amp0"])
+        r.paulirot(f["flip"], f["phase"], f["phi"])
+        assert np.array_equal(r.get_state(), f["amp1"])
+    with Register(9, p2.PREC_FP32) as r:
+        r.set_state(f["amp0"])
+        r.paulirot(f["flip"], f["phase"], f["phi"])
+        assert np.max(np.abs(r.get_state() - f["amp1"])) < FP32_TOL
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 6, 7, 9, 12, 14])
+@pytest.mark.parametrize("fusion", [(5, 0), (1, 1), (3, 0), (4, 2)])
+def test_random_rotations_bit_exact(n, fusion, oracle_lib):
+    rng = np.random.Generator(np.random.PCG64(7 * n + fusion[0]))
+    amp = _rand_state(rng, n)
+    flip, phase, phi = _rand_rots(rng, n, 120)
+    want = oracle_lib.rotate(amp, n, flip, phase, phi)
+    with Register(n, p2.PREC_FP64) as r:
+        r.set_fusion(*fusion)
+        r.set_state(amp)
+        r.paulirot(flip, phase, phi, batch=37)
+        got = r.get_state()
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("n", [3, 10, 15])
+def test_fp32_state_close(n, oracle_lib):
+    rng = np.random.Generator(np.random.PCG64(1000 + n))
+    amp = _rand_state(rng, n)
+    flip, phase, phi = _rand_rots(rng, n, 200)
+    want = oracle_lib.rotate(amp, n, flip, phase, phi)
+    with Register(n, p2.PREC_FP32) as r:
+        assert r.precision == p2.PREC_FP32
+        r.set_state(amp)
+        r.paulirot(flip, phase, phi)
+        got = r.get_state()
+        nrm = r.norm2()
+    err = np.max(np.abs(got - want))
+    assert err < FP32_TOL * max(1.0, np.max(np.abs(want)) * 10), err
+    assert abs(nrm - 1.0) < 1e-5
+
+
+def test_identity_rotation_is_phase():
+    """test/t-qreg.c:139-166: P = I multiplies every amplitude by e^{i phi}."""
+    rng = np.random.Generator(np.random.PCG64(1))
+    amp = rng.random(1 << 13) + 1j * rng.random(1 << 13)
+    with Register(13) as r:
+        r.set_state(amp)
+        r.paulirot([0], [0], [0.711])
+        got = r.get_state()
+    assert np.max(np.abs(got - amp * np.exp(1j * 0.711))) < 1e-14
+
+
+def test_y_and_yyy_explicit():
+    """test/t-qreg.c:168-232: exp(i a Y)|0> and exp(i a YYY)|000>."""
+    a = 0.11
+    with Register(1) as r:
+        r.zero()
+        r.setamps([0], [2.0])
+        r.paulirot([1], [1], [a])
+        z = r.getamps([0, 1])
+    assert abs(z[0] - 2 * math.cos(a)) < 1e-14
+    assert abs(z[1] + 2 * math.sin(a)) < 1e-14
+    with Register(3) as r:
+        r.zero()
+        r.setamps([0], [2.0])
+        r.paulirot([7], [7], [a])
+        z = r.getamps([0, 7])
+    assert abs(z[0] - 2 * math.cos(a)) < 1e-14
+    assert abs(z[1] - 2 * math.sin(a)) < 1e-14
+
+
+def test_get_set_zero_roundtrip():
+    rng = np.random.Generator(np.random.PCG64(2))
+    n = 13
+    amp = rng.random(1 << n) + 1j * rng.random(1 << n)
+    with Register(n) as r:
+        idx = np.arange(1 << n, dtype=np.uint64)
+        r.setamps(idx, amp)
+        assert np.array_equal(r.getamps(idx), amp)
+        r.zero()
+        assert not np.any(r.get_state())
+        # later writes win on duplicate indices, as sequential setamp
+        r.setamps([5, 5, 9], [1.0, 2.0, 3.0])
+        assert np.array_equal(r.getamps([5, 9]), [2.0, 3.0])
+        with pytest.raises(RuntimeError):
+            r.getamps([1 << n])
+
+
+def test_deterministic_across_runs():
+    """test/t-qreg.c:456-503: identical inputs give identical bits."""
+    rng = np.random.Generator(np.random.PCG64(3))
+    amp = _rand_state(rng, 12)
+    flip, phase, phi = _rand_rots(rng, 12, 300)
+    outs = []
+    for _ in range(2):
+        with Register(12) as r:
+            r.set_state(amp)
+            r.paulirot(flip, phase, phi)
+            outs.append(r.get_state())
+    assert np.array_equal(outs[0], outs[1])
+
+
+def test_stats_count_passes():
+    t = workloads.jw_terms(16, 256, seed=5)
+    with Register(16) as r:
+        r.reset_stats()
+        r.paulirot(t.flip, t.phase, np.full(len(t), 0.01))
+        r.synchronize()
+        st = r.stats()
+    assert st["rotations"] == 256
+    assert 0 < st["passes"] < 256
+    assert st["bytes"] == st["passes"] * 2 * (1 << 16) * 16
+
+
+# ---- drivers -----------------------------------------------------------
+
+
+def _driver_case(c):
+    t = Terms(np.array(c["flip"], dtype=np.uint64),
+              np.array(c["phase"], dtype=np.uint64), np.array(c["cf"]))
+    d = Dets(np.array(c["det_idx"], dtype=np.uint64),
+             np.array([_cz(v) for v in c["det_cf"]]))
+    return t, d
+
+
+def test_drivers_match_golden(golden):
+    for c in golden["drivers"]:
+        t, d = _driver_case(c)
+        n = c["nqb"]
+        if c["kind"] in ("trott", "trott2"):
+            p2.set_term_order(0 if c["lex"] else 1)
+            fn = p2.trott if c["kind"] == "trott" else p2.trott2
+            z = fn(n, t, d, c["steps"], c["delta"])
+        elif c["kind"] == "qdrift":
+            p2.set_term_order(0)
+            z = p2.qdrift(n, t, d, c["samples"], c["depth"], c["step_size"],
+                          c["seed"])
+        else:
+            p2.set_term_order(0)
+            z = p2.cmpsit(n, t, d, c["samples"], c["steps"], c["length"],
+                          c["depth"], c["angle_det"], c["angle_rand"],
+                          c["seed"])
+        want = np.array([_cz(v) for v in c["z"]])
+        assert np.all(np.abs(z - want) <= 1e-12 * np.maximum(1, abs(want)))
+        assert np.array_equal(z, want), c["kind"]
+    p2.set_term_order(0)
+
+
+def test_trotter12_golden(golden):
+    cfg = workloads.trotter12()
+    z = p2.trott(12, cfg["terms"], cfg["dets"], cfg["steps"], cfg["delta"])
+    want = np.array([_cz(v) for v in golden["trotter12"]["z"]])
+    assert np.array_equal(z, want)
+
+
+def test_trotter12_fp32(golden):
+    cfg = workloads.trotter12()
+    p2.set_precision(p2.PREC_FP32)
+    try:
+        z = p2.trott(12, cfg["terms"], cfg["dets"], cfg["steps"],
+                     cfg["delta"])
+    finally:
+        p2.set_precision(p2.PREC_FP64)
+    want = np.array([_cz(v) for v in golden["trotter12"]["z"]])
+    assert np.max(np.abs(z - want)) < FP32_TOL
+
+
+@pytest.mark.parametrize("order2", [False, True])
+def test_trott_jw_vs_oracle(order2, oracle_lib):
+    t = workloads.jw_terms(12, 300, seed=11)
+    d = workloads.hamming_dets(12, 6, 6, seed=12)
+    fn = p2.trott2 if order2 else p2.trott
+    z = fn(12, t, d, 5, 0.2)
+    want = oracle_lib.trott(12, t.flip, t.phase, t.cf, d.idx, d.cf, 5, 0.2,
+                            order2=order2)
+    assert np.array_equal(z, want)
+
+
+def test_qdrift_cmpsit_vs_oracle(oracle_lib):
+    t = workloads.jw_terms(11, 500, seed=13)
+    d = workloads.hamming_dets(11, 3, 5, seed=14)
+    z = p2.qdrift(11, t, d, 5, 300, 0.01, 0xABC)
+    want = oracle_lib.qdrift(11, t.flip, t.phase, t.cf, d.idx, d.cf, 5, 300,
+                             0.01, 0xABC)
+    assert np.array_equal(z, want)
+    z = p2.cmpsit(11, t, d, 2, 3, 50, 100, 0.05, 0.002, 0xDEF)
+    want = oracle_lib.cmpsit(11, t.flip, t.phase, t.cf, d.idx, d.cf, 2, 3,
+                             50, 100, 0.05, 0.002, 0xDEF)
+    assert np.array_equal(z, want)
+
+
+def test_flip_order_vs_oracle_given_order(oracle_lib):
+    t = workloads.jw_terms(13, 400, seed=15)
+    d = workloads.hamming_dets(13, 4, 6, seed=16)
+    p2.set_term_order(2)
+    try:
+        z = p2.trott2(13, t, d, 3, 0.1)
+    finally:
+        p2.set_term_order(0)
+    s = workloads.sort_by_flip(t)
+    want = oracle_lib.trott(13, s.flip, s.phase, s.cf, d.idx, d.cf, 3, 0.1,
+                            order2=True, sort_lex=False)
+    assert np.array_equal(z, want)
+
+
+def test_empty_hamiltonian_and_edges():
+    t = Terms(np.zeros(0, np.uint64), np.zeros(0, np.uint64), np.zeros(0))
+    d = Dets(np.array([3], np.uint64), np.array([1.0 + 0j]))
+    z = p2.trott(4, t, d, 3, 0.1)
+    assert np.array_equal(z, np.ones(3, dtype=complex))
+    with pytest.raises(RuntimeError):  # qdrift needs a non-empty CDF
+        p2.qdrift(4, t, d, 1, 4, 0.1, 1)
+
+
+# ---- one-shot entry (python/tests/test_phase2.py of the reference) -----
+
+
+def test_phase2_run_golden(golden):
+    for c in golden["phase2_run"]:
+        if c["rc"] != 0:
+            with pytest.raises(ValueError):
+                p2.run(c["paulis"], c["coeffs"], c["delta"], c["psi"])
+            continue
+        z = p2.run(c["paulis"], c["coeffs"], c["delta"], c["psi"])
+        assert z == _cz(c["z"]), c
+
+
+def test_phase2_run_analytic():
+    TOL = 1e-12
+    assert isinstance(p2.run(["Z0"], [1.0], 0.1, "0"), complex)
+    a = 0.3
+    z = p2.run(["Z0"], [1.0], a, "0")
+    assert abs(z - complex(math.cos(a), math.sin(a))) < TOL
+    z = p2.run(["Z0"], [1.0], 0.7, "1")
+    assert abs(z - complex(math.cos(0.7), -math.sin(0.7))) < TOL
+    z = p2.run(["X0", "X0"], [1.0, 1.0], 0.4, "0")
+    assert abs(z.real - math.cos(0.8)) < TOL
+    h = [0.1 * (k + 1) for k in range(10)]
+    z = p2.run([f"X{k}" for k in range(10)], h, 0.05, "0" * 10)
+    assert abs(z.real - math.prod(math.cos(0.05 * x) for x in h)) < TOL
+    assert abs(p2.run([], [], 1.0, "00") - 1.0) < TOL
+    assert abs(p2.run(["Z0"], [1.0], math.pi / 2, "0") - 1j) < TOL
+    for bad in ((["Z0"], [1.0, 2.0], 0.1, "0"), (["W0"], [1.0], 0.1, "0"),
+                (["X5"], [1.0], 0.1, "0"), (["Z0"], [1.0], 0.1, "2")):
+        with pytest.raises(ValueError):
+            p2.run(*bad)
+    args = (["X0", "Z1"], [0.3, -0.7], 0.25, "01")
+    assert p2.run(*args) == p2.run(*args)
+
+
+# ---- wide registers: exact sparse checks, size-independent properties --
+
+
+@pytest.mark.parametrize("n,prec", [(26, 0), (30, 0), (30, 1), (33, 0)])
+def test_wide_register_sparse_exact(n, prec):
+    t = workloads.jw_terms(n, 400, seed=20 + n)
+    rng = np.random.Generator(np.random.PCG64(n))
+    pick = rng.choice(len(t), 10, replace=False)
+    flip, phase = t.flip[pick], t.phase[pick]
+    flip[3] = 1 << (n - 1) | 1   # top and bottom qubit
+    phase[3] = 1 << (n - 2)
+    flip[6] = 0                  # one diagonal term
+    phi = rng.uniform(-1, 1, 10)
+    start = {int(1 << (n - 1)) | 5: 0.6 + 0.0j, 3: 0.0 + 0.8j}
+    want = dict(start)
+    for k in range(10):
+        want = sparse_rotate(want, int(flip[k]), int(phase[k]), float(phi[k]))
+    idx = np.array(sorted(want), dtype=np.uint64)
+    with Register(n, prec) as r:
+        r.zero()
+        r.setamps(list(start), list(start.values()))
+        r.paulirot(flip, phase, phi)
+        got = r.getamps(idx)
+        nrm = r.norm2()
+    exp = np.array([want[int(i)] for i in idx])
+    if prec == 0:
+        assert np.array_equal(got, exp)
+        assert abs(nrm - 1.0) < 1e-12
+    else:
+        assert np.max(np.abs(got - exp)) < FP32_TOL
+
+
+def test_fused_equals_plain_and_inverse_at_scale():
+    """24 qubits, dense state: fused FP64 == one-rotation-per-pass FP64 bit
+    for bit; applying the reversed sequence at -phi restores the state."""
+    n = 24
+    rng = np.random.Generator(np.random.PCG64(24))
+    amp = _rand_state(rng, n)
+    t = workloads.jw_terms(n, 600, seed=24)
+    phi = rng.uniform(-0.5, 0.5, len(t))
+    outs = []
+    for fusion in ((5, 0), (1, 1)):
+        with Register(n) as r:
+            r.set_fusion(*fusion)
+            r.set_state(amp)
+            r.paulirot(t.flip, t.phase, phi)
+            outs.append(r.get_state())
+            if fusion == (5, 0):
+                r.paulirot(t.flip[::-1], t.phase[::-1], -phi[::-1])
+                back = r.get_state()
+                nrm = r.norm2()
+    assert np.array_equal(outs[0], outs[1])
+    assert np.max(np.abs(back - amp)) < 1e-12
+    assert abs(nrm - 1.0) < 1e-12
+
+
+def test_inner_dense_matches_numpy():
+    rng = np.random.Generator(np.random.PCG64(31))
+    n = 16
+    a, b = _rand_state(rng, n), _rand_state(rng, n)
+    with Register(n) as r:
+        r.set_state(a)
+        z = r.inner_dense(b)
+    assert abs(z - np.vdot(b, a)) < 1e-13
