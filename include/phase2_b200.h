@@ -120,6 +120,39 @@ int qreg_set_timing(struct qreg *reg, int on);
  * for callers that record CUDA events around library calls. */
 void *qreg_stream(const struct qreg *reg);
 
+/* ---- allocation-free reduction ------------------------------------------ */
+
+/*
+ * sum |a_i|^2 of a state the caller already holds in device memory,
+ * without allocating anything.  This entry point has no counterpart in the
+ * reference.
+ *
+ * It exists for callers that cannot call cudaMalloc: code whose device
+ * memory is owned by its own pool or arena and may not allocate outside
+ * it, and latency-critical loops that cannot afford the implicit device
+ * synchronisation cudaMalloc/cudaFree bring.  qreg_norm2 computes the same
+ * sum but allocates its partials buffer on first use.
+ *
+ *   d_state  device pointer to namp amplitudes: complex128 (prec =
+ *            PHASE2_PREC_FP64) or complex64 (PHASE2_PREC_FP32)
+ *   namp     1 .. 2^34 (the fixed scratch holds 8192 partial sums of up
+ *            to 2^21 amplitudes each); larger sizes return -1 with an error
+ *   d_out    device pointer to 2 doubles; receives {sum, 0}
+ *   stream   cudaStream_t (NULL = legacy default stream); the call is
+ *            asynchronous on it
+ *
+ * The per-block partial sums live in a static device array (about
+ * 128 KiB) that every GPU loading the library holds until the process
+ * exits.  The first call on a device looks up that array's address and
+ * caches it; make that first call before starting any stream capture.
+ * All calls share the array: two calls whose kernels overlap on the GPU
+ * (different streams, no ordering between them) race on it and may
+ * return wrong sums.  Calls ordered on one stream are safe; nothing in the
+ * array needs to start at zero.  Returns 0 (launched) or -1.
+ */
+int phase2_norm2_noalloc(const void *d_state, int prec, uint64_t namp,
+	double *d_out, void *stream);
+
 /* ---- planner (host) ----------------------------------------------------- */
 
 /* One rotation exp(i phi P) with P = (flip, phase). */

@@ -896,3 +896,75 @@ extern "C" void *p2d_stream(const struct p2_dev *d)
 {
 	return (void *)d->stream;
 }
+
+/* ---- allocation-free norm (phase2_norm2_noalloc) ------------------------ */
+
+/*
+ * Per-block partial sums for phase2_norm2_noalloc live in this file-scope
+ * device array instead of memory obtained from cudaMalloc.  Every GPU that
+ * loads the library holds it (about 128 KiB) until the process exits.
+ * Host code must not use the symbol as an address: on the host it names a
+ * stand-in, so the device address is looked up per device with
+ * cudaGetSymbolAddress and passed to the kernels.
+ */
+#define P2_NOALLOC_MAX_BLOCKS 8192
+#define P2_NOALLOC_CHUNK (UINT64_C(1) << 21)
+#define P2_NOALLOC_MAX_AMPS ((uint64_t)P2_NOALLOC_MAX_BLOCKS * P2_NOALLOC_CHUNK)
+#define P2_NOALLOC_MAX_DEVICES 64
+
+static __device__ __align__(256) double
+	p2_noalloc_scratch[2 * P2_NOALLOC_MAX_BLOCKS];
+
+static double *p2_noalloc_addr[P2_NOALLOC_MAX_DEVICES];
+
+extern "C" int phase2_norm2_noalloc(const void *d_state, int prec,
+	uint64_t namp, double *d_out, void *stream)
+{
+	if (!d_state || !d_out) {
+		log_error("phase2_norm2_noalloc: NULL state or output pointer");
+		return -1;
+	}
+	if (prec != PHASE2_PREC_FP64 && prec != PHASE2_PREC_FP32) {
+		log_error("phase2_norm2_noalloc: unknown precision %d", prec);
+		return -1;
+	}
+	if (namp == 0 || namp > P2_NOALLOC_MAX_AMPS) {
+		log_error("phase2_norm2_noalloc: %llu amplitudes outside"
+			  " [1, %llu]: the fixed scratch holds %d partial sums"
+			  " of up to %llu amplitudes each",
+			(unsigned long long)namp,
+			(unsigned long long)P2_NOALLOC_MAX_AMPS,
+			P2_NOALLOC_MAX_BLOCKS,
+			(unsigned long long)P2_NOALLOC_CHUNK);
+		return -1;
+	}
+	int dev = 0;
+	CUDA_OK(cudaGetDevice(&dev), "phase2_norm2_noalloc: current device");
+	if (dev < 0 || dev >= P2_NOALLOC_MAX_DEVICES) {
+		log_error("phase2_norm2_noalloc: device %d beyond the %d"
+			  " supported", dev, P2_NOALLOC_MAX_DEVICES);
+		return -1;
+	}
+	if (!p2_noalloc_addr[dev]) {
+		/* first call on this device: resolve the array's address */
+		double *ptr = NULL;
+		CUDA_OK(cudaGetSymbolAddress((void **)&ptr, p2_noalloc_scratch),
+			"phase2_norm2_noalloc: scratch address");
+		p2_noalloc_addr[dev] = ptr;
+	}
+	double *part = p2_noalloc_addr[dev];
+	const cudaStream_t s = (cudaStream_t)stream;
+	/* Each block writes its own two slots before the final kernel reads
+	 * them (stream order), so the array needs no clearing. */
+	const unsigned blocks =
+		(unsigned)((namp + P2_NOALLOC_CHUNK - 1) / P2_NOALLOC_CHUNK);
+	if (prec == PHASE2_PREC_FP64)
+		k_reduce_partial<<<blocks, P2_RED_TPB, 0, s>>>(
+			(const double2 *)d_state, NULL, namp, part);
+	else
+		k_reduce_partial<<<blocks, P2_RED_TPB, 0, s>>>(
+			(const float2 *)d_state, NULL, namp, part);
+	k_reduce_final<<<1, P2_RED_TPB, 0, s>>>(part, blocks, d_out);
+	CUDA_OK(cudaGetLastError(), "phase2_norm2_noalloc: launch");
+	return 0;
+}
