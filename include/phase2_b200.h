@@ -51,6 +51,15 @@ int qreg_precision(const struct qreg *reg);
 int phase2_set_fusion(int max_span, int max_rots);
 int qreg_set_fusion(struct qreg *reg, int max_span, int max_rots);
 
+/* Launch choice of the pass kernel for one precision and span M (0..5):
+ * variant 0 loads each thread's cosets straight into registers, variant 1
+ * prefetches the next coset into shared memory with cp.async while the
+ * current one is computed; per_sm caps resident blocks per SM in the grid
+ * (0 = default).  Process-wide; the autotuner (phase2_b200/autotune.py)
+ * sets these from its measurements.  0 or -1. */
+int phase2_tune_set(int prec, int span, int variant, int per_sm);
+int phase2_tune_get(int prec, int span, int *variant, int *per_sm);
+
 /* ---- term order --------------------------------------------------------- */
 
 /* Order used by trott_init / trott2_init and the deterministic part of
@@ -172,24 +181,35 @@ struct phase2_pass {
 	uint8_t piv[PHASE2_MAX_SPAN]; /* pivot bits, ascending */
 	uint8_t pad[3];
 	uint64_t basis[PHASE2_MAX_SPAN];
+	double scale;      /* scaled form: product of the per-rotation factors */
 };
 
 /* Rotation record in slot coordinates: the partner of slot u is u ^ U; the
  * sign bit of slot u for a thread with representative x is
- * bit u of smask XOR parity(x & z); odd = 1 multiplies the partner by i. */
+ * bit u of smask XOR parity(x & z); odd = 1 multiplies the partner by i.
+ *
+ * form 0 (exact, FP64 state):  a_u <- c a_u + (+-s) p_u
+ * form 1 (scaled, |c| >= |s|): y_u <- y_u + (+-s/c) p_u,  factor c
+ * form 2 (scaled, |c| <  |s|): y_u <- (c/s) y_u + (+-1) p_u, factor s
+ * with p_u the partner (times i when odd); in the scaled forms `c` holds
+ * the ratio and the pass multiplies every amplitude by `scale` (the product
+ * of the factors) once, when it stores. */
 struct phase2_rot_rec {
 	uint64_t z;
 	double c, s;
 	uint32_t smask;
-	uint16_t U;
+	uint8_t U;
+	uint8_t W;    /* bit k = parity(basis[k] & z): smask bit u = bit 0 of
+		       * smask XOR parity(u & W) */
 	uint8_t odd;
-	uint8_t pad;
+	uint8_t form;
 };
 
-/* Plan n rotations for an nqb-qubit register.  Writes at most n passes and
- * n records; returns the number of passes, or -1. */
+/* Plan n rotations for an nqb-qubit register of precision prec (FP64:
+ * exact form; FP32: scaled forms).  Writes at most n passes and n records;
+ * returns the number of passes, or -1. */
 long phase2_plan(uint32_t nqb, const struct phase2_rot_in *rots, size_t n,
-	int max_span, int max_rots, struct phase2_pass *passes,
+	int max_span, int max_rots, int prec, struct phase2_pass *passes,
 	struct phase2_rot_rec *recs);
 
 /* ---- misc --------------------------------------------------------------- */

@@ -317,7 +317,8 @@ def cmpsit(nqb, terms, dets, samples, steps, length, depth, angle_det,
 # ---- planner (host only) -----------------------------------------------
 
 
-def plan(nqb: int, flip, phase, phi, max_span: int = 5, max_rots: int = 0):
+def plan(nqb: int, flip, phase, phi, max_span: int = 5, max_rots: int = 0,
+         prec: int = PREC_FP64):
     """Run the host planner; returns (passes, records) as lists of dicts."""
     L = lib()
     n = len(phi)
@@ -327,12 +328,13 @@ def plan(nqb: int, flip, phase, phi, max_span: int = 5, max_rots: int = 0):
             float(phi[k])
     passes = (_ffi.Pass * max(n, 1))()
     recs = (_ffi.RotRec * max(n, 1))()
-    np_ = L.phase2_plan(nqb, rin, n, max_span, max_rots, passes, recs)
+    np_ = L.phase2_plan(nqb, rin, n, max_span, max_rots, prec, passes, recs)
     if np_ < 0:
         raise ValueError("phase2_plan failed")
     out_p = [{"span": p.span, "nrot": p.nrot, "rot_off": p.rot_off,
-              "piv": list(p.piv)[:p.span], "basis": list(p.basis)[:p.span]}
+              "piv": list(p.piv)[:p.span], "basis": list(p.basis)[:p.span],
+              "scale": p.scale}
              for p in passes[:np_]]
     out_r = [{"z": r.z, "c": r.c, "s": r.s, "smask": r.smask, "U": r.U,
-              "odd": r.odd} for r in recs[:n]]
+              "odd": r.odd, "form": r.form} for r in recs[:n]]
     return out_p, out_r

@@ -144,13 +144,14 @@ MAX_SPAN = 5
 class Pass(C.Structure):
     _fields_ = [("span", C.c_uint32), ("nrot", C.c_uint32),
                 ("rot_off", C.c_uint32), ("piv", C.c_uint8 * MAX_SPAN),
-                ("pad", C.c_uint8 * 3), ("basis", C.c_uint64 * MAX_SPAN)]
+                ("pad", C.c_uint8 * 3), ("basis", C.c_uint64 * MAX_SPAN),
+                ("scale", C.c_double)]
 
 
 class RotRec(C.Structure):
     _fields_ = [("z", C.c_uint64), ("c", C.c_double), ("s", C.c_double),
-                ("smask", C.c_uint32), ("U", C.c_uint16),
-                ("odd", C.c_uint8), ("pad", C.c_uint8)]
+                ("smask", C.c_uint32), ("U", C.c_uint8), ("W", C.c_uint8),
+                ("odd", C.c_uint8), ("form", C.c_uint8)]
 
 
 class Stats(C.Structure):
@@ -266,7 +267,12 @@ _SIGS = {
     "phase2_set_term_order": (C.c_int, [C.c_int]),
     "phase2_get_term_order": (C.c_int, []),
     "phase2_plan": (C.c_long, [C.c_uint32, _P(RotIn), C.c_size_t, C.c_int,
-                               C.c_int, _P(Pass), _P(RotRec)]),
+                               C.c_int, C.c_int, _P(Pass), _P(RotRec)]),
+    "phase2_norm2_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_uint64,
+                                       C.c_void_p, C.c_void_p]),
+    "phase2_tune_set": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int]),
+    "phase2_tune_get": (C.c_int, [C.c_int, C.c_int, _P(C.c_int),
+                                  _P(C.c_int)]),
     "phase2_version": (C.c_char_p, []),
     "phase2_sizeof": (C.c_size_t, [C.c_int]),
 }

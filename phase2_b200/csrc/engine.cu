@@ -109,15 +109,41 @@ __host__ __device__ constexpr int p2_hibit(int v)
 	return v <= 1 ? 0 : 1 + p2_hibit(v >> 1);
 }
 
-/* One rotation on the 2^M slots of a coset.  sm bit u = sign of slot u. */
+/* k with a zero bit inserted at position h (pair index -> lower slot). */
+__host__ __device__ constexpr int p2_ins0(int g, int h)
+{
+	return ((g >> h) << (h + 1)) | (g & ((1 << h) - 1));
+}
+
+/* Bit u of sm moved to the sign position (u is a compile-time constant
+ * after unrolling: one shift and one mask, independent per slot). */
+__device__ __forceinline__ uint32_t p2_bitmask(uint32_t sm, int u)
+{
+	return (sm << (31 - u)) & 0x80000000u;
+}
+
+/* v with the sign mask (0 or 1 << 31) XORed into its high word. */
+__device__ __forceinline__ double p2_sgn(double v, uint32_t mask)
+{
+	return __hiloint2double(__double2hiint(v) ^ (int)mask,
+		__double2loint(v));
+}
+
+/*
+ * One rotation on the 2^M slots of a coset (FP64 state, exact rounding).
+ * The sign of slot u is bit u of sm (the thread's parity already folded
+ * in); each slot's sign is extracted independently so the per-slot work
+ * has no serial dependency.
+ */
 template <int M, int U, int ODD, bool EXACT>
 __device__ __forceinline__ void p2_rot(double (&re)[1 << M],
-	double (&im)[1 << M], double c, double s, uint32_t sm)
+	double (&im)[1 << M], double c, double s, uint32_t sm, uint32_t W)
 {
+	(void)W;
 	if constexpr (U == 0) {
 #pragma unroll
 		for (int u = 0; u < (1 << M); ++u) {
-			const double su = (sm >> u & 1u) ? -s : s;
+			const double su = p2_sgn(s, p2_bitmask(sm, u));
 			double tr, ti;
 			if constexpr (ODD) {
 				tr = p2_mul<EXACT>(-su, im[u]);
@@ -132,12 +158,11 @@ __device__ __forceinline__ void p2_rot(double (&re)[1 << M],
 	} else {
 		constexpr int H = p2_hibit(U);
 #pragma unroll
-		for (int u = 0; u < (1 << M); ++u) {
-			if (u >> H & 1)
-				continue;
+		for (int k = 0; k < (1 << (M - 1)); ++k) {
+			const int u = p2_ins0(k, H);
 			const int w = u ^ U;
-			const double su = (sm >> u & 1u) ? -s : s;
-			const double sw = (sm >> w & 1u) ? -s : s;
+			const double su = p2_sgn(s, p2_bitmask(sm, u));
+			const double sw = p2_sgn(s, p2_bitmask(sm, w));
 			double tur, tui, twr, twi;
 			if constexpr (ODD) {
 				tur = p2_mul<EXACT>(-su, im[w]);
@@ -162,17 +187,105 @@ __device__ __forceinline__ void p2_rot(double (&re)[1 << M],
 	}
 }
 
+/*
+ * Scaled rotation (FP32 storage).  All amplitudes carry a common pending
+ * factor, applied once per pass at the store, so one FMA per component:
+ *   COT = 0:  y_u <- y_u + (+-r) p_u          (r = s/c, factor c)
+ *   COT = 1:  y_u <- r y_u + (+-1) p_u        (r = c/s, factor s)
+ * p_u = y_{u^U}, times i when ODD; the sign is bit u of sm.
+ */
+template <int M, int U, int ODD, int COT>
+__device__ __forceinline__ void p2_rot_scaled(double (&re)[1 << M],
+	double (&im)[1 << M], double r, uint32_t sm, uint32_t W)
+{
+	(void)W;
+	if constexpr (U == 0) {
+#pragma unroll
+		for (int u = 0; u < (1 << M); ++u) {
+			const uint32_t sg = p2_bitmask(sm, u);
+			const double pr = ODD ? -im[u] : re[u];
+			const double pi = ODD ? re[u] : im[u];
+			if constexpr (!COT) {
+				const double ru = p2_sgn(r, sg);
+				re[u] = fma(ru, pr, re[u]);
+				im[u] = fma(ru, pi, im[u]);
+			} else {
+				re[u] = fma(r, re[u], p2_sgn(pr, sg));
+				im[u] = fma(r, im[u], p2_sgn(pi, sg));
+			}
+		}
+	} else {
+		constexpr int H = p2_hibit(U);
+#pragma unroll
+		for (int k = 0; k < (1 << (M - 1)); ++k) {
+			const int u = p2_ins0(k, H);
+			const int w = u ^ U;
+			const uint32_t sg = p2_bitmask(sm, u);
+			const uint32_t sw = p2_bitmask(sm, w);
+			const double pur = ODD ? -im[w] : re[w];
+			const double pui = ODD ? re[w] : im[w];
+			const double pwr = ODD ? -im[u] : re[u];
+			const double pwi = ODD ? re[u] : im[u];
+			double nur, nui, nwr, nwi;
+			if constexpr (!COT) {
+				const double ru = p2_sgn(r, sg), rw = p2_sgn(r, sw);
+				nur = fma(ru, pur, re[u]);
+				nui = fma(ru, pui, im[u]);
+				nwr = fma(rw, pwr, re[w]);
+				nwi = fma(rw, pwi, im[w]);
+			} else {
+				nur = fma(r, re[u], p2_sgn(pur, sg));
+				nui = fma(r, im[u], p2_sgn(pui, sg));
+				nwr = fma(r, re[w], p2_sgn(pwr, sw));
+				nwi = fma(r, im[w], p2_sgn(pwi, sw));
+			}
+			re[u] = nur;
+			im[u] = nui;
+			re[w] = nwr;
+			im[w] = nwi;
+		}
+	}
+}
+
+#define P2_CASE_S(K)                                                           \
+	case K:                                                                \
+		if constexpr ((K) < (4 << M))                                  \
+			p2_rot_scaled<M, ((K) >> 2), (((K) >> 1) & 1),         \
+				((K)&1)>(re, im, r, sm, W);                    \
+		break;
+#define P2_CASE_S8(B)                                                          \
+	P2_CASE_S(B + 0) P2_CASE_S(B + 1) P2_CASE_S(B + 2) P2_CASE_S(B + 3)    \
+	P2_CASE_S(B + 4) P2_CASE_S(B + 5) P2_CASE_S(B + 6) P2_CASE_S(B + 7)
+
+/* key = U << 2 | odd << 1 | cot */
+template <int M>
+__device__ __forceinline__ void p2_apply_scaled(uint32_t key,
+	double (&re)[1 << M], double (&im)[1 << M], double r, uint32_t sm,
+	uint32_t W)
+{
+	switch (key) {
+		P2_CASE_S8(0) P2_CASE_S8(8) P2_CASE_S8(16) P2_CASE_S8(24)
+		P2_CASE_S8(32) P2_CASE_S8(40) P2_CASE_S8(48) P2_CASE_S8(56)
+		P2_CASE_S8(64) P2_CASE_S8(72) P2_CASE_S8(80) P2_CASE_S8(88)
+		P2_CASE_S8(96) P2_CASE_S8(104) P2_CASE_S8(112) P2_CASE_S8(120)
+	default:
+		break;
+	}
+}
+#undef P2_CASE_S8
+#undef P2_CASE_S
+
 #define P2_CASE(K)                                                             \
 	case K:                                                                \
 		if constexpr ((K) < (2 << M))                                  \
 			p2_rot<M, ((K) >> 1), ((K)&1), EXACT>(re, im, c, s,    \
-				sm);                                           \
+				sm, W);                                        \
 		break;
 
 /* key = U << 1 | odd; a jump table over the (U, odd) variants. */
 template <int M, bool EXACT>
 __device__ __forceinline__ void p2_apply(uint32_t key, double (&re)[1 << M],
-	double (&im)[1 << M], double c, double s, uint32_t sm)
+	double (&im)[1 << M], double c, double s, uint32_t sm, uint32_t W)
 {
 	switch (key) {
 		P2_CASE(0) P2_CASE(1) P2_CASE(2) P2_CASE(3) P2_CASE(4)
@@ -237,43 +350,214 @@ __device__ __forceinline__ uint64_t p2_slot_off(int u, const uint64_t *basis)
 
 /* ---- the pass kernel ---------------------------------------------------- */
 
-template <int M, typename ST, bool EXACT>
-__global__ void __launch_bounds__(P2_TPB) k_pass(ST *__restrict__ st,
-	uint64_t nrep, struct phase2_pass p,
-	const struct phase2_rot_rec *__restrict__ recs)
+/* Threads per block: 128, except FP64 with 32 slots per thread (64 keeps
+ * three blocks of two prefetch stages within shared memory). */
+__host__ __device__ constexpr int p2_tpb(int m, int elem_bytes)
 {
+	return (m >= 5 && elem_bytes == 16) ? 64 : P2_TPB;
+}
+
+/* Resident blocks per SM the register allocation should allow: 2^M FP64
+ * complex values need 4 * 2^M registers per thread. */
+__host__ __device__ constexpr int p2_min_blocks(int m)
+{
+	return m >= 5 ? 1 : (m == 4 ? 4 : (m == 3 ? 6 : 8));
+}
+
+/* Representative number t -> index x: zeros inserted at the pivots. */
+template <int M>
+__device__ __forceinline__ uint64_t p2_rep(uint64_t t,
+	const struct phase2_pass &p)
+{
+	uint64_t x = t;
+#pragma unroll
+	for (int k = 0; k < M; ++k) {
+		const uint32_t q = p.piv[k];
+		x = ((x >> q) << (q + 1)) | (x & ((UINT64_C(1) << q) - 1));
+	}
+	return x;
+}
+
+/* Asynchronous global -> shared copy of one amplitude. */
+__device__ __forceinline__ void p2_cp_async(float2 *smem, const float2 *g)
+{
+	const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+	asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s),
+		"l"(g)
+		: "memory");
+}
+
+__device__ __forceinline__ void p2_cp_async(double2 *smem, const double2 *g)
+{
+	const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s),
+		"l"(g)
+		: "memory");
+}
+
+__device__ __forceinline__ void p2_cp_commit()
+{
+	asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+template <int N> __device__ __forceinline__ void p2_cp_wait()
+{
+	asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+/* The run of rotations of one pass on one coset held in registers, then
+ * the pass-wide factor of the scaled forms. */
+template <int M, bool EXACT>
+__device__ __forceinline__ void p2_apply_run(double (&re)[1 << M],
+	double (&im)[1 << M], uint64_t x, const struct phase2_rot_rec *srec,
+	uint32_t nrot, double scale)
+{
+	for (uint32_t r = 0; r < nrot; ++r) {
+		const uint64_t z = srec[r].z;
+		const uint32_t px = (uint32_t)(__popcll(x & z) & 1);
+		const uint32_t sm = srec[r].smask ^ (0u - px);
+		if constexpr (EXACT) {
+			const uint32_t key =
+				((uint32_t)srec[r].U << 1) | srec[r].odd;
+			p2_apply<M, EXACT>(key, re, im, srec[r].c, srec[r].s,
+				sm, srec[r].W);
+		} else {
+			const uint32_t key = ((uint32_t)srec[r].U << 2) |
+				((uint32_t)srec[r].odd << 1) |
+				(srec[r].form == 2 ? 1u : 0u);
+			p2_apply_scaled<M>(key, re, im, srec[r].c, sm,
+				srec[r].W);
+		}
+	}
+	if constexpr (!EXACT) {
+#pragma unroll
+		for (int u = 0; u < (1 << M); ++u) {
+			re[u] *= scale;
+			im[u] *= scale;
+		}
+	}
+}
+
+/* Stage layout [slot][thread]: a warp's accesses to one slot are 32
+ * consecutive elements, conflict-free. */
+template <int M, typename ST>
+__device__ __forceinline__ void p2_prefetch(ST *stage, const ST *st,
+	uint64_t x, const uint64_t (&pb)[M > 0 ? M : 1])
+{
+#pragma unroll
+	for (int u = 0; u < (1 << M); ++u)
+		p2_cp_async(&stage[u * blockDim.x + threadIdx.x],
+			st + (x ^ p2_slot_off<M>(u, pb)));
+}
+
+/*
+ * One pass.  Persistent grid: each thread walks representatives
+ * t, t + stride, ...; while it applies the rotations to coset t in
+ * registers, the 2^M amplitudes of coset t + stride are already on their
+ * way into its own shared-memory stage (cp.async), so every warp keeps
+ * loads in flight during its compute.  A thread only ever reads the stage
+ * slots it copied itself: cp.async.wait_group orders them, no block
+ * barrier is needed inside the loop.  The next prefetch into a stage is
+ * issued after the values read from it have been consumed (in-order issue),
+ * so the stage is never overwritten early.
+ */
+template <int M, typename ST, bool EXACT>
+__global__ void __launch_bounds__(p2_tpb(M, sizeof(ST)), p2_min_blocks(M))
+	k_pass_pf(ST *__restrict__ st, uint64_t nrep, struct phase2_pass p,
+		const struct phase2_rot_rec *__restrict__ recs)
+{
+	extern __shared__ __align__(16) unsigned char p2_dyn[];
+	ST *const stage = (ST *)p2_dyn;
 	__shared__ struct phase2_rot_rec srec[P2_MAX_ROTS_PER_PASS];
+	__shared__ uint64_t sbasis[PHASE2_MAX_SPAN];
 	for (uint32_t r = threadIdx.x; r < p.nrot; r += blockDim.x)
 		srec[r] = recs[p.rot_off + r];
+	if (threadIdx.x == 0) {
+#pragma unroll
+		for (int k = 0; k < M; ++k)
+			sbasis[k] = p.basis[k];
+	}
 	__syncthreads();
+	uint64_t pb[M > 0 ? M : 1];
+#pragma unroll
+	for (int k = 0; k < M; ++k)
+		pb[k] = p.basis[k];
+
+	const uint32_t nst = (1u << M) * blockDim.x; /* elements per stage */
+	const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+	uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (t < nrep)
+		p2_prefetch<M>(stage, st, p2_rep<M>(t, p), pb);
+	p2_cp_commit();
+	uint32_t cur = 0;
+	for (; t < nrep; t += stride) {
+		const uint64_t tn = t + stride;
+		if (tn < nrep)
+			p2_prefetch<M>(stage + (cur ^ 1) * nst, st,
+				p2_rep<M>(tn, p), pb);
+		p2_cp_commit();
+		p2_cp_wait<1>();
+
+		const uint64_t x = p2_rep<M>(t, p);
+		double re[1 << M], im[1 << M];
+		const ST *const mine = stage + cur * nst + threadIdx.x;
+#pragma unroll
+		for (int u = 0; u < (1 << M); ++u) {
+			const ST v = mine[u * blockDim.x];
+			re[u] = (double)v.x;
+			im[u] = (double)v.y;
+		}
+
+		p2_apply_run<M, EXACT>(re, im, x, srec, p.nrot, p.scale);
+		/* Slot addresses are recomputed from the shared copy of the
+		 * basis rather than kept live across the rotations. */
+#pragma unroll
+		for (int u = 0; u < (1 << M); ++u)
+			p2_st(st, x ^ p2_slot_off<M>(u, sbasis), re[u], im[u]);
+		cur ^= 1;
+	}
+	p2_cp_wait<0>();
+}
+
+/*
+ * One pass, direct variant: each thread loads its coset straight from HBM
+ * into registers (all 2^M loads issued back to back), applies the run and
+ * stores; latency is hidden by the other resident warps only.  The grid
+ * covers every representative once (no persistent loop state).
+ */
+template <int M, typename ST, bool EXACT>
+__global__ void __launch_bounds__(P2_TPB,
+	(M >= 5 && sizeof(ST) == 8) ? 3 : p2_min_blocks(M))
+	k_pass(ST *__restrict__ st, uint64_t nrep, struct phase2_pass p,
+		const struct phase2_rot_rec *__restrict__ recs)
+{
+	__shared__ struct phase2_rot_rec srec[P2_MAX_ROTS_PER_PASS];
+	__shared__ uint64_t sbasis[PHASE2_MAX_SPAN];
+	for (uint32_t r = threadIdx.x; r < p.nrot; r += blockDim.x)
+		srec[r] = recs[p.rot_off + r];
+	if (threadIdx.x == 0) {
+#pragma unroll
+		for (int k = 0; k < M; ++k)
+			sbasis[k] = p.basis[k];
+	}
+	__syncthreads();
+	uint64_t pb[M > 0 ? M : 1];
+#pragma unroll
+	for (int k = 0; k < M; ++k)
+		pb[k] = p.basis[k];
 
 	const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
 	for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
 		t < nrep; t += stride) {
-		/* representative: zeros inserted at the pivots (ascending) */
-		uint64_t x = t;
-#pragma unroll
-		for (int k = 0; k < M; ++k) {
-			const uint32_t q = p.piv[k];
-			x = ((x >> q) << (q + 1)) | (x & ((UINT64_C(1) << q) - 1));
-		}
+		const uint64_t x = p2_rep<M>(t, p);
 		double re[1 << M], im[1 << M];
 #pragma unroll
 		for (int u = 0; u < (1 << M); ++u)
-			p2_ld(st, x ^ p2_slot_off<M>(u, p.basis), re[u], im[u]);
-
-		for (uint32_t r = 0; r < p.nrot; ++r) {
-			const uint64_t z = srec[r].z;
-			const uint32_t px = (uint32_t)(__popcll(x & z) & 1);
-			const uint32_t sm = srec[r].smask ^ (0u - px);
-			const uint32_t key =
-				((uint32_t)srec[r].U << 1) | srec[r].odd;
-			p2_apply<M, EXACT>(key, re, im, srec[r].c, srec[r].s, sm);
-		}
-
+			p2_ld(st, x ^ p2_slot_off<M>(u, pb), re[u], im[u]);
+		p2_apply_run<M, EXACT>(re, im, x, srec, p.nrot, p.scale);
 #pragma unroll
 		for (int u = 0; u < (1 << M); ++u)
-			p2_st(st, x ^ p2_slot_off<M>(u, p.basis), re[u], im[u]);
+			p2_st(st, x ^ p2_slot_off<M>(u, sbasis), re[u], im[u]);
 	}
 }
 
@@ -301,29 +585,6 @@ __global__ void k_scatter(ST *__restrict__ st, const uint64_t *__restrict__ idx,
 	if (blockIdx.x == 0 && threadIdx.x == 0)
 		for (size_t i = 0; i < n; ++i)
 			p2_st(st, idx[i], val[2 * i], val[2 * i + 1]);
-}
-
-template <typename ST>
-__global__ void k_widen(const ST *__restrict__ st, double2 *__restrict__ out,
-	uint64_t n)
-{
-	const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-	for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-		i < n; i += stride) {
-		double re, im;
-		p2_ld(st, i, re, im);
-		out[i] = make_double2(re, im);
-	}
-}
-
-template <typename ST>
-__global__ void k_narrow(ST *__restrict__ st, const double2 *__restrict__ in,
-	uint64_t n)
-{
-	const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-	for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-		i < n; i += stride)
-		p2_st(st, i, in[i].x, in[i].y);
 }
 
 /* Neumaier: s + c carries the running sum and its rounding error. */
@@ -647,17 +908,21 @@ extern "C" int p2d_get_state(struct p2_dev *d, double *out)
 		CUDA_OK(cudaStreamSynchronize(d->stream), "download state");
 		return 0;
 	}
-	double2 *tmp = NULL;
-	CUDA_OK(cudaMalloc((void **)&tmp, bytes), "alloc widen buffer");
-	k_widen<<<grid_for(d, d->namp, 256, 16), 256, 0, d->stream>>>(
-		(const float2 *)d->state, tmp, d->namp);
-	d->launches++;
-	cudaError_t e = cudaMemcpyAsync(out, tmp, bytes,
-		cudaMemcpyDeviceToHost, d->stream);
-	if (e == cudaSuccess)
-		e = cudaStreamSynchronize(d->stream);
-	cudaFree(tmp);
-	CUDA_OK(e, "download widened state");
+	/* FP32: download the raw complex64 values into the upper half of
+	 * `out` and widen forward in place (element i is read before the
+	 * 16 bytes at 16 i are written, and never overlaps a later one). */
+	float *raw = (float *)((char *)out + d->namp * sizeof(float2));
+	CUDA_OK(cudaMemcpyAsync(raw, d->state, d->namp * sizeof(float2),
+			cudaMemcpyDeviceToHost, d->stream),
+		"download state");
+	CUDA_OK(cudaStreamSynchronize(d->stream), "download state");
+	d->d2h_bytes += d->namp * sizeof(float2);
+	for (uint64_t i = 0; i < d->namp; i++) {
+		const float re = raw[2 * i], im = raw[2 * i + 1];
+		out[2 * i] = (double)re;
+		out[2 * i + 1] = (double)im;
+	}
+	(void)bytes;
 	return 0;
 }
 
@@ -672,29 +937,103 @@ extern "C" int p2d_set_state(struct p2_dev *d, const double *in)
 		CUDA_OK(cudaStreamSynchronize(d->stream), "upload state");
 		return 0;
 	}
-	double2 *tmp = NULL;
-	CUDA_OK(cudaMalloc((void **)&tmp, bytes), "alloc narrow buffer");
-	cudaError_t e = cudaMemcpyAsync(tmp, in, bytes, cudaMemcpyHostToDevice,
-		d->stream);
-	if (e == cudaSuccess) {
-		k_narrow<<<grid_for(d, d->namp, 256, 16), 256, 0, d->stream>>>(
-			(float2 *)d->state, tmp, d->namp);
-		d->launches++;
-		e = cudaStreamSynchronize(d->stream);
+	/* FP32: round to nearest on the host (as __double2float_rn), upload */
+	float *raw = (float *)malloc(d->namp * sizeof(float2));
+	if (!raw) {
+		log_error("set_state: host buffer of %zu bytes",
+			(size_t)(d->namp * sizeof(float2)));
+		return -1;
 	}
-	cudaFree(tmp);
+	for (uint64_t i = 0; i < 2 * d->namp; i++)
+		raw[i] = (float)in[i];
+	cudaError_t e = cudaMemcpyAsync(d->state, raw,
+		d->namp * sizeof(float2), cudaMemcpyHostToDevice, d->stream);
+	if (e == cudaSuccess)
+		e = cudaStreamSynchronize(d->stream);
+	free(raw);
 	CUDA_OK(e, "upload narrowed state");
+	d->h2d_bytes += d->namp * sizeof(float2);
+	(void)bytes;
 	return 0;
 }
 
+/*
+ * Launch table: per precision and span, which pass kernel runs (0 direct,
+ * 1 shared-memory prefetch) and how many blocks per SM the grid holds
+ * (0: the direct kernel's default of 16, the prefetch kernel's occupancy).
+ * Set by phase2_tune_set (the autotuner) or left at these defaults.
+ */
+struct p2_tune_entry {
+	int variant;
+	int per_sm;
+};
+static struct p2_tune_entry p2_tune[2][PHASE2_MAX_SPAN + 1];
+
+extern "C" int phase2_tune_set(int prec, int span, int variant, int per_sm)
+{
+	if ((prec != PHASE2_PREC_FP64 && prec != PHASE2_PREC_FP32) || span < 0 ||
+		span > PHASE2_MAX_SPAN || variant < 0 || variant > 1 ||
+		per_sm < 0 || per_sm > 64)
+		return -1;
+	p2_tune[prec][span].variant = variant;
+	p2_tune[prec][span].per_sm = per_sm;
+	return 0;
+}
+
+extern "C" int phase2_tune_get(int prec, int span, int *variant, int *per_sm)
+{
+	if ((prec != PHASE2_PREC_FP64 && prec != PHASE2_PREC_FP32) || span < 0 ||
+		span > PHASE2_MAX_SPAN)
+		return -1;
+	*variant = p2_tune[prec][span].variant;
+	*per_sm = p2_tune[prec][span].per_sm;
+	return 0;
+}
+
+/* Resolved configuration of the prefetch kernel (shared memory opt-in and
+ * resident blocks per SM), once per instantiation. */
+struct p2_kcfg {
+	int ready;
+	int tpb;
+	size_t smem;
+	int per_sm;
+};
+
 template <int M, typename ST, bool EXACT>
-static void launch_pass_t(struct p2_dev *d, const struct phase2_pass &p,
+static int launch_pass_t(struct p2_dev *d, const struct phase2_pass &p,
 	const struct phase2_rot_rec *recs)
 {
 	const uint64_t nrep = d->namp >> M;
-	const unsigned grid = grid_for(d, nrep, P2_TPB, 16);
-	k_pass<M, ST, EXACT><<<grid, P2_TPB, 0, d->stream>>>(
+	const struct p2_tune_entry te = p2_tune[d->prec][M];
+	if (te.variant == 0) {
+		const unsigned per_sm = te.per_sm ? (unsigned)te.per_sm : 16u;
+		const unsigned grid = grid_for(d, nrep, P2_TPB, per_sm);
+		k_pass<M, ST, EXACT><<<grid, P2_TPB, 0, d->stream>>>(
+			(ST *)d->state, nrep, p, recs);
+		return 0;
+	}
+	static struct p2_kcfg cfg;
+	if (!cfg.ready) {
+		cfg.tpb = p2_tpb(M, (int)sizeof(ST));
+		cfg.smem = 2 * ((size_t)1 << M) * cfg.tpb * sizeof(ST);
+		CUDA_OK(cudaFuncSetAttribute(k_pass_pf<M, ST, EXACT>,
+				cudaFuncAttributeMaxDynamicSharedMemorySize,
+				(int)cfg.smem),
+			"pass kernel shared memory");
+		int per_sm = 0;
+		CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm,
+				k_pass_pf<M, ST, EXACT>, cfg.tpb, cfg.smem),
+			"pass kernel occupancy");
+		cfg.per_sm = per_sm > 0 ? per_sm : 1;
+		cfg.ready = 1;
+	}
+	const unsigned per_sm = te.per_sm && te.per_sm < cfg.per_sm
+		? (unsigned)te.per_sm
+		: (unsigned)cfg.per_sm;
+	const unsigned grid = grid_for(d, nrep, (unsigned)cfg.tpb, per_sm);
+	k_pass_pf<M, ST, EXACT><<<grid, cfg.tpb, cfg.smem, d->stream>>>(
 		(ST *)d->state, nrep, p, recs);
+	return 0;
 }
 
 template <typename ST, bool EXACT>
@@ -703,28 +1042,21 @@ static int launch_pass(struct p2_dev *d, const struct phase2_pass &p,
 {
 	switch (p.span) {
 	case 0:
-		launch_pass_t<0, ST, EXACT>(d, p, recs);
-		break;
+		return launch_pass_t<0, ST, EXACT>(d, p, recs);
 	case 1:
-		launch_pass_t<1, ST, EXACT>(d, p, recs);
-		break;
+		return launch_pass_t<1, ST, EXACT>(d, p, recs);
 	case 2:
-		launch_pass_t<2, ST, EXACT>(d, p, recs);
-		break;
+		return launch_pass_t<2, ST, EXACT>(d, p, recs);
 	case 3:
-		launch_pass_t<3, ST, EXACT>(d, p, recs);
-		break;
+		return launch_pass_t<3, ST, EXACT>(d, p, recs);
 	case 4:
-		launch_pass_t<4, ST, EXACT>(d, p, recs);
-		break;
+		return launch_pass_t<4, ST, EXACT>(d, p, recs);
 	case 5:
-		launch_pass_t<5, ST, EXACT>(d, p, recs);
-		break;
+		return launch_pass_t<5, ST, EXACT>(d, p, recs);
 	default:
 		log_error("pass span %u unsupported", p.span);
 		return -1;
 	}
-	return 0;
 }
 
 static int recs_reserve(struct p2_dev *d, size_t n)

@@ -24,6 +24,16 @@ extern struct p2_settings p2_cfg;
 void p2_settings_from_env(void);
 
 /* reg->backend */
+/*
+ * Work on a register is kept in program order with two host queues:
+ * rotations (q) and amplitude writes (w*).  At most one of them is
+ * non-empty: queuing into one drains the other first.  Reads drain both.
+ * Registers of up to P2_HOST_COPY_QB qubits keep a host copy of the state
+ * (host_copy) after a read, valid until the next change, so that long runs
+ * of single-amplitude reads cost one download.
+ */
+#define P2_HOST_COPY_QB 16
+
 struct p2_qreg {
 	struct p2_dev *dev;
 	int prec;
@@ -34,6 +44,11 @@ struct p2_qreg {
 	struct phase2_pass *passes;
 	struct phase2_rot_rec *recs;
 	size_t plan_cap;
+	uint64_t *widx;
+	double *wval;
+	size_t wlen, wcap;
+	double *host_copy;
+	int host_copy_valid;
 };
 
 /* Sticky error of a register (0 ok, -1 failed). */

@@ -23,9 +23,10 @@ extern "C" {
 /* Queued rotations that trigger an automatic flush. */
 #define P2_QUEUE_FLUSH 8192
 
+/* scaled = 1 emits the FP32 forms (struct phase2_rot_rec, forms 1 and 2). */
 long p2_plan(uint32_t nqb, const struct phase2_rot_in *rots, size_t n,
-	int max_span, int max_rots, int pad_span, struct phase2_pass *passes,
-	struct phase2_rot_rec *recs);
+	int max_span, int max_rots, int pad_span, int scaled,
+	struct phase2_pass *passes, struct phase2_rot_rec *recs);
 
 /* ---- device engine ------------------------------------------------------ */
 

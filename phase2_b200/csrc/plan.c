@@ -115,7 +115,7 @@ static inline int parity64(uint64_t v)
 /* Close the open pass: pad the basis with unit vectors (more amplitudes per
  * thread, contiguous along low qubits), fix pivots, fill slot masks. */
 static void builder_close(struct pass_builder *b, uint32_t nqb, int pad_to,
-	const struct phase2_rot_in *rots, struct phase2_pass *pass,
+	int scaled, const struct phase2_rot_in *rots, struct phase2_pass *pass,
 	struct phase2_rot_rec *recs)
 {
 	for (uint32_t q = 0; b->m < pad_to && q < nqb; q++) {
@@ -133,6 +133,7 @@ static void builder_close(struct pass_builder *b, uint32_t nqb, int pad_to,
 		pass->basis[k] = b->basis[k];
 	}
 	const uint32_t nslot = UINT32_C(1) << b->m;
+	double scale = 1.0;
 	for (uint32_t r = 0; r < b->nrot; r++) {
 		struct phase2_rot_rec *rec = &recs[b->first_rec + r];
 		const struct phase2_rot_in *in = &rots[b->first_rec + r];
@@ -147,22 +148,44 @@ static void builder_close(struct pass_builder *b, uint32_t nqb, int pad_to,
 					(kbase >> 1))
 				<< u;
 		rec->smask = smask;
+		rec->W = (uint8_t)W;
 		rec->odd = (uint8_t)(kbase & 1);
+		rec->form = 0;
+		if (scaled) {
+			/* Every amplitude is multiplied by c in this rotation;
+			 * carry the larger of |c|, |s| as a pass-wide factor and
+			 * keep the ratio, so the kernel needs one FMA per
+			 * component.  |factor| >= 1/sqrt(2), so 256 rotations
+			 * shrink the scale by at most 2^-128. */
+			const double c = rec->c, s = rec->s;
+			if (fabs(c) >= fabs(s)) {
+				rec->form = 1;
+				rec->c = s / c;
+				scale *= c;
+			} else {
+				rec->form = 2;
+				rec->c = c / s;
+				scale *= s;
+			}
+		}
 	}
+	pass->scale = scale;
 }
 
 long phase2_plan(uint32_t nqb, const struct phase2_rot_in *rots, size_t n,
-	int max_span, int max_rots, struct phase2_pass *passes,
+	int max_span, int max_rots, int prec, struct phase2_pass *passes,
 	struct phase2_rot_rec *recs)
 {
+	if (prec != PHASE2_PREC_FP64 && prec != PHASE2_PREC_FP32)
+		return -1;
 	return p2_plan(nqb, rots, n, max_span, max_rots, P2_DEFAULT_PAD_SPAN,
-		passes, recs);
+		prec == PHASE2_PREC_FP32, passes, recs);
 }
 
 /* Records are emitted in input order: recs[i] describes rots[i]. */
 long p2_plan(uint32_t nqb, const struct phase2_rot_in *rots, size_t n,
-	int max_span, int max_rots, int pad_span, struct phase2_pass *passes,
-	struct phase2_rot_rec *recs)
+	int max_span, int max_rots, int pad_span, int scaled,
+	struct phase2_pass *passes, struct phase2_rot_rec *recs)
 {
 	if (nqb == 0 || nqb > QREG_MAX_WIDTH)
 		return -1;
@@ -198,8 +221,8 @@ long p2_plan(uint32_t nqb, const struct phase2_rot_in *rots, size_t n,
 				fits = 0;
 		}
 		if (!fits) {
-			builder_close(&b, nqb, pad_span, rots, &passes[npass],
-				recs);
+			builder_close(&b, nqb, pad_span, scaled, rots,
+				&passes[npass], recs);
 			npass++;
 			builder_reset(&b, i);
 			if (f != 0)
@@ -211,12 +234,14 @@ long p2_plan(uint32_t nqb, const struct phase2_rot_in *rots, size_t n,
 		rec->z = rots[i].phase;
 		rec->c = cos(rots[i].phi);
 		rec->s = sin(rots[i].phi);
-		rec->U = (uint16_t)U;
-		rec->pad = 0;
+		rec->U = (uint8_t)U;
+		rec->W = 0;
+		rec->form = 0;
 		b.nrot++;
 	}
 	if (b.nrot > 0) {
-		builder_close(&b, nqb, pad_span, rots, &passes[npass], recs);
+		builder_close(&b, nqb, pad_span, scaled, rots, &passes[npass],
+			recs);
 		npass++;
 	}
 	return npass;

@@ -7,10 +7,16 @@
  * into two buffers, two rotation launches per term and a recombination
  * (phase2/qreg_cuda_lo.cu:111-131).  With one rank the exchange is a self
  * copy and the second buffer is identically zero, so all of that reduces
- * to applying the rotations in order to the one state; this file queues
- * them and hands planned passes to the engine.  Observing calls drain the
- * queue first, so the state seen by any caller is the one the reference
- * would produce.
+ * to applying the rotations in order to the one state.
+ *
+ * Execution model: rotations and amplitude writes are queued on the host
+ * in program order and executed in batches -- rotations as planned passes
+ * (plan.c), writes as one scatter launch.  Every call that observes the
+ * state (getamp, sync, norms, stats) drains the queues first, so callers
+ * see exactly the state the reference would hold at that point.  Small
+ * registers keep a host copy after a read so that runs of single-amplitude
+ * reads (the reference's tests read whole states one amplitude at a time)
+ * cost one download.
  */
 #include <complex.h>
 #include <stdint.h>
@@ -67,6 +73,13 @@ int qreg_init_prec(struct qreg *reg, uint32_t nqb, int prec)
 	reg->qb_hi = 0;
 	reg->namp = UINT64_C(1) << nqb;
 	reg->backend = b;
+	if (nqb <= P2_HOST_COPY_QB) {
+		b->host_copy = calloc(2 * reg->namp, sizeof(double));
+		if (!b->host_copy) {
+			qreg_free(reg);
+			return -1;
+		}
+	}
 	if (nqb <= QREG_EAGER_SHADOW_QB) {
 		reg->amp = calloc(reg->namp, sizeof *reg->amp);
 		if (!reg->amp) {
@@ -91,6 +104,9 @@ void qreg_free(struct qreg *reg)
 		free(b->q);
 		free(b->passes);
 		free(b->recs);
+		free(b->widx);
+		free(b->wval);
+		free(b->host_copy);
 		free(b);
 	}
 	free(reg->amp);
@@ -104,23 +120,23 @@ int qreg_precision(const struct qreg *reg)
 	return b ? b->prec : -1;
 }
 
-int qreg_set_fusion(struct qreg *reg, int max_span, int max_rots)
+/* Launch the queued amplitude writes (one scatter, later writes win). */
+static int drain_writes(struct p2_qreg *b)
 {
-	struct p2_qreg *b = B(reg);
-	if (!b || max_span < 1 || max_span > PHASE2_MAX_SPAN || max_rots < 0)
-		return -1;
-	if (qreg_flush(reg) < 0)
-		return -1;
-	b->max_span = max_span;
-	b->max_rots = max_rots;
-	return 0;
+	if (b->wlen == 0)
+		return b->error;
+	if (p2d_set(b->dev, b->widx, b->wval, b->wlen) < 0) {
+		log_error("qreg: %zu amplitude writes failed", b->wlen);
+		b->error = -1;
+	}
+	b->wlen = 0;
+	return b->error;
 }
 
-int qreg_flush(struct qreg *reg)
+/* Plan and launch the queued rotations (asynchronously). */
+static int drain_rotations(struct qreg *reg)
 {
 	struct p2_qreg *b = B(reg);
-	if (!b)
-		return -1;
 	if (b->qlen == 0)
 		return b->error;
 	if (b->plan_cap < b->qlen) {
@@ -140,14 +156,38 @@ int qreg_flush(struct qreg *reg)
 		b->plan_cap = b->qlen;
 	}
 	const long np = p2_plan(reg->qb_lo, b->q, b->qlen, b->max_span,
-		b->max_rots, P2_DEFAULT_PAD_SPAN, b->passes, b->recs);
+		b->max_rots, P2_DEFAULT_PAD_SPAN, b->prec == PHASE2_PREC_FP32,
+		b->passes, b->recs);
 	if (np < 0 || p2d_run(b->dev, b->passes, (size_t)np, b->recs,
 			      b->qlen) < 0) {
-		log_error("qreg_flush: %zu rotations failed", b->qlen);
+		log_error("qreg: %zu rotations failed", b->qlen);
 		b->error = -1;
 	}
 	b->qlen = 0;
 	return b->error;
+}
+
+int qreg_flush(struct qreg *reg)
+{
+	struct p2_qreg *b = B(reg);
+	if (!b)
+		return -1;
+	/* at most one queue is non-empty; order does not matter here */
+	drain_writes(b);
+	drain_rotations(reg);
+	return b->error;
+}
+
+int qreg_set_fusion(struct qreg *reg, int max_span, int max_rots)
+{
+	struct p2_qreg *b = B(reg);
+	if (!b || max_span < 1 || max_span > PHASE2_MAX_SPAN || max_rots < 0)
+		return -1;
+	if (qreg_flush(reg) < 0)
+		return -1;
+	b->max_span = max_span;
+	b->max_rots = max_rots;
+	return 0;
 }
 
 int qreg_synchronize(struct qreg *reg)
@@ -164,8 +204,11 @@ void qreg_paulirot(struct qreg *reg, struct paulis code_hi,
 	const struct paulis *codes_lo, const double *phis, size_t ncodes)
 {
 	struct p2_qreg *b = B(reg);
-	if (!b)
+	if (!b || ncodes == 0)
 		return;
+	if (drain_writes(b) < 0)
+		return;
+	b->host_copy_valid = 0;
 	/* Operators beyond the register's qubits are dropped, as the
 	 * reference's hi/lo split does (phase2/paulis.c:165-180). */
 	const uint64_t m = reg->qb_lo >= 64 ? ~UINT64_C(0)
@@ -188,31 +231,77 @@ void qreg_paulirot(struct qreg *reg, struct paulis code_hi,
 		r->phase = (code_hi.pak[1] | codes_lo[k].pak[1]) & m;
 		r->phi = phis[k];
 		if (b->qlen >= P2_QUEUE_FLUSH)
-			qreg_flush(reg);
+			drain_rotations(reg);
 	}
-}
-
-int qreg_getamps(struct qreg *reg, const uint64_t *idx, _Complex double *z,
-	size_t n)
-{
-	struct p2_qreg *b = B(reg);
-	if (!b || qreg_flush(reg) < 0)
-		return -1;
-	/* _Complex double is laid out as two doubles (re, im) */
-	if (p2d_get(b->dev, idx, (double *)z, n) < 0) {
-		b->error = -1;
-		return -1;
-	}
-	return 0;
 }
 
 int qreg_setamps(struct qreg *reg, const uint64_t *idx,
 	const _Complex double *z, size_t n)
 {
 	struct p2_qreg *b = B(reg);
-	if (!b || qreg_flush(reg) < 0)
+	if (!b)
 		return -1;
-	if (p2d_set(b->dev, idx, (const double *)z, n) < 0) {
+	for (size_t i = 0; i < n; i++)
+		if (idx[i] >= reg->namp) {
+			log_error("qreg_setamps: index %llu out of range",
+				(unsigned long long)idx[i]);
+			return -1;
+		}
+	if (drain_rotations(reg) < 0)
+		return -1;
+	if (b->wlen + n > b->wcap) {
+		size_t cap = b->wcap ? b->wcap : 256;
+		while (cap < b->wlen + n)
+			cap *= 2;
+		uint64_t *wi = realloc(b->widx, sizeof *wi * cap);
+		if (wi)
+			b->widx = wi;
+		double *wv = realloc(b->wval, sizeof *wv * 2 * cap);
+		if (wv)
+			b->wval = wv;
+		if (!wi || !wv) {
+			b->error = -1;
+			return -1;
+		}
+		b->wcap = cap;
+	}
+	memcpy(b->widx + b->wlen, idx, sizeof *idx * n);
+	memcpy(b->wval + 2 * b->wlen, z, sizeof(double) * 2 * n);
+	b->wlen += n;
+	b->host_copy_valid = 0;
+	return 0;
+}
+
+int qreg_getamps(struct qreg *reg, const uint64_t *idx, _Complex double *z,
+	size_t n)
+{
+	struct p2_qreg *b = B(reg);
+	if (!b)
+		return -1;
+	for (size_t i = 0; i < n; i++)
+		if (idx[i] >= reg->namp) {
+			log_error("qreg_getamps: index %llu out of range",
+				(unsigned long long)idx[i]);
+			return -1;
+		}
+	if (qreg_flush(reg) < 0)
+		return -1;
+	double *out = (double *)z; /* _Complex double = (re, im) */
+	if (b->host_copy) {
+		if (!b->host_copy_valid) {
+			if (p2d_get_state(b->dev, b->host_copy) < 0) {
+				b->error = -1;
+				return -1;
+			}
+			b->host_copy_valid = 1;
+		}
+		for (size_t i = 0; i < n; i++) {
+			out[2 * i] = b->host_copy[2 * idx[i]];
+			out[2 * i + 1] = b->host_copy[2 * idx[i] + 1];
+		}
+		return 0;
+	}
+	if (p2d_get(b->dev, idx, out, n) < 0) {
 		b->error = -1;
 		return -1;
 	}
@@ -238,10 +327,18 @@ void qreg_zero(struct qreg *reg)
 	struct p2_qreg *b = B(reg);
 	if (!b)
 		return;
-	/* queued rotations act on a state about to be overwritten */
+	/* queued work acts on a state about to be overwritten */
 	b->qlen = 0;
-	if (p2d_zero(b->dev) < 0)
+	b->wlen = 0;
+	if (p2d_zero(b->dev) < 0) {
 		b->error = -1;
+		b->host_copy_valid = 0;
+		return;
+	}
+	if (b->host_copy) {
+		memset(b->host_copy, 0, sizeof(double) * 2 * reg->namp);
+		b->host_copy_valid = 1;
+	}
 }
 
 int qreg_get_state(struct qreg *reg, double *out)
@@ -249,6 +346,10 @@ int qreg_get_state(struct qreg *reg, double *out)
 	struct p2_qreg *b = B(reg);
 	if (!b || qreg_flush(reg) < 0)
 		return -1;
+	if (b->host_copy && b->host_copy_valid) {
+		memcpy(out, b->host_copy, sizeof(double) * 2 * reg->namp);
+		return 0;
+	}
 	return p2d_get_state(b->dev, out);
 }
 
@@ -258,6 +359,8 @@ int qreg_set_state(struct qreg *reg, const double *in)
 	if (!b)
 		return -1;
 	b->qlen = 0;
+	b->wlen = 0;
+	b->host_copy_valid = 0;
 	return p2d_set_state(b->dev, in);
 }
 

@@ -40,20 +40,30 @@ def emulate(amp: np.ndarray, nqb: int, passes, recs) -> np.ndarray:
             offs.append(o)
         idx = x[:, None] ^ np.array(offs, dtype=np.uint64)[None, :]
         R, I = re[idx], im[idx]
+        scaled = False
         for r in recs[p["rot_off"]:p["rot_off"] + p["nrot"]]:
             px = _parity(x & np.uint64(r["z"]))
             sm = (np.int64(r["smask"]) ^ (-px)) & 0xFFFFFFFF
             c, s, U, odd = r["c"], r["s"], r["U"], r["odd"]
+            form = r.get("form", 0)
+            scaled = scaled or form != 0
             nR, nI = R.copy(), I.copy()
             for u in range(1 << M):
                 w = u ^ U
-                su = np.where((sm >> u) & 1, -s, s)
-                if odd:
-                    tr, ti = (-su) * I[:, w], su * R[:, w]
-                else:
-                    tr, ti = su * R[:, w], su * I[:, w]
-                nR[:, u] = c * R[:, u] + tr
-                nI[:, u] = c * I[:, u] + ti
+                sig = np.where((sm >> u) & 1, -1.0, 1.0)
+                pr, pi = (-I[:, w], R[:, w]) if odd else (R[:, w], I[:, w])
+                if form == 0:
+                    su = sig * s
+                    nR[:, u] = c * R[:, u] + su * pr
+                    nI[:, u] = c * I[:, u] + su * pi
+                elif form == 1:   # y + (+-s/c) p, factor c
+                    nR[:, u] = R[:, u] + sig * c * pr
+                    nI[:, u] = I[:, u] + sig * c * pi
+                else:             # (c/s) y + (+-1) p, factor s
+                    nR[:, u] = c * R[:, u] + sig * pr
+                    nI[:, u] = c * I[:, u] + sig * pi
             R, I = nR, nI
+        if scaled:
+            R, I = R * p["scale"], I * p["scale"]
         re[idx], im[idx] = R, I
     return re + 1j * im

@@ -214,6 +214,21 @@ def test_planner_emulation_bit_exact(n, span, max_rots, oracle_lib):
     assert np.array_equal(got, want)
 
 
+@pytest.mark.parametrize("n", [2, 6, 11])
+def test_planner_scaled_forms(n, oracle_lib):
+    """FP32 plans (scaled forms, pass-wide factor) reproduce the oracle to
+    FP64 rounding when executed in FP64; angles cover both forms."""
+    rng = np.random.Generator(np.random.PCG64(500 + n))
+    flip, phase, phi = _rand_rotations(rng, n, 80)
+    amp = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+    passes, recs = plan(n, flip, phase, phi, 5, 0, prec=1)
+    forms = {r["form"] for r in recs}
+    assert forms == {1, 2}
+    got = emulate(amp, n, passes, recs)
+    want = oracle_lib.rotate(amp, n, flip, phase, phi)
+    assert np.max(np.abs(got - want)) < 1e-12 * np.max(np.abs(want))
+
+
 def test_planner_fuses_jw_runs():
     t = workloads.jw_terms(20, 2000, seed=4)
     phi = np.full(len(t), 0.01)
@@ -227,7 +242,7 @@ def test_planner_fuses_jw_runs():
 def test_planner_rejects_bad_width():
     L = lib()
     rin = (_ffi.RotIn * 1)()
-    assert L.phase2_plan(0, rin, 1, 5, 0, (_ffi.Pass * 1)(),
+    assert L.phase2_plan(0, rin, 1, 5, 0, 0, (_ffi.Pass * 1)(),
                          (_ffi.RotRec * 1)()) == -1
 
 

@@ -13,6 +13,7 @@ Tolerances:
                  (one FP32 rounding per pass, FP64 arithmetic inside).
 """
 
+import ctypes as C
 import math
 
 import numpy as np
@@ -80,6 +81,41 @@ def test_random_rotations_bit_exact(n, fusion, oracle_lib):
         r.paulirot(flip, phase, phi, batch=37)
         got = r.get_state()
     assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("n", [5, 11, 17])
+def test_both_kernel_variants(variant, n, oracle_lib):
+    """Direct-load and shared-memory-prefetch pass kernels give the same
+    bits (FP64) and the same FP32 results for every span."""
+    from phase2_b200._ffi import lib
+    L = lib()
+    saved = []
+    for prec in (0, 1):
+        for m in range(6):
+            v, s = C.c_int(), C.c_int()
+            L.phase2_tune_get(prec, m, C.byref(v), C.byref(s))
+            saved.append((prec, m, v.value, s.value))
+            L.phase2_tune_set(prec, m, variant, 0)
+    try:
+        rng = np.random.Generator(np.random.PCG64(300 + n))
+        amp = _rand_state(rng, n)
+        flip, phase, phi = _rand_rots(rng, n, 150)
+        want = oracle_lib.rotate(amp, n, flip, phase, phi)
+        for span in (2, 3, 4, 5):
+            with Register(n, p2.PREC_FP64) as r:
+                r.set_fusion(span, 0)
+                r.set_state(amp)
+                r.paulirot(flip, phase, phi)
+                assert np.array_equal(r.get_state(), want)
+            with Register(n, p2.PREC_FP32) as r:
+                r.set_fusion(span, 0)
+                r.set_state(amp)
+                r.paulirot(flip, phase, phi)
+                assert np.max(np.abs(r.get_state() - want)) < FP32_TOL
+    finally:
+        for prec, m, v, s in saved:
+            L.phase2_tune_set(prec, m, v, s)
 
 
 @pytest.mark.parametrize("n", [3, 10, 15])
