@@ -78,6 +78,27 @@ int phase2_get_term_order(void);
 /* Stable sort by (flip mask, phase mask). */
 void circ_hamil_sort_flip(struct circ_hamil *hm);
 
+/* ---- batched drivers ------------------------------------------------------ */
+
+/*
+ * Run n independent, already initialised problems of one kind together:
+ * each keeps its own register (its own CUDA stream), and the host advances
+ * them in lockstep, enqueuing instance i's next step as soon as its
+ * current overlap has been read, so the GPU overlaps the instances' work
+ * (and replays each instance's repeated step plan from a CUDA graph).
+ * Results land in each problem's ct.vals and step writer exactly as the
+ * single-problem *_simul calls would produce them.  0, or -1 if any
+ * instance failed (the others still run to completion).
+ */
+struct trott;
+struct trott2;
+struct qdrift;
+struct cmpsit;
+int trott_simul_batch(struct trott *const *tts, size_t n);
+int trott2_simul_batch(struct trott2 *const *t2s, size_t n);
+int qdrift_simul_batch(struct qdrift *const *qds, size_t n);
+int cmpsit_simul_batch(struct cmpsit *const *cps, size_t n);
+
 /* ---- execution control and bulk access ---------------------------------- */
 
 /* Launch all queued rotations (asynchronously).  0 or -1. */
@@ -116,6 +137,10 @@ struct phase2_stats {
 	double pass_ms;     /* device time of timed pass launches (CUDA events) */
 	uint64_t h2d_bytes; /* host-to-device bytes copied for this register */
 	uint64_t d2h_bytes; /* device-to-host bytes copied for this register */
+	uint64_t graph_replays; /* flushes launched from a captured CUDA graph
+				 * (a plan seen before, e.g. every Trotter
+				 * step after the second; registers of up to
+				 * 24 qubits) */
 };
 
 int qreg_get_stats(const struct qreg *reg, struct phase2_stats *st);

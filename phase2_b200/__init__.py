@@ -291,6 +291,54 @@ def _run_driver(kind: str, nqb: int, terms: Terms, dets: Dets, **kw):
     return (vals, stats) if kw.get("with_stats") else vals
 
 
+_KIND = {"trott": (_ffi.Trott, "steps"), "trott2": (_ffi.Trott2, "steps"),
+         "qdrift": (_ffi.Qdrift, None), "cmpsit": (_ffi.Cmpsit, None)}
+
+
+def _driver_data(kind: str, p: dict):
+    if kind in ("trott", "trott2"):
+        return _ffi.TrottData(p["steps"], p["delta"])
+    if kind == "qdrift":
+        return _ffi.QdriftData(p["samples"], p["depth"], p["step_size"],
+                               p["seed"])
+    return _ffi.CmpsitData(p["samples"], p["steps"], p["length"], p["depth"],
+                           p["angle_det"], p["angle_rand"], p["seed"])
+
+
+def batch(kind: str, problems: list[dict], with_stats: bool = False):
+    """Run independent problems of one driver kind together through
+    <kind>_simul_batch.  Each problem dict holds nqb, terms, dets and the
+    driver's parameters (as the single-problem helpers take them)."""
+    world_ensure()
+    L = lib()
+    cls = _KIND[kind][0]
+    objs = []
+    try:
+        for p in problems:
+            obj = cls()
+            hm, md = _hamil(p["nqb"], p["terms"]), _muldet(p["dets"])
+            dt = _driver_data(kind, p)
+            if getattr(L, f"{kind}_init")(
+                    C.byref(obj), C.byref(dt), hm, _ffi.STPREP_MULTIDET,
+                    C.cast(C.pointer(md), C.c_void_p), None) != 0:
+                raise RuntimeError(f"{kind}_init failed")
+            objs.append(obj)
+        arr = (C.c_void_p * max(1, len(objs)))(
+            *[C.cast(C.pointer(o), C.c_void_p) for o in objs])
+        if getattr(L, f"{kind}_simul_batch")(arr, len(objs)) != 0:
+            raise RuntimeError(f"{kind}_simul_batch failed")
+        vals = [_values(o.ct.vals) for o in objs]
+        stats = []
+        for o in objs:
+            st = _ffi.Stats()
+            L.qreg_get_stats(C.byref(o.ct.reg), C.byref(st))
+            stats.append({k: getattr(st, k) for k, _ in _ffi.Stats._fields_})
+    finally:
+        for o in objs:
+            getattr(L, f"{kind}_free")(C.byref(o))
+    return (vals, stats) if with_stats else vals
+
+
 def trott(nqb, terms, dets, steps, delta, **kw):
     return _run_driver("trott", nqb, terms, dets, steps=steps, delta=delta,
                        **kw)

@@ -158,7 +158,8 @@ class Stats(C.Structure):
     _fields_ = [("rotations", C.c_uint64), ("passes", C.c_uint64),
                 ("launches", C.c_uint64), ("bytes", C.c_uint64),
                 ("timed_passes", C.c_uint64), ("pass_ms", C.c_double),
-                ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64)]
+                ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64),
+                ("graph_replays", C.c_uint64)]
 
 
 LAYOUT = {0: Qreg, 1: Circ, 2: Trott, 3: Trott2, 4: Qdrift, 5: Cmpsit,
@@ -270,6 +271,10 @@ _SIGS = {
                                C.c_int, C.c_int, _P(Pass), _P(RotRec)]),
     "phase2_norm2_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_uint64,
                                        C.c_void_p, C.c_void_p]),
+    "trott_simul_batch": (C.c_int, [_P(C.c_void_p), C.c_size_t]),
+    "trott2_simul_batch": (C.c_int, [_P(C.c_void_p), C.c_size_t]),
+    "qdrift_simul_batch": (C.c_int, [_P(C.c_void_p), C.c_size_t]),
+    "cmpsit_simul_batch": (C.c_int, [_P(C.c_void_p), C.c_size_t]),
     "phase2_tune_set": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int]),
     "phase2_tune_get": (C.c_int, [C.c_int, C.c_int, _P(C.c_int),
                                   _P(C.c_int)]),

@@ -346,3 +346,127 @@ int cmpsit_simul(struct cmpsit *cp)
 	}
 	return 0;
 }
+
+/* ---- batched drivers (include/phase2_b200.h) ---------------------------- */
+
+/* One instance of a batch: its circuit, writer, the next output slot, and
+ * the function that queues the work producing output slot `idx`. */
+struct batch_item {
+	void *obj;
+	struct circ *ct;
+	struct phase2_step_writer *sw;
+	int (*enqueue)(void *obj, size_t idx);
+	size_t next;
+	int failed;
+};
+
+static int trott_enqueue(void *obj, size_t idx)
+{
+	struct trott *tt = obj;
+	if (idx == 0 && circ_prepst(&tt->ct) < 0)
+		return -1;
+	return circ_step(&tt->ct, &tt->ct.hm, tt->dt.delta);
+}
+
+static int trott2_enqueue(void *obj, size_t idx)
+{
+	struct trott2 *t2 = obj;
+	const double half = t2->dt.delta / 2.0;
+	if (idx == 0 && circ_prepst(&t2->ct) < 0)
+		return -1;
+	if (circ_step(&t2->ct, &t2->ct.hm, half) < 0)
+		return -1;
+	return circ_step_reverse(&t2->ct, &t2->ct.hm, half);
+}
+
+static int qdrift_enqueue(void *obj, size_t idx)
+{
+	struct qdrift *qd = obj;
+	(void)idx;
+	if (circ_prepst(&qd->ct) < 0)
+		return -1;
+	qdrift_draw(qd);
+	return circ_step(&qd->ct, &qd->ranct.hm_ran, asin(qd->dt.step_size));
+}
+
+static int cmpsit_enqueue(void *obj, size_t idx)
+{
+	struct cmpsit *cp = obj;
+	(void)idx;
+	if (circ_prepst(&cp->ct) < 0)
+		return -1;
+	for (size_t s = 0; s < cp->dt.steps; s++) {
+		if (cmpsit_sample(cp) < 0 ||
+			circ_step(&cp->ct, &cp->ranct.hm_smpl, 0.5) < 0)
+			return -1;
+		if (cmpsit_sample(cp) < 0 ||
+			circ_step_reverse(&cp->ct, &cp->ranct.hm_smpl, 0.5) < 0)
+			return -1;
+	}
+	return 0;
+}
+
+static void batch_launch(struct batch_item *it)
+{
+	if (it->enqueue(it->obj, it->next) < 0 || qreg_flush(&it->ct->reg) < 0) {
+		log_error("batch: instance failed at output %zu", it->next);
+		it->failed = 1;
+	}
+}
+
+/* Queue output 0 everywhere, then repeatedly read each instance's pending
+ * output and immediately queue its next one. */
+static int run_batch(struct batch_item *items, size_t n)
+{
+	for (size_t i = 0; i < n; i++)
+		if (items[i].ct->vals.len > 0)
+			batch_launch(&items[i]);
+	int active = 1;
+	while (active) {
+		active = 0;
+		for (size_t i = 0; i < n; i++) {
+			struct batch_item *it = &items[i];
+			struct circ_values *vals = &it->ct->vals;
+			if (it->failed || it->next >= vals->len)
+				continue;
+			active = 1;
+			vals->z[it->next] = circ_measure(it->ct);
+			if (p2_qreg_error(&it->ct->reg) < 0 ||
+				emit(it->sw, it->next, vals->z[it->next]) < 0) {
+				it->failed = 1;
+				continue;
+			}
+			if (++it->next < vals->len)
+				batch_launch(it);
+		}
+	}
+	int rc = 0;
+	for (size_t i = 0; i < n; i++)
+		if (items[i].failed)
+			rc = -1;
+	return rc;
+}
+
+#define BATCH_ENTRY(NAME, TYPE, ENQ)                                           \
+	int NAME(TYPE *const *objs, size_t n)                                  \
+	{                                                                      \
+		if (n == 0)                                                    \
+			return 0;                                              \
+		struct batch_item *items = calloc(n, sizeof *items);           \
+		if (!items)                                                    \
+			return -1;                                             \
+		for (size_t i = 0; i < n; i++) {                               \
+			items[i].obj = objs[i];                                \
+			items[i].ct = &objs[i]->ct;                            \
+			items[i].sw = objs[i]->sw;                             \
+			items[i].enqueue = ENQ;                                \
+		}                                                              \
+		const int rc = run_batch(items, n);                            \
+		free(items);                                                   \
+		return rc;                                                     \
+	}
+
+BATCH_ENTRY(trott_simul_batch, struct trott, trott_enqueue)
+BATCH_ENTRY(trott2_simul_batch, struct trott2, trott2_enqueue)
+BATCH_ENTRY(qdrift_simul_batch, struct qdrift, qdrift_enqueue)
+BATCH_ENTRY(cmpsit_simul_batch, struct cmpsit, cmpsit_enqueue)

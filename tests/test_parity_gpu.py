@@ -299,6 +299,52 @@ def test_flip_order_vs_oracle_given_order(oracle_lib):
     assert np.array_equal(z, want)
 
 
+def test_graph_replay_is_exact(oracle_lib):
+    """Repeated Trotter steps replay a captured CUDA graph; the result is
+    unchanged (bit-identical to the oracle)."""
+    t = workloads.jw_terms(14, 200, seed=41)
+    d = workloads.hamming_dets(14, 3, 7, seed=42)
+    z, st = p2.trott(14, t, d, 8, 0.1, with_stats=True)
+    assert st["graph_replays"] >= 5
+    want = oracle_lib.trott(14, t.flip, t.phase, t.cf, d.idx, d.cf, 8, 0.1)
+    assert np.array_equal(z, want)
+
+
+def test_batched_drivers_match_single(oracle_lib):
+    """Independent problems of uneven size run together; every result is
+    bit-identical to the oracle run of that problem alone."""
+    probs = []
+    for k, n in enumerate((8, 13, 10, 15, 9, 12)):
+        t = workloads.jw_terms(n, 40 + 30 * k, seed=500 + k)
+        d = workloads.hamming_dets(n, 1 + k % 3, n // 2, seed=600 + k)
+        probs.append(dict(nqb=n, terms=t, dets=d, steps=3 + k, delta=0.1,
+                          samples=2 + k % 2, depth=50 + 10 * k,
+                          step_size=0.02, seed=700 + k))
+    for kind in ("trott", "trott2"):
+        got = p2.batch(kind, probs)
+        for p, z in zip(probs, got):
+            t, d = p["terms"], p["dets"]
+            want = oracle_lib.trott(p["nqb"], t.flip, t.phase, t.cf, d.idx,
+                                    d.cf, p["steps"], p["delta"],
+                                    order2=kind == "trott2")
+            assert np.array_equal(z, want), kind
+    got = p2.batch("qdrift", probs)
+    for p, z in zip(probs, got):
+        t, d = p["terms"], p["dets"]
+        want = oracle_lib.qdrift(p["nqb"], t.flip, t.phase, t.cf, d.idx,
+                                 d.cf, p["samples"], p["depth"],
+                                 p["step_size"], p["seed"])
+        assert np.array_equal(z, want)
+    cm = [dict(p, samples=2, steps=2, length=8, depth=20, angle_det=0.05,
+               angle_rand=0.01) for p in probs]
+    got = p2.batch("cmpsit", cm)
+    for p, z in zip(cm, got):
+        t, d = p["terms"], p["dets"]
+        want = oracle_lib.cmpsit(p["nqb"], t.flip, t.phase, t.cf, d.idx,
+                                 d.cf, 2, 2, 8, 20, 0.05, 0.01, p["seed"])
+        assert np.array_equal(z, want)
+
+
 def test_empty_hamiltonian_and_edges():
     t = Terms(np.zeros(0, np.uint64), np.zeros(0, np.uint64), np.zeros(0))
     d = Dets(np.array([3], np.uint64), np.array([1.0 + 0j]))
