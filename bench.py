@@ -298,6 +298,10 @@ def gpu_arm(args) -> None:
         dev_ms / args.steps / 1e3) / 1e9
     cpu = _cpu_baseline() if (rank == 0 and ws == 1 and not args.quick) \
         else None
+    extra = {}
+    if rank == 0 and not args.quick:
+        extra["fp32_error"] = fp32_error_study()
+        extra["batched"] = batched_study()
     if rank != 0:
         return
     clocks = clk.summary()
@@ -337,8 +341,76 @@ def gpu_arm(args) -> None:
         "fp32_fused_vs_fp64_plain": (value / arms["fp64_plain"]["value"]
                                      if arms.get("fp64_plain") else None),
         "overlaps": [[z.real, z.imag] for z in zs[:2]],
+        **extra,
     }
     print(json.dumps(line), flush=True)
+
+
+def fp32_error_study(nqb: int = 20, nterms: int = 300, steps: int = 1000,
+                     delta: float = 0.05) -> dict:
+    """Second-order Trotter with a JW Hamiltonian (lexicographic order, 4
+    determinants), FP32 and FP64 states side by side; error of every
+    step's overlap against the FP64 run, which is bit-identical to the CPU
+    oracle (tests/test_parity_gpu.py)."""
+    import numpy as np
+
+    import phase2_b200 as p2
+    from phase2_b200 import workloads
+    t = workloads.jw_terms(nqb, nterms, seed=0xE220)
+    d = workloads.hamming_dets(nqb, 4, nqb // 2, seed=0xE221)
+    p2.set_precision(p2.PREC_FP64)
+    t0 = time.perf_counter()
+    z64 = p2.trott2(nqb, t, d, steps, delta)
+    p2.set_precision(p2.PREC_FP32)
+    try:
+        z32 = p2.trott2(nqb, t, d, steps, delta)
+    finally:
+        p2.set_precision(p2.PREC_FP64)
+    err = np.abs(z32 - z64)
+    at = {str(s): float(err[s - 1]) for s in (1, 10, 100, 1000)
+          if s <= steps}
+    return {"workload": (f"trott2 {nqb} qubits, {nterms} JW terms, "
+                         f"4 determinants, delta {delta}"),
+            "steps": steps, "rotations": 2 * nterms * steps,
+            "max_abs_err": float(err.max()), "err_at_step": at,
+            "final_overlap_fp64": [float(z64[-1].real), float(z64[-1].imag)],
+            "seconds": time.perf_counter() - t0}
+
+
+def batched_study(ninst: int = 64, step_cap: int = 4, seed: int = 0xBA7C4):
+    """Independent trott problems of uneven size run together: qubits
+    U{18..24}, JW terms log-uniform in [1e3, 5e4], steps U{16..512} capped
+    at step_cap for a bounded run, FP32 state, one determinant each.
+    Aggregate rot.amp/s over the batch (wall clock around the batch
+    call)."""
+    import numpy as np
+
+    import phase2_b200 as p2
+    from phase2_b200 import workloads
+    rng = np.random.Generator(np.random.PCG64(seed))
+    probs, work = [], 0
+    for k in range(ninst):
+        n = int(rng.integers(18, 25))
+        nt = int(round(10 ** rng.uniform(3, np.log10(5e4))))
+        steps = min(int(rng.integers(16, 513)), step_cap)
+        t = workloads.jw_terms(n, nt, seed=seed + k)
+        d = workloads.hamming_dets(n, 1, n // 2, seed=seed + 1000 + k)
+        probs.append(dict(nqb=n, terms=t, dets=d, steps=steps, delta=0.05))
+        work += steps * nt * (1 << n)
+    p2.set_precision(p2.PREC_FP32)
+    try:
+        p2.batch("trott", probs[:2])  # warm the kernels
+        t0 = time.perf_counter()
+        _, stats = p2.batch("trott", probs, with_stats=True)
+        wall = time.perf_counter() - t0
+    finally:
+        p2.set_precision(p2.PREC_FP64)
+    return {"workload": (f"{ninst} trott instances, 18-24 qubits, 1e3-5e4 "
+                         f"JW terms, {step_cap} steps each, FP32 state"),
+            "rot_amp": work, "seconds": wall,
+            "value": work / wall, "unit": UNIT,
+            "passes": int(sum(s["passes"] for s in stats)),
+            "graph_replays": int(sum(s["graph_replays"] for s in stats))}
 
 
 # ---- the reference arm -------------------------------------------------

@@ -345,6 +345,23 @@ def test_batched_drivers_match_single(oracle_lib):
         assert np.array_equal(z, want)
 
 
+def test_sharded_qdrift_equals_single_run():
+    """Replica sharding (phase2_b200.replicas): the blocks of 3 ranks,
+    each with its generator advanced to its first sample, concatenate to
+    the single-process run bit for bit."""
+    from phase2_b200 import replicas
+    t = workloads.jw_terms(12, 150, seed=61)
+    d = workloads.hamming_dets(12, 2, 6, seed=62)
+    full = p2.qdrift(12, t, d, 8, 40, 0.03, 0x600D)
+    parts = []
+    for rank in range(3):
+        start, z = replicas.qdrift_local(12, t, d, 8, 40, 0.03, 0x600D,
+                                         rank, 3)
+        parts.append((start, z))
+    got = np.concatenate([z for _, z in sorted(parts, key=lambda b: b[0])])
+    assert np.array_equal(got, full)
+
+
 def test_empty_hamiltonian_and_edges():
     t = Terms(np.zeros(0, np.uint64), np.zeros(0, np.uint64), np.zeros(0))
     d = Dets(np.array([3], np.uint64), np.array([1.0 + 0j]))
