@@ -32,6 +32,8 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <type_traits>
+
 #define LOG_SUBSYS "engine"
 #include "log.h"
 
@@ -581,6 +583,164 @@ __global__ void __launch_bounds__(P2_TPB,
 	}
 }
 
+/* ---- split pass kernel (FP32 storage) ----------------------------------- */
+
+/* y <- y + (+-r) p  or  y <- r y + (+-1) p, p = partner (times i if ODD) */
+template <int ODD, int COT>
+__device__ __forceinline__ void p2_split_upd(double &yr, double &yi,
+	double qr, double qi, double r, uint32_t sg)
+{
+	const double pr = ODD ? -qi : qr;
+	const double pi = ODD ? qr : qi;
+	if constexpr (!COT) {
+		const double rv = p2_sgn(r, sg);
+		yr = fma(rv, pr, yr);
+		yi = fma(rv, pi, yi);
+	} else {
+		yr = fma(r, yr, p2_sgn(pr, sg));
+		yi = fma(r, yi, p2_sgn(pi, sg));
+	}
+}
+
+/*
+ * Scaled rotation on a coset shared by two adjacent lanes: this lane holds
+ * the 2^(M-1) slots whose top slot bit equals its lane parity (`half`);
+ * slot u = v | half << (M-1).  A rotation whose partner stays in the lane
+ * (top bit of U clear) is the ordinary pair update on the local slots;
+ * otherwise every local slot's partner is fetched from the other lane with
+ * one shuffle per component and each lane updates only its own slots.
+ * sm holds this lane's signs (bit v = sign of local slot v).
+ */
+template <int M, int U, int ODD, int COT>
+__device__ __forceinline__ void p2_rot_split(double (&re)[1 << (M - 1)],
+	double (&im)[1 << (M - 1)], double r, uint32_t sm, unsigned mask)
+{
+	constexpr int MH = M - 1;
+	constexpr int TOP = 1 << MH;
+	if constexpr ((U & TOP) == 0) {
+		p2_rot_scaled<MH, U, ODD, COT>(re, im, r, sm, 0u);
+	} else {
+		/* Local slots v and v ^ UL exchange with the other lane's
+		 * v ^ UL and v: fetch both before either is overwritten. */
+		constexpr int UL = U & (TOP - 1);
+#pragma unroll
+		for (int v = 0; v < (1 << MH); ++v) {
+			const int v2 = v ^ UL;
+			if (v2 < v)
+				continue;
+			const double ar = __shfl_xor_sync(mask, re[v2], 1);
+			const double ai = __shfl_xor_sync(mask, im[v2], 1);
+			double br = 0.0, bi = 0.0;
+			if (v2 != v) {
+				br = __shfl_xor_sync(mask, re[v], 1);
+				bi = __shfl_xor_sync(mask, im[v], 1);
+			}
+			p2_split_upd<ODD, COT>(re[v], im[v], ar, ai, r,
+				p2_bitmask(sm, v));
+			if (v2 != v)
+				p2_split_upd<ODD, COT>(re[v2], im[v2], br, bi, r,
+					p2_bitmask(sm, v2));
+		}
+	}
+}
+
+#define P2_CASE_P(K)                                                           \
+	case K:                                                                \
+		if constexpr ((K) < (4 << M))                                  \
+			p2_rot_split<M, ((K) >> 2), (((K) >> 1) & 1),          \
+				((K)&1)>(re, im, r, sm, mask);                 \
+		break;
+#define P2_CASE_P8(B)                                                          \
+	P2_CASE_P(B + 0) P2_CASE_P(B + 1) P2_CASE_P(B + 2) P2_CASE_P(B + 3)    \
+	P2_CASE_P(B + 4) P2_CASE_P(B + 5) P2_CASE_P(B + 6) P2_CASE_P(B + 7)
+
+template <int M>
+__device__ __forceinline__ void p2_apply_split(uint32_t key,
+	double (&re)[1 << (M - 1)], double (&im)[1 << (M - 1)], double r,
+	uint32_t sm, unsigned mask)
+{
+	switch (key) {
+		P2_CASE_P8(0) P2_CASE_P8(8) P2_CASE_P8(16) P2_CASE_P8(24)
+		P2_CASE_P8(32) P2_CASE_P8(40) P2_CASE_P8(48) P2_CASE_P8(56)
+		P2_CASE_P8(64) P2_CASE_P8(72) P2_CASE_P8(80) P2_CASE_P8(88)
+		P2_CASE_P8(96) P2_CASE_P8(104) P2_CASE_P8(112) P2_CASE_P8(120)
+	default:
+		break;
+	}
+}
+#undef P2_CASE_P8
+#undef P2_CASE_P
+
+/*
+ * One FP32 pass with each coset shared by a lane pair (variant 2): half
+ * the registers per thread of k_pass, so twice the resident warps to hide
+ * load and arithmetic latency.  Both lanes of a pair always have the same
+ * representative, so they enter and leave the loop together and every
+ * shuffle pairs two active lanes.
+ */
+template <int M>
+__global__ void __launch_bounds__(P2_TPB, M >= 5 ? 4 : 6)
+	k_pass_split(float2 *__restrict__ st, uint64_t nrep,
+		struct phase2_pass p,
+		const struct phase2_rot_rec *__restrict__ recs)
+{
+	__shared__ struct phase2_rot_rec srec[P2_MAX_ROTS_PER_PASS];
+	__shared__ uint64_t sbasis[PHASE2_MAX_SPAN];
+	for (uint32_t r = threadIdx.x; r < p.nrot; r += blockDim.x)
+		srec[r] = recs[p.rot_off + r];
+	if (threadIdx.x == 0) {
+#pragma unroll
+		for (int k = 0; k < M; ++k)
+			sbasis[k] = p.basis[k];
+	}
+	__syncthreads();
+	constexpr int MH = M - 1;
+	const uint32_t half = threadIdx.x & 1u;
+	uint64_t pb[MH > 0 ? MH : 1];
+#pragma unroll
+	for (int k = 0; k < MH; ++k)
+		pb[k] = p.basis[k];
+	const uint64_t top = half ? p.basis[MH] : 0;
+
+	const uint64_t stride = ((uint64_t)gridDim.x * blockDim.x) >> 1;
+	for (uint64_t t = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 1;
+		t < nrep; t += stride) {
+		const unsigned mask = __activemask();
+		const uint64_t x = p2_rep<M>(t, p) ^ top;
+		double re[1 << MH], im[1 << MH];
+#pragma unroll
+		for (int v = 0; v < (1 << MH); ++v)
+			p2_ld(st, x ^ p2_slot_off<MH>(v, pb), re[v], im[v]);
+		for (uint32_t r = 0; r < p.nrot; ++r) {
+			const uint64_t z = srec[r].z;
+			const uint32_t px = (uint32_t)(__popcll(x & z) & 1);
+			/* x includes the top basis vector for the upper lane, so
+			 * px already carries parity(top & z): local sign bits are
+			 * the lower half of smask with that parity folded in */
+			uint32_t sm = srec[r].smask;
+			if (half)
+				sm = (sm >> (1u << MH)) ^
+					(((uint32_t)__popcll(top & z) & 1u) ?
+							0xffffffffu : 0u);
+			sm ^= 0u - px;
+			const uint32_t key = ((uint32_t)srec[r].U << 2) |
+				((uint32_t)srec[r].odd << 1) |
+				(srec[r].form == 2 ? 1u : 0u);
+			p2_apply_split<M>(key, re, im, srec[r].c, sm, mask);
+		}
+#pragma unroll
+		for (int v = 0; v < (1 << MH); ++v) {
+			re[v] *= p.scale;
+			im[v] *= p.scale;
+		}
+		const uint64_t xs = p2_rep<M>(t, p) ^
+			(half ? sbasis[MH] : UINT64_C(0));
+#pragma unroll
+		for (int v = 0; v < (1 << MH); ++v)
+			p2_st(st, xs ^ p2_slot_off<MH>(v, sbasis), re[v], im[v]);
+	}
+}
+
 /* ---- small kernels ------------------------------------------------------ */
 
 template <typename ST>
@@ -1007,7 +1167,7 @@ static struct p2_tune_entry p2_tune[2][PHASE2_MAX_SPAN + 1] = {
 extern "C" int phase2_tune_set(int prec, int span, int variant, int per_sm)
 {
 	if ((prec != PHASE2_PREC_FP64 && prec != PHASE2_PREC_FP32) || span < 0 ||
-		span > PHASE2_MAX_SPAN || variant < 0 || variant > 1 ||
+		span > PHASE2_MAX_SPAN || variant < 0 || variant > 2 ||
 		per_sm < 0 || per_sm > 64)
 		return -1;
 	p2_tune[prec][span].variant = variant;
@@ -1040,7 +1200,16 @@ static int launch_pass_t(struct p2_dev *d, const struct phase2_pass &p,
 {
 	const uint64_t nrep = d->namp >> M;
 	const struct p2_tune_entry te = p2_tune[d->prec][M];
-	if (te.variant == 0) {
+	if constexpr (std::is_same<ST, float2>::value && M >= 2) {
+		if (te.variant == 2) {
+			const unsigned per_sm = te.per_sm ? (unsigned)te.per_sm : 16u;
+			const unsigned grid = grid_for(d, 2 * nrep, P2_TPB, per_sm);
+			k_pass_split<M><<<grid, P2_TPB, 0, d->stream>>>(
+				(float2 *)d->state, nrep, p, recs);
+			return 0;
+		}
+	}
+	if (te.variant != 1) {
 		const unsigned per_sm = te.per_sm ? (unsigned)te.per_sm : 16u;
 		const unsigned grid = grid_for(d, nrep, P2_TPB, per_sm);
 		k_pass<M, ST, EXACT><<<grid, P2_TPB, 0, d->stream>>>(
