@@ -51,6 +51,53 @@ def cplx(z) -> list:
     return [float(np.real(z)), float(np.imag(z))]
 
 
+H2O_DUMP = Path("/root/reference/test/data/H2O_CAS56.h5dump")
+
+
+def _dataset_values(text: str, name: str) -> list[float]:
+    """Numbers of DATASET `name` in an h5dump text (index prefixes
+    like "(12):" or "(3,0):" removed)."""
+    import re
+    start = text.index(f'DATASET "{name}"')
+    body = text[text.index("DATA {", start) + 6:]
+    body = body[:body.index("}")]
+    body = re.sub(r"\(\s*\d+(\s*,\s*\d+)*\s*\):", " ", body)
+    return [float(v) for v in body.replace(",", " ").split()]
+
+
+def h2o_fixture() -> dict:
+    """The reference's 10-qubit water CAS(5,6) Hamiltonian (251 terms) and
+    determinant from test/data/H2O_CAS56.h5dump, loaded as the reference's
+    data_hamil_load / data_muldet_load do (ph2run/data.c:515-540, 625-660):
+    coefficient times the `normalization` attribute, byte j of a row is the
+    operator on qubit j (I=0, X=1, Y=2, Z=3), determinant bit j = byte j."""
+    import re
+    text = H2O_DUMP.read_text()
+    i = text.index('ATTRIBUTE "normalization"')
+    norm = float(re.search(r"\(0\):\s*([-0-9.eE+]+)", text[i:]).group(1))
+    coeffs = _dataset_values(text, "coeffs")[:251]
+    paulis = [int(v) for v in _dataset_values(text, "paulis")]
+    sp = text.index('GROUP "state_prep"')
+    det_cf = _dataset_values(text[sp:], "coeffs")
+    det_bits = [int(v) for v in _dataset_values(text[sp:], "dets")]
+    nqb = 10
+    flip, phase = [], []
+    for t in range(len(coeffs)):
+        f = p = 0
+        for j in range(nqb):
+            b = paulis[t * nqb + j]
+            if b in (1, 2):
+                f |= 1 << j
+            if b in (2, 3):
+                p |= 1 << j
+        flip.append(f)
+        phase.append(p)
+    idx = sum(b << j for j, b in enumerate(det_bits))
+    return {"nqb": nqb, "flip": flip, "phase": phase,
+            "cf": [c * norm for c in coeffs], "det_idx": [idx],
+            "det_cf": [[det_cf[0], det_cf[1]]], "normalization": norm}
+
+
 def main() -> None:
     ref = Reference()
     L = ref.L
@@ -225,6 +272,24 @@ def main() -> None:
     z = ref.trott(12, t.flip, t.phase, t.cf, d.idx, d.cf, cfg["steps"],
                   cfg["delta"], order2=False, sort_lex=True)
     gold["trotter12"] = {"z": [cplx(v) for v in z]}
+
+    # -- the reference's water fixture through all four drivers
+    h = h2o_fixture()
+    fl = np.array(h["flip"], dtype=np.uint64)
+    ph = np.array(h["phase"], dtype=np.uint64)
+    cf = np.array(h["cf"])
+    di = np.array(h["det_idx"], dtype=np.uint64)
+    dc = np.array([complex(*c) for c in h["det_cf"]])
+    h["trott"] = [cplx(v) for v in ref.trott(10, fl, ph, cf, di, dc, 12,
+                                            0.5)]
+    h["trott2"] = [cplx(v) for v in ref.trott(10, fl, ph, cf, di, dc, 12,
+                                             0.5, order2=True)]
+    h["qdrift"] = [cplx(v) for v in ref.qdrift(10, fl, ph, cf, di, dc, 6,
+                                              300, 0.01, 0xC0FFEE)]
+    h["cmpsit"] = [cplx(v) for v in ref.cmpsit(10, fl, ph, cf, di, dc, 3,
+                                              4, 60, 50, 0.1, 0.02,
+                                              0xBEEF)]
+    gold["h2o"] = h
 
     (OUT / "golden.json").write_text(json.dumps(gold, indent=0))
 

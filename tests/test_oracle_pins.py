@@ -98,6 +98,38 @@ def test_trotter12(golden, oracle_lib):
     assert np.array_equal(z, want)
 
 
+def h2o_case(golden):
+    """The reference's water CAS(5,6) fixture as numpy arrays."""
+    h = golden["h2o"]
+    return (h["nqb"], np.array(h["flip"], dtype=np.uint64),
+            np.array(h["phase"], dtype=np.uint64), np.array(h["cf"]),
+            np.array(h["det_idx"], dtype=np.uint64),
+            np.array([_cz(v) for v in h["det_cf"]]))
+
+
+def test_h2o_fixture(golden, oracle_lib):
+    h = golden["h2o"]
+    n, fl, ph, cf, di, dc = h2o_case(golden)
+    assert n == 10 and len(cf) == 251 and int(di[0]) == 0b0011100111
+    # Pauli strings are distinct; the identity is not among them (its
+    # coefficient is the file's separate `offset` attribute).
+    assert len(set(zip(fl.tolist(), ph.tolist()))) == 251
+    assert not np.any((fl == 0) & (ph == 0))
+    runs = {
+        "trott": oracle_lib.trott(n, fl, ph, cf, di, dc, 12, 0.5),
+        "trott2": oracle_lib.trott(n, fl, ph, cf, di, dc, 12, 0.5,
+                                   order2=True),
+        "qdrift": oracle_lib.qdrift(n, fl, ph, cf, di, dc, 6, 300, 0.01,
+                                    0xC0FFEE),
+        "cmpsit": oracle_lib.cmpsit(n, fl, ph, cf, di, dc, 3, 4, 60, 50, 0.1,
+                                    0.02, 0xBEEF),
+    }
+    for kind, z in runs.items():
+        want = np.array([_cz(v) for v in h[kind]])
+        assert np.array_equal(z, want), kind
+        assert np.all(np.abs(z) <= 1 + 1e-12), kind
+
+
 needs_ref = pytest.mark.skipif(not REF_SO.is_file(),
                                reason="oracle/_ref not built here")
 

@@ -83,11 +83,12 @@ def test_random_rotations_bit_exact(n, fusion, oracle_lib):
     assert np.array_equal(got, want)
 
 
-@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("variant", [0, 1, 2])
 @pytest.mark.parametrize("n", [5, 11, 17])
 def test_both_kernel_variants(variant, n, oracle_lib):
-    """Direct-load and shared-memory-prefetch pass kernels give the same
-    bits (FP64) and the same FP32 results for every span."""
+    """Direct-load, shared-memory-prefetch and lane-split pass kernels give
+    the same bits (FP64; the split variant is FP32-only and FP64 falls back
+    to direct loads) and the same FP32 results for every span."""
     from phase2_b200._ffi import lib
     L = lib()
     saved = []
@@ -259,6 +260,50 @@ def test_trotter12_fp32(golden):
         p2.set_precision(p2.PREC_FP64)
     want = np.array([_cz(v) for v in golden["trotter12"]["z"]])
     assert np.max(np.abs(z - want)) < FP32_TOL
+
+
+def _h2o(golden):
+    h = golden["h2o"]
+    return h, Terms(np.array(h["flip"], dtype=np.uint64),
+                    np.array(h["phase"], dtype=np.uint64),
+                    np.array(h["cf"])), \
+        Dets(np.array(h["det_idx"], dtype=np.uint64),
+             np.array([_cz(v) for v in h["det_cf"]]))
+
+
+def _h2o_runs(t, d):
+    return {
+        "trott": lambda: p2.trott(10, t, d, 12, 0.5),
+        "trott2": lambda: p2.trott2(10, t, d, 12, 0.5),
+        "qdrift": lambda: p2.qdrift(10, t, d, 6, 300, 0.01, 0xC0FFEE),
+        "cmpsit": lambda: p2.cmpsit(10, t, d, 3, 4, 60, 50, 0.1, 0.02,
+                                    0xBEEF),
+    }
+
+
+@pytest.mark.parametrize("fusion", [(1, 1), (5, 0)])
+def test_h2o_fixture_fp64(golden, fusion):
+    """The reference's water CAS(5,6) Hamiltonian (251 terms, 10 qubits)
+    through all four drivers: bit-identical to the reference's outputs."""
+    h, t, d = _h2o(golden)
+    p2.set_fusion(*fusion)
+    try:
+        for kind, run in _h2o_runs(t, d).items():
+            want = np.array([_cz(v) for v in h[kind]])
+            assert np.array_equal(run(), want), kind
+    finally:
+        p2.set_fusion(5, 0)
+
+
+def test_h2o_fixture_fp32(golden):
+    h, t, d = _h2o(golden)
+    p2.set_precision(p2.PREC_FP32)
+    try:
+        for kind, run in _h2o_runs(t, d).items():
+            want = np.array([_cz(v) for v in h[kind]])
+            assert np.max(np.abs(run() - want)) < FP32_TOL, kind
+    finally:
+        p2.set_precision(p2.PREC_FP64)
 
 
 @pytest.mark.parametrize("order2", [False, True])
