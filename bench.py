@@ -184,7 +184,7 @@ def _ffi_stats(p2, obj):
 
 
 def _traffic_per_launch():
-    p = ROOT / "profiles" / "k_pass_traffic.json"
+    p = ROOT / "profiles" / "k_pass_lift32_traffic.json"
     if p.is_file():
         try:
             return json.loads(p.read_text()).get("bytes_per_launch_30q_fp32")
@@ -268,17 +268,22 @@ def gpu_arm(args) -> None:
     cmp_depth = max(64, min(depth, args.cmp_depth))
     cmp_cfg = dict(cfg, depth=cmp_depth)
     arms = {}
-    for name, prec, fusion in (("fp64_plain", p2.PREC_FP64, (1, 1)),
-                               ("fp64_fused", p2.PREC_FP64, (5, 0)),
-                               ("fp32_plain", p2.PREC_FP32, (1, 1))):
+    form0 = p2.get_fp32_form()
+    for name, prec, fusion, form in (
+            ("fp64_plain", p2.PREC_FP64, (1, 1), form0),
+            ("fp64_fused", p2.PREC_FP64, (5, 0), form0),
+            ("fp32_plain", p2.PREC_FP32, (1, 1), form0),
+            ("fp32_fused_f64arith", p2.PREC_FP32, (5, 0), p2.FORM_LIFTED)):
         if args.quick and name != "fp64_plain":
             continue
+        p2.set_fp32_form(form)
         o = _qdrift_obj(p2, cmp_cfg, prec, fusion, seed + 7)
         try:
             _run_steps(p2, o, 1, timing=False)
             ms, _, s, _ = _run_steps(p2, o, 1, timing=True)
         finally:
             p2.lib().qdrift_free(C.byref(o))
+            p2.set_fp32_form(form0)
         ms = _max_over_ranks(ms, ws)
         elem = 16 if prec == p2.PREC_FP64 else 8
         arms[name] = {
@@ -300,7 +305,14 @@ def gpu_arm(args) -> None:
         else None
     extra = {}
     if rank == 0 and not args.quick:
-        extra["fp32_error"] = fp32_error_study()
+        extra["fp32_error"] = {}
+        for fname, form in (("f32_arith", p2.FORM_LIFTED_F32),
+                            ("f64_arith", p2.FORM_LIFTED)):
+            p2.set_fp32_form(form)
+            try:
+                extra["fp32_error"][fname] = fp32_error_study()
+            finally:
+                p2.set_fp32_form(form0)
         extra["batched"] = batched_study()
     if rank != 0:
         return
@@ -309,8 +321,9 @@ def gpu_arm(args) -> None:
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "storage": "complex64 state (f32), f64 rotation arithmetic",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "storage": ("complex64 state; rotations in FP32 FMAs (lifted "
+                    "form); angles, cos/sin, norms and overlaps in FP64"),
         "data": "synthetic (seeded JW-like Hamiltonian, no dataset)",
         "config": {
             "workload": (f"qdrift {nqb} qubits, {len(cfg['terms'])} JW "
@@ -327,7 +340,7 @@ def gpu_arm(args) -> None:
                      "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"],
                      "peak_source": peaks["source"],
-                     "kernel": "k_pass<M,float2,false>",
+                     "kernel": "k_pass_lift32<M,uint32_t>",
                      "bytes_per_launch": bytes_per_launch,
                      "launch_ms": launch_ms,
                      "traffic": _traffic_per_launch()},

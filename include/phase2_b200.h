@@ -22,9 +22,9 @@ extern "C" {
 /* ---- precision ---------------------------------------------------------- */
 
 /* FP64: complex128 state, rotations bit-identical to the reference CPU
- * path.  FP32: complex64 state (half the HBM bytes per sweep); cos/sin,
- * the rotation arithmetic inside a pass, norms and overlaps stay FP64, and
- * each amplitude is rounded to FP32 once per pass. */
+ * path.  FP32: complex64 state (half the HBM bytes per sweep); angles and
+ * cos/sin are computed in FP64, norms and overlaps are FP64 reductions, and
+ * the rotation arithmetic follows the FP32 form (phase2_set_fp32_form). */
 enum phase2_prec {
 	PHASE2_PREC_FP64 = 0,
 	PHASE2_PREC_FP32 = 1,
@@ -35,6 +35,15 @@ enum phase2_prec {
  * ("fp32"/"fp64") read at world_init.  Returns 0 or -1. */
 int phase2_set_precision(int prec);
 int phase2_get_precision(void);
+
+/* Arithmetic of FP32 passes (enum phase2_form below), both rotating each
+ * amplitude pair by three in-place shears:
+ *   PHASE2_FORM_LIFTED_F32 (default) FP32 FMAs on FP32 coefficients;
+ *   PHASE2_FORM_LIFTED      FP64 arithmetic, one rounding to FP32 per pass.
+ * Also PHASE2_FP32_FORM=lifted_f32|lifted at world_init.  Applies to
+ * rotations planned afterwards.  0 or -1. */
+int phase2_set_fp32_form(int form);
+int phase2_get_fp32_form(void);
 
 /* qreg_init at an explicit precision. */
 int qreg_init_prec(struct qreg *reg, uint32_t nqb, int prec);
@@ -204,21 +213,35 @@ struct phase2_pass {
 	uint32_t nrot;     /* rotations in this pass */
 	uint32_t rot_off;  /* first rotation record */
 	uint8_t piv[PHASE2_MAX_SPAN]; /* pivot bits, ascending */
-	uint8_t pad[3];
+	uint8_t form;      /* PHASE2_FORM_* of every record of the pass */
+	uint8_t pad[2];
 	uint64_t basis[PHASE2_MAX_SPAN];
-	double scale;      /* scaled form: product of the per-rotation factors */
+	double scale;      /* lifted forms: +-1, applied at the store */
+};
+
+/* Arithmetic of a pass (struct phase2_pass.form). */
+enum phase2_form {
+	PHASE2_FORM_EXACT = 0,      /* FP64 state: the reference's update,
+				     * records of form 0 */
+	PHASE2_FORM_LIFTED = 1,     /* FP32 state, records of form 1, FP64
+				     * arithmetic */
+	PHASE2_FORM_LIFTED_F32 = 2, /* FP32 state, records of form 1 with FP32
+				     * s, FP32 arithmetic */
 };
 
 /* Rotation record in slot coordinates: the partner of slot u is u ^ U; the
  * sign bit of slot u for a thread with representative x is
  * bit u of smask XOR parity(x & z); odd = 1 multiplies the partner by i.
  *
- * form 0 (exact, FP64 state):  a_u <- c a_u + (+-s) p_u
- * form 1 (scaled, |c| >= |s|): y_u <- y_u + (+-s/c) p_u,  factor c
- * form 2 (scaled, |c| <  |s|): y_u <- (c/s) y_u + (+-1) p_u, factor s
- * with p_u the partner (times i when odd); in the scaled forms `c` holds
- * the ratio and the pass multiplies every amplitude by `scale` (the product
- * of the factors) once, when it stores. */
+ * form 0 (exact, FP64 state):   a_u <- c a_u + (+-s) p_u,
+ *     p_u the partner (times i when odd);
+ * form 1 (lifted, FP32 state):  three in-place shears of the pair,
+ *     y_u += t q_u y_w;  y_w += s q_w y_u;  y_u += t q_u y_w,
+ *     q_u = (+-1)(odd ? i : 1), q_w = -conj(q_u), t = (1 - cos phi) / s
+ *     held in `c`; a rotation with cos(phi) < 0 is stored as
+ *     exp(i(phi -+ pi)P) and the pass negates every amplitude once per such
+ *     rotation (`scale` = +-1).  For PHASE2_FORM_LIFTED_F32 passes s is an
+ *     FP32 value and t is taken against it. */
 struct phase2_rot_rec {
 	uint64_t z;
 	double c, s;
@@ -231,7 +254,7 @@ struct phase2_rot_rec {
 };
 
 /* Plan n rotations for an nqb-qubit register of precision prec (FP64:
- * exact form; FP32: scaled forms).  Writes at most n passes and n records;
+ * exact form; FP32: the process's FP32 form, lifted by default).  Writes at most n passes and n records;
  * returns the number of passes, or -1. */
 long phase2_plan(uint32_t nqb, const struct phase2_rot_in *rots, size_t n,
 	int max_span, int max_rots, int prec, struct phase2_pass *passes,

@@ -26,6 +26,7 @@ __all__ = ["run", "world_ensure", "Register", "Terms", "Dets", "trott",
 
 PREC_FP64 = _ffi.PREC_FP64
 PREC_FP32 = _ffi.PREC_FP32
+FORM_EXACT, FORM_LIFTED, FORM_LIFTED_F32 = 0, 1, 2
 _WORLD_SEED = 0x2B200C0DE5EED001
 
 
@@ -62,6 +63,17 @@ def run(paulis: list[str], coeffs: list[float], delta: float,
 def set_precision(prec: int) -> None:
     if lib().phase2_set_precision(prec) != 0:
         raise ValueError(f"bad precision {prec}")
+
+
+def set_fp32_form(form: int) -> None:
+    """Arithmetic of FP32 passes: FORM_LIFTED_F32 (default, FP32 FMAs) or
+    FORM_LIFTED (FP64 arithmetic, one rounding to FP32 per pass)."""
+    if lib().phase2_set_fp32_form(form) != 0:
+        raise ValueError(f"bad FP32 form {form}")
+
+
+def get_fp32_form() -> int:
+    return lib().phase2_get_fp32_form()
 
 
 def set_fusion(max_span: int, max_rots: int = 0) -> None:
@@ -381,7 +393,7 @@ def plan(nqb: int, flip, phase, phi, max_span: int = 5, max_rots: int = 0,
         raise ValueError("phase2_plan failed")
     out_p = [{"span": p.span, "nrot": p.nrot, "rot_off": p.rot_off,
               "piv": list(p.piv)[:p.span], "basis": list(p.basis)[:p.span],
-              "scale": p.scale}
+              "scale": p.scale, "form": p.form}
              for p in passes[:np_]]
     out_r = [{"z": r.z, "c": r.c, "s": r.s, "smask": r.smask, "U": r.U,
               "odd": r.odd, "form": r.form} for r in recs[:n]]

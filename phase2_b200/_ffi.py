@@ -144,7 +144,8 @@ MAX_SPAN = 5
 class Pass(C.Structure):
     _fields_ = [("span", C.c_uint32), ("nrot", C.c_uint32),
                 ("rot_off", C.c_uint32), ("piv", C.c_uint8 * MAX_SPAN),
-                ("pad", C.c_uint8 * 3), ("basis", C.c_uint64 * MAX_SPAN),
+                ("form", C.c_uint8), ("pad", C.c_uint8 * 2),
+                ("basis", C.c_uint64 * MAX_SPAN),
                 ("scale", C.c_double)]
 
 
@@ -264,6 +265,8 @@ _SIGS = {
                              _P(C.c_double)]),
     "phase2_set_precision": (C.c_int, [C.c_int]),
     "phase2_get_precision": (C.c_int, []),
+    "phase2_set_fp32_form": (C.c_int, [C.c_int]),
+    "phase2_get_fp32_form": (C.c_int, []),
     "phase2_set_fusion": (C.c_int, [C.c_int, C.c_int]),
     "phase2_set_term_order": (C.c_int, [C.c_int]),
     "phase2_get_term_order": (C.c_int, []),

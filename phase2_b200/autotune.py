@@ -1,9 +1,10 @@
 """Autotuner for the pass kernel launch table and the fusion cap.
 
 For each state precision and span M (amplitudes per thread = 2^M) it times
-passes of both kernel variants (direct loads / shared-memory prefetch) and
-several grid densities on probe rotations whose flip masks span exactly M
-dimensions, then keeps the fastest.  It then compares fusion caps
+passes of the kernel variants (FP64: direct loads / shared-memory prefetch;
+FP32: the lifted kernel of the current FP32 form) at several grid densities
+on probe rotations whose flip masks span exactly M dimensions, then keeps
+the fastest.  It then compares fusion caps
 (max_span 4 vs 5) on a stream of qDRIFT-like draws, by rotations per second.
 
 Results are written as JSON (``save``) and applied to the running library
@@ -26,7 +27,9 @@ from . import PREC_FP32, PREC_FP64, Register, lib, world_ensure
 
 DEFAULT_FILE = Path(__file__).resolve().parent / "tuning_b200.json"
 PRECS = {"fp64": PREC_FP64, "fp32": PREC_FP32}
-GRIDS = {0: [0, 4, 8, 32], 1: [0, 1]}  # variant -> per_sm candidates
+# per precision: variant -> per_sm candidates
+GRIDS = {"fp64": {0: [0, 4, 8, 32], 1: [0, 1]},
+         "fp32": {0: [0, 8, 16, 32]}}
 
 
 def _probe_rotations(nqb: int, M: int, groups: int, seed: int):
@@ -71,7 +74,7 @@ def sweep_launch(nqb: int, groups: int = 12, reps: int = 2) -> dict:
                 flip, phase, phi = _probe_rotations(nqb, M, groups, 7 + M)
                 best = None
                 trials = []
-                for variant, grids in GRIDS.items():
+                for variant, grids in GRIDS[pname].items():
                     for per_sm in grids:
                         L.phase2_tune_set(prec, M, variant, per_sm)
                         _time_passes(reg, flip[:M + 1], phase[:M + 1],

@@ -4,22 +4,24 @@
  * The state vector is one flat array of 2^n complex amplitudes in HBM,
  * complex128 (double2) or complex64 (float2), updated in place.
  *
- * Hot kernel: k_pass<M, Storage, EXACT>.  One launch = one HBM sweep that
- * applies a planned run of rotations (plan.c).  Each thread owns whole
- * cosets x + span(basis[0..M-1]): it loads the 2^M amplitudes of a coset
- * into FP64 registers, applies every rotation of the run in order (partners
- * of a rotation are always inside the coset), and writes them back.  Warp
+ * Hot kernels: k_pass<M> (FP64 state), k_pass_lift32<M> and k_pass_lift<M>
+ * (FP32 state).  One launch = one HBM sweep that applies a planned run of
+ * rotations (plan.c).  Each thread owns whole cosets
+ * x + span(basis[0..M-1]): it loads the 2^M amplitudes of a coset into
+ * registers, applies every rotation of the run in order (partners of a
+ * rotation are always inside the coset), and writes them back.  Warp
  * lanes take consecutive representatives x, so for each slot the warp
  * touches one contiguous 256 B (FP32) or 512 B (FP64) segment: coalesced,
  * one read and one write of every amplitude per pass, no shared-memory
  * staging of amplitudes.  It is a streaming pair sweep on CUDA cores; there
  * is no contraction for the tensor cores to do.
  *
- * EXACT (FP64 storage): products and sums are rounded separately with
+ * FP64 state: products and sums are rounded separately with
  * __dmul_rn/__dadd_rn, never fused, so every amplitude is bit-identical to
  * the reference CPU update a_i <- c a_i + i conj(s z) a_j
- * (phase2/qreg_qreg.c:149-160).  FP32 storage computes in FP64 with FMA and
- * rounds to FP32 once per pass.
+ * (phase2/qreg_qreg.c:149-160).  FP32 state: each pair is rotated by three
+ * in-place shears (the lifted form), in FP32 FMAs (k_pass_lift32, the
+ * default) or in FP64 with one rounding to FP32 per pass (k_pass_lift).
  *
  * Other kernels: gather/scatter of a few amplitudes (overlap, state prep),
  * and a two-stage FP64 sum of squares / inner product (warp-shuffle tree
@@ -31,8 +33,6 @@
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
-
-#include <type_traits>
 
 #define LOG_SUBSYS "engine"
 #include "log.h"
@@ -107,23 +107,17 @@ struct p2_dev {
 
 /* ---- arithmetic --------------------------------------------------------- */
 
-template <bool EXACT>
+/* Products and sums rounded separately (no FMA contraction), as the
+ * reference's CPU build computes them. */
 __device__ __forceinline__ double p2_mul(double a, double b)
 {
-	if constexpr (EXACT)
-		return __dmul_rn(a, b);
-	else
-		return a * b;
+	return __dmul_rn(a, b);
 }
 
-/* c*x + t: two roundings (EXACT) or one (FMA). */
-template <bool EXACT>
+/* c*x + t with two roundings. */
 __device__ __forceinline__ double p2_cxt(double c, double x, double t)
 {
-	if constexpr (EXACT)
-		return __dadd_rn(__dmul_rn(c, x), t);
-	else
-		return fma(c, x, t);
+	return __dadd_rn(__dmul_rn(c, x), t);
 }
 
 __host__ __device__ constexpr int p2_hibit(int v)
@@ -157,7 +151,7 @@ __device__ __forceinline__ double p2_sgn(double v, uint32_t mask)
  * in); each slot's sign is extracted independently so the per-slot work
  * has no serial dependency.
  */
-template <int M, int U, int ODD, bool EXACT>
+template <int M, int U, int ODD>
 __device__ __forceinline__ void p2_rot(double (&re)[1 << M],
 	double (&im)[1 << M], double c, double s, uint32_t sm, uint32_t W)
 {
@@ -168,14 +162,14 @@ __device__ __forceinline__ void p2_rot(double (&re)[1 << M],
 			const double su = p2_sgn(s, p2_bitmask(sm, u));
 			double tr, ti;
 			if constexpr (ODD) {
-				tr = p2_mul<EXACT>(-su, im[u]);
-				ti = p2_mul<EXACT>(su, re[u]);
+				tr = p2_mul(-su, im[u]);
+				ti = p2_mul(su, re[u]);
 			} else {
-				tr = p2_mul<EXACT>(su, re[u]);
-				ti = p2_mul<EXACT>(su, im[u]);
+				tr = p2_mul(su, re[u]);
+				ti = p2_mul(su, im[u]);
 			}
-			re[u] = p2_cxt<EXACT>(c, re[u], tr);
-			im[u] = p2_cxt<EXACT>(c, im[u], ti);
+			re[u] = p2_cxt(c, re[u], tr);
+			im[u] = p2_cxt(c, im[u], ti);
 		}
 	} else {
 		constexpr int H = p2_hibit(U);
@@ -187,20 +181,20 @@ __device__ __forceinline__ void p2_rot(double (&re)[1 << M],
 			const double sw = p2_sgn(s, p2_bitmask(sm, w));
 			double tur, tui, twr, twi;
 			if constexpr (ODD) {
-				tur = p2_mul<EXACT>(-su, im[w]);
-				tui = p2_mul<EXACT>(su, re[w]);
-				twr = p2_mul<EXACT>(-sw, im[u]);
-				twi = p2_mul<EXACT>(sw, re[u]);
+				tur = p2_mul(-su, im[w]);
+				tui = p2_mul(su, re[w]);
+				twr = p2_mul(-sw, im[u]);
+				twi = p2_mul(sw, re[u]);
 			} else {
-				tur = p2_mul<EXACT>(su, re[w]);
-				tui = p2_mul<EXACT>(su, im[w]);
-				twr = p2_mul<EXACT>(sw, re[u]);
-				twi = p2_mul<EXACT>(sw, im[u]);
+				tur = p2_mul(su, re[w]);
+				tui = p2_mul(su, im[w]);
+				twr = p2_mul(sw, re[u]);
+				twi = p2_mul(sw, im[u]);
 			}
-			const double nur = p2_cxt<EXACT>(c, re[u], tur);
-			const double nui = p2_cxt<EXACT>(c, im[u], tui);
-			const double nwr = p2_cxt<EXACT>(c, re[w], twr);
-			const double nwi = p2_cxt<EXACT>(c, im[w], twi);
+			const double nur = p2_cxt(c, re[u], tur);
+			const double nui = p2_cxt(c, im[u], tui);
+			const double nwr = p2_cxt(c, re[w], twr);
+			const double nwi = p2_cxt(c, im[w], twi);
 			re[u] = nur;
 			im[u] = nui;
 			re[w] = nwr;
@@ -208,104 +202,15 @@ __device__ __forceinline__ void p2_rot(double (&re)[1 << M],
 		}
 	}
 }
-
-/*
- * Scaled rotation (FP32 storage).  All amplitudes carry a common pending
- * factor, applied once per pass at the store, so one FMA per component:
- *   COT = 0:  y_u <- y_u + (+-r) p_u          (r = s/c, factor c)
- *   COT = 1:  y_u <- r y_u + (+-1) p_u        (r = c/s, factor s)
- * p_u = y_{u^U}, times i when ODD; the sign is bit u of sm.
- */
-template <int M, int U, int ODD, int COT>
-__device__ __forceinline__ void p2_rot_scaled(double (&re)[1 << M],
-	double (&im)[1 << M], double r, uint32_t sm, uint32_t W)
-{
-	(void)W;
-	if constexpr (U == 0) {
-#pragma unroll
-		for (int u = 0; u < (1 << M); ++u) {
-			const uint32_t sg = p2_bitmask(sm, u);
-			const double pr = ODD ? -im[u] : re[u];
-			const double pi = ODD ? re[u] : im[u];
-			if constexpr (!COT) {
-				const double ru = p2_sgn(r, sg);
-				re[u] = fma(ru, pr, re[u]);
-				im[u] = fma(ru, pi, im[u]);
-			} else {
-				re[u] = fma(r, re[u], p2_sgn(pr, sg));
-				im[u] = fma(r, im[u], p2_sgn(pi, sg));
-			}
-		}
-	} else {
-		constexpr int H = p2_hibit(U);
-#pragma unroll
-		for (int k = 0; k < (1 << (M - 1)); ++k) {
-			const int u = p2_ins0(k, H);
-			const int w = u ^ U;
-			const uint32_t sg = p2_bitmask(sm, u);
-			const uint32_t sw = p2_bitmask(sm, w);
-			const double pur = ODD ? -im[w] : re[w];
-			const double pui = ODD ? re[w] : im[w];
-			const double pwr = ODD ? -im[u] : re[u];
-			const double pwi = ODD ? re[u] : im[u];
-			double nur, nui, nwr, nwi;
-			if constexpr (!COT) {
-				const double ru = p2_sgn(r, sg), rw = p2_sgn(r, sw);
-				nur = fma(ru, pur, re[u]);
-				nui = fma(ru, pui, im[u]);
-				nwr = fma(rw, pwr, re[w]);
-				nwi = fma(rw, pwi, im[w]);
-			} else {
-				nur = fma(r, re[u], p2_sgn(pur, sg));
-				nui = fma(r, im[u], p2_sgn(pui, sg));
-				nwr = fma(r, re[w], p2_sgn(pwr, sw));
-				nwi = fma(r, im[w], p2_sgn(pwi, sw));
-			}
-			re[u] = nur;
-			im[u] = nui;
-			re[w] = nwr;
-			im[w] = nwi;
-		}
-	}
-}
-
-#define P2_CASE_S(K)                                                           \
-	case K:                                                                \
-		if constexpr ((K) < (4 << M))                                  \
-			p2_rot_scaled<M, ((K) >> 2), (((K) >> 1) & 1),         \
-				((K)&1)>(re, im, r, sm, W);                    \
-		break;
-#define P2_CASE_S8(B)                                                          \
-	P2_CASE_S(B + 0) P2_CASE_S(B + 1) P2_CASE_S(B + 2) P2_CASE_S(B + 3)    \
-	P2_CASE_S(B + 4) P2_CASE_S(B + 5) P2_CASE_S(B + 6) P2_CASE_S(B + 7)
-
-/* key = U << 2 | odd << 1 | cot */
-template <int M>
-__device__ __forceinline__ void p2_apply_scaled(uint32_t key,
-	double (&re)[1 << M], double (&im)[1 << M], double r, uint32_t sm,
-	uint32_t W)
-{
-	switch (key) {
-		P2_CASE_S8(0) P2_CASE_S8(8) P2_CASE_S8(16) P2_CASE_S8(24)
-		P2_CASE_S8(32) P2_CASE_S8(40) P2_CASE_S8(48) P2_CASE_S8(56)
-		P2_CASE_S8(64) P2_CASE_S8(72) P2_CASE_S8(80) P2_CASE_S8(88)
-		P2_CASE_S8(96) P2_CASE_S8(104) P2_CASE_S8(112) P2_CASE_S8(120)
-	default:
-		break;
-	}
-}
-#undef P2_CASE_S8
-#undef P2_CASE_S
 
 #define P2_CASE(K)                                                             \
 	case K:                                                                \
 		if constexpr ((K) < (2 << M))                                  \
-			p2_rot<M, ((K) >> 1), ((K)&1), EXACT>(re, im, c, s,    \
-				sm, W);                                        \
+			p2_rot<M, ((K) >> 1), ((K)&1)>(re, im, c, s, sm, W);   \
 		break;
 
 /* key = U << 1 | odd; a jump table over the (U, odd) variants. */
-template <int M, bool EXACT>
+template <int M>
 __device__ __forceinline__ void p2_apply(uint32_t key, double (&re)[1 << M],
 	double (&im)[1 << M], double c, double s, uint32_t sm, uint32_t W)
 {
@@ -372,11 +277,11 @@ __device__ __forceinline__ uint64_t p2_slot_off(int u, const uint64_t *basis)
 
 /* ---- the pass kernel ---------------------------------------------------- */
 
-/* Threads per block: 128, except FP64 with 32 slots per thread (64 keeps
- * three blocks of two prefetch stages within shared memory). */
-__host__ __device__ constexpr int p2_tpb(int m, int elem_bytes)
+/* Threads per block of the FP64 prefetch kernel: 128, or 64 with 32 slots
+ * per thread (three blocks of two stages then fit in shared memory). */
+__host__ __device__ constexpr int p2_tpb(int m)
 {
-	return (m >= 5 && elem_bytes == 16) ? 64 : P2_TPB;
+	return m >= 5 ? 64 : P2_TPB;
 }
 
 /* Resident blocks per SM the register allocation should allow: 2^M FP64
@@ -401,14 +306,6 @@ __device__ __forceinline__ uint64_t p2_rep(uint64_t t,
 }
 
 /* Asynchronous global -> shared copy of one amplitude. */
-__device__ __forceinline__ void p2_cp_async(float2 *smem, const float2 *g)
-{
-	const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-	asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s),
-		"l"(g)
-		: "memory");
-}
-
 __device__ __forceinline__ void p2_cp_async(double2 *smem, const double2 *g)
 {
 	const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -427,43 +324,25 @@ template <int N> __device__ __forceinline__ void p2_cp_wait()
 	asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-/* The run of rotations of one pass on one coset held in registers, then
- * the pass-wide factor of the scaled forms. */
-template <int M, bool EXACT>
+/* The run of rotations of one pass on one coset held in registers. */
+template <int M>
 __device__ __forceinline__ void p2_apply_run(double (&re)[1 << M],
 	double (&im)[1 << M], uint64_t x, const struct phase2_rot_rec *srec,
-	uint32_t nrot, double scale)
+	uint32_t nrot)
 {
 	for (uint32_t r = 0; r < nrot; ++r) {
 		const uint64_t z = srec[r].z;
 		const uint32_t px = (uint32_t)(__popcll(x & z) & 1);
 		const uint32_t sm = srec[r].smask ^ (0u - px);
-		if constexpr (EXACT) {
-			const uint32_t key =
-				((uint32_t)srec[r].U << 1) | srec[r].odd;
-			p2_apply<M, EXACT>(key, re, im, srec[r].c, srec[r].s,
-				sm, srec[r].W);
-		} else {
-			const uint32_t key = ((uint32_t)srec[r].U << 2) |
-				((uint32_t)srec[r].odd << 1) |
-				(srec[r].form == 2 ? 1u : 0u);
-			p2_apply_scaled<M>(key, re, im, srec[r].c, sm,
-				srec[r].W);
-		}
-	}
-	if constexpr (!EXACT) {
-#pragma unroll
-		for (int u = 0; u < (1 << M); ++u) {
-			re[u] *= scale;
-			im[u] *= scale;
-		}
+		const uint32_t key = ((uint32_t)srec[r].U << 1) | srec[r].odd;
+		p2_apply<M>(key, re, im, srec[r].c, srec[r].s, sm, srec[r].W);
 	}
 }
 
 /* Stage layout [slot][thread]: a warp's accesses to one slot are 32
  * consecutive elements, conflict-free. */
-template <int M, typename ST>
-__device__ __forceinline__ void p2_prefetch(ST *stage, const ST *st,
+template <int M>
+__device__ __forceinline__ void p2_prefetch(double2 *stage, const double2 *st,
 	uint64_t x, const uint64_t (&pb)[M > 0 ? M : 1])
 {
 #pragma unroll
@@ -483,13 +362,13 @@ __device__ __forceinline__ void p2_prefetch(ST *stage, const ST *st,
  * issued after the values read from it have been consumed (in-order issue),
  * so the stage is never overwritten early.
  */
-template <int M, typename ST, bool EXACT>
-__global__ void __launch_bounds__(p2_tpb(M, sizeof(ST)), p2_min_blocks(M))
-	k_pass_pf(ST *__restrict__ st, uint64_t nrep, struct phase2_pass p,
+template <int M>
+__global__ void __launch_bounds__(p2_tpb(M), p2_min_blocks(M))
+	k_pass_pf(double2 *__restrict__ st, uint64_t nrep, struct phase2_pass p,
 		const struct phase2_rot_rec *__restrict__ recs)
 {
 	extern __shared__ __align__(16) unsigned char p2_dyn[];
-	ST *const stage = (ST *)p2_dyn;
+	double2 *const stage = (double2 *)p2_dyn;
 	__shared__ struct phase2_rot_rec srec[P2_MAX_ROTS_PER_PASS];
 	__shared__ uint64_t sbasis[PHASE2_MAX_SPAN];
 	for (uint32_t r = threadIdx.x; r < p.nrot; r += blockDim.x)
@@ -522,15 +401,15 @@ __global__ void __launch_bounds__(p2_tpb(M, sizeof(ST)), p2_min_blocks(M))
 
 		const uint64_t x = p2_rep<M>(t, p);
 		double re[1 << M], im[1 << M];
-		const ST *const mine = stage + cur * nst + threadIdx.x;
+		const double2 *const mine = stage + cur * nst + threadIdx.x;
 #pragma unroll
 		for (int u = 0; u < (1 << M); ++u) {
-			const ST v = mine[u * blockDim.x];
-			re[u] = (double)v.x;
-			im[u] = (double)v.y;
+			const double2 v = mine[u * blockDim.x];
+			re[u] = v.x;
+			im[u] = v.y;
 		}
 
-		p2_apply_run<M, EXACT>(re, im, x, srec, p.nrot, p.scale);
+		p2_apply_run<M>(re, im, x, srec, p.nrot);
 		/* Slot addresses are recomputed from the shared copy of the
 		 * basis rather than kept live across the rotations. */
 #pragma unroll
@@ -547,10 +426,9 @@ __global__ void __launch_bounds__(p2_tpb(M, sizeof(ST)), p2_min_blocks(M))
  * stores; latency is hidden by the other resident warps only.  The grid
  * covers every representative once (no persistent loop state).
  */
-template <int M, typename ST, bool EXACT>
-__global__ void __launch_bounds__(P2_TPB,
-	(M >= 5 && sizeof(ST) == 8) ? 3 : p2_min_blocks(M))
-	k_pass(ST *__restrict__ st, uint64_t nrep, struct phase2_pass p,
+template <int M>
+__global__ void __launch_bounds__(P2_TPB, p2_min_blocks(M))
+	k_pass(double2 *__restrict__ st, uint64_t nrep, struct phase2_pass p,
 		const struct phase2_rot_rec *__restrict__ recs)
 {
 	__shared__ struct phase2_rot_rec srec[P2_MAX_ROTS_PER_PASS];
@@ -576,168 +454,409 @@ __global__ void __launch_bounds__(P2_TPB,
 #pragma unroll
 		for (int u = 0; u < (1 << M); ++u)
 			p2_ld(st, x ^ p2_slot_off<M>(u, pb), re[u], im[u]);
-		p2_apply_run<M, EXACT>(re, im, x, srec, p.nrot, p.scale);
+		p2_apply_run<M>(re, im, x, srec, p.nrot);
 #pragma unroll
 		for (int u = 0; u < (1 << M); ++u)
 			p2_st(st, x ^ p2_slot_off<M>(u, sbasis), re[u], im[u]);
 	}
 }
 
-/* ---- split pass kernel (FP32 storage) ----------------------------------- */
-
-/* y <- y + (+-r) p  or  y <- r y + (+-1) p, p = partner (times i if ODD) */
-template <int ODD, int COT>
-__device__ __forceinline__ void p2_split_upd(double &yr, double &yi,
-	double qr, double qi, double r, uint32_t sg)
-{
-	const double pr = ODD ? -qi : qr;
-	const double pi = ODD ? qr : qi;
-	if constexpr (!COT) {
-		const double rv = p2_sgn(r, sg);
-		yr = fma(rv, pr, yr);
-		yi = fma(rv, pi, yi);
-	} else {
-		yr = fma(r, yr, p2_sgn(pr, sg));
-		yi = fma(r, yi, p2_sgn(pi, sg));
-	}
-}
+/* ---- lifted pass kernel (FP32 storage) ---------------------------------- */
 
 /*
- * Scaled rotation on a coset shared by two adjacent lanes: this lane holds
- * the 2^(M-1) slots whose top slot bit equals its lane parity (`half`);
- * slot u = v | half << (M-1).  A rotation whose partner stays in the lane
- * (top bit of U clear) is the ordinary pair update on the local slots;
- * otherwise every local slot's partner is fetched from the other lane with
- * one shuffle per component and each lane updates only its own slots.
- * sm holds this lane's signs (bit v = sign of local slot v).
+ * One lifted rotation on the 2^M slots of a coset.  A pair (u, w = u ^ U)
+ * with sign sigma (bit u of sm) is rotated by three in-place shears,
+ *   y_u += t q_u y_w;  y_w += s q_w y_u;  y_u += t q_u y_w,
+ * q_u = sigma (odd ? i : 1), q_w = -conj(q_u), t = tan(phi/2): every update
+ * writes the register it reads, so a case needs no temporaries and leaves
+ * no moves behind.  The partner is held as sigma * y_w during the shears
+ * (its sign bits flipped in place), which makes all six FMAs sign-free.
+ * U = 0 (the string is diagonal on the coset, and then odd = 1) is the
+ * phase c + i sigma s, applied to (re, sigma im) by the same three shears.
  */
-template <int M, int U, int ODD, int COT>
-__device__ __forceinline__ void p2_rot_split(double (&re)[1 << (M - 1)],
-	double (&im)[1 << (M - 1)], double r, uint32_t sm, unsigned mask)
+template <int M, int U, int ODD>
+__device__ __forceinline__ void p2_rot_lift(double (&re)[1 << M],
+	double (&im)[1 << M], double t, double s, uint32_t sm)
 {
-	constexpr int MH = M - 1;
-	constexpr int TOP = 1 << MH;
-	if constexpr ((U & TOP) == 0) {
-		p2_rot_scaled<MH, U, ODD, COT>(re, im, r, sm, 0u);
-	} else {
-		/* Local slots v and v ^ UL exchange with the other lane's
-		 * v ^ UL and v: fetch both before either is overwritten. */
-		constexpr int UL = U & (TOP - 1);
+	if constexpr (U == 0) {
 #pragma unroll
-		for (int v = 0; v < (1 << MH); ++v) {
-			const int v2 = v ^ UL;
-			if (v2 < v)
-				continue;
-			const double ar = __shfl_xor_sync(mask, re[v2], 1);
-			const double ai = __shfl_xor_sync(mask, im[v2], 1);
-			double br = 0.0, bi = 0.0;
-			if (v2 != v) {
-				br = __shfl_xor_sync(mask, re[v], 1);
-				bi = __shfl_xor_sync(mask, im[v], 1);
+		for (int u = 0; u < (1 << M); ++u) {
+			const uint32_t g = p2_bitmask(sm, u);
+			if constexpr (ODD) {
+				double v = p2_sgn(im[u], g);
+				re[u] = fma(-t, v, re[u]);
+				v = fma(s, re[u], v);
+				re[u] = fma(-t, v, re[u]);
+				im[u] = p2_sgn(v, g);
+			} else {
+				/* (c +- s) y with c = 1 - t s; a Hermitian string
+				 * that is diagonal on the coset never has it */
+				const double k = p2_sgn(s, g) + fma(-t, s, 1.0);
+				re[u] *= k;
+				im[u] *= k;
 			}
-			p2_split_upd<ODD, COT>(re[v], im[v], ar, ai, r,
-				p2_bitmask(sm, v));
-			if (v2 != v)
-				p2_split_upd<ODD, COT>(re[v2], im[v2], br, bi, r,
-					p2_bitmask(sm, v2));
+		}
+	} else {
+		constexpr int H = p2_hibit(U);
+#pragma unroll
+		for (int k = 0; k < (1 << (M - 1)); ++k) {
+			const int u = p2_ins0(k, H);
+			const int w = u ^ U;
+			const uint32_t g = p2_bitmask(sm, u);
+			double wr = p2_sgn(re[w], g), wi = p2_sgn(im[w], g);
+			if constexpr (ODD) {
+				re[u] = fma(-t, wi, re[u]);
+				im[u] = fma(t, wr, im[u]);
+				wr = fma(-s, im[u], wr);
+				wi = fma(s, re[u], wi);
+				re[u] = fma(-t, wi, re[u]);
+				im[u] = fma(t, wr, im[u]);
+			} else {
+				re[u] = fma(t, wr, re[u]);
+				im[u] = fma(t, wi, im[u]);
+				wr = fma(-s, re[u], wr);
+				wi = fma(-s, im[u], wi);
+				re[u] = fma(t, wr, re[u]);
+				im[u] = fma(t, wi, im[u]);
+			}
+			re[w] = p2_sgn(wr, g);
+			im[w] = p2_sgn(wi, g);
 		}
 	}
 }
 
-#define P2_CASE_P(K)                                                           \
+#define P2_CASE_L(K)                                                           \
 	case K:                                                                \
-		if constexpr ((K) < (4 << M))                                  \
-			p2_rot_split<M, ((K) >> 2), (((K) >> 1) & 1),          \
-				((K)&1)>(re, im, r, sm, mask);                 \
+		if constexpr ((K) < (2 << M))                                  \
+			p2_rot_lift<M, ((K) >> 1), ((K)&1)>(re, im, t, s, sm); \
 		break;
-#define P2_CASE_P8(B)                                                          \
-	P2_CASE_P(B + 0) P2_CASE_P(B + 1) P2_CASE_P(B + 2) P2_CASE_P(B + 3)    \
-	P2_CASE_P(B + 4) P2_CASE_P(B + 5) P2_CASE_P(B + 6) P2_CASE_P(B + 7)
 
+/* key = U << 1 | odd */
 template <int M>
-__device__ __forceinline__ void p2_apply_split(uint32_t key,
-	double (&re)[1 << (M - 1)], double (&im)[1 << (M - 1)], double r,
-	uint32_t sm, unsigned mask)
+__device__ __forceinline__ void p2_apply_lift(uint32_t key,
+	double (&re)[1 << M], double (&im)[1 << M], double t, double s,
+	uint32_t sm)
 {
 	switch (key) {
-		P2_CASE_P8(0) P2_CASE_P8(8) P2_CASE_P8(16) P2_CASE_P8(24)
-		P2_CASE_P8(32) P2_CASE_P8(40) P2_CASE_P8(48) P2_CASE_P8(56)
-		P2_CASE_P8(64) P2_CASE_P8(72) P2_CASE_P8(80) P2_CASE_P8(88)
-		P2_CASE_P8(96) P2_CASE_P8(104) P2_CASE_P8(112) P2_CASE_P8(120)
+		P2_CASE_L(0) P2_CASE_L(1) P2_CASE_L(2) P2_CASE_L(3)
+		P2_CASE_L(4) P2_CASE_L(5) P2_CASE_L(6) P2_CASE_L(7)
+		P2_CASE_L(8) P2_CASE_L(9) P2_CASE_L(10) P2_CASE_L(11)
+		P2_CASE_L(12) P2_CASE_L(13) P2_CASE_L(14) P2_CASE_L(15)
+		P2_CASE_L(16) P2_CASE_L(17) P2_CASE_L(18) P2_CASE_L(19)
+		P2_CASE_L(20) P2_CASE_L(21) P2_CASE_L(22) P2_CASE_L(23)
+		P2_CASE_L(24) P2_CASE_L(25) P2_CASE_L(26) P2_CASE_L(27)
+		P2_CASE_L(28) P2_CASE_L(29) P2_CASE_L(30) P2_CASE_L(31)
+		P2_CASE_L(32) P2_CASE_L(33) P2_CASE_L(34) P2_CASE_L(35)
+		P2_CASE_L(36) P2_CASE_L(37) P2_CASE_L(38) P2_CASE_L(39)
+		P2_CASE_L(40) P2_CASE_L(41) P2_CASE_L(42) P2_CASE_L(43)
+		P2_CASE_L(44) P2_CASE_L(45) P2_CASE_L(46) P2_CASE_L(47)
+		P2_CASE_L(48) P2_CASE_L(49) P2_CASE_L(50) P2_CASE_L(51)
+		P2_CASE_L(52) P2_CASE_L(53) P2_CASE_L(54) P2_CASE_L(55)
+		P2_CASE_L(56) P2_CASE_L(57) P2_CASE_L(58) P2_CASE_L(59)
+		P2_CASE_L(60) P2_CASE_L(61) P2_CASE_L(62) P2_CASE_L(63)
 	default:
 		break;
 	}
 }
-#undef P2_CASE_P8
-#undef P2_CASE_P
+#undef P2_CASE_L
+
+/* A lifted record as the kernel reads it from shared memory. */
+struct p2_lift_rec {
+	double t, s;
+	uint64_t z;
+	uint32_t sm;  /* smask */
+	uint32_t key; /* U << 1 | odd */
+};
+
+__device__ __forceinline__ uint32_t p2_parity(uint32_t v)
+{
+	return (uint32_t)__popc(v) & 1u;
+}
+
+__device__ __forceinline__ uint32_t p2_parity(uint64_t v)
+{
+	return (uint32_t)__popcll(v) & 1u;
+}
+
+/* x, with its value hidden from the optimiser: store addresses recomputed
+ * from it are not merged with the load addresses, which would otherwise
+ * stay live (2^M 64-bit pointers) across the whole run of rotations. */
+__device__ __forceinline__ uint32_t p2_opaque(uint32_t x)
+{
+	asm volatile("" : "+r"(x));
+	return x;
+}
+
+__device__ __forceinline__ uint64_t p2_opaque(uint64_t x)
+{
+	asm volatile("" : "+l"(x));
+	return x;
+}
+
+/* Representative number t -> index x in index type IT (32-bit when the
+ * register has at most 31 qubits, so that no shift reaches 32). */
+template <int M, typename IT>
+__device__ __forceinline__ IT p2_rep_t(IT t, const struct phase2_pass &p)
+{
+	IT x = t;
+#pragma unroll
+	for (int k = 0; k < M; ++k) {
+		const uint32_t q = p.piv[k];
+		x = ((x >> q) << (q + 1)) | (x & (((IT)1 << q) - 1));
+	}
+	return x;
+}
 
 /*
- * One FP32 pass with each coset shared by a lane pair (variant 2): half
- * the registers per thread of k_pass, so twice the resident warps to hide
- * load and arithmetic latency.  Both lanes of a pair always have the same
- * representative, so they enter and leave the loop together and every
- * shuffle pairs two active lanes.
+ * One FP32 pass in the lifted form: each thread loads its coset straight
+ * from HBM (2^M independent 8-byte loads, coalesced across the warp),
+ * widens to FP64, applies the run of rotations in registers and narrows
+ * once at the store.  Index arithmetic is 32-bit when IT is uint32_t.
+ * At M = 5, three resident blocks cap a thread at 168 registers (a few
+ * spilled); measured faster than two blocks with no spills.
  */
-template <int M>
-__global__ void __launch_bounds__(P2_TPB, M >= 5 ? 4 : 6)
-	k_pass_split(float2 *__restrict__ st, uint64_t nrep,
+template <int M, typename IT>
+__global__ void __launch_bounds__(P2_TPB, M >= 5 ? 3 : p2_min_blocks(M))
+	k_pass_lift(float2 *__restrict__ st, uint64_t nrep,
 		struct phase2_pass p,
 		const struct phase2_rot_rec *__restrict__ recs)
 {
-	__shared__ struct phase2_rot_rec srec[P2_MAX_ROTS_PER_PASS];
-	__shared__ uint64_t sbasis[PHASE2_MAX_SPAN];
-	for (uint32_t r = threadIdx.x; r < p.nrot; r += blockDim.x)
-		srec[r] = recs[p.rot_off + r];
-	if (threadIdx.x == 0) {
-#pragma unroll
-		for (int k = 0; k < M; ++k)
-			sbasis[k] = p.basis[k];
+	__shared__ struct p2_lift_rec srec[P2_MAX_ROTS_PER_PASS];
+	for (uint32_t r = threadIdx.x; r < p.nrot; r += blockDim.x) {
+		const struct phase2_rot_rec in = recs[p.rot_off + r];
+		struct p2_lift_rec o;
+		o.t = in.c;
+		o.s = in.s;
+		o.z = in.z;
+		o.sm = in.smask;
+		o.key = ((uint32_t)in.U << 1) | in.odd;
+		srec[r] = o;
 	}
 	__syncthreads();
-	constexpr int MH = M - 1;
-	const uint32_t half = threadIdx.x & 1u;
-	uint64_t pb[MH > 0 ? MH : 1];
+	IT pb[M > 0 ? M : 1];
 #pragma unroll
-	for (int k = 0; k < MH; ++k)
-		pb[k] = p.basis[k];
-	const uint64_t top = half ? p.basis[MH] : 0;
+	for (int k = 0; k < M; ++k)
+		pb[k] = (IT)p.basis[k];
+	const bool neg = p.scale < 0;
+	const uint32_t nrot = p.nrot;
 
-	const uint64_t stride = ((uint64_t)gridDim.x * blockDim.x) >> 1;
-	for (uint64_t t = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 1;
+	const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+	for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
 		t < nrep; t += stride) {
-		const unsigned mask = __activemask();
-		const uint64_t x = p2_rep<M>(t, p) ^ top;
-		double re[1 << MH], im[1 << MH];
+		const IT x = p2_rep_t<M, IT>((IT)t, p);
+		double re[1 << M], im[1 << M];
 #pragma unroll
-		for (int v = 0; v < (1 << MH); ++v)
-			p2_ld(st, x ^ p2_slot_off<MH>(v, pb), re[v], im[v]);
-		for (uint32_t r = 0; r < p.nrot; ++r) {
-			const uint64_t z = srec[r].z;
-			const uint32_t px = (uint32_t)(__popcll(x & z) & 1);
-			/* x includes the top basis vector for the upper lane, so
-			 * px already carries parity(top & z): local sign bits are
-			 * the lower half of smask with that parity folded in */
-			uint32_t sm = srec[r].smask;
-			if (half)
-				sm = (sm >> (1u << MH)) ^
-					(((uint32_t)__popcll(top & z) & 1u) ?
-							0xffffffffu : 0u);
-			sm ^= 0u - px;
-			const uint32_t key = ((uint32_t)srec[r].U << 2) |
-				((uint32_t)srec[r].odd << 1) |
-				(srec[r].form == 2 ? 1u : 0u);
-			p2_apply_split<M>(key, re, im, srec[r].c, sm, mask);
+		for (int u = 0; u < (1 << M); ++u) {
+			IT off = 0;
+#pragma unroll
+			for (int k = 0; k < M; ++k)
+				if (u >> k & 1)
+					off ^= pb[k];
+			const float2 v = st[x ^ off];
+			re[u] = (double)v.x;
+			im[u] = (double)v.y;
 		}
-#pragma unroll
-		for (int v = 0; v < (1 << MH); ++v) {
-			re[v] *= p.scale;
-			im[v] *= p.scale;
+		for (uint32_t r = 0; r < nrot; ++r) {
+			const struct p2_lift_rec q = srec[r];
+			const uint32_t sm = q.sm ^ (0u - p2_parity(x & (IT)q.z));
+			p2_apply_lift<M>(q.key, re, im, q.t, q.s, sm);
 		}
-		const uint64_t xs = p2_rep<M>(t, p) ^
-			(half ? sbasis[MH] : UINT64_C(0));
+		if (neg) {
 #pragma unroll
-		for (int v = 0; v < (1 << MH); ++v)
-			p2_st(st, xs ^ p2_slot_off<MH>(v, sbasis), re[v], im[v]);
+			for (int u = 0; u < (1 << M); ++u) {
+				re[u] = -re[u];
+				im[u] = -im[u];
+			}
+		}
+		const IT xs = p2_opaque(x);
+#pragma unroll
+		for (int u = 0; u < (1 << M); ++u) {
+			IT off = 0;
+#pragma unroll
+			for (int k = 0; k < M; ++k)
+				if (u >> k & 1)
+					off ^= pb[k];
+			st[xs ^ off] = make_float2(__double2float_rn(re[u]),
+				__double2float_rn(im[u]));
+		}
+	}
+}
+
+/* ---- lifted pass kernel, FP32 arithmetic -------------------------------- */
+
+__device__ __forceinline__ float p2_fsgn(float v, uint32_t mask)
+{
+	return __int_as_float(__float_as_int(v) ^ (int)mask);
+}
+
+/*
+ * The lifted rotation of p2_rot_lift with the amplitudes in FP32 registers
+ * and FP32 FMAs.  s reaches the kernel as an FP32 value and t = (1 - cos
+ * phi) / s in FP64 (plan.c); the angle of the three shears is fixed by the
+ * product t s (their trace is 2 (1 - t s)), so rounding t to FP32 leaves a
+ * relative angle error of at most 2^-25.  The signs go onto the
+ * coefficients (one XOR each on a 32-bit register).
+ */
+template <int M, int U, int ODD>
+__device__ __forceinline__ void p2_rot_lift32(float (&re)[1 << M],
+	float (&im)[1 << M], float t, float s, uint32_t sm)
+{
+	if constexpr (U == 0) {
+#pragma unroll
+		for (int u = 0; u < (1 << M); ++u) {
+			const uint32_t g = p2_bitmask(sm, u);
+			const float st = p2_fsgn(t, g), ss = p2_fsgn(s, g);
+			if constexpr (ODD) {
+				re[u] = fmaf(-st, im[u], re[u]);
+				im[u] = fmaf(ss, re[u], im[u]);
+				re[u] = fmaf(-st, im[u], re[u]);
+			} else {
+				/* (c +- s) y with c = 1 - t s; a Hermitian string
+				 * that is diagonal on the coset never has it */
+				const float k = ss + fmaf(-t, s, 1.f);
+				re[u] *= k;
+				im[u] *= k;
+			}
+		}
+	} else {
+		constexpr int H = p2_hibit(U);
+#pragma unroll
+		for (int k = 0; k < (1 << (M - 1)); ++k) {
+			const int u = p2_ins0(k, H);
+			const int w = u ^ U;
+			const uint32_t g = p2_bitmask(sm, u);
+			const float st = p2_fsgn(t, g), ss = p2_fsgn(s, g);
+			if constexpr (ODD) {
+				re[u] = fmaf(-st, im[w], re[u]);
+				im[u] = fmaf(st, re[w], im[u]);
+				re[w] = fmaf(-ss, im[u], re[w]);
+				im[w] = fmaf(ss, re[u], im[w]);
+				re[u] = fmaf(-st, im[w], re[u]);
+				im[u] = fmaf(st, re[w], im[u]);
+			} else {
+				re[u] = fmaf(st, re[w], re[u]);
+				im[u] = fmaf(st, im[w], im[u]);
+				re[w] = fmaf(-ss, re[u], re[w]);
+				im[w] = fmaf(-ss, im[u], im[w]);
+				re[u] = fmaf(st, re[w], re[u]);
+				im[u] = fmaf(st, im[w], im[u]);
+			}
+		}
+	}
+}
+
+/* A lifted record as the FP32 kernel reads it. */
+struct p2_lift32_rec {
+	float t, s;
+	uint64_t z;
+	uint32_t sm;  /* smask */
+	uint32_t key; /* U << 1 | odd */
+};
+
+#define P2_CASE_L32(K)                                                         \
+	case K:                                                                \
+		if constexpr ((K) < (2 << M))                                  \
+			p2_rot_lift32<M, ((K) >> 1), ((K)&1)>(re, im, q.t,     \
+				q.s, sm);                                      \
+		break;
+
+template <int M>
+__device__ __forceinline__ void p2_apply_lift32(const struct p2_lift32_rec &q,
+	float (&re)[1 << M], float (&im)[1 << M], uint32_t sm)
+{
+	switch (q.key) {
+		P2_CASE_L32(0) P2_CASE_L32(1) P2_CASE_L32(2) P2_CASE_L32(3)
+		P2_CASE_L32(4) P2_CASE_L32(5) P2_CASE_L32(6) P2_CASE_L32(7)
+		P2_CASE_L32(8) P2_CASE_L32(9) P2_CASE_L32(10) P2_CASE_L32(11)
+		P2_CASE_L32(12) P2_CASE_L32(13) P2_CASE_L32(14) P2_CASE_L32(15)
+		P2_CASE_L32(16) P2_CASE_L32(17) P2_CASE_L32(18) P2_CASE_L32(19)
+		P2_CASE_L32(20) P2_CASE_L32(21) P2_CASE_L32(22) P2_CASE_L32(23)
+		P2_CASE_L32(24) P2_CASE_L32(25) P2_CASE_L32(26) P2_CASE_L32(27)
+		P2_CASE_L32(28) P2_CASE_L32(29) P2_CASE_L32(30) P2_CASE_L32(31)
+		P2_CASE_L32(32) P2_CASE_L32(33) P2_CASE_L32(34) P2_CASE_L32(35)
+		P2_CASE_L32(36) P2_CASE_L32(37) P2_CASE_L32(38) P2_CASE_L32(39)
+		P2_CASE_L32(40) P2_CASE_L32(41) P2_CASE_L32(42) P2_CASE_L32(43)
+		P2_CASE_L32(44) P2_CASE_L32(45) P2_CASE_L32(46) P2_CASE_L32(47)
+		P2_CASE_L32(48) P2_CASE_L32(49) P2_CASE_L32(50) P2_CASE_L32(51)
+		P2_CASE_L32(52) P2_CASE_L32(53) P2_CASE_L32(54) P2_CASE_L32(55)
+		P2_CASE_L32(56) P2_CASE_L32(57) P2_CASE_L32(58) P2_CASE_L32(59)
+		P2_CASE_L32(60) P2_CASE_L32(61) P2_CASE_L32(62) P2_CASE_L32(63)
+	default:
+		break;
+	}
+}
+#undef P2_CASE_L32
+
+/* Resident blocks per SM the FP32-arithmetic kernel is built for
+ * (2^M FP32 complex values take 2^(M+1) registers per thread). */
+__host__ __device__ constexpr int p2_lift32_blocks(int m)
+{
+	return m >= 5 ? 5 : (m == 4 ? 6 : 8);
+}
+
+/*
+ * One FP32 pass in the lifted form with FP32 arithmetic: loads go straight
+ * into FP32 registers, the run is applied with FP32 FMAs, stores write the
+ * registers back.  Half the registers of k_pass_lift (20 resident warps
+ * per SM at M = 5) and no conversions.
+ */
+template <int M, typename IT>
+__global__ void __launch_bounds__(P2_TPB, p2_lift32_blocks(M))
+	k_pass_lift32(float2 *__restrict__ st, uint64_t nrep,
+		struct phase2_pass p,
+		const struct phase2_rot_rec *__restrict__ recs)
+{
+	__shared__ struct p2_lift32_rec srec[P2_MAX_ROTS_PER_PASS];
+	for (uint32_t r = threadIdx.x; r < p.nrot; r += blockDim.x) {
+		const struct phase2_rot_rec in = recs[p.rot_off + r];
+		struct p2_lift32_rec o;
+		o.t = (float)in.c;
+		o.s = (float)in.s; /* an FP32 value: exact */
+		o.z = in.z;
+		o.sm = in.smask;
+		o.key = ((uint32_t)in.U << 1) | in.odd;
+		srec[r] = o;
+	}
+	__syncthreads();
+	IT pb[M > 0 ? M : 1];
+#pragma unroll
+	for (int k = 0; k < M; ++k)
+		pb[k] = (IT)p.basis[k];
+	const uint32_t negm = p.scale < 0 ? 0x80000000u : 0u;
+	const uint32_t nrot = p.nrot;
+
+	const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+	for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+		t < nrep; t += stride) {
+		const IT x = p2_rep_t<M, IT>((IT)t, p);
+		float re[1 << M], im[1 << M];
+#pragma unroll
+		for (int u = 0; u < (1 << M); ++u) {
+			IT off = 0;
+#pragma unroll
+			for (int k = 0; k < M; ++k)
+				if (u >> k & 1)
+					off ^= pb[k];
+			const float2 v = st[x ^ off];
+			re[u] = v.x;
+			im[u] = v.y;
+		}
+		for (uint32_t r = 0; r < nrot; ++r) {
+			const struct p2_lift32_rec q = srec[r];
+			const uint32_t sm = q.sm ^ (0u - p2_parity(x & (IT)q.z));
+			p2_apply_lift32<M>(q, re, im, sm);
+		}
+		const IT xs = p2_opaque(x);
+#pragma unroll
+		for (int u = 0; u < (1 << M); ++u) {
+			IT off = 0;
+#pragma unroll
+			for (int k = 0; k < M; ++k)
+				if (u >> k & 1)
+					off ^= pb[k];
+			st[xs ^ off] = make_float2(p2_fsgn(re[u], negm),
+				p2_fsgn(im[u], negm));
+		}
 	}
 }
 
@@ -1147,10 +1266,12 @@ extern "C" int p2d_set_state(struct p2_dev *d, const double *in)
 }
 
 /*
- * Launch table: per precision and span, which pass kernel runs (0 direct,
- * 1 shared-memory prefetch) and how many blocks per SM the grid holds
- * (0: the direct kernel's default of 16, the prefetch kernel's occupancy).
- * Set by phase2_tune_set (the autotuner) or left at these defaults.
+ * Launch table: per precision and span, which pass kernel runs and how many
+ * blocks per SM the grid holds.  FP64: variant 0 direct loads, 1 shared-
+ * memory prefetch (per_sm 0: 16 for the direct kernel, the occupancy for
+ * the prefetch kernel).  FP32: the lifted kernels, variant 0 only (per_sm
+ * 0: 16).  Set by phase2_tune_set (the autotuner) or left at these
+ * defaults.
  */
 struct p2_tune_entry {
 	int variant;
@@ -1160,15 +1281,17 @@ static struct p2_tune_entry p2_tune[2][PHASE2_MAX_SPAN + 1] = {
 	/* FP64: direct loads, 32 blocks per SM (measured 93-96 % of HBM
 	 * peak for every span at 28 qubits on B200) */
 	{ { 0, 32 }, { 0, 32 }, { 0, 32 }, { 0, 32 }, { 0, 32 }, { 0, 32 } },
-	/* FP32: prefetch for spans 2-4, direct for 0, 1 and 5 */
-	{ { 0, 32 }, { 0, 32 }, { 1, 0 }, { 1, 0 }, { 1, 0 }, { 0, 32 } },
+	/* FP32: 32 blocks per SM (k_pass_lift32 at span 5: 95 % of HBM peak
+	 * at 28 and 30 qubits, ahead of 16 and 8) */
+	{ { 0, 32 }, { 0, 32 }, { 0, 32 }, { 0, 32 }, { 0, 32 }, { 0, 32 } },
 };
 
 extern "C" int phase2_tune_set(int prec, int span, int variant, int per_sm)
 {
 	if ((prec != PHASE2_PREC_FP64 && prec != PHASE2_PREC_FP32) || span < 0 ||
-		span > PHASE2_MAX_SPAN || variant < 0 || variant > 2 ||
-		per_sm < 0 || per_sm > 64)
+		span > PHASE2_MAX_SPAN || variant < 0 ||
+		variant > (prec == PHASE2_PREC_FP64 ? 1 : 0) || per_sm < 0 ||
+		per_sm > 64)
 		return -1;
 	p2_tune[prec][span].variant = variant;
 	p2_tune[prec][span].per_sm = per_sm;
@@ -1194,39 +1317,31 @@ struct p2_kcfg {
 	int per_sm;
 };
 
-template <int M, typename ST, bool EXACT>
+/* One FP64 pass: direct (variant 0) or prefetch (variant 1) kernel. */
+template <int M>
 static int launch_pass_t(struct p2_dev *d, const struct phase2_pass &p,
 	const struct phase2_rot_rec *recs)
 {
 	const uint64_t nrep = d->namp >> M;
-	const struct p2_tune_entry te = p2_tune[d->prec][M];
-	if constexpr (std::is_same<ST, float2>::value && M >= 2) {
-		if (te.variant == 2) {
-			const unsigned per_sm = te.per_sm ? (unsigned)te.per_sm : 16u;
-			const unsigned grid = grid_for(d, 2 * nrep, P2_TPB, per_sm);
-			k_pass_split<M><<<grid, P2_TPB, 0, d->stream>>>(
-				(float2 *)d->state, nrep, p, recs);
-			return 0;
-		}
-	}
+	const struct p2_tune_entry te = p2_tune[PHASE2_PREC_FP64][M];
+	double2 *const sv = (double2 *)d->state;
 	if (te.variant != 1) {
 		const unsigned per_sm = te.per_sm ? (unsigned)te.per_sm : 16u;
 		const unsigned grid = grid_for(d, nrep, P2_TPB, per_sm);
-		k_pass<M, ST, EXACT><<<grid, P2_TPB, 0, d->stream>>>(
-			(ST *)d->state, nrep, p, recs);
+		k_pass<M><<<grid, P2_TPB, 0, d->stream>>>(sv, nrep, p, recs);
 		return 0;
 	}
 	static struct p2_kcfg cfg;
 	if (!cfg.ready) {
-		cfg.tpb = p2_tpb(M, (int)sizeof(ST));
-		cfg.smem = 2 * ((size_t)1 << M) * cfg.tpb * sizeof(ST);
-		CUDA_OK(cudaFuncSetAttribute(k_pass_pf<M, ST, EXACT>,
+		cfg.tpb = p2_tpb(M);
+		cfg.smem = 2 * ((size_t)1 << M) * cfg.tpb * sizeof(double2);
+		CUDA_OK(cudaFuncSetAttribute(k_pass_pf<M>,
 				cudaFuncAttributeMaxDynamicSharedMemorySize,
 				(int)cfg.smem),
 			"pass kernel shared memory");
 		int per_sm = 0;
 		CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm,
-				k_pass_pf<M, ST, EXACT>, cfg.tpb, cfg.smem),
+				k_pass_pf<M>, cfg.tpb, cfg.smem),
 			"pass kernel occupancy");
 		cfg.per_sm = per_sm > 0 ? per_sm : 1;
 		cfg.ready = 1;
@@ -1235,28 +1350,67 @@ static int launch_pass_t(struct p2_dev *d, const struct phase2_pass &p,
 		? (unsigned)te.per_sm
 		: (unsigned)cfg.per_sm;
 	const unsigned grid = grid_for(d, nrep, (unsigned)cfg.tpb, per_sm);
-	k_pass_pf<M, ST, EXACT><<<grid, cfg.tpb, cfg.smem, d->stream>>>(
-		(ST *)d->state, nrep, p, recs);
+	k_pass_pf<M><<<grid, cfg.tpb, cfg.smem, d->stream>>>(sv, nrep, p, recs);
 	return 0;
 }
 
-template <typename ST, bool EXACT>
+/* One FP32 pass in the lifted form of the pass: FP32 arithmetic
+ * (k_pass_lift32) or FP64 arithmetic (k_pass_lift); 32-bit index
+ * arithmetic up to 31 qubits. */
+template <int M>
+static int launch_lift_t(struct p2_dev *d, const struct phase2_pass &p,
+	const struct phase2_rot_rec *recs)
+{
+	const uint64_t nrep = d->namp >> M;
+	const struct p2_tune_entry te = p2_tune[PHASE2_PREC_FP32][M];
+	const unsigned per_sm = te.per_sm ? (unsigned)te.per_sm : 16u;
+	const unsigned grid = grid_for(d, nrep, P2_TPB, per_sm);
+	float2 *const sv = (float2 *)d->state;
+	const bool narrow = d->nqb <= 31;
+	if (p.form == PHASE2_FORM_LIFTED_F32) {
+		if (narrow)
+			k_pass_lift32<M, uint32_t>
+				<<<grid, P2_TPB, 0, d->stream>>>(sv, nrep, p, recs);
+		else
+			k_pass_lift32<M, uint64_t>
+				<<<grid, P2_TPB, 0, d->stream>>>(sv, nrep, p, recs);
+	} else if (p.form == PHASE2_FORM_LIFTED) {
+		if (narrow)
+			k_pass_lift<M, uint32_t>
+				<<<grid, P2_TPB, 0, d->stream>>>(sv, nrep, p, recs);
+		else
+			k_pass_lift<M, uint64_t>
+				<<<grid, P2_TPB, 0, d->stream>>>(sv, nrep, p, recs);
+	} else {
+		log_error("FP32 pass of form %u unsupported", p.form);
+		return -1;
+	}
+	return 0;
+}
+
 static int launch_pass(struct p2_dev *d, const struct phase2_pass &p,
 	const struct phase2_rot_rec *recs)
 {
+	const bool f64 = d->prec == PHASE2_PREC_FP64;
 	switch (p.span) {
 	case 0:
-		return launch_pass_t<0, ST, EXACT>(d, p, recs);
+		return f64 ? launch_pass_t<0>(d, p, recs)
+			   : launch_lift_t<0>(d, p, recs);
 	case 1:
-		return launch_pass_t<1, ST, EXACT>(d, p, recs);
+		return f64 ? launch_pass_t<1>(d, p, recs)
+			   : launch_lift_t<1>(d, p, recs);
 	case 2:
-		return launch_pass_t<2, ST, EXACT>(d, p, recs);
+		return f64 ? launch_pass_t<2>(d, p, recs)
+			   : launch_lift_t<2>(d, p, recs);
 	case 3:
-		return launch_pass_t<3, ST, EXACT>(d, p, recs);
+		return f64 ? launch_pass_t<3>(d, p, recs)
+			   : launch_lift_t<3>(d, p, recs);
 	case 4:
-		return launch_pass_t<4, ST, EXACT>(d, p, recs);
+		return f64 ? launch_pass_t<4>(d, p, recs)
+			   : launch_lift_t<4>(d, p, recs);
 	case 5:
-		return launch_pass_t<5, ST, EXACT>(d, p, recs);
+		return f64 ? launch_pass_t<5>(d, p, recs)
+			   : launch_lift_t<5>(d, p, recs);
 	default:
 		log_error("pass span %u unsupported", p.span);
 		return -1;
@@ -1302,10 +1456,7 @@ static int launch_all(struct p2_dev *d, const struct phase2_pass *passes,
 	size_t npass, const struct phase2_rot_rec *d_recs)
 {
 	for (size_t i = 0; i < npass; i++) {
-		const int rc = d->prec == PHASE2_PREC_FP64
-			? launch_pass<double2, true>(d, passes[i], d_recs)
-			: launch_pass<float2, false>(d, passes[i], d_recs);
-		if (rc < 0)
+		if (launch_pass(d, passes[i], d_recs) < 0)
 			return -1;
 	}
 	return 0;

@@ -19,6 +19,7 @@ struct p2_settings {
 	int max_span;
 	int max_rots;
 	int order;
+	int fp32_form; /* enum phase2_form used for FP32 registers */
 };
 extern struct p2_settings p2_cfg;
 void p2_settings_from_env(void);

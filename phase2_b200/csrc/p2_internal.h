@@ -23,10 +23,14 @@ extern "C" {
 /* Queued rotations that trigger an automatic flush. */
 #define P2_QUEUE_FLUSH 8192
 
-/* scaled = 1 emits the FP32 forms (struct phase2_rot_rec, forms 1 and 2). */
+/* form: enum phase2_form of every pass (and the records it implies). */
 long p2_plan(uint32_t nqb, const struct phase2_rot_in *rots, size_t n,
-	int max_span, int max_rots, int pad_span, int scaled,
+	int max_span, int max_rots, int pad_span, int form,
 	struct phase2_pass *passes, struct phase2_rot_rec *recs);
+
+/* Pass form for a state precision: exact for FP64, the process's FP32
+ * form (phase2_set_fp32_form) for FP32. */
+int p2_form_for(int prec);
 
 /* ---- device engine ------------------------------------------------------ */
 

@@ -112,10 +112,25 @@ static inline int parity64(uint64_t v)
 	return __builtin_popcountll(v) & 1;
 }
 
+/*
+ * Coefficients of a lifted rotation applied with FP32 arithmetic (c >= 0):
+ * s is rounded to FP32 and t = (1 - c) / fl32(s) is kept in FP64, so the
+ * product t * fl32(s), which fixes the rotation angle (the three shears
+ * have trace 2 (1 - t s)), equals 1 - cos(phi) to FP64 accuracy; the
+ * kernel's rounding of t to FP32 is then the only error in the angle
+ * (relative, at most 2^-25).  1 - c is formed as s^2 / (1 + c).
+ */
+static void lift_f32(double c, double s, double *t_out, double *s_out)
+{
+	const float s32 = (float)s;
+	*s_out = s32;
+	*t_out = s32 == 0.0f ? 0.0 : s * s / (1.0 + c) / (double)s32;
+}
+
 /* Close the open pass: pad the basis with unit vectors (more amplitudes per
  * thread, contiguous along low qubits), fix pivots, fill slot masks. */
 static void builder_close(struct pass_builder *b, uint32_t nqb, int pad_to,
-	int scaled, const struct phase2_rot_in *rots, struct phase2_pass *pass,
+	int form, const struct phase2_rot_in *rots, struct phase2_pass *pass,
 	struct phase2_rot_rec *recs)
 {
 	for (uint32_t q = 0; b->m < pad_to && q < nqb; q++) {
@@ -151,25 +166,30 @@ static void builder_close(struct pass_builder *b, uint32_t nqb, int pad_to,
 		rec->W = (uint8_t)W;
 		rec->odd = (uint8_t)(kbase & 1);
 		rec->form = 0;
-		if (scaled) {
-			/* Every amplitude is multiplied by c in this rotation;
-			 * carry the larger of |c|, |s| as a pass-wide factor and
-			 * keep the ratio, so the kernel needs one FMA per
-			 * component.  |factor| >= 1/sqrt(2), so 256 rotations
-			 * shrink the scale by at most 2^-128. */
-			const double c = rec->c, s = rec->s;
-			if (fabs(c) >= fabs(s)) {
-				rec->form = 1;
-				rec->c = s / c;
-				scale *= c;
+		if (form == PHASE2_FORM_LIFTED ||
+			form == PHASE2_FORM_LIFTED_F32) {
+			/* Three shears per pair (no temporaries, no pass-wide
+			 * factor): t = tan(phi/2) = s / (1 + c), computed with
+			 * c >= 0 so it stays in [-1, 1]; for c < 0 the rotation
+			 * is exp(i(phi -+ pi)P) times -1, and the -1 goes to
+			 * the pass. */
+			double c = rec->c, s = rec->s;
+			if (c < 0) {
+				c = -c;
+				s = -s;
+				scale = -scale;
+			}
+			rec->form = 1;
+			if (form == PHASE2_FORM_LIFTED_F32) {
+				lift_f32(c, s, &rec->c, &rec->s);
 			} else {
-				rec->form = 2;
-				rec->c = c / s;
-				scale *= s;
+				rec->c = s / (1.0 + c);
+				rec->s = s;
 			}
 		}
 	}
 	pass->scale = scale;
+	pass->form = (uint8_t)form;
 }
 
 long phase2_plan(uint32_t nqb, const struct phase2_rot_in *rots, size_t n,
@@ -179,12 +199,12 @@ long phase2_plan(uint32_t nqb, const struct phase2_rot_in *rots, size_t n,
 	if (prec != PHASE2_PREC_FP64 && prec != PHASE2_PREC_FP32)
 		return -1;
 	return p2_plan(nqb, rots, n, max_span, max_rots, P2_DEFAULT_PAD_SPAN,
-		prec == PHASE2_PREC_FP32, passes, recs);
+		p2_form_for(prec), passes, recs);
 }
 
 /* Records are emitted in input order: recs[i] describes rots[i]. */
 long p2_plan(uint32_t nqb, const struct phase2_rot_in *rots, size_t n,
-	int max_span, int max_rots, int pad_span, int scaled,
+	int max_span, int max_rots, int pad_span, int form,
 	struct phase2_pass *passes, struct phase2_rot_rec *recs)
 {
 	if (nqb == 0 || nqb > QREG_MAX_WIDTH)
@@ -221,7 +241,7 @@ long p2_plan(uint32_t nqb, const struct phase2_rot_in *rots, size_t n,
 				fits = 0;
 		}
 		if (!fits) {
-			builder_close(&b, nqb, pad_span, scaled, rots,
+			builder_close(&b, nqb, pad_span, form, rots,
 				&passes[npass], recs);
 			npass++;
 			builder_reset(&b, i);
@@ -240,7 +260,7 @@ long p2_plan(uint32_t nqb, const struct phase2_rot_in *rots, size_t n,
 		b.nrot++;
 	}
 	if (b.nrot > 0) {
-		builder_close(&b, nqb, pad_span, scaled, rots, &passes[npass],
+		builder_close(&b, nqb, pad_span, form, rots, &passes[npass],
 			recs);
 		npass++;
 	}

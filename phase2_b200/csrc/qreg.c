@@ -156,7 +156,7 @@ static int drain_rotations(struct qreg *reg)
 		b->plan_cap = b->qlen;
 	}
 	const long np = p2_plan(reg->qb_lo, b->q, b->qlen, b->max_span,
-		b->max_rots, P2_DEFAULT_PAD_SPAN, b->prec == PHASE2_PREC_FP32,
+		b->max_rots, P2_DEFAULT_PAD_SPAN, p2_form_for(b->prec),
 		b->passes, b->recs);
 	if (np < 0 || p2d_run(b->dev, b->passes, (size_t)np, b->recs,
 			      b->qlen) < 0) {

@@ -17,6 +17,7 @@ struct p2_settings p2_cfg = {
 	.max_span = PHASE2_MAX_SPAN,
 	.max_rots = 0,
 	.order = PHASE2_ORDER_LEX,
+	.fp32_form = PHASE2_FORM_LIFTED_F32,
 };
 
 void p2_settings_from_env(void)
@@ -30,6 +31,33 @@ void p2_settings_from_env(void)
 		else
 			log_warn("PHASE2_PRECISION=%s not understood", p);
 	}
+	const char *f = getenv("PHASE2_FP32_FORM");
+	if (f && *f) {
+		if (!strcmp(f, "lifted"))
+			p2_cfg.fp32_form = PHASE2_FORM_LIFTED;
+		else if (!strcmp(f, "lifted_f32"))
+			p2_cfg.fp32_form = PHASE2_FORM_LIFTED_F32;
+		else
+			log_warn("PHASE2_FP32_FORM=%s not understood", f);
+	}
+}
+
+int phase2_set_fp32_form(int form)
+{
+	if (form != PHASE2_FORM_LIFTED && form != PHASE2_FORM_LIFTED_F32)
+		return -1;
+	p2_cfg.fp32_form = form;
+	return 0;
+}
+
+int phase2_get_fp32_form(void)
+{
+	return p2_cfg.fp32_form;
+}
+
+int p2_form_for(int prec)
+{
+	return prec == PHASE2_PREC_FP32 ? p2_cfg.fp32_form : PHASE2_FORM_EXACT;
 }
 
 int phase2_set_precision(int prec)

@@ -15,6 +15,7 @@ import subprocess
 import numpy as np
 import pytest
 
+import phase2_b200 as p2
 from phase2_b200 import _ffi, plan, workloads
 from phase2_b200._ffi import lib
 
@@ -215,18 +216,35 @@ def test_planner_emulation_bit_exact(n, span, max_rots, oracle_lib):
 
 
 @pytest.mark.parametrize("n", [2, 6, 11])
-def test_planner_scaled_forms(n, oracle_lib):
-    """FP32 plans (scaled forms, pass-wide factor) reproduce the oracle to
-    FP64 rounding when executed in FP64; angles cover both forms."""
+@pytest.mark.parametrize("form", [p2.FORM_LIFTED, p2.FORM_LIFTED_F32])
+def test_planner_fp32_forms(n, form, oracle_lib):
+    """FP32 plans (lifted shears with a pass-wide sign) reproduce the
+    oracle when executed in FP64: to FP64 rounding with FP64 coefficients,
+    and to the rounding of s to FP32 (relative angle error <= 2^-24 per
+    rotation) with the FP32-arithmetic coefficients; angles in [-pi, pi]
+    cover both signs of cos."""
     rng = np.random.Generator(np.random.PCG64(500 + n))
     flip, phase, phi = _rand_rotations(rng, n, 80)
     amp = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
-    passes, recs = plan(n, flip, phase, phi, 5, 0, prec=1)
-    forms = {r["form"] for r in recs}
-    assert forms == {1, 2}
+    old = p2.get_fp32_form()
+    p2.set_fp32_form(form)
+    try:
+        passes, recs = plan(n, flip, phase, phi, 5, 0, prec=1)
+    finally:
+        p2.set_fp32_form(old)
+    assert {r["form"] for r in recs} == {1}
+    assert {p["form"] for p in passes} == {form}
+    assert {p["scale"] for p in passes} <= {1.0, -1.0}
+    assert all(abs(r["c"]) <= 1.0 + 1e-7 for r in recs)
     got = emulate(amp, n, passes, recs)
     want = oracle_lib.rotate(amp, n, flip, phase, phi)
-    assert np.max(np.abs(got - want)) < 1e-12 * np.max(np.abs(want))
+    if form == p2.FORM_LIFTED:
+        tol = 1e-12
+    else:
+        assert all(np.float32(r["s"]) == r["s"] for r in recs)
+        # t * s = 1 - cos(phi) exactly: s rounding only tilts the shears
+        tol = 80 * 2.0 ** -24
+    assert np.max(np.abs(got - want)) < tol * np.max(np.abs(want))
 
 
 def test_planner_fuses_jw_runs():

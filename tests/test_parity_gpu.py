@@ -9,8 +9,9 @@ Tolerances:
   FP64 state  -- bit-identical (np.array_equal) to the oracle; the bar the
                  path is held to is 1e-12 relative per overlap, which
                  bit-identity implies.
-  FP32 state  -- 1e-5 absolute per amplitude / overlap for short runs
-                 (one FP32 rounding per pass, FP64 arithmetic inside).
+  FP32 state  -- 1e-5 absolute per amplitude / overlap for short runs, for
+                 both FP32 forms (FP32 arithmetic: a few FP32 roundings per
+                 rotation; FP64 arithmetic: one FP32 rounding per pass).
 """
 
 import ctypes as C
@@ -45,6 +46,16 @@ def _rand_rots(rng, n, k, diag_frac=0.2):
     return t.flip, t.phase, rng.uniform(-math.pi, math.pi, k)
 
 
+@pytest.fixture(params=[p2.FORM_LIFTED_F32, p2.FORM_LIFTED],
+                ids=["f32arith", "f64arith"])
+def fp32_form(request):
+    """Run an FP32 test under each FP32 arithmetic form."""
+    old = p2.get_fp32_form()
+    p2.set_fp32_form(request.param)
+    yield request.param
+    p2.set_fp32_form(old)
+
+
 @pytest.fixture(scope="module", autouse=True)
 def _world():
     p2.world_ensure()
@@ -56,7 +67,7 @@ def _world():
 # ---- register level ----------------------------------------------------
 
 
-def test_paulirot_golden_fixture():
+def test_paulirot_golden_fixture(fp32_form):
     f = np.load(GOLDEN / "paulirot.npz")
     with Register(9, p2.PREC_FP64) as r:
         r.set_state(f["amp0"])
@@ -83,12 +94,12 @@ def test_random_rotations_bit_exact(n, fusion, oracle_lib):
     assert np.array_equal(got, want)
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2])
+@pytest.mark.parametrize("variant,per_sm", [(0, 0), (1, 0), (0, 4)])
 @pytest.mark.parametrize("n", [5, 11, 17])
-def test_both_kernel_variants(variant, n, oracle_lib):
-    """Direct-load, shared-memory-prefetch and lane-split pass kernels give
-    the same bits (FP64; the split variant is FP32-only and FP64 falls back
-    to direct loads) and the same FP32 results for every span."""
+def test_launch_variants(variant, per_sm, n, fp32_form, oracle_lib):
+    """The direct-load and shared-memory-prefetch FP64 kernels give the
+    same bits for every span, at several grid densities; the FP32 lifted
+    kernels (one variant) stay within tolerance at the same densities."""
     from phase2_b200._ffi import lib
     L = lib()
     saved = []
@@ -97,7 +108,9 @@ def test_both_kernel_variants(variant, n, oracle_lib):
             v, s = C.c_int(), C.c_int()
             L.phase2_tune_get(prec, m, C.byref(v), C.byref(s))
             saved.append((prec, m, v.value, s.value))
-            L.phase2_tune_set(prec, m, variant, 0)
+            assert L.phase2_tune_set(prec, m, variant if prec == 0 else 0,
+                                     per_sm) == 0
+        assert L.phase2_tune_set(1, 5, 1, 0) == -1
     try:
         rng = np.random.Generator(np.random.PCG64(300 + n))
         amp = _rand_state(rng, n)
@@ -120,7 +133,7 @@ def test_both_kernel_variants(variant, n, oracle_lib):
 
 
 @pytest.mark.parametrize("n", [3, 10, 15])
-def test_fp32_state_close(n, oracle_lib):
+def test_fp32_state_close(n, fp32_form, oracle_lib):
     rng = np.random.Generator(np.random.PCG64(1000 + n))
     amp = _rand_state(rng, n)
     flip, phase, phi = _rand_rots(rng, n, 200)
@@ -250,7 +263,7 @@ def test_trotter12_golden(golden):
     assert np.array_equal(z, want)
 
 
-def test_trotter12_fp32(golden):
+def test_trotter12_fp32(golden, fp32_form):
     cfg = workloads.trotter12()
     p2.set_precision(p2.PREC_FP32)
     try:
@@ -295,7 +308,7 @@ def test_h2o_fixture_fp64(golden, fusion):
         p2.set_fusion(5, 0)
 
 
-def test_h2o_fixture_fp32(golden):
+def test_h2o_fixture_fp32(golden, fp32_form):
     h, t, d = _h2o(golden)
     p2.set_precision(p2.PREC_FP32)
     try:
@@ -455,7 +468,8 @@ def test_phase2_run_analytic():
 # ---- wide registers: exact sparse checks, size-independent properties --
 
 
-@pytest.mark.parametrize("n,prec", [(26, 0), (30, 0), (30, 1), (33, 0)])
+@pytest.mark.parametrize("n,prec", [(26, 0), (30, 0), (30, 1), (32, 1),
+                                    (33, 0)])
 def test_wide_register_sparse_exact(n, prec):
     t = workloads.jw_terms(n, 400, seed=20 + n)
     rng = np.random.Generator(np.random.PCG64(n))
