@@ -394,8 +394,10 @@ def batched_study(ninst: int = 64, step_cap: int = 4, seed: int = 0xBA7C4):
     """Independent trott problems of uneven size run together: qubits
     U{18..24}, JW terms log-uniform in [1e3, 5e4], steps U{16..512} capped
     at step_cap for a bounded run, FP32 state, one determinant each.
-    Aggregate rot.amp/s over the batch (wall clock around the batch
-    call)."""
+    Aggregate rot.amp/s over the batch (wall clock around the batch call,
+    recording/planning and result download included), once in one
+    persistent launch and once on per-instance streams; HBM GB/s counts
+    2 * 2^n * 8 bytes per pass (small instances are partly L2-resident)."""
     import numpy as np
 
     import phase2_b200 as p2
@@ -410,20 +412,30 @@ def batched_study(ninst: int = 64, step_cap: int = 4, seed: int = 0xBA7C4):
         d = workloads.hamming_dets(n, 1, n // 2, seed=seed + 1000 + k)
         probs.append(dict(nqb=n, terms=t, dets=d, steps=steps, delta=0.05))
         work += steps * nt * (1 << n)
+    out = {"workload": (f"{ninst} trott instances, 18-24 qubits, 1e3-5e4 "
+                        f"JW terms, {step_cap} steps each, FP32 state"),
+           "rot_amp": work, "unit": UNIT}
     p2.set_precision(p2.PREC_FP32)
     try:
-        p2.batch("trott", probs[:2])  # warm the kernels
-        t0 = time.perf_counter()
-        _, stats = p2.batch("trott", probs, with_stats=True)
-        wall = time.perf_counter() - t0
+        for mode, persistent in (("persistent", True), ("streams", False)):
+            p2.set_batch_persistent(persistent)
+            p2.batch("trott", probs[:2])  # warm the kernels
+            t0 = time.perf_counter()
+            _, stats = p2.batch("trott", probs, with_stats=True)
+            wall = time.perf_counter() - t0
+            hbm = sum(s["bytes"] for s in stats)
+            out[mode] = {
+                "seconds": wall, "value": work / wall,
+                "hbm_gbs_wall": hbm / wall / 1e9,
+                "launches": int(sum(s["launches"] for s in stats)),
+                "passes": int(sum(s["passes"] for s in stats)),
+                "graph_replays": int(sum(s["graph_replays"]
+                                         for s in stats))}
     finally:
+        p2.set_batch_persistent(True)
         p2.set_precision(p2.PREC_FP64)
-    return {"workload": (f"{ninst} trott instances, 18-24 qubits, 1e3-5e4 "
-                         f"JW terms, {step_cap} steps each, FP32 state"),
-            "rot_amp": work, "seconds": wall,
-            "value": work / wall, "unit": UNIT,
-            "passes": int(sum(s["passes"] for s in stats)),
-            "graph_replays": int(sum(s["graph_replays"] for s in stats))}
+    out["value"] = out["persistent"]["value"]
+    return out
 
 
 # ---- the reference arm -------------------------------------------------

@@ -90,13 +90,25 @@ void circ_hamil_sort_flip(struct circ_hamil *hm);
 /* ---- batched drivers ------------------------------------------------------ */
 
 /*
- * Run n independent, already initialised problems of one kind together:
- * each keeps its own register (its own CUDA stream), and the host advances
- * them in lockstep, enqueuing instance i's next step as soon as its
- * current overlap has been read, so the GPU overlaps the instances' work
- * (and replays each instance's repeated step plan from a CUDA graph).
- * Results land in each problem's ct.vals and step writer exactly as the
- * single-problem *_simul calls would produce them.  0, or -1 if any
+ * Batched drivers run in one of two ways.  Persistent (default, when every
+ * instance is an FP32 register of at most 31 qubits and the FP32 form is
+ * PHASE2_FORM_LIFTED_F32): each instance's steps are recorded as a program
+ * and all programs run in ONE persistent kernel launch that schedules
+ * (instance, op, tile) work over all SMs.  Otherwise, or after
+ * phase2_set_batch_persistent(0): per-instance streams as described below.
+ */
+int phase2_set_batch_persistent(int on);
+
+/*
+ * Run n independent, already initialised problems of one kind together.
+ * Persistent mode (above): one launch for all instances and all their
+ * steps.  Stream mode: each keeps its own register (its own CUDA stream),
+ * and the host advances them in lockstep, enqueuing instance i's next step
+ * as soon as its current overlap has been read, so the GPU overlaps the
+ * instances' work (and replays each instance's repeated step plan from a
+ * CUDA graph).  Either way results land in each problem's ct.vals and step
+ * writer as the single-problem *_simul calls would produce them (the
+ * writer is called after the launch in persistent mode).  0, or -1 if any
  * instance failed (the others still run to completion).
  */
 struct trott;

@@ -76,6 +76,12 @@ def get_fp32_form() -> int:
     return lib().phase2_get_fp32_form()
 
 
+def set_batch_persistent(on: bool) -> None:
+    """Batched drivers: one persistent launch for all instances (default,
+    FP32 registers in the FP32-arithmetic form) or per-instance streams."""
+    lib().phase2_set_batch_persistent(1 if on else 0)
+
+
 def set_fusion(max_span: int, max_rots: int = 0) -> None:
     if lib().phase2_set_fusion(max_span, max_rots) != 0:
         raise ValueError("bad fusion setting")

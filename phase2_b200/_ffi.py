@@ -266,6 +266,7 @@ _SIGS = {
     "phase2_set_precision": (C.c_int, [C.c_int]),
     "phase2_get_precision": (C.c_int, []),
     "phase2_set_fp32_form": (C.c_int, [C.c_int]),
+    "phase2_set_batch_persistent": (C.c_int, [C.c_int]),
     "phase2_get_fp32_form": (C.c_int, []),
     "phase2_set_fusion": (C.c_int, [C.c_int, C.c_int]),
     "phase2_set_term_order": (C.c_int, [C.c_int]),

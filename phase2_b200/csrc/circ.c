@@ -270,6 +270,15 @@ int circ_step_reverse(struct circ *ct, const struct circ_hamil *hm,
 	return circ_step_generic(ct, hm, omega, 1);
 }
 
+_Complex double p2_circ_overlap(const struct circ_muldet *md,
+	const _Complex double *a)
+{
+	_Complex double pr = 0.0;
+	for (size_t d = 0; d < md->len; d++)
+		pr += a[d] * conj(md->dets[d].cf);
+	return pr;
+}
+
 _Complex double circ_measure(struct circ *ct)
 {
 	if (ct->stprep_kind != STPREP_MULTIDET)
@@ -288,12 +297,10 @@ _Complex double circ_measure(struct circ *ct)
 	}
 	for (size_t d = 0; d < md->len; d++)
 		idx[d] = md->dets[d].idx;
-	if (qreg_getamps(&ct->reg, idx, a, md->len) < 0) {
+	if (qreg_getamps(&ct->reg, idx, a, md->len) < 0)
 		log_error("circ_measure: gather failed");
-	} else {
-		for (size_t d = 0; d < md->len; d++)
-			pr += a[d] * conj(md->dets[d].cf);
-	}
+	else
+		pr = p2_circ_overlap(md, a);
 	free(idx);
 	free(a);
 	return pr;

@@ -414,9 +414,120 @@ static void batch_launch(struct batch_item *it)
 	}
 }
 
+/*
+ * One persistent launch for the whole batch (FP32 registers in the
+ * FP32-arithmetic form): each instance's work is recorded as a program
+ * (its enqueue calls, then a gather of its determinant amplitudes per
+ * output), all programs run in p2d_batch_run, and every output is then
+ * formed on the host from its gathered amplitudes with circ_measure's
+ * expression.  Instances whose recording fails are left out and reported.
+ */
+static int run_batch_persistent(struct batch_item *items, size_t n)
+{
+	struct p2_prog *progs = calloc(n, sizeof *progs);
+	const struct p2_prog **pp = calloc(n, sizeof *pp);
+	struct p2_dev **devs = calloc(n, sizeof *devs);
+	long **gat = calloc(n, sizeof *gat);
+	size_t *who = calloc(n, sizeof *who);
+	double *gout = NULL;
+	int rc = -1;
+	if (!progs || !pp || !devs || !gat || !who)
+		goto out;
+	size_t m = 0, ng = 0;
+	for (size_t i = 0; i < n; i++) {
+		struct batch_item *it = &items[i];
+		struct qreg *reg = &it->ct->reg;
+		const struct circ_muldet *md = &it->ct->md;
+		const size_t len = it->ct->vals.len;
+		uint64_t *didx = malloc(sizeof *didx * (md->len ? md->len : 1));
+		gat[i] = malloc(sizeof **gat * (len ? len : 1));
+		if (!didx || !gat[i] || p2_qreg_record(reg, &progs[i]) < 0) {
+			free(didx);
+			it->failed = 1;
+			continue;
+		}
+		for (size_t d = 0; d < md->len; d++)
+			didx[d] = md->dets[d].idx;
+		for (size_t k = 0; k < len && !it->failed; k++) {
+			if (it->enqueue(it->obj, k) < 0)
+				it->failed = 1;
+			else if ((gat[i][k] = p2_qreg_record_gather(reg, didx,
+					  md->len)) < 0)
+				it->failed = 1;
+		}
+		free(didx);
+		if (p2_qreg_record_end(reg) < 0)
+			it->failed = 1;
+		if (it->failed) {
+			log_error("batch: instance %zu could not be recorded", i);
+			continue;
+		}
+		devs[m] = p2_qreg_dev(reg);
+		pp[m] = &progs[i];
+		who[m++] = i;
+		ng += progs[i].ng;
+	}
+	gout = malloc(sizeof(double) * 2 * (ng ? ng : 1));
+	if (!gout)
+		goto out;
+	if (p2d_batch_run(devs, pp, m, gout, NULL) < 0) {
+		for (size_t j = 0; j < m; j++)
+			items[who[j]].failed = 1;
+		goto out;
+	}
+	size_t base = 0;
+	for (size_t j = 0; j < m; j++) {
+		struct batch_item *it = &items[who[j]];
+		struct circ_values *vals = &it->ct->vals;
+		for (size_t k = 0; k < vals->len; k++) {
+			const _Complex double *a = (const _Complex double *)(gout +
+				2 * (base + (size_t)gat[who[j]][k]));
+			vals->z[k] = p2_circ_overlap(&it->ct->md, a);
+			if (emit(it->sw, k, vals->z[k]) < 0) {
+				it->failed = 1;
+				break;
+			}
+		}
+		base += pp[j]->ng;
+	}
+	rc = 0;
+out:
+	for (size_t i = 0; i < n; i++) {
+		if (progs)
+			p2_prog_free(&progs[i]);
+		if (gat)
+			free(gat[i]);
+		if (rc < 0)
+			items[i].failed = 1;
+	}
+	free(progs);
+	free(pp);
+	free(devs);
+	free(gat);
+	free(who);
+	free(gout);
+	for (size_t i = 0; i < n; i++)
+		if (items[i].failed)
+			rc = -1;
+	return rc;
+}
+
+/* Whether every instance can run in one persistent launch. */
+static int batch_persistent_ok(const struct batch_item *items, size_t n)
+{
+	if (!p2_cfg.batch_persistent ||
+		p2_form_for(PHASE2_PREC_FP32) != PHASE2_FORM_LIFTED_F32)
+		return 0;
+	for (size_t i = 0; i < n; i++)
+		if (!p2d_batch_ok(p2_qreg_dev(&items[i].ct->reg)) ||
+			items[i].ct->stprep_kind != STPREP_MULTIDET)
+			return 0;
+	return 1;
+}
+
 /* Queue output 0 everywhere, then repeatedly read each instance's pending
  * output and immediately queue its next one. */
-static int run_batch(struct batch_item *items, size_t n)
+static int run_batch_streams(struct batch_item *items, size_t n)
 {
 	for (size_t i = 0; i < n; i++)
 		if (items[i].ct->vals.len > 0)
@@ -461,7 +572,9 @@ static int run_batch(struct batch_item *items, size_t n)
 			items[i].sw = objs[i]->sw;                             \
 			items[i].enqueue = ENQ;                                \
 		}                                                              \
-		const int rc = run_batch(items, n);                            \
+		const int rc = batch_persistent_ok(items, n)                   \
+			? run_batch_persistent(items, n)                       \
+			: run_batch_streams(items, n);                         \
 		free(items);                                                   \
 		return rc;                                                     \
 	}

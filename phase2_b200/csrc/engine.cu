@@ -794,6 +794,65 @@ __host__ __device__ constexpr int p2_lift32_blocks(int m)
 	return m >= 5 ? 5 : (m == 4 ? 6 : 8);
 }
 
+/* A lifted record repacked for the FP32 kernels' shared memory. */
+__device__ __forceinline__ struct p2_lift32_rec p2_lift32_of(
+	const struct phase2_rot_rec &in)
+{
+	struct p2_lift32_rec o;
+	o.t = (float)in.c;
+	o.s = (float)in.s; /* an FP32 value: exact */
+	o.z = in.z;
+	o.sm = in.smask;
+	o.key = ((uint32_t)in.U << 1) | in.odd;
+	return o;
+}
+
+/*
+ * One coset of a lifted FP32 pass: load the 2^M amplitudes x ^ off(u)
+ * into FP32 registers, apply the run of rotations, store them (negated
+ * when negm has the sign bit).  CG: loads and stores at L2 only (the
+ * persistent batch kernel, whose blocks read what other blocks of the same
+ * launch wrote).
+ */
+template <int M, typename IT, bool CG>
+__device__ __forceinline__ void p2_lift32_coset(float2 *__restrict__ st, IT x,
+	const IT (&pb)[M > 0 ? M : 1], const struct p2_lift32_rec *srec,
+	uint32_t nrot, uint32_t negm)
+{
+	float re[1 << M], im[1 << M];
+#pragma unroll
+	for (int u = 0; u < (1 << M); ++u) {
+		IT off = 0;
+#pragma unroll
+		for (int k = 0; k < M; ++k)
+			if (u >> k & 1)
+				off ^= pb[k];
+		const float2 v = CG ? __ldcg(st + (x ^ off)) : st[x ^ off];
+		re[u] = v.x;
+		im[u] = v.y;
+	}
+	for (uint32_t r = 0; r < nrot; ++r) {
+		const struct p2_lift32_rec q = srec[r];
+		const uint32_t sm = q.sm ^ (0u - p2_parity(x & (IT)q.z));
+		p2_apply_lift32<M>(q, re, im, sm);
+	}
+	const IT xs = p2_opaque(x);
+#pragma unroll
+	for (int u = 0; u < (1 << M); ++u) {
+		IT off = 0;
+#pragma unroll
+		for (int k = 0; k < M; ++k)
+			if (u >> k & 1)
+				off ^= pb[k];
+		const float2 v = make_float2(p2_fsgn(re[u], negm),
+			p2_fsgn(im[u], negm));
+		if (CG)
+			__stcg(st + (xs ^ off), v);
+		else
+			st[xs ^ off] = v;
+	}
+}
+
 /*
  * One FP32 pass in the lifted form with FP32 arithmetic: loads go straight
  * into FP32 registers, the run is applied with FP32 FMAs, stores write the
@@ -807,16 +866,8 @@ __global__ void __launch_bounds__(P2_TPB, p2_lift32_blocks(M))
 		const struct phase2_rot_rec *__restrict__ recs)
 {
 	__shared__ struct p2_lift32_rec srec[P2_MAX_ROTS_PER_PASS];
-	for (uint32_t r = threadIdx.x; r < p.nrot; r += blockDim.x) {
-		const struct phase2_rot_rec in = recs[p.rot_off + r];
-		struct p2_lift32_rec o;
-		o.t = (float)in.c;
-		o.s = (float)in.s; /* an FP32 value: exact */
-		o.z = in.z;
-		o.sm = in.smask;
-		o.key = ((uint32_t)in.U << 1) | in.odd;
-		srec[r] = o;
-	}
+	for (uint32_t r = threadIdx.x; r < p.nrot; r += blockDim.x)
+		srec[r] = p2_lift32_of(recs[p.rot_off + r]);
 	__syncthreads();
 	IT pb[M > 0 ? M : 1];
 #pragma unroll
@@ -827,36 +878,197 @@ __global__ void __launch_bounds__(P2_TPB, p2_lift32_blocks(M))
 
 	const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
 	for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-		t < nrep; t += stride) {
-		const IT x = p2_rep_t<M, IT>((IT)t, p);
-		float re[1 << M], im[1 << M];
+		t < nrep; t += stride)
+		p2_lift32_coset<M, IT, false>(st, p2_rep_t<M, IT>((IT)t, p),
+			pb, srec, nrot, negm);
+}
+
+/* ---- persistent batch kernel -------------------------------------------- */
+
+/*
+ * Many registers' recorded programs (p2_internal.h) in one launch.  Every
+ * op of a program is cut into tiles (a pass: 128 cosets, one per thread;
+ * a zero: 4096 amplitudes; a write or gather: one tile); op k+1 of a
+ * program starts only when every tile of op k is done, programs are
+ * independent.  Each program has a ticket, (op << 32) | next tile: a block
+ * claims a tile with one atomicAdd, and the block that completes the last
+ * tile of an op publishes the next op by resetting the ticket.  Blocks
+ * look for work across programs starting from the last one they served,
+ * so small programs interleave and the GPU stays busy without a launch per
+ * pass.  Waiting is bounded: a block that finds nothing to claim for
+ * idle_limit consecutive rounds (about a microsecond each) raises status
+ * and returns, so a scheduling fault ends the launch instead of hanging it.
+ *
+ * Ordering: a tile's stores are made visible (each thread fences, then the
+ * block barrier) before its completion count; the finisher fences before
+ * publishing the next op; a claimer fences after its claim.  State loads
+ * and stores go through L2 only (ld/st .cg), since L1 is not coherent
+ * across SMs.
+ */
+#define P2_BATCH_ZERO_TILE (P2_TPB * 32)
+
+struct p2_binst {
+	float2 *state;
+	uint64_t namp;
+	uint32_t op_off, nops;
+};
+
+struct p2_bctl {
+	unsigned long long ticket;
+	unsigned int done;
+	unsigned int pad;
+};
+
+template <int M>
+__device__ __forceinline__ void p2_batch_pass_tile(float2 *st,
+	const struct phase2_pass &p, uint64_t t, const struct p2_lift32_rec *srec)
+{
+	uint32_t pb[M > 0 ? M : 1];
 #pragma unroll
-		for (int u = 0; u < (1 << M); ++u) {
-			IT off = 0;
-#pragma unroll
-			for (int k = 0; k < M; ++k)
-				if (u >> k & 1)
-					off ^= pb[k];
-			const float2 v = st[x ^ off];
-			re[u] = v.x;
-			im[u] = v.y;
+	for (int k = 0; k < M; ++k)
+		pb[k] = (uint32_t)p.basis[k];
+	p2_lift32_coset<M, uint32_t, true>(st, p2_rep_t<M, uint32_t>(
+		(uint32_t)t, p), pb, srec, p.nrot,
+		p.scale < 0 ? 0x80000000u : 0u);
+}
+
+__global__ void __launch_bounds__(P2_TPB, 4)
+	k_batch(const struct p2_binst *__restrict__ inst, uint32_t ninst,
+		const struct p2_op *__restrict__ ops,
+		const struct phase2_pass *__restrict__ passes,
+		const struct phase2_rot_rec *__restrict__ recs,
+		const uint64_t *__restrict__ widx,
+		const double *__restrict__ wval,
+		const uint64_t *__restrict__ gidx, double2 *__restrict__ gout,
+		struct p2_bctl *ctl, unsigned int *status,
+		unsigned int idle_limit)
+{
+	__shared__ struct p2_lift32_rec srec[P2_MAX_ROTS_PER_PASS];
+	__shared__ uint32_t s_inst, s_seq, s_tile;
+	__shared__ int s_what; /* 0 nothing claimable yet, 1 work, 2 exit */
+	uint32_t cursor = blockIdx.x % ninst;
+	unsigned int idle = 0;
+	for (;;) {
+		if (threadIdx.x == 0) {
+			int what = 2;
+			for (uint32_t k = 0; k < ninst; ++k) {
+				const uint32_t i = cursor + k < ninst
+					? cursor + k
+					: cursor + k - ninst;
+				const uint32_t nops = inst[i].nops;
+				const unsigned long long tk =
+					*(volatile unsigned long long *)&ctl[i]
+						 .ticket;
+				if ((uint32_t)(tk >> 32) >= nops)
+					continue; /* program finished */
+				what = 0;
+				const uint32_t off = inst[i].op_off;
+				if ((uint32_t)tk >=
+					ops[off + (uint32_t)(tk >> 32)].ntiles)
+					continue; /* all tiles taken */
+				const unsigned long long got =
+					atomicAdd(&ctl[i].ticket, 1ull);
+				const uint32_t seq = (uint32_t)(got >> 32);
+				const uint32_t tile = (uint32_t)got;
+				if (seq < nops && tile < ops[off + seq].ntiles) {
+					__threadfence();
+					s_inst = i;
+					s_seq = seq;
+					s_tile = tile;
+					cursor = i;
+					what = 1;
+					break;
+				}
+			}
+			if (what == 0) {
+				if (++idle > idle_limit) {
+					atomicOr(status, 1u);
+					what = 2;
+				} else {
+					__nanosleep(1000);
+				}
+			} else if (what == 1) {
+				idle = 0;
+			}
+			s_what = what;
 		}
-		for (uint32_t r = 0; r < nrot; ++r) {
-			const struct p2_lift32_rec q = srec[r];
-			const uint32_t sm = q.sm ^ (0u - p2_parity(x & (IT)q.z));
-			p2_apply_lift32<M>(q, re, im, sm);
+		__syncthreads();
+		const int what = s_what;
+		if (what == 2)
+			return;
+		if (what == 1) {
+			const uint32_t i = s_inst, seq = s_seq, tile = s_tile;
+			float2 *const st = inst[i].state;
+			const uint64_t namp = inst[i].namp;
+			const struct p2_op op = ops[inst[i].op_off + seq];
+			if (op.kind == P2_OP_PASS) {
+				const struct phase2_pass p = passes[op.a];
+				for (uint32_t r = threadIdx.x; r < p.nrot;
+					r += blockDim.x)
+					srec[r] = p2_lift32_of(recs[p.rot_off + r]);
+				__syncthreads();
+				const uint64_t t =
+					(uint64_t)tile * P2_TPB + threadIdx.x;
+				if (t < (namp >> p.span)) {
+					switch (p.span) {
+					case 0:
+						p2_batch_pass_tile<0>(st, p, t, srec);
+						break;
+					case 1:
+						p2_batch_pass_tile<1>(st, p, t, srec);
+						break;
+					case 2:
+						p2_batch_pass_tile<2>(st, p, t, srec);
+						break;
+					case 3:
+						p2_batch_pass_tile<3>(st, p, t, srec);
+						break;
+					case 4:
+						p2_batch_pass_tile<4>(st, p, t, srec);
+						break;
+					default:
+						p2_batch_pass_tile<5>(st, p, t, srec);
+						break;
+					}
+				}
+			} else if (op.kind == P2_OP_ZERO) {
+				const uint64_t base =
+					(uint64_t)tile * P2_BATCH_ZERO_TILE;
+				for (uint32_t k = threadIdx.x;
+					k < P2_BATCH_ZERO_TILE; k += blockDim.x)
+					if (base + k < namp)
+						__stcg(st + base + k,
+							make_float2(0.f, 0.f));
+			} else if (op.kind == P2_OP_WRITE) {
+				/* in order: later writes win */
+				if (threadIdx.x == 0)
+					for (uint32_t e = op.a; e < op.a + op.b; ++e)
+						__stcg(st + widx[e],
+							make_float2(
+								(float)wval[2 * e],
+								(float)wval[2 * e + 1]));
+			} else {
+				for (uint32_t d = threadIdx.x; d < op.b;
+					d += blockDim.x) {
+					const float2 v =
+						__ldcg(st + gidx[op.a + d]);
+					gout[op.a + d] = make_double2(v.x, v.y);
+				}
+			}
+			__threadfence();
+			__syncthreads();
+			if (threadIdx.x == 0) {
+				const unsigned int d =
+					atomicAdd(&ctl[i].done, 1u) + 1u;
+				if (d == op.ntiles) {
+					atomicExch(&ctl[i].done, 0u);
+					__threadfence();
+					atomicExch(&ctl[i].ticket,
+						(unsigned long long)(seq + 1) << 32);
+				}
+			}
 		}
-		const IT xs = p2_opaque(x);
-#pragma unroll
-		for (int u = 0; u < (1 << M); ++u) {
-			IT off = 0;
-#pragma unroll
-			for (int k = 0; k < M; ++k)
-				if (u >> k & 1)
-					off ^= pb[k];
-			st[xs ^ off] = make_float2(p2_fsgn(re[u], negm),
-				p2_fsgn(im[u], negm));
-		}
+		__syncthreads();
 	}
 }
 
@@ -1695,6 +1907,201 @@ extern "C" void p2d_set_timing(struct p2_dev *d, int on)
 extern "C" void *p2d_stream(const struct p2_dev *d)
 {
 	return (void *)d->stream;
+}
+
+/* ---- batched persistent execution --------------------------------------- */
+
+extern "C" int p2d_batch_ok(const struct p2_dev *d)
+{
+	return d && d->prec == PHASE2_PREC_FP32 && d->nqb <= 31;
+}
+
+static size_t p2_align256(size_t v)
+{
+	return (v + 255) & ~(size_t)255;
+}
+
+/* Idle scheduling rounds (each sleeps ~1 us) before a block gives up. */
+#define P2_BATCH_IDLE_LIMIT 2000000u
+
+extern "C" int p2d_batch_run(struct p2_dev *const *devs,
+	const struct p2_prog *const *progs, size_t n, double *gout,
+	double *kernel_ms)
+{
+	if (n == 0)
+		return 0;
+	size_t nops = 0, npass = 0, nrec = 0, nw = 0, ng = 0;
+	for (size_t i = 0; i < n; i++) {
+		if (!p2d_batch_ok(devs[i]) || progs[i]->error) {
+			log_error("batch: program %zu cannot run batched", i);
+			return -1;
+		}
+		nops += progs[i]->nops;
+		npass += progs[i]->npass;
+		nrec += progs[i]->nrec;
+		nw += progs[i]->nw;
+		ng += progs[i]->ng;
+	}
+	if (n > UINT32_MAX || nops > UINT32_MAX || npass > UINT32_MAX ||
+		nrec > UINT32_MAX || nw > UINT32_MAX || ng > UINT32_MAX) {
+		log_error("batch: program too large");
+		return -1;
+	}
+	/* one device buffer: uploaded part, then outputs and control */
+	const size_t o_inst = 0;
+	const size_t o_ops = p2_align256(o_inst + n * sizeof(struct p2_binst));
+	const size_t o_pass = p2_align256(o_ops + nops * sizeof(struct p2_op));
+	const size_t o_rec =
+		p2_align256(o_pass + npass * sizeof(struct phase2_pass));
+	const size_t o_widx =
+		p2_align256(o_rec + nrec * sizeof(struct phase2_rot_rec));
+	const size_t o_wval = p2_align256(o_widx + nw * sizeof(uint64_t));
+	const size_t o_gidx = p2_align256(o_wval + 2 * nw * sizeof(double));
+	const size_t up = p2_align256(o_gidx + ng * sizeof(uint64_t));
+	const size_t o_gout = up;
+	const size_t o_ctl = p2_align256(o_gout + ng * sizeof(double2));
+	const size_t o_status = p2_align256(o_ctl + n * sizeof(struct p2_bctl));
+	const size_t total = o_status + 256;
+
+	unsigned char *h = (unsigned char *)malloc(up);
+	if (!h)
+		return -1;
+	struct p2_binst *hi = (struct p2_binst *)(h + o_inst);
+	struct p2_op *ho = (struct p2_op *)(h + o_ops);
+	struct phase2_pass *hp = (struct phase2_pass *)(h + o_pass);
+	struct phase2_rot_rec *hr = (struct phase2_rot_rec *)(h + o_rec);
+	uint64_t *hwi = (uint64_t *)(h + o_widx);
+	double *hwv = (double *)(h + o_wval);
+	uint64_t *hgi = (uint64_t *)(h + o_gidx);
+	size_t bo = 0, bp = 0, br = 0, bw = 0, bg = 0;
+	for (size_t i = 0; i < n; i++) {
+		const struct p2_prog *pg = progs[i];
+		struct p2_dev *d = devs[i];
+		hi[i].state = (float2 *)d->state;
+		hi[i].namp = d->namp;
+		hi[i].op_off = (uint32_t)bo;
+		hi[i].nops = (uint32_t)pg->nops;
+		for (size_t k = 0; k < pg->npass; k++) {
+			hp[bp + k] = pg->passes[k];
+			hp[bp + k].rot_off += (uint32_t)br;
+		}
+		for (size_t k = 0; k < pg->nops; k++) {
+			struct p2_op op = pg->ops[k];
+			switch (op.kind) {
+			case P2_OP_PASS: {
+				op.a += (uint32_t)bp;
+				const uint64_t nrep = d->namp >> hp[op.a].span;
+				op.ntiles = (uint32_t)((nrep + P2_TPB - 1) /
+					P2_TPB);
+				break;
+			}
+			case P2_OP_ZERO:
+				op.ntiles = (uint32_t)((d->namp +
+						       P2_BATCH_ZERO_TILE - 1) /
+					P2_BATCH_ZERO_TILE);
+				break;
+			case P2_OP_WRITE:
+				op.a += (uint32_t)bw;
+				op.ntiles = 1;
+				break;
+			default:
+				op.a += (uint32_t)bg;
+				op.ntiles = 1;
+				break;
+			}
+			ho[bo + k] = op;
+		}
+		if (pg->nrec)
+			memcpy(hr + br, pg->recs, pg->nrec * sizeof *hr);
+		if (pg->nw) {
+			memcpy(hwi + bw, pg->widx, pg->nw * sizeof *hwi);
+			memcpy(hwv + 2 * bw, pg->wval,
+				2 * pg->nw * sizeof *hwv);
+		}
+		if (pg->ng)
+			memcpy(hgi + bg, pg->gidx, pg->ng * sizeof *hgi);
+		bo += pg->nops;
+		bp += pg->npass;
+		br += pg->nrec;
+		bw += pg->nw;
+		bg += pg->ng;
+	}
+
+	struct p2_dev *d0 = devs[0];
+	unsigned char *dbuf = NULL;
+	cudaError_t e = cudaSuccess;
+	for (size_t i = 0; i < n && e == cudaSuccess; i++)
+		e = cudaStreamSynchronize(devs[i]->stream);
+	if (e == cudaSuccess)
+		e = cudaMalloc((void **)&dbuf, total);
+	if (e == cudaSuccess)
+		e = cudaMemcpy(dbuf, h, up, cudaMemcpyHostToDevice);
+	free(h);
+	if (e == cudaSuccess)
+		e = cudaMemset(dbuf + o_ctl, 0, total - o_ctl);
+	int per_sm = 0;
+	if (e == cudaSuccess)
+		e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm,
+			k_batch, P2_TPB, 0);
+	if (e != cudaSuccess) {
+		cudaFree(dbuf);
+		log_error("batch: setup: %s", cudaGetErrorString(e));
+		return -1;
+	}
+	const unsigned grid =
+		(unsigned)d0->sm_count * (unsigned)(per_sm > 0 ? per_sm : 1);
+	cudaEventRecord(d0->t0, d0->stream);
+	k_batch<<<grid, P2_TPB, 0, d0->stream>>>(
+		(const struct p2_binst *)(dbuf + o_inst), (uint32_t)n,
+		(const struct p2_op *)(dbuf + o_ops),
+		(const struct phase2_pass *)(dbuf + o_pass),
+		(const struct phase2_rot_rec *)(dbuf + o_rec),
+		(const uint64_t *)(dbuf + o_widx),
+		(const double *)(dbuf + o_wval),
+		(const uint64_t *)(dbuf + o_gidx), (double2 *)(dbuf + o_gout),
+		(struct p2_bctl *)(dbuf + o_ctl),
+		(unsigned int *)(dbuf + o_status), P2_BATCH_IDLE_LIMIT);
+	e = cudaGetLastError();
+	cudaEventRecord(d0->t1, d0->stream);
+	unsigned int status = 0;
+	if (e == cudaSuccess)
+		e = cudaStreamSynchronize(d0->stream);
+	if (e == cudaSuccess)
+		e = cudaMemcpy(&status, dbuf + o_status, sizeof status,
+			cudaMemcpyDeviceToHost);
+	if (e == cudaSuccess && ng)
+		e = cudaMemcpy(gout, dbuf + o_gout, ng * sizeof(double2),
+			cudaMemcpyDeviceToHost);
+	float ms = 0.0f;
+	if (e == cudaSuccess)
+		e = cudaEventElapsedTime(&ms, d0->t0, d0->t1);
+	cudaFree(dbuf);
+	if (e != cudaSuccess) {
+		log_error("batch: %s", cudaGetErrorString(e));
+		return -1;
+	}
+	if (status) {
+		log_error("batch: a block found no work for %u rounds",
+			P2_BATCH_IDLE_LIMIT);
+		return -1;
+	}
+	if (kernel_ms)
+		*kernel_ms = ms;
+	for (size_t i = 0; i < n; i++) {
+		struct p2_dev *d = devs[i];
+		const struct p2_prog *pg = progs[i];
+		uint64_t np = 0;
+		for (size_t k = 0; k < pg->nops; k++)
+			np += pg->ops[k].kind == P2_OP_PASS;
+		d->passes += np;
+		d->rotations += pg->rotations;
+		d->h2d_bytes += pg->nrec * sizeof(struct phase2_rot_rec) +
+			pg->nw * (sizeof(uint64_t) + 2 * sizeof(double));
+		d->d2h_bytes += pg->ng * sizeof(double2);
+	}
+	d0->launches += 1;
+	d0->h2d_bytes += o_pass; /* program tables */
+	return 0;
 }
 
 /* ---- allocation-free norm (phase2_norm2_noalloc) ------------------------ */

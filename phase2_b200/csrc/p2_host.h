@@ -8,6 +8,7 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include "phase2/circ.h"
 #include "phase2/qreg.h"
 #include "phase2_b200.h"
 
@@ -20,6 +21,7 @@ struct p2_settings {
 	int max_rots;
 	int order;
 	int fp32_form; /* enum phase2_form used for FP32 registers */
+	int batch_persistent; /* batched drivers: one persistent launch */
 };
 extern struct p2_settings p2_cfg;
 void p2_settings_from_env(void);
@@ -50,9 +52,27 @@ struct p2_qreg {
 	size_t wlen, wcap;
 	double *host_copy;
 	int host_copy_valid;
+	struct p2_prog *rec; /* recording instead of executing, or NULL */
 };
 
 /* Sticky error of a register (0 ok, -1 failed). */
 int p2_qreg_error(const struct qreg *reg);
+
+/*
+ * Recording (batched persistent execution, drivers.c): between
+ * p2_qreg_record and p2_qreg_record_end, zero, writes and rotation flushes
+ * of the register are appended to *pg instead of running; reads of the
+ * state are errors except p2_qreg_record_gather, which records a gather
+ * and returns the output index of its first amplitude (or -1).
+ */
+int p2_qreg_record(struct qreg *reg, struct p2_prog *pg);
+long p2_qreg_record_gather(struct qreg *reg, const uint64_t *idx, size_t n);
+int p2_qreg_record_end(struct qreg *reg);
+struct p2_dev *p2_qreg_dev(const struct qreg *reg);
+
+/* sum_d a[d] * conj(cf_d) over the circuit's determinants, the expression
+ * of circ_measure (a: the determinant amplitudes in order). */
+_Complex double p2_circ_overlap(const struct circ_muldet *md,
+	const _Complex double *a);
 
 #endif /* P2_HOST_H */

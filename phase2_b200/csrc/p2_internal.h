@@ -66,6 +66,72 @@ void p2d_stats_reset(struct p2_dev *d);
 void p2d_set_timing(struct p2_dev *d, int on);
 void *p2d_stream(const struct p2_dev *d);
 
+/* ---- recorded programs (batched persistent execution) ------------------- */
+
+/*
+ * A register can record, instead of execute, what would run on it: a list
+ * of ops over its state.  Many registers' programs then run together in one
+ * persistent launch (p2d_batch_run).
+ */
+enum p2_op_kind {
+	P2_OP_ZERO = 0,   /* state <- 0 */
+	P2_OP_WRITE = 1,  /* writes a .. a+b-1 of widx/wval, in order */
+	P2_OP_PASS = 2,   /* pass a of passes */
+	P2_OP_GATHER = 3, /* amplitudes gidx[a .. a+b-1] -> output a .. a+b-1 */
+};
+
+struct p2_op {
+	uint32_t kind;
+	uint32_t a, b;
+	uint32_t ntiles; /* work tiles of the op (set by p2d_batch_run) */
+};
+
+/* A distinct flush plan of a program: later identical flushes reuse it. */
+struct p2_plan_ref {
+	uint64_t hash;
+	uint32_t pass_off, npass, rec_off, nrec;
+};
+
+struct p2_prog {
+	struct p2_op *ops;
+	size_t nops, ops_cap;
+	struct phase2_pass *passes; /* rot_off relative to recs */
+	size_t npass, pass_cap;
+	struct phase2_rot_rec *recs;
+	size_t nrec, rec_cap;
+	uint64_t *widx;
+	double *wval; /* (re, im) per write */
+	size_t nw, w_cap;
+	uint64_t *gidx;
+	size_t ng, g_cap;
+	struct p2_plan_ref *plans;
+	size_t nplans, plans_cap;
+	uint64_t rotations; /* rotations in the PASS ops */
+	int error;
+};
+
+void p2_prog_free(struct p2_prog *pg);
+int p2_prog_zero(struct p2_prog *pg);
+int p2_prog_write(struct p2_prog *pg, const uint64_t *idx, const double *val,
+	size_t n);
+/* Append a flush plan's passes (records rot_off-relative to recs). */
+int p2_prog_plan(struct p2_prog *pg, const struct phase2_pass *passes,
+	size_t npass, const struct phase2_rot_rec *recs, size_t nrec);
+/* Gather n amplitudes; returns the output index of the first, or -1. */
+long p2_prog_gather(struct p2_prog *pg, const uint64_t *idx, size_t n);
+
+/* Whether a register's programs can run in p2d_batch_run (FP32 state in
+ * the FP32-arithmetic lifted form, at most 31 qubits). */
+int p2d_batch_ok(const struct p2_dev *d);
+
+/* Run n recorded programs, program i on register devs[i], in one
+ * persistent launch; gout receives every program's gathered amplitudes
+ * (FP64 re, im) in program order.  *kernel_ms (if non-NULL) gets the
+ * launch's device time.  0 or -1. */
+int p2d_batch_run(struct p2_dev *const *devs,
+	const struct p2_prog *const *progs, size_t n, double *gout,
+	double *kernel_ms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -120,11 +120,26 @@ int qreg_precision(const struct qreg *reg)
 	return b ? b->prec : -1;
 }
 
+/* Reads of the state are not possible while the register records. */
+static int recording(const struct p2_qreg *b, const char *what)
+{
+	if (!b->rec)
+		return 0;
+	log_error("%s: register is recording a batch program", what);
+	return 1;
+}
+
 /* Launch the queued amplitude writes (one scatter, later writes win). */
 static int drain_writes(struct p2_qreg *b)
 {
 	if (b->wlen == 0)
 		return b->error;
+	if (b->rec) {
+		if (p2_prog_write(b->rec, b->widx, b->wval, b->wlen) < 0)
+			b->error = -1;
+		b->wlen = 0;
+		return b->error;
+	}
 	if (p2d_set(b->dev, b->widx, b->wval, b->wlen) < 0) {
 		log_error("qreg: %zu amplitude writes failed", b->wlen);
 		b->error = -1;
@@ -158,8 +173,12 @@ static int drain_rotations(struct qreg *reg)
 	const long np = p2_plan(reg->qb_lo, b->q, b->qlen, b->max_span,
 		b->max_rots, P2_DEFAULT_PAD_SPAN, p2_form_for(b->prec),
 		b->passes, b->recs);
-	if (np < 0 || p2d_run(b->dev, b->passes, (size_t)np, b->recs,
-			      b->qlen) < 0) {
+	if (np >= 0 && b->rec) {
+		if (p2_prog_plan(b->rec, b->passes, (size_t)np, b->recs,
+			    b->qlen) < 0)
+			b->error = -1;
+	} else if (np < 0 || p2d_run(b->dev, b->passes, (size_t)np, b->recs,
+				    b->qlen) < 0) {
 		log_error("qreg: %zu rotations failed", b->qlen);
 		b->error = -1;
 	}
@@ -195,7 +214,7 @@ int qreg_synchronize(struct qreg *reg)
 	struct p2_qreg *b = B(reg);
 	if (!b || qreg_flush(reg) < 0)
 		return -1;
-	if (p2d_sync(b->dev) < 0)
+	if (!b->rec && p2d_sync(b->dev) < 0)
 		b->error = -1;
 	return b->error;
 }
@@ -276,7 +295,7 @@ int qreg_getamps(struct qreg *reg, const uint64_t *idx, _Complex double *z,
 	size_t n)
 {
 	struct p2_qreg *b = B(reg);
-	if (!b)
+	if (!b || recording(b, "qreg_getamps"))
 		return -1;
 	for (size_t i = 0; i < n; i++)
 		if (idx[i] >= reg->namp) {
@@ -330,6 +349,11 @@ void qreg_zero(struct qreg *reg)
 	/* queued work acts on a state about to be overwritten */
 	b->qlen = 0;
 	b->wlen = 0;
+	if (b->rec) {
+		if (p2_prog_zero(b->rec) < 0)
+			b->error = -1;
+		return;
+	}
 	if (p2d_zero(b->dev) < 0) {
 		b->error = -1;
 		b->host_copy_valid = 0;
@@ -344,7 +368,7 @@ void qreg_zero(struct qreg *reg)
 int qreg_get_state(struct qreg *reg, double *out)
 {
 	struct p2_qreg *b = B(reg);
-	if (!b || qreg_flush(reg) < 0)
+	if (!b || recording(b, "qreg_get_state") || qreg_flush(reg) < 0)
 		return -1;
 	if (b->host_copy && b->host_copy_valid) {
 		memcpy(out, b->host_copy, sizeof(double) * 2 * reg->namp);
@@ -356,7 +380,7 @@ int qreg_get_state(struct qreg *reg, double *out)
 int qreg_set_state(struct qreg *reg, const double *in)
 {
 	struct p2_qreg *b = B(reg);
-	if (!b)
+	if (!b || recording(b, "qreg_set_state"))
 		return -1;
 	b->qlen = 0;
 	b->wlen = 0;
@@ -393,7 +417,7 @@ void qreg_sync_device_to_host(struct qreg *reg)
 int qreg_norm2(struct qreg *reg, double *out)
 {
 	struct p2_qreg *b = B(reg);
-	if (!b || qreg_flush(reg) < 0)
+	if (!b || recording(b, "qreg_norm2") || qreg_flush(reg) < 0)
 		return -1;
 	return p2d_norm2(b->dev, out);
 }
@@ -401,9 +425,54 @@ int qreg_norm2(struct qreg *reg, double *out)
 int qreg_inner_dense(struct qreg *reg, const double *trial, double out[2])
 {
 	struct p2_qreg *b = B(reg);
-	if (!b || qreg_flush(reg) < 0)
+	if (!b || recording(b, "qreg_inner_dense") || qreg_flush(reg) < 0)
 		return -1;
 	return p2d_inner_dense(b->dev, trial, out);
+}
+
+int p2_qreg_record(struct qreg *reg, struct p2_prog *pg)
+{
+	struct p2_qreg *b = B(reg);
+	if (!b || b->rec || qreg_flush(reg) < 0)
+		return -1;
+	b->rec = pg;
+	b->host_copy_valid = 0;
+	return 0;
+}
+
+long p2_qreg_record_gather(struct qreg *reg, const uint64_t *idx, size_t n)
+{
+	struct p2_qreg *b = B(reg);
+	if (!b || !b->rec || qreg_flush(reg) < 0)
+		return -1;
+	for (size_t i = 0; i < n; i++)
+		if (idx[i] >= reg->namp) {
+			log_error("gather: index %llu out of range",
+				(unsigned long long)idx[i]);
+			return -1;
+		}
+	const long at = p2_prog_gather(b->rec, idx, n);
+	if (at < 0)
+		b->error = -1;
+	return at;
+}
+
+int p2_qreg_record_end(struct qreg *reg)
+{
+	struct p2_qreg *b = B(reg);
+	if (!b || !b->rec)
+		return -1;
+	qreg_flush(reg);
+	if (b->rec->error)
+		b->error = -1;
+	b->rec = NULL;
+	return b->error;
+}
+
+struct p2_dev *p2_qreg_dev(const struct qreg *reg)
+{
+	const struct p2_qreg *b = B(reg);
+	return b ? b->dev : NULL;
 }
 
 int qreg_get_stats(const struct qreg *reg, struct phase2_stats *st)

@@ -18,6 +18,7 @@ struct p2_settings p2_cfg = {
 	.max_rots = 0,
 	.order = PHASE2_ORDER_LEX,
 	.fp32_form = PHASE2_FORM_LIFTED_F32,
+	.batch_persistent = 1,
 };
 
 void p2_settings_from_env(void)
@@ -53,6 +54,12 @@ int phase2_set_fp32_form(int form)
 int phase2_get_fp32_form(void)
 {
 	return p2_cfg.fp32_form;
+}
+
+int phase2_set_batch_persistent(int on)
+{
+	p2_cfg.batch_persistent = on ? 1 : 0;
+	return 0;
 }
 
 int p2_form_for(int prec)

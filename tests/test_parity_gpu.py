@@ -403,6 +403,73 @@ def test_batched_drivers_match_single(oracle_lib):
         assert np.array_equal(z, want)
 
 
+def _uneven_problems():
+    probs = []
+    for k, n in enumerate((8, 13, 10, 15, 9, 12, 18, 11)):
+        t = workloads.jw_terms(n, 40 + 30 * k, seed=900 + k)
+        d = workloads.hamming_dets(n, 1 + k % 3, n // 2, seed=950 + k)
+        probs.append(dict(nqb=n, terms=t, dets=d, steps=2 + k % 5,
+                          delta=0.1, samples=1 + k % 3, depth=30 + 7 * k,
+                          step_size=0.02, seed=990 + k, length=6,
+                          angle_det=0.05, angle_rand=0.01))
+    return probs
+
+
+@pytest.mark.parametrize("kind", ["trott", "trott2", "qdrift", "cmpsit"])
+def test_persistent_batch(kind, oracle_lib):
+    """FP32 batches in one persistent launch: bit-identical to the same
+    batch run on per-instance streams (same plans, same per-coset
+    arithmetic), within the FP32 tolerance of the FP64 oracle, and one
+    kernel launch for the whole batch."""
+    probs = _uneven_problems()
+    if kind == "cmpsit":
+        probs = [dict(p, samples=2, steps=2, depth=12) for p in probs]
+    p2.set_precision(p2.PREC_FP32)
+    try:
+        p2.set_batch_persistent(True)
+        got, stats = p2.batch(kind, probs, with_stats=True)
+        p2.set_batch_persistent(False)
+        ref = p2.batch(kind, probs)
+    finally:
+        p2.set_batch_persistent(True)
+        p2.set_precision(p2.PREC_FP64)
+    assert sum(s["launches"] for s in stats) == 1
+    assert all(s["passes"] > 0 for s in stats)
+    for p, z, r in zip(probs, got, ref):
+        assert np.array_equal(z, r), kind
+        t, d = p["terms"], p["dets"]
+        if kind in ("trott", "trott2"):
+            want = oracle_lib.trott(p["nqb"], t.flip, t.phase, t.cf, d.idx,
+                                    d.cf, p["steps"], p["delta"],
+                                    order2=kind == "trott2")
+        elif kind == "qdrift":
+            want = oracle_lib.qdrift(p["nqb"], t.flip, t.phase, t.cf, d.idx,
+                                     d.cf, p["samples"], p["depth"],
+                                     p["step_size"], p["seed"])
+        else:
+            want = oracle_lib.cmpsit(p["nqb"], t.flip, t.phase, t.cf, d.idx,
+                                     d.cf, 2, 2, p["length"], 12,
+                                     p["angle_det"], p["angle_rand"],
+                                     p["seed"])
+        assert np.max(np.abs(z - want)) < FP32_TOL, kind
+
+
+def test_persistent_batch_empty_and_single():
+    """Edge cases: an empty batch, one instance, an instance with no
+    outputs (zero steps) beside others."""
+    assert p2.batch("trott", []) == []
+    probs = _uneven_problems()[:3]
+    probs[1] = dict(probs[1], steps=0)
+    p2.set_precision(p2.PREC_FP32)
+    try:
+        one = p2.batch("trott", probs[:1])
+        got = p2.batch("trott", probs)
+    finally:
+        p2.set_precision(p2.PREC_FP64)
+    assert np.array_equal(one[0], got[0])
+    assert len(got[1]) == 0
+
+
 def test_sharded_qdrift_equals_single_run():
     """Replica sharding (phase2_b200.replicas): the blocks of 3 ranks,
     each with its generator advanced to its first sample, concatenate to
