@@ -1,10 +1,14 @@
 """Benchmark of the phase2 state-vector hot path on B200.
 
 Metric: Pauli-rotation x amplitudes per second (and HBM GB/s) at 30 qubits,
-FP32 state with FP64 arithmetic ("FP32-batched": fused passes) against the
-plain FP64 path (one rotation per pass), on the qDRIFT workload: 30 qubits,
-100,000 Jordan-Wigner-like terms (seeded synthetic, phase2_b200.workloads),
-4096 draws per sample, step_size 1e-3.
+FP32 state ("FP32-batched": fused passes, rotations as three FP32 shears
+per pair; angles, cos/sin and overlaps in FP64) against the plain FP64 path
+(one rotation per pass), on the qDRIFT workload: 30 qubits, 100,000
+Jordan-Wigner-like terms (seeded synthetic, phase2_b200.workloads), 4096
+draws per sample, step_size 1e-3.  The line also carries comparison arms
+(FP64 plain/fused, FP32 plain, FP32 with FP64 arithmetic, and the
+reference's own CUDA kernel built from its sources), the FP32 error study
+and the batched study.
 
 A step is one qDRIFT sample through the library's C-ABI driver
 (qdrift_simul): state prep, 4096 rotations, overlap.  ``value`` is timed
@@ -193,6 +197,30 @@ def _traffic_per_launch():
     return None
 
 
+def _reference_gpu(nqb: int, nrot: int = 16, reps: int = 3):
+    """The reference's own CUDA backend (phase2/qreg_cuda_lo.cu: one thread
+    per amplitude, two kernelPauliRot launches per rotation for its amp and
+    buf slabs, plus the mix/add/exchange of a flush), compiled from its
+    sources for sm_100a (oracle/Makefile ref-cuda) and timed with the same
+    driver as the CPU baseline: one flush of nrot JW-like rotations on an
+    nqb-qubit FP64 register, min of reps, device-synchronised."""
+    exe = ROOT / "oracle" / "_ref" / "ref_bench_cuda"
+    if not exe.is_file():
+        return None
+    try:
+        out = subprocess.run([str(exe), str(nqb), str(nrot), str(reps)],
+                             capture_output=True, text=True, timeout=600)
+        best, rate = out.stdout.split()[-2:]
+    except (subprocess.SubprocessError, ValueError, OSError):
+        return None
+    namp = 1 << nqb
+    return {"value": float(rate), "unit": UNIT, "rotations": nrot,
+            "seconds_per_flush": float(best),
+            "kernel_gbs_effective": nrot * 2 * namp * 16 / float(best) / 1e9,
+            "what": ("reference CUDA backend, FP64, one flush of "
+                     f"{nrot} rotations at {nqb} qubits")}
+
+
 def _cpu_baseline(nrot: int = 8, reps: int = 2, max_qb: int = 25) -> dict:
     """Reference CPU qreg_paulirot on R processes x one 2^(30-log2 R) slab.
 
@@ -293,6 +321,10 @@ def gpu_arm(args) -> None:
             "kernel_gbs": (s["passes"] * 2 * namp * elem / 1e9) /
             (s["pass_ms"] / 1e3) if s["pass_ms"] else None}
     p2.set_precision(p2.PREC_FP64)
+    if rank == 0 and not args.quick:
+        ref_gpu = _reference_gpu(nqb)
+        if ref_gpu:
+            arms["reference_gpu_fp64"] = ref_gpu
 
     peaks = _peaks()
     passes_per_step = st["passes"] / args.steps
@@ -424,9 +456,13 @@ def batched_study(ninst: int = 64, step_cap: int = 4, seed: int = 0xBA7C4):
             _, stats = p2.batch("trott", probs, with_stats=True)
             wall = time.perf_counter() - t0
             hbm = sum(s["bytes"] for s in stats)
+            kms = sum(s["pass_ms"] for s in stats)
             out[mode] = {
                 "seconds": wall, "value": work / wall,
                 "hbm_gbs_wall": hbm / wall / 1e9,
+                "kernel_seconds": kms / 1e3 if persistent else None,
+                "hbm_gbs_kernel": (hbm / (kms / 1e3) / 1e9
+                                   if persistent and kms else None),
                 "launches": int(sum(s["launches"] for s in stats)),
                 "passes": int(sum(s["passes"] for s in stats)),
                 "graph_replays": int(sum(s["graph_replays"]

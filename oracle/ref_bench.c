@@ -11,6 +11,12 @@
  * batch.  Prints one line: "<best_seconds> <rot_amp_per_s>" with the
  * minimum over repeats (the reference's own min-of-K convention,
  * bench/bench.h).
+ *
+ * Built with REF_BENCH_CUDA against the reference's CUDA backend
+ * (oracle/Makefile ref-cuda) it times the reference's own GPU kernels
+ * (phase2/qreg_cuda_lo.cu); qreg_paulirot only launches them, so every
+ * timed call ends with a device synchronisation, and one untimed call
+ * comes first (module load).
  */
 #define _POSIX_C_SOURCE 200809L
 
@@ -21,6 +27,13 @@
 #include <time.h>
 
 #include "phase2.h"
+
+#ifdef REF_BENCH_CUDA
+#include <cuda_runtime_api.h>
+#define DEVICE_SYNC() cudaDeviceSynchronize()
+#else
+#define DEVICE_SYNC() ((void)0)
+#endif
 
 static double now(void)
 {
@@ -71,9 +84,14 @@ int main(int argc, char **argv)
 	}
 	const struct paulis hi = paulis_new();
 	double best = 1e300;
+#ifdef REF_BENCH_CUDA
+	qreg_paulirot(&reg, hi, lo, phi, nrot);
+	DEVICE_SYNC();
+#endif
 	for (int r = 0; r < reps; r++) {
 		const double t0 = now();
 		qreg_paulirot(&reg, hi, lo, phi, nrot);
+		DEVICE_SYNC();
 		const double dt = now() - t0;
 		if (dt < best)
 			best = dt;

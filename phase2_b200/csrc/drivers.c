@@ -18,12 +18,16 @@
  * identical to the reference for equal seeds.  The deterministic term
  * order follows phase2_get_term_order() (lexicographic by default).
  */
+#define _POSIX_C_SOURCE 200809L /* clock_gettime */
+
 #include <complex.h>
 #include <float.h>
 #include <math.h>
+#include <pthread.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 
 #define LOG_SUBSYS "circ"
 #include "log.h"
@@ -422,8 +426,83 @@ static void batch_launch(struct batch_item *it)
  * formed on the host from its gathered amplitudes with circ_measure's
  * expression.  Instances whose recording fails are left out and reported.
  */
+/* Record instance i's program (all its outputs): its enqueue calls, then a
+ * gather of the determinant amplitudes per output (gat[k]: output index of
+ * output k's first amplitude).  Touches only the instance's own objects
+ * and no device state, so instances record in parallel. */
+static void record_one(struct batch_item *it, struct p2_prog *pg, long **gat)
+{
+	struct qreg *reg = &it->ct->reg;
+	const struct circ_muldet *md = &it->ct->md;
+	const size_t len = it->ct->vals.len;
+	uint64_t *didx = malloc(sizeof *didx * (md->len ? md->len : 1));
+	*gat = malloc(sizeof **gat * (len ? len : 1));
+	if (!didx || !*gat || p2_qreg_record(reg, pg) < 0) {
+		free(didx);
+		it->failed = 1;
+		return;
+	}
+	for (size_t d = 0; d < md->len; d++)
+		didx[d] = md->dets[d].idx;
+	for (size_t k = 0; k < len && !it->failed; k++) {
+		if (it->enqueue(it->obj, k) < 0)
+			it->failed = 1;
+		else if (((*gat)[k] = p2_qreg_record_gather(reg, didx,
+				  md->len)) < 0)
+			it->failed = 1;
+	}
+	free(didx);
+	if (p2_qreg_record_end(reg) < 0)
+		it->failed = 1;
+}
+
+struct record_pool {
+	struct batch_item *items;
+	struct p2_prog *progs;
+	long **gat;
+	size_t n;
+	size_t next; /* next instance to record (atomic) */
+};
+
+static void *record_worker(void *arg)
+{
+	struct record_pool *rp = arg;
+	for (;;) {
+		const size_t i = __atomic_fetch_add(&rp->next, 1,
+			__ATOMIC_RELAXED);
+		if (i >= rp->n)
+			return NULL;
+		record_one(&rp->items[i], &rp->progs[i], &rp->gat[i]);
+	}
+}
+
+/* Host threads that record a batch: one per instance up to 16. */
+#define P2_RECORD_THREADS 16
+
+static void record_all(struct batch_item *items, struct p2_prog *progs,
+	long **gat, size_t n)
+{
+	struct record_pool rp = { items, progs, gat, n, 0 };
+	pthread_t th[P2_RECORD_THREADS];
+	size_t nt = n < P2_RECORD_THREADS ? n : P2_RECORD_THREADS, started = 0;
+	for (size_t k = 1; k < nt; k++)
+		if (pthread_create(&th[started], NULL, record_worker, &rp) == 0)
+			started++;
+	record_worker(&rp);
+	for (size_t k = 0; k < started; k++)
+		pthread_join(th[k], NULL);
+}
+
+static double wall_s(void)
+{
+	struct timespec ts;
+	clock_gettime(CLOCK_MONOTONIC, &ts);
+	return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
 static int run_batch_persistent(struct batch_item *items, size_t n)
 {
+	const double t0 = wall_s();
 	struct p2_prog *progs = calloc(n, sizeof *progs);
 	const struct p2_prog **pp = calloc(n, sizeof *pp);
 	struct p2_dev **devs = calloc(n, sizeof *devs);
@@ -433,36 +512,16 @@ static int run_batch_persistent(struct batch_item *items, size_t n)
 	int rc = -1;
 	if (!progs || !pp || !devs || !gat || !who)
 		goto out;
+	record_all(items, progs, gat, n);
+	const double t1 = wall_s();
 	size_t m = 0, ng = 0;
 	for (size_t i = 0; i < n; i++) {
 		struct batch_item *it = &items[i];
-		struct qreg *reg = &it->ct->reg;
-		const struct circ_muldet *md = &it->ct->md;
-		const size_t len = it->ct->vals.len;
-		uint64_t *didx = malloc(sizeof *didx * (md->len ? md->len : 1));
-		gat[i] = malloc(sizeof **gat * (len ? len : 1));
-		if (!didx || !gat[i] || p2_qreg_record(reg, &progs[i]) < 0) {
-			free(didx);
-			it->failed = 1;
-			continue;
-		}
-		for (size_t d = 0; d < md->len; d++)
-			didx[d] = md->dets[d].idx;
-		for (size_t k = 0; k < len && !it->failed; k++) {
-			if (it->enqueue(it->obj, k) < 0)
-				it->failed = 1;
-			else if ((gat[i][k] = p2_qreg_record_gather(reg, didx,
-					  md->len)) < 0)
-				it->failed = 1;
-		}
-		free(didx);
-		if (p2_qreg_record_end(reg) < 0)
-			it->failed = 1;
 		if (it->failed) {
 			log_error("batch: instance %zu could not be recorded", i);
 			continue;
 		}
-		devs[m] = p2_qreg_dev(reg);
+		devs[m] = p2_qreg_dev(&it->ct->reg);
 		pp[m] = &progs[i];
 		who[m++] = i;
 		ng += progs[i].ng;
@@ -470,11 +529,16 @@ static int run_batch_persistent(struct batch_item *items, size_t n)
 	gout = malloc(sizeof(double) * 2 * (ng ? ng : 1));
 	if (!gout)
 		goto out;
-	if (p2d_batch_run(devs, pp, m, gout, NULL) < 0) {
+	double kms = 0.0;
+	if (p2d_batch_run(devs, pp, m, gout, &kms) < 0) {
 		for (size_t j = 0; j < m; j++)
 			items[who[j]].failed = 1;
 		goto out;
 	}
+	if (getenv("PHASE2_BATCH_TIMING"))
+		log_info("batch: %zu programs, record %.3f s, launch+copy %.3f s"
+			 " (kernel %.3f s)",
+			m, t1 - t0, wall_s() - t1, kms / 1e3);
 	size_t base = 0;
 	for (size_t j = 0; j < m; j++) {
 		struct batch_item *it = &items[who[j]];

@@ -53,6 +53,13 @@ struct p2_qreg {
 	double *host_copy;
 	int host_copy_valid;
 	struct p2_prog *rec; /* recording instead of executing, or NULL */
+	/* input of the plan held in passes/recs (a flush whose queue is
+	 * byte-identical, with the same settings, reuses it: every Trotter
+	 * step after the first) */
+	struct phase2_rot_in *plan_q;
+	size_t plan_qlen, plan_qcap;
+	long plan_np;
+	int plan_span, plan_rots, plan_form;
 };
 
 /* Sticky error of a register (0 ok, -1 failed). */

@@ -107,6 +107,8 @@ struct p2_prog {
 	struct p2_plan_ref *plans;
 	size_t nplans, plans_cap;
 	uint64_t rotations; /* rotations in the PASS ops */
+	long last_plan;     /* plans[] index of the last p2_prog_plan (valid
+			     * when nplans > 0) */
 	int error;
 };
 
@@ -114,9 +116,11 @@ void p2_prog_free(struct p2_prog *pg);
 int p2_prog_zero(struct p2_prog *pg);
 int p2_prog_write(struct p2_prog *pg, const uint64_t *idx, const double *val,
 	size_t n);
-/* Append a flush plan's passes (records rot_off-relative to recs). */
+/* Append a flush plan's passes (records rot_off-relative to recs);
+ * same_as_last: the caller knows it equals the previous call's plan. */
 int p2_prog_plan(struct p2_prog *pg, const struct phase2_pass *passes,
-	size_t npass, const struct phase2_rot_rec *recs, size_t nrec);
+	size_t npass, const struct phase2_rot_rec *recs, size_t nrec,
+	int same_as_last);
 /* Gather n amplitudes; returns the output index of the first, or -1. */
 long p2_prog_gather(struct p2_prog *pg, const uint64_t *idx, size_t n);
 

@@ -112,14 +112,22 @@ static int same_plan(const struct p2_prog *pg, const struct p2_plan_ref *r,
 }
 
 int p2_prog_plan(struct p2_prog *pg, const struct phase2_pass *passes,
-	size_t npass, const struct phase2_rot_rec *recs, size_t nrec)
+	size_t npass, const struct phase2_rot_rec *recs, size_t nrec,
+	int same_as_last)
 {
 	if (pg->error || npass == 0)
 		return pg->error;
-	uint64_t h = fnv1a(UINT64_C(0xcbf29ce484222325), passes,
-		npass * sizeof *passes);
-	h = fnv1a(h, recs, nrec * sizeof *recs);
 	const struct p2_plan_ref *hit = NULL;
+	if (same_as_last && pg->last_plan >= 0 && pg->nplans > 0 &&
+		pg->plans[pg->last_plan].npass == npass &&
+		pg->plans[pg->last_plan].nrec == nrec)
+		hit = &pg->plans[pg->last_plan];
+	uint64_t h = 0;
+	if (!hit) {
+		h = fnv1a(UINT64_C(0xcbf29ce484222325), passes,
+			npass * sizeof *passes);
+		h = fnv1a(h, recs, nrec * sizeof *recs);
+	}
 	for (size_t k = 0; k < pg->nplans && !hit; k++)
 		if (pg->plans[k].hash == h &&
 			same_plan(pg, &pg->plans[k], passes, npass, recs, nrec))
@@ -151,6 +159,7 @@ int p2_prog_plan(struct p2_prog *pg, const struct phase2_pass *passes,
 		pg->nrec += nrec;
 		hit = r;
 	}
+	pg->last_plan = hit - pg->plans;
 	for (size_t i = 0; i < npass; i++) {
 		if (push_op(pg, P2_OP_PASS, hit->pass_off + (uint32_t)i, 0) < 0)
 			return -1;

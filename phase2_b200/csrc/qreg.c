@@ -104,6 +104,7 @@ void qreg_free(struct qreg *reg)
 		free(b->q);
 		free(b->passes);
 		free(b->recs);
+		free(b->plan_q);
 		free(b->widx);
 		free(b->wval);
 		free(b->host_copy);
@@ -148,6 +149,27 @@ static int drain_writes(struct p2_qreg *b)
 	return b->error;
 }
 
+/* Keep a copy of the queue just planned (the plan cache's key). */
+static void remember_plan(struct p2_qreg *b, long np, int form)
+{
+	b->plan_qlen = 0;
+	if (np < 0)
+		return;
+	if (b->plan_qcap < b->qlen) {
+		free(b->plan_q);
+		b->plan_q = malloc(sizeof *b->plan_q * b->qlen);
+		b->plan_qcap = b->plan_q ? b->qlen : 0;
+		if (!b->plan_q)
+			return;
+	}
+	memcpy(b->plan_q, b->q, sizeof *b->q * b->qlen);
+	b->plan_qlen = b->qlen;
+	b->plan_np = np;
+	b->plan_span = b->max_span;
+	b->plan_rots = b->max_rots;
+	b->plan_form = form;
+}
+
 /* Plan and launch the queued rotations (asynchronously). */
 static int drain_rotations(struct qreg *reg)
 {
@@ -169,13 +191,25 @@ static int drain_rotations(struct qreg *reg)
 			return -1;
 		}
 		b->plan_cap = b->qlen;
+		b->plan_qlen = 0; /* the held plan is gone */
 	}
-	const long np = p2_plan(reg->qb_lo, b->q, b->qlen, b->max_span,
-		b->max_rots, P2_DEFAULT_PAD_SPAN, p2_form_for(b->prec),
-		b->passes, b->recs);
+	const int form = p2_form_for(b->prec);
+	/* the same queue under the same settings plans to the same passes:
+	 * reuse the plan still held in passes/recs */
+	const int same = b->plan_q && b->plan_qlen == b->qlen &&
+		b->plan_span == b->max_span && b->plan_rots == b->max_rots &&
+		b->plan_form == form &&
+		memcmp(b->plan_q, b->q, sizeof *b->q * b->qlen) == 0;
+	long np = b->plan_np;
+	if (!same) {
+		np = p2_plan(reg->qb_lo, b->q, b->qlen, b->max_span,
+			b->max_rots, P2_DEFAULT_PAD_SPAN, form, b->passes,
+			b->recs);
+		remember_plan(b, np, form);
+	}
 	if (np >= 0 && b->rec) {
 		if (p2_prog_plan(b->rec, b->passes, (size_t)np, b->recs,
-			    b->qlen) < 0)
+			    b->qlen, same) < 0)
 			b->error = -1;
 	} else if (np < 0 || p2d_run(b->dev, b->passes, (size_t)np, b->recs,
 				    b->qlen) < 0) {
