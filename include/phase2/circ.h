@@ -15,6 +15,7 @@
 
 #include "phase2/paulis.h"
 #include "phase2/qreg.h"
+#include "phase2/state_prep_coeff.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -71,7 +72,7 @@ struct data_coeff_matrix {
 	struct data_coeff_block *blocks;
 };
 
-/* Reference: circ.h:169-178 (without the coefficient-matrix scratch). */
+/* Reference: circ.h:169-178. */
 struct circ {
 	struct circ_hamil hm;
 	struct circ_muldet md;
@@ -80,6 +81,7 @@ struct circ {
 	struct qreg reg;
 	enum stprep_kind stprep_kind;
 	struct data_coeff_matrix cm;
+	struct state_prep_coeff_scratch sp_scratch;
 };
 
 /* Carriers (reference: circ.h:202-226).  _init: 0 or -1; _free idempotent. */

@@ -42,6 +42,21 @@ def term_records(flip, phase, cf) -> np.ndarray:
     return rec
 
 
+def coeff_arrays(cm):
+    """(ncomp, weights, Ca, Cb) flat float64 arrays of a coefficient-matrix
+    state given as an object with n_sites, n_alpha, n_beta, C_alpha (list),
+    C_beta (list or None), weights (list or None)."""
+    ncomp = 0 if cm.weights is None else len(cm.weights)
+    w = np.asarray(cm.weights if ncomp else [1.0], dtype=np.float64)
+    ca = np.concatenate([np.ascontiguousarray(a, dtype=np.float64).ravel()
+                         for a in cm.C_alpha])
+    cb = None
+    if cm.C_beta is not None:
+        cb = np.concatenate([np.ascontiguousarray(b, dtype=np.float64).ravel()
+                             for b in cm.C_beta])
+    return ncomp, w, ca, cb
+
+
 def _dets(idx, cf):
     idx = np.ascontiguousarray(idx, dtype=np.uint64)
     cf = np.ascontiguousarray(cf, dtype=np.complex128).view(np.float64)
@@ -93,7 +108,36 @@ class Oracle:
         L.orc_phase2_run.argtypes = [_P(C.c_char_p), _D, C.c_size_t,
                                      C.c_double, C.c_char_p, _D, _D]
         L.orc_phase2_run.restype = C.c_int
+        cm_args = [C.c_uint32] * 4 + [C.c_int, C.c_size_t, _D, _D, _D]
+        L.orc_coeff_expand_all.argtypes = cm_args + [_D]
+        L.orc_coeff_expand_all.restype = C.c_int
+        L.orc_coeff_inner.argtypes = cm_args + [_D, _D]
+        L.orc_coeff_inner.restype = C.c_int
         self.L = L
+
+    # -- coefficient-matrix trial state
+    def coeff_expand(self, nqb, cm) -> np.ndarray:
+        ncomp, w, ca, cb = coeff_arrays(cm)
+        amp = np.zeros(1 << nqb, dtype=np.complex128)
+        if self.L.orc_coeff_expand_all(
+                nqb, cm.n_sites, cm.n_alpha, cm.n_beta, int(cm.tapered),
+                ncomp, _dptr(w), _dptr(ca),
+                None if cb is None else _dptr(cb),
+                _dptr(amp.view(np.float64))):
+            raise RuntimeError("oracle coeff_expand failed")
+        return amp
+
+    def coeff_inner(self, nqb, cm, amp) -> complex:
+        ncomp, w, ca, cb = coeff_arrays(cm)
+        a = np.ascontiguousarray(amp, dtype=np.complex128)
+        out = np.zeros(2)
+        if self.L.orc_coeff_inner(
+                nqb, cm.n_sites, cm.n_alpha, cm.n_beta, int(cm.tapered),
+                ncomp, _dptr(w), _dptr(ca),
+                None if cb is None else _dptr(cb),
+                _dptr(a.view(np.float64)), _dptr(out)):
+            raise RuntimeError("oracle coeff_inner failed")
+        return complex(out[0], out[1])
 
     # -- primitives
     def rng_sequence(self, seed: int, n: int) -> list[int]:
@@ -213,7 +257,35 @@ class Reference:
         L.phase2_run.argtypes = [_P(C.c_char_p), _D, C.c_size_t, C.c_double,
                                  C.c_char_p, _D, _D]
         L.phase2_run.restype = C.c_int
+        cm_args = [C.c_uint32] * 4 + [C.c_int, C.c_size_t, _D, _D, _D]
+        L.refh_coeff_expand_all.argtypes = cm_args + [_D]
+        L.refh_coeff_expand_all.restype = C.c_int
+        L.refh_coeff_inner.argtypes = cm_args + [_D, _D]
+        L.refh_coeff_inner.restype = C.c_int
         self.L = L
+
+    def coeff_expand(self, nqb, cm) -> np.ndarray:
+        ncomp, w, ca, cb = coeff_arrays(cm)
+        amp = np.zeros(1 << nqb, dtype=np.complex128)
+        if self.L.refh_coeff_expand_all(
+                nqb, cm.n_sites, cm.n_alpha, cm.n_beta, int(cm.tapered),
+                ncomp, _dptr(w), _dptr(ca),
+                None if cb is None else _dptr(cb),
+                _dptr(amp.view(np.float64))):
+            raise RuntimeError("reference coeff_expand failed")
+        return amp
+
+    def coeff_inner(self, nqb, cm, amp) -> complex:
+        ncomp, w, ca, cb = coeff_arrays(cm)
+        a = np.ascontiguousarray(amp, dtype=np.complex128)
+        out = np.zeros(2)
+        if self.L.refh_coeff_inner(
+                nqb, cm.n_sites, cm.n_alpha, cm.n_beta, int(cm.tapered),
+                ncomp, _dptr(w), _dptr(ca),
+                None if cb is None else _dptr(cb),
+                _dptr(a.view(np.float64)), _dptr(out)):
+            raise RuntimeError("reference coeff_inner failed")
+        return complex(out[0], out[1])
 
     def paulirot(self, amp, nqb, flip, phase, phi):
         a = np.ascontiguousarray(amp, dtype=np.complex128).copy()

@@ -545,3 +545,228 @@ double orc_norm2(const double *amp, uint32_t nqb)
 		s += amp[i] * amp[i];
 	return s;
 }
+
+/* ---- coefficient-matrix trial state ------------------------------------ */
+
+#define ORC_CM_MAX_K 32
+
+/* k-subsets of {0..n-1} in lex order (lib/combinations.c:45-98); returns
+ * the count, tuples of k entries in out (NULL: count only). */
+static size_t orc_subsets(uint32_t n, uint32_t k, uint32_t *out)
+{
+	uint32_t c[ORC_CM_MAX_K];
+	if (k > n || k > ORC_CM_MAX_K)
+		return 0;
+	for (uint32_t i = 0; i < k; i++)
+		c[i] = i;
+	size_t m = 0;
+	for (;;) {
+		if (out)
+			memcpy(out + m * (k ? k : 1), c, sizeof(uint32_t) * k);
+		m++;
+		int32_t j = (int32_t)k - 1;
+		while (j >= 0 && c[j] == n - k + (uint32_t)j)
+			j--;
+		if (j < 0)
+			return m;
+		c[j]++;
+		for (uint32_t i = (uint32_t)j + 1; i < k; i++)
+			c[i] = c[i - 1] + 1;
+	}
+}
+
+/* LU with partial pivoting (lib/det_small.c:27-71); a is overwritten. */
+static double orc_det(double *a, uint32_t n)
+{
+	if (n == 0)
+		return 1.0;
+	double det = 1.0;
+	for (uint32_t k = 0; k < n; k++) {
+		uint32_t piv = k;
+		double mx = fabs(a[k * n + k]);
+		for (uint32_t i = k + 1; i < n; i++)
+			if (fabs(a[i * n + k]) > mx) {
+				mx = fabs(a[i * n + k]);
+				piv = i;
+			}
+		if (mx == 0.0)
+			return 0.0;
+		if (piv != k) {
+			for (uint32_t j = k; j < n; j++) {
+				const double t = a[k * n + j];
+				a[k * n + j] = a[piv * n + j];
+				a[piv * n + j] = t;
+			}
+			det = -det;
+		}
+		const double p = a[k * n + k];
+		det *= p;
+		const double ip = 1.0 / p;
+		for (uint32_t i = k + 1; i < n; i++) {
+			const double f = a[i * n + k] * ip;
+			if (f == 0.0)
+				continue;
+			for (uint32_t j = k + 1; j < n; j++)
+				a[i * n + j] -= f * a[k * n + j];
+		}
+	}
+	return det;
+}
+
+/* det(C[tuple, :]) for each tuple (state_prep_coeff.c:102-122). */
+static void orc_tuple_dets(const double *C, uint32_t k, const uint32_t *tup,
+	size_t m, double *out)
+{
+	double a[ORC_CM_MAX_K * ORC_CM_MAX_K];
+	for (size_t i = 0; i < m; i++) {
+		for (uint32_t r = 0; r < k; r++)
+			for (uint32_t c = 0; c < k; c++)
+				a[r * k + c] = C[tup[i * k + r] * k + c];
+		out[i] = orc_det(a, k);
+	}
+}
+
+struct orc_cm {
+	uint32_t n_sites, na, nb;
+	size_t Ma, Mb;
+	uint32_t *ta, *tb;
+	double *da, *db;
+};
+
+static int orc_cm_init(struct orc_cm *s, uint32_t nqb, uint32_t n_sites,
+	uint32_t na, uint32_t nb, int tapered)
+{
+	memset(s, 0, sizeof *s);
+	if (na > n_sites || nb > n_sites || n_sites == 0 || n_sites > 32 ||
+		(tapered ? 2 * n_sites - 2 : 2 * n_sites) > nqb)
+		return -1;
+	s->n_sites = n_sites;
+	s->na = na;
+	s->nb = nb;
+	s->Ma = orc_subsets(n_sites, na, NULL);
+	s->Mb = orc_subsets(n_sites, nb, NULL);
+	s->ta = malloc(sizeof *s->ta * s->Ma * (na ? na : 1));
+	s->tb = malloc(sizeof *s->tb * s->Mb * (nb ? nb : 1));
+	s->da = malloc(sizeof *s->da * s->Ma);
+	s->db = malloc(sizeof *s->db * s->Mb);
+	if (!s->ta || !s->tb || !s->da || !s->db)
+		return -1;
+	orc_subsets(n_sites, na, s->ta);
+	orc_subsets(n_sites, nb, s->tb);
+	return 0;
+}
+
+static void orc_cm_free(struct orc_cm *s)
+{
+	free(s->ta);
+	free(s->tb);
+	free(s->da);
+	free(s->db);
+}
+
+/* Index of tuple pair (i, j): alpha bits, beta bits above n_sites, and
+ * for tapered states bits 0 and n_sites dropped (state_prep_coeff.c:34-54). */
+static uint64_t orc_cm_index(const struct orc_cm *s, size_t i, size_t j,
+	int tapered)
+{
+	uint64_t idx = 0;
+	for (uint32_t r = 0; r < s->na; r++)
+		idx |= UINT64_C(1) << s->ta[i * s->na + r];
+	for (uint32_t r = 0; r < s->nb; r++)
+		idx |= UINT64_C(1) << (s->n_sites + s->tb[j * s->nb + r]);
+	if (tapered) {
+		const uint64_t lo =
+			(idx >> 1) & ((UINT64_C(1) << (s->n_sites - 1)) - 1);
+		idx = lo | ((idx >> (s->n_sites + 1)) << (s->n_sites - 1));
+	}
+	return idx;
+}
+
+/* One block: write (accumulate 0) or add the products weight * da * db
+ * not below 1e-12 in magnitude (state_prep_coeff.c:156-196). */
+static void orc_cm_block(struct orc_cm *s, const double *Ca, const double *Cb,
+	double weight, int tapered, int accumulate, double *amp)
+{
+	orc_tuple_dets(Ca, s->na, s->ta, s->Ma, s->da);
+	orc_tuple_dets(Cb ? Cb : Ca, s->nb, s->tb, s->Mb, s->db);
+	for (size_t i = 0; i < s->Ma; i++)
+		for (size_t j = 0; j < s->Mb; j++) {
+			const double cf = weight * s->da[i] * s->db[j];
+			if (fabs(cf) < 1.0e-12)
+				continue;
+			const uint64_t idx = orc_cm_index(s, i, j, tapered);
+			if (accumulate) {
+				amp[2 * idx] += cf;
+			} else {
+				amp[2 * idx] = cf;
+				amp[2 * idx + 1] = 0.0;
+			}
+		}
+}
+
+int orc_coeff_expand_all(uint32_t nqb, uint32_t n_sites, uint32_t na,
+	uint32_t nb, int tapered, size_t ncomp, const double *w,
+	const double *Ca, const double *Cb, double *amp)
+{
+	struct orc_cm s;
+	if (orc_cm_init(&s, nqb, n_sites, na, nb, tapered) < 0) {
+		orc_cm_free(&s);
+		return -1;
+	}
+	memset(amp, 0, sizeof(double) * 2 * (UINT64_C(1) << nqb));
+	if (ncomp == 0)
+		orc_cm_block(&s, Ca, Cb, 1.0, tapered, 0, amp);
+	for (size_t k = 0; k < ncomp; k++)
+		orc_cm_block(&s, Ca + k * (size_t)n_sites * na,
+			Cb ? Cb + k * (size_t)n_sites * nb : NULL, w[k], tapered,
+			1, amp);
+	orc_cm_free(&s);
+	return 0;
+}
+
+/* Sequential sum of cf * a over one block (state_prep_coeff.c:199-244). */
+static void orc_cm_inner_block(struct orc_cm *s, const double *Ca,
+	const double *Cb, double weight, int tapered, const double *amp,
+	double *re, double *im)
+{
+	orc_tuple_dets(Ca, s->na, s->ta, s->Ma, s->da);
+	orc_tuple_dets(Cb ? Cb : Ca, s->nb, s->tb, s->Mb, s->db);
+	double ar = 0.0, ai = 0.0;
+	for (size_t i = 0; i < s->Ma; i++)
+		for (size_t j = 0; j < s->Mb; j++) {
+			const double cf = weight * s->da[i] * s->db[j];
+			if (fabs(cf) < 1.0e-12)
+				continue;
+			const uint64_t idx = orc_cm_index(s, i, j, tapered);
+			ar += cf * amp[2 * idx];
+			ai += cf * amp[2 * idx + 1];
+		}
+	*re = ar;
+	*im = ai;
+}
+
+int orc_coeff_inner(uint32_t nqb, uint32_t n_sites, uint32_t na, uint32_t nb,
+	int tapered, size_t ncomp, const double *w, const double *Ca,
+	const double *Cb, const double *amp, double *out)
+{
+	struct orc_cm s;
+	if (orc_cm_init(&s, nqb, n_sites, na, nb, tapered) < 0) {
+		orc_cm_free(&s);
+		return -1;
+	}
+	double pr = 0.0, pi = 0.0, zr, zi;
+	if (ncomp == 0) {
+		orc_cm_inner_block(&s, Ca, Cb, 1.0, tapered, amp, &pr, &pi);
+	}
+	for (size_t k = 0; k < ncomp; k++) {
+		orc_cm_inner_block(&s, Ca + k * (size_t)n_sites * na,
+			Cb ? Cb + k * (size_t)n_sites * nb : NULL, w[k], tapered,
+			amp, &zr, &zi);
+		pr += zr;
+		pi += zi;
+	}
+	out[0] = pr;
+	out[1] = pi;
+	orc_cm_free(&s);
+	return 0;
+}

@@ -104,4 +104,21 @@ int orc_phase2_run(const char **pauli_strs, const double *coeffs,
 /* Squared norm with a plain sequential sum (diagnostics). */
 double orc_norm2(const double *amp, uint32_t nqb);
 
+/*
+ * Coefficient-matrix trial state (phase2/state_prep_coeff.c:156-325).
+ * Blocks: ncomp weights w with matrices Ca + k*n_sites*na and
+ * Cb + k*n_sites*nb (Cb NULL = closed shell, C_beta = C_alpha); ncomp == 0
+ * is the single block of weight 1.0 carried by Ca/Cb.
+ * orc_coeff_expand_all: amp (2*2^nqb doubles) <- the expanded state
+ * (state_prep_coeff_expand_all).  orc_coeff_inner: out <- sum over blocks
+ * of the sequential inner product with amp (circ.c:315-336).  -1 on bad
+ * sizes.
+ */
+int orc_coeff_expand_all(uint32_t nqb, uint32_t n_sites, uint32_t na,
+	uint32_t nb, int tapered, size_t ncomp, const double *w,
+	const double *Ca, const double *Cb, double *amp);
+int orc_coeff_inner(uint32_t nqb, uint32_t n_sites, uint32_t na, uint32_t nb,
+	int tapered, size_t ncomp, const double *w, const double *Ca,
+	const double *Cb, const double *amp, double *out);
+
 #endif /* PHASE2_ORACLE_H */

@@ -7,7 +7,9 @@
  * make_golden.py and the not-gpu pin tests) calls these to obtain answers
  * from the unmodified reference code: qreg_paulirot (phase2/qreg.c:135-142),
  * trott_simul (circ/trott.c:44-65), trott2_simul (circ/trott2.c:44-74),
- * qdrift_simul (circ/qdrift.c:105-134), cmpsit_simul (circ/cmpsit.c:208-235).
+ * qdrift_simul (circ/qdrift.c:105-134), cmpsit_simul (circ/cmpsit.c:208-235),
+ * and the coefficient-matrix state prep and overlap
+ * (phase2/state_prep_coeff.c:156-325).
  *
  * Term records use the reference layout struct circ_hamil_term
  * {double cf; struct paulis op;} (include/phase2/circ.h:48-55).
@@ -23,6 +25,7 @@
 #include "circ/trott.h"
 #include "circ/trott2.h"
 #include "phase2.h"
+#include "phase2/state_prep_coeff.h"
 
 #include "circ_cache.h"
 
@@ -215,5 +218,112 @@ int refh_cmpsit(uint32_t nqb, const void *terms, size_t nterms,
 	const int rc = cmpsit_simul(&cp);
 	store_vals(&cp.ct.vals, out_z);
 	cmpsit_free(&cp);
+	return rc;
+}
+
+/*
+ * Coefficient-matrix trial state (phase2/state_prep_coeff.c:156-325) on an
+ * nqb-qubit reference register.  Blocks: ncomp weights w and matrices
+ * Ca[k*n_sites*na ...], Cb[k*n_sites*nb ...] (Cb NULL = closed shell).
+ * ncomp == 0 means one block of weight 1.0 carried by Ca/Cb (the
+ * single-block case of data_coeff_matrix).
+ *
+ * refh_coeff_expand_all: the state after state_prep_coeff_expand_all
+ * (2*2^nqb doubles out).
+ * refh_coeff_inner: amp (in) is loaded into the register, then the sum of
+ * state_prep_coeff_inner over the blocks in order, as circ.c measure_coeff
+ * does (out: 2 doubles).
+ */
+static void fill_cm(struct data_coeff_matrix *cm, struct data_coeff_block *bl,
+	uint32_t nqb, uint32_t n_sites, uint32_t na, uint32_t nb, int tapered,
+	size_t ncomp, const double *w, const double *Ca, const double *Cb)
+{
+	memset(cm, 0, sizeof *cm);
+	cm->nqb = nqb;
+	cm->n_sites = n_sites;
+	cm->n_alpha = na;
+	cm->n_beta = nb;
+	cm->closed_shell = Cb == NULL;
+	cm->tapered = tapered;
+	cm->n_components = ncomp;
+	if (ncomp == 0) {
+		cm->C_alpha = Ca;
+		cm->C_beta = Cb;
+		return;
+	}
+	for (size_t k = 0; k < ncomp; k++) {
+		bl[k].cf = w[k];
+		bl[k].C_alpha = Ca + k * (size_t)n_sites * na;
+		bl[k].C_beta = Cb ? Cb + k * (size_t)n_sites * nb : NULL;
+	}
+	cm->blocks = bl;
+}
+
+int refh_coeff_expand_all(uint32_t nqb, uint32_t n_sites, uint32_t na,
+	uint32_t nb, int tapered, size_t ncomp, const double *w,
+	const double *Ca, const double *Cb, double *amp)
+{
+	if (ensure_world() < 0)
+		return -1;
+	struct qreg reg;
+	if (qreg_init(&reg, nqb) < 0)
+		return -1;
+	struct data_coeff_block *bl = calloc(ncomp ? ncomp : 1, sizeof *bl);
+	struct data_coeff_matrix cm;
+	struct state_prep_coeff_scratch sc;
+	int rc = -1;
+	if (bl && state_prep_coeff_scratch_init(&sc, n_sites, na, nb) == 0) {
+		fill_cm(&cm, bl, nqb, n_sites, na, nb, tapered, ncomp, w, Ca,
+			Cb);
+		rc = state_prep_coeff_expand_all(&reg, &sc, &cm);
+		for (uint64_t i = 0; i < reg.namp; i++) {
+			amp[2 * i] = creal(reg.amp[i]);
+			amp[2 * i + 1] = cimag(reg.amp[i]);
+		}
+		state_prep_coeff_scratch_free(&sc);
+	}
+	free(bl);
+	qreg_free(&reg);
+	return rc;
+}
+
+int refh_coeff_inner(uint32_t nqb, uint32_t n_sites, uint32_t na,
+	uint32_t nb, int tapered, size_t ncomp, const double *w,
+	const double *Ca, const double *Cb, const double *amp, double *out)
+{
+	if (ensure_world() < 0)
+		return -1;
+	struct qreg reg;
+	if (qreg_init(&reg, nqb) < 0)
+		return -1;
+	for (uint64_t i = 0; i < reg.namp; i++)
+		reg.amp[i] = CMPLX(amp[2 * i], amp[2 * i + 1]);
+	struct data_coeff_block *bl = calloc(ncomp ? ncomp : 1, sizeof *bl);
+	struct data_coeff_matrix cm;
+	struct state_prep_coeff_scratch sc;
+	int rc = -1;
+	if (bl && state_prep_coeff_scratch_init(&sc, n_sites, na, nb) == 0) {
+		fill_cm(&cm, bl, nqb, n_sites, na, nb, tapered, ncomp, w, Ca,
+			Cb);
+		_Complex double pr = 0.0, z = 0.0;
+		rc = 0;
+		if (ncomp == 0) {
+			rc = state_prep_coeff_inner(&reg, &sc, Ca, Cb, 1.0,
+				tapered, &z);
+			pr = z;
+		} else {
+			for (size_t k = 0; k < ncomp && rc == 0; k++) {
+				rc = state_prep_coeff_inner(&reg, &sc,
+					bl[k].C_alpha, bl[k].C_beta, bl[k].cf,
+					tapered, &z);
+				pr += z;
+			}
+		}
+		out[0] = creal(pr);
+		out[1] = cimag(pr);
+		state_prep_coeff_scratch_free(&sc);
+	}
+	free(bl);
+	qreg_free(&reg);
 	return rc;
 }

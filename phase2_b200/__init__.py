@@ -123,6 +123,84 @@ class Dets:
         return len(self.idx)
 
 
+@dataclass
+class CoeffMatrix:
+    """Coefficient-matrix trial state (Slater-Condon expansion): blocks of
+    real orbital coefficients C_alpha[k] (n_sites x n_alpha) and C_beta[k]
+    (n_sites x n_beta; None = closed shell, C_beta = C_alpha) with weights
+    (None = the single block of weight 1).  tapered drops qubits 0 and
+    n_sites.  Used as the initial state / overlap trial of the drivers in
+    place of Dets."""
+    n_sites: int
+    n_alpha: int
+    n_beta: int
+    C_alpha: list
+    C_beta: list | None = None
+    weights: list | None = None
+    tapered: bool = False
+
+    def blocks(self):
+        nb = len(self.C_alpha)
+        w = self.weights if self.weights is not None else [1.0]
+        cb = self.C_beta if self.C_beta is not None else [None] * nb
+        return list(zip(w, self.C_alpha, cb))
+
+
+_libc = None
+
+
+def _malloc_copy(arr) -> int:
+    """A malloc'ed copy of a float64 array (the library frees it)."""
+    global _libc
+    if _libc is None:
+        _libc = C.CDLL(None)
+        _libc.malloc.restype = C.c_void_p
+        _libc.malloc.argtypes = [C.c_size_t]
+    a = np.ascontiguousarray(arr, dtype=np.float64)
+    p = _libc.malloc(max(1, a.nbytes))
+    if not p:
+        raise MemoryError("malloc")
+    C.memmove(p, a.ctypes.data, a.nbytes)
+    return p
+
+
+def _coeff_matrix(nqb: int, cm: CoeffMatrix) -> _ffi.CoeffMatrix:
+    """struct data_coeff_matrix with malloc'ed arrays, adopted by circ_init
+    (freed by data_coeff_matrix_free)."""
+    out = _ffi.CoeffMatrix()
+    out.nqb, out.n_sites = nqb, cm.n_sites
+    out.n_alpha, out.n_beta = cm.n_alpha, cm.n_beta
+    out.closed_shell = 1 if cm.C_beta is None else 0
+    out.tapered = 1 if cm.tapered else 0
+    if cm.weights is None:
+        out.n_components = 0
+        out.C_alpha = _malloc_copy(cm.C_alpha[0])
+        out.C_beta = (None if cm.C_beta is None
+                      else _malloc_copy(cm.C_beta[0]))
+        out.blocks = None
+        return out
+    n = len(cm.weights)
+    out.n_components = n
+    out.C_alpha = out.C_beta = None
+    bl = _libc.malloc(C.sizeof(_ffi.CoeffBlock) * n)
+    arr = (_ffi.CoeffBlock * n).from_address(bl)
+    for k, (w, ca, cb) in enumerate(cm.blocks()):
+        arr[k].cf = float(w)
+        arr[k].C_alpha = _malloc_copy(ca)
+        arr[k].C_beta = None if cb is None else _malloc_copy(cb)
+    out.blocks = bl
+    return out
+
+
+def _initial_state(nqb: int, dets):
+    """(stprep kind, pointer, keep-alive) for Dets or CoeffMatrix."""
+    if isinstance(dets, CoeffMatrix):
+        cm = _coeff_matrix(nqb, dets)
+        return _ffi.STPREP_COEFF_MATRIX, C.cast(C.pointer(cm), C.c_void_p), cm
+    md = _muldet(dets)
+    return _ffi.STPREP_MULTIDET, C.cast(C.pointer(md), C.c_void_p), md
+
+
 def _hamil(nqb: int, terms: Terms) -> _ffi.CircHamil:
     L = lib()
     hm = _ffi.CircHamil()
@@ -257,6 +335,50 @@ class Register:
             raise RuntimeError("qreg_inner_dense failed")
         return complex(out[0], out[1])
 
+    def _coeff_call(self, fn, cm: CoeffMatrix, *tail):
+        sc = _ffi.CoeffScratch()
+        if self._L.state_prep_coeff_scratch_init(
+                C.byref(sc), cm.n_sites, cm.n_alpha, cm.n_beta) != 0:
+            raise ValueError("coefficient matrix sizes out of range")
+        try:
+            return fn(sc, *tail)
+        finally:
+            self._L.state_prep_coeff_scratch_free(C.byref(sc))
+
+    def coeff_expand(self, cm: CoeffMatrix) -> None:
+        """Zero the register and expand the trial state on the device
+        (state_prep_coeff_expand_all)."""
+        m = _coeff_matrix(self.nqb, cm)
+        try:
+            def run(sc):
+                if self._L.state_prep_coeff_expand_all(
+                        C.byref(self.reg), C.byref(sc), C.byref(m)) != 0:
+                    raise RuntimeError("state_prep_coeff_expand_all failed")
+            self._coeff_call(run, cm)
+        finally:
+            self._L.data_coeff_matrix_free(C.byref(m))
+
+    def coeff_inner(self, cm: CoeffMatrix) -> complex:
+        """<trial|psi> summed over the blocks in order (device reduction;
+        the measure of the coefficient-matrix drivers)."""
+        def run(sc):
+            tot = 0j
+            for w, ca, cb in cm.blocks():
+                a = np.ascontiguousarray(ca, dtype=np.float64)
+                b = (None if cb is None
+                     else np.ascontiguousarray(cb, dtype=np.float64))
+                z = (C.c_double * 2)()
+                if self._L.state_prep_coeff_inner(
+                        C.byref(self.reg), C.byref(sc),
+                        a.ctypes.data_as(C.POINTER(C.c_double)),
+                        None if b is None else
+                        b.ctypes.data_as(C.POINTER(C.c_double)),
+                        float(w), int(cm.tapered), z) != 0:
+                    raise RuntimeError("state_prep_coeff_inner failed")
+                tot += complex(z[0], z[1])
+            return tot
+        return self._coeff_call(run, cm)
+
     def set_timing(self, on: bool) -> None:
         self._L.qreg_set_timing(C.byref(self.reg), int(on))
 
@@ -272,10 +394,11 @@ class Register:
 # ---- drivers -----------------------------------------------------------
 
 
-def _run_driver(kind: str, nqb: int, terms: Terms, dets: Dets, **kw):
+def _run_driver(kind: str, nqb: int, terms: Terms, dets, **kw):
     world_ensure()
     L = lib()
-    hm, md = _hamil(nqb, terms), _muldet(dets)
+    hm = _hamil(nqb, terms)
+    sp_kind, sp_ptr, _keep = _initial_state(nqb, dets)
     if kind in ("trott", "trott2"):
         obj = (_ffi.Trott if kind == "trott" else _ffi.Trott2)()
         dt = _ffi.TrottData(kw["steps"], kw["delta"])
@@ -289,8 +412,7 @@ def _run_driver(kind: str, nqb: int, terms: Terms, dets: Dets, **kw):
                              kw["depth"], kw["angle_det"], kw["angle_rand"],
                              kw["seed"])
     init = getattr(L, f"{kind}_init")
-    if init(C.byref(obj), C.byref(dt), hm, _ffi.STPREP_MULTIDET,
-            C.cast(C.pointer(md), C.c_void_p), None) != 0:
+    if init(C.byref(obj), C.byref(dt), hm, sp_kind, sp_ptr, None) != 0:
         raise RuntimeError(f"{kind}_init failed")
     try:
         if kw.get("fusion") is not None:
@@ -334,11 +456,12 @@ def batch(kind: str, problems: list[dict], with_stats: bool = False):
     try:
         for p in problems:
             obj = cls()
-            hm, md = _hamil(p["nqb"], p["terms"]), _muldet(p["dets"])
+            hm = _hamil(p["nqb"], p["terms"])
+            sp_kind, sp_ptr, _keep = _initial_state(p["nqb"], p["dets"])
             dt = _driver_data(kind, p)
             if getattr(L, f"{kind}_init")(
-                    C.byref(obj), C.byref(dt), hm, _ffi.STPREP_MULTIDET,
-                    C.cast(C.pointer(md), C.c_void_p), None) != 0:
+                    C.byref(obj), C.byref(dt), hm, sp_kind, sp_ptr,
+                    None) != 0:
                 raise RuntimeError(f"{kind}_init failed")
             objs.append(obj)
         arr = (C.c_void_p * max(1, len(objs)))(

@@ -68,11 +68,24 @@ class CoeffMatrix(C.Structure):
                 ("C_beta", C.c_void_p), ("blocks", C.c_void_p)]
 
 
+class CoeffBlock(C.Structure):
+    _fields_ = [("cf", C.c_double), ("C_alpha", C.c_void_p),
+                ("C_beta", C.c_void_p)]
+
+
+class CoeffScratch(C.Structure):
+    _fields_ = [("n_sites", C.c_uint32), ("n_alpha", C.c_uint32),
+                ("n_beta", C.c_uint32), ("tup_a", C.c_void_p),
+                ("tup_b", C.c_void_p), ("det_a", C.c_void_p),
+                ("det_b", C.c_void_p), ("Ma", C.c_size_t),
+                ("Mb", C.c_size_t)]
+
+
 class Circ(C.Structure):
     _fields_ = [("hm", CircHamil), ("md", CircMuldet),
                 ("cache", C.c_void_p), ("vals", CircValues),
                 ("reg", Qreg), ("stprep_kind", C.c_int),
-                ("cm", CoeffMatrix)]
+                ("cm", CoeffMatrix), ("sp_scratch", CoeffScratch)]
 
 
 class TrottData(C.Structure):
@@ -170,6 +183,7 @@ PREC_FP64 = 0
 PREC_FP32 = 1
 ORDER_LEX, ORDER_GIVEN, ORDER_FLIP = 0, 1, 2
 STPREP_MULTIDET = 1
+STPREP_COEFF_MATRIX = 2
 WORLD_READY = 0
 
 # ---- loading -----------------------------------------------------------
@@ -267,6 +281,18 @@ _SIGS = {
     "phase2_get_precision": (C.c_int, []),
     "phase2_set_fp32_form": (C.c_int, [C.c_int]),
     "phase2_set_batch_persistent": (C.c_int, [C.c_int]),
+    "state_prep_coeff_scratch_init": (C.c_int, [C.c_void_p, C.c_uint32,
+                                                C.c_uint32, C.c_uint32]),
+    "state_prep_coeff_scratch_free": (None, [C.c_void_p]),
+    "state_prep_coeff_expand_all": (C.c_int, [C.c_void_p, C.c_void_p,
+                                              C.c_void_p]),
+    "state_prep_coeff_expand": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_void_p, C.c_double, C.c_int,
+                                          C.c_int]),
+    "state_prep_coeff_inner": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_void_p, C.c_double, C.c_int,
+                                         C.c_void_p]),
+    "data_coeff_matrix_free": (None, [C.c_void_p]),
     "phase2_get_fp32_form": (C.c_int, []),
     "phase2_set_fusion": (C.c_int, [C.c_int, C.c_int]),
     "phase2_set_term_order": (C.c_int, [C.c_int]),

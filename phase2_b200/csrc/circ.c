@@ -12,6 +12,10 @@
  *                      (circ.c:338-350), evaluated on the host from one
  *                      batched device gather, with the same expression so
  *                      the FP64 result is bit-identical.
+ *
+ * and for the coefficient-matrix state (state_prep.c, on the device):
+ * circ_prepst expands it (circ.c:225-229), circ_measure sums the blocks'
+ * inner products in order (circ.c:303-336).
  */
 #include <complex.h>
 #include <stdint.h>
@@ -147,10 +151,12 @@ void circ_values_free(struct circ_values *vals)
 
 static void free_payload(struct circ *ct, enum stprep_kind kind)
 {
-	if (kind == STPREP_MULTIDET)
+	if (kind == STPREP_MULTIDET) {
 		circ_muldet_free(&ct->md);
-	else if (kind == STPREP_COEFF_MATRIX)
+	} else if (kind == STPREP_COEFF_MATRIX) {
 		data_coeff_matrix_free(&ct->cm);
+		state_prep_coeff_scratch_free(&ct->sp_scratch);
+	}
 }
 
 int circ_init(struct circ *ct, struct circ_hamil hm, enum stprep_kind sp_kind,
@@ -158,6 +164,7 @@ int circ_init(struct circ *ct, struct circ_hamil hm, enum stprep_kind sp_kind,
 {
 	memset(&ct->md, 0, sizeof ct->md);
 	memset(&ct->cm, 0, sizeof ct->cm);
+	memset(&ct->sp_scratch, 0, sizeof ct->sp_scratch);
 	memset(&ct->reg, 0, sizeof ct->reg);
 	memset(&ct->vals, 0, sizeof ct->vals);
 	ct->cache = NULL;
@@ -170,9 +177,12 @@ int circ_init(struct circ *ct, struct circ_hamil hm, enum stprep_kind sp_kind,
 		break;
 	case STPREP_COEFF_MATRIX:
 		ct->cm = *(const struct data_coeff_matrix *)sp_data;
-		log_error("circ_init: coefficient-matrix state prep is not"
-			  " supported by this library");
-		goto err;
+		if (state_prep_coeff_scratch_init(&ct->sp_scratch,
+			    ct->cm.n_sites, ct->cm.n_alpha, ct->cm.n_beta) < 0) {
+			log_error("circ_init: sp_scratch init failed");
+			goto err;
+		}
+		break;
 	default:
 		log_error("circ_init: unknown state-prep kind %d", (int)sp_kind);
 		goto err;
@@ -215,6 +225,9 @@ void circ_free(struct circ *ct)
 
 int circ_prepst(struct circ *ct)
 {
+	if (ct->stprep_kind == STPREP_COEFF_MATRIX)
+		return state_prep_coeff_expand_all(&ct->reg, &ct->sp_scratch,
+			&ct->cm);
 	if (ct->stprep_kind != STPREP_MULTIDET)
 		return -1;
 	qreg_zero(&ct->reg);
@@ -279,8 +292,34 @@ _Complex double p2_circ_overlap(const struct circ_muldet *md,
 	return pr;
 }
 
+/* <trial | evolved> of a coefficient-matrix trial state: the single block,
+ * or the sum over blocks in order (reference: circ.c:315-336). */
+static _Complex double measure_coeff(struct circ *ct)
+{
+	const struct data_coeff_matrix *cm = &ct->cm;
+	_Complex double pr = 0.0, z;
+	if (cm->n_components == 0) {
+		if (state_prep_coeff_inner(&ct->reg, &ct->sp_scratch,
+			    cm->C_alpha, cm->closed_shell ? NULL : cm->C_beta,
+			    1.0, cm->tapered, &z) == 0)
+			pr = z;
+		return pr;
+	}
+	for (size_t k = 0; k < cm->n_components; k++) {
+		const struct data_coeff_block *b = &cm->blocks[k];
+		if (state_prep_coeff_inner(&ct->reg, &ct->sp_scratch,
+			    b->C_alpha, cm->closed_shell ? NULL : b->C_beta,
+			    b->cf, cm->tapered, &z) < 0)
+			z = 0.0;
+		pr += z;
+	}
+	return pr;
+}
+
 _Complex double circ_measure(struct circ *ct)
 {
+	if (ct->stprep_kind == STPREP_COEFF_MATRIX)
+		return measure_coeff(ct);
 	if (ct->stprep_kind != STPREP_MULTIDET)
 		return 0.0;
 	const struct circ_muldet *md = &ct->md;

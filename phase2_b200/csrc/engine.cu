@@ -83,6 +83,9 @@ struct p2_dev {
 	double *d_part;
 	size_t part_cap;
 
+	unsigned char *d_cm; /* coefficient-matrix tables */
+	size_t cm_cap;
+
 	int timing;
 	cudaEvent_t t0, t1;
 
@@ -1133,6 +1136,31 @@ __device__ __forceinline__ double p2_warp_sum(double v)
 	return v;
 }
 
+/* A block's two compensated per-thread sums -> part[2*block + {0,1}]:
+ * warp-shuffle tree, then one pass over the warp totals in shared memory. */
+__device__ __forceinline__ void p2_block_sum2(double vr, double vi,
+	double *__restrict__ part)
+{
+	vr = p2_warp_sum(vr);
+	vi = p2_warp_sum(vi);
+	__shared__ double wr[P2_RED_TPB / 32], wi[P2_RED_TPB / 32];
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	if (lane == 0) {
+		wr[warp] = vr;
+		wi[warp] = vi;
+	}
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double s0 = 0.0, c0 = 0.0, s1 = 0.0, c1 = 0.0;
+		for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+			p2_neumaier(s0, c0, wr[w]);
+			p2_neumaier(s1, c1, wi[w]);
+		}
+		part[2 * blockIdx.x] = s0 + c0;
+		part[2 * blockIdx.x + 1] = s1 + c1;
+	}
+}
+
 /* Stage 1: per-block sums of |a|^2 (trial == NULL) or of conj(trial) * a,
  * written to part[2*block + {0,1}].  Each thread accumulates its strided
  * elements with compensation, then a warp-shuffle tree and one pass over
@@ -1156,23 +1184,94 @@ __global__ void __launch_bounds__(P2_RED_TPB) k_reduce_partial(
 			p2_neumaier(sr, cr, re * re + im * im);
 		}
 	}
-	double vr = p2_warp_sum(sr + cr), vi = p2_warp_sum(si + ci);
-	__shared__ double wr[P2_RED_TPB / 32], wi[P2_RED_TPB / 32];
-	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	if (lane == 0) {
-		wr[warp] = vr;
-		wi[warp] = vi;
-	}
-	__syncthreads();
-	if (threadIdx.x == 0) {
-		double s0 = 0.0, c0 = 0.0, s1 = 0.0, c1 = 0.0;
-		for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-			p2_neumaier(s0, c0, wr[w]);
-			p2_neumaier(s1, c1, wi[w]);
+	p2_block_sum2(sr + cr, si + ci, part);
+}
+
+/* ---- coefficient-matrix trial states (state_prep.c) --------------------- */
+
+/* Index of an (alpha | beta) occupation: tapered drops bits 0 and n_sites
+ * and compacts the rest (reference: state_prep_coeff.c:47-54). */
+__device__ __forceinline__ uint64_t p2_cm_index(uint64_t full,
+	uint32_t n_sites, int tapered)
+{
+	if (!tapered)
+		return full;
+	const uint64_t lo =
+		(full >> 1) & ((UINT64_C(1) << (n_sites - 1)) - 1);
+	return lo | ((full >> (n_sites + 1)) << (n_sites - 1));
+}
+
+/* Slater-Condon expansion: for pair (i, j) every block k whose
+ * c = (w_k * det_a_k[i]) * det_b_k[j] is not below 1e-12 in magnitude is
+ * added, in block order, to the amplitude (accumulate) or to a first
+ * assignment; products and sums rounded separately, as the reference's
+ * host loop (state_prep_coeff.c:171-193).  Distinct pairs have distinct
+ * indices (fixed particle numbers), so no two threads write one
+ * amplitude. */
+template <typename ST>
+__global__ void k_cm_expand(ST *__restrict__ st,
+	const uint64_t *__restrict__ occ_a, const uint64_t *__restrict__ occ_b,
+	uint64_t Ma, uint64_t Mb, const double *__restrict__ w,
+	const double *__restrict__ det_a, const double *__restrict__ det_b,
+	uint32_t ncomp, uint32_t n_sites, int tapered, int accumulate)
+{
+	const uint64_t n = Ma * Mb;
+	const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+	for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+		p < n; p += stride) {
+		const uint64_t i = p / Mb, j = p - i * Mb;
+		const uint64_t idx =
+			p2_cm_index(occ_a[i] | occ_b[j], n_sites, tapered);
+		double re = 0.0, im = 0.0;
+		bool hit = false;
+		for (uint32_t k = 0; k < ncomp; ++k) {
+			const double cf = __dmul_rn(
+				__dmul_rn(w[k], det_a[k * Ma + i]),
+				det_b[k * Mb + j]);
+			if (fabs(cf) < 1.0e-12)
+				continue;
+			if (!hit) {
+				hit = true;
+				if (accumulate) {
+					p2_ld(st, idx, re, im);
+					re = __dadd_rn(re, cf);
+				} else {
+					re = cf;
+				}
+			} else {
+				re = __dadd_rn(re, cf);
+			}
 		}
-		part[2 * blockIdx.x] = s0 + c0;
-		part[2 * blockIdx.x + 1] = s1 + c1;
+		if (hit)
+			p2_st(st, idx, re, im);
 	}
+}
+
+/* Overlap of the real trial state with the register: per-block partial
+ * sums of c * a[idx] over the pairs (compensated), then k_reduce_final. */
+template <typename ST>
+__global__ void __launch_bounds__(P2_RED_TPB) k_cm_inner(
+	const ST *__restrict__ st, const uint64_t *__restrict__ occ_a,
+	const uint64_t *__restrict__ occ_b, uint64_t Ma, uint64_t Mb, double w,
+	const double *__restrict__ det_a, const double *__restrict__ det_b,
+	uint32_t n_sites, int tapered, double *__restrict__ part)
+{
+	double sr = 0.0, cr = 0.0, si = 0.0, ci = 0.0;
+	const uint64_t n = Ma * Mb;
+	const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+	for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+		p < n; p += stride) {
+		const uint64_t i = p / Mb, j = p - i * Mb;
+		const double cf = __dmul_rn(__dmul_rn(w, det_a[i]), det_b[j]);
+		if (fabs(cf) < 1.0e-12)
+			continue;
+		double re, im;
+		p2_ld(st, p2_cm_index(occ_a[i] | occ_b[j], n_sites, tapered),
+			re, im);
+		p2_neumaier(sr, cr, __dmul_rn(cf, re));
+		p2_neumaier(si, ci, __dmul_rn(cf, im));
+	}
+	p2_block_sum2(sr + cr, si + ci, part);
 }
 
 /* Stage 2: one block combines nblk partials (compensated). */
@@ -1328,6 +1427,7 @@ extern "C" void p2d_destroy(struct p2_dev *d)
 	cudaFreeHost(d->h_idx);
 	cudaFreeHost(d->h_val);
 	cudaFree(d->d_part);
+	cudaFree(d->d_cm);
 	for (int k = 0; k < P2_GRAPH_SLOTS; k++) {
 		struct p2_graph *g = &d->graphs[k];
 		if (g->exec)
@@ -1829,9 +1929,9 @@ extern "C" int p2d_run(struct p2_dev *d, const struct phase2_pass *passes,
 	return 0;
 }
 
-static int reduce(struct p2_dev *d, const double2 *trial, double out[2])
+/* Partial-sum buffer for `blocks` reduction blocks plus the result. */
+static int part_reserve(struct p2_dev *d, unsigned blocks)
 {
-	const unsigned blocks = grid_for(d, d->namp, P2_RED_TPB, 4);
 	if (d->part_cap < 2 * (size_t)blocks + 2) {
 		CUDA_OK(cudaStreamSynchronize(d->stream), "sync before partials");
 		cudaFree(d->d_part);
@@ -1842,24 +1942,131 @@ static int reduce(struct p2_dev *d, const double2 *trial, double out[2])
 			"alloc partials");
 		d->part_cap = 2 * (size_t)blocks + 2;
 	}
-	if (d->prec == PHASE2_PREC_FP64)
-		k_reduce_partial<<<blocks, P2_RED_TPB, 0, d->stream>>>(
-			(const double2 *)d->state, trial, d->namp, d->d_part);
-	else
-		k_reduce_partial<<<blocks, P2_RED_TPB, 0, d->stream>>>(
-			(const float2 *)d->state, trial, d->namp, d->d_part);
+	return 0;
+}
+
+/* Run k_reduce_final over `blocks` partials and download the result. */
+static int reduce_finish(struct p2_dev *d, unsigned blocks, double out[2])
+{
 	k_reduce_final<<<1, P2_RED_TPB, 0, d->stream>>>(d->d_part, blocks,
 		d->d_part + 2 * (size_t)blocks);
-	d->launches += 2;
+	d->launches += 1;
 	CUDA_OK(cudaGetLastError(), "reduce launch");
 	double h[2];
 	CUDA_OK(cudaMemcpyAsync(h, d->d_part + 2 * (size_t)blocks, sizeof h,
 			cudaMemcpyDeviceToHost, d->stream),
 		"download reduction");
 	CUDA_OK(cudaStreamSynchronize(d->stream), "reduce");
+	d->d2h_bytes += sizeof h;
 	out[0] = h[0];
 	out[1] = h[1];
 	return 0;
+}
+
+static int reduce(struct p2_dev *d, const double2 *trial, double out[2])
+{
+	const unsigned blocks = grid_for(d, d->namp, P2_RED_TPB, 4);
+	if (part_reserve(d, blocks) < 0)
+		return -1;
+	if (d->prec == PHASE2_PREC_FP64)
+		k_reduce_partial<<<blocks, P2_RED_TPB, 0, d->stream>>>(
+			(const double2 *)d->state, trial, d->namp, d->d_part);
+	else
+		k_reduce_partial<<<blocks, P2_RED_TPB, 0, d->stream>>>(
+			(const float2 *)d->state, trial, d->namp, d->d_part);
+	d->launches += 1;
+	return reduce_finish(d, blocks, out);
+}
+
+/* Upload the expansion tables (occupations, weights, determinants) into
+ * the register's table buffer; *p receives the five device pointers. */
+static int cm_upload(struct p2_dev *d, const uint64_t *occ_a, size_t Ma,
+	const uint64_t *occ_b, size_t Mb, const double *w, size_t ncomp,
+	const double *det_a, const double *det_b, void *p[5])
+{
+	const size_t sz[5] = { Ma * sizeof(uint64_t), Mb * sizeof(uint64_t),
+		ncomp * sizeof(double), ncomp * Ma * sizeof(double),
+		ncomp * Mb * sizeof(double) };
+	const void *src[5] = { occ_a, occ_b, w, det_a, det_b };
+	size_t off[5], total = 0;
+	for (int k = 0; k < 5; k++) {
+		off[k] = total;
+		total += (sz[k] + 255) & ~(size_t)255;
+	}
+	if (total > d->cm_cap) {
+		CUDA_OK(cudaStreamSynchronize(d->stream), "sync before tables");
+		cudaFree(d->d_cm);
+		d->d_cm = NULL;
+		d->cm_cap = 0;
+		CUDA_OK(cudaMalloc((void **)&d->d_cm, total), "alloc tables");
+		d->cm_cap = total;
+	}
+	for (int k = 0; k < 5; k++) {
+		p[k] = d->d_cm + off[k];
+		if (sz[k])
+			CUDA_OK(cudaMemcpyAsync(p[k], src[k], sz[k],
+					cudaMemcpyHostToDevice, d->stream),
+				"upload tables");
+	}
+	d->h2d_bytes += sz[0] + sz[1] + sz[2] + sz[3] + sz[4];
+	return 0;
+}
+
+extern "C" int p2d_cm_expand(struct p2_dev *d, uint32_t n_sites, int tapered,
+	int accumulate, const uint64_t *occ_a, size_t Ma, const uint64_t *occ_b,
+	size_t Mb, const double *w, const double *det_a, const double *det_b,
+	size_t ncomp)
+{
+	if (Ma == 0 || Mb == 0 || ncomp == 0)
+		return 0;
+	void *p[5];
+	if (cm_upload(d, occ_a, Ma, occ_b, Mb, w, ncomp, det_a, det_b, p) < 0)
+		return -1;
+	const uint64_t n = (uint64_t)Ma * Mb;
+	const unsigned grid = grid_for(d, n, P2_TPB, 8);
+	if (d->prec == PHASE2_PREC_FP64)
+		k_cm_expand<<<grid, P2_TPB, 0, d->stream>>>((double2 *)d->state,
+			(const uint64_t *)p[0], (const uint64_t *)p[1], Ma, Mb,
+			(const double *)p[2], (const double *)p[3],
+			(const double *)p[4], (uint32_t)ncomp, n_sites, tapered,
+			accumulate);
+	else
+		k_cm_expand<<<grid, P2_TPB, 0, d->stream>>>((float2 *)d->state,
+			(const uint64_t *)p[0], (const uint64_t *)p[1], Ma, Mb,
+			(const double *)p[2], (const double *)p[3],
+			(const double *)p[4], (uint32_t)ncomp, n_sites, tapered,
+			accumulate);
+	d->launches += 1;
+	CUDA_OK(cudaGetLastError(), "expansion launch");
+	return 0;
+}
+
+extern "C" int p2d_cm_inner(struct p2_dev *d, uint32_t n_sites, int tapered,
+	const uint64_t *occ_a, size_t Ma, const uint64_t *occ_b, size_t Mb,
+	double w, const double *det_a, const double *det_b, double out[2])
+{
+	out[0] = out[1] = 0.0;
+	if (Ma == 0 || Mb == 0)
+		return 0;
+	void *p[5];
+	if (cm_upload(d, occ_a, Ma, occ_b, Mb, &w, 1, det_a, det_b, p) < 0)
+		return -1;
+	const uint64_t n = (uint64_t)Ma * Mb;
+	const unsigned blocks = grid_for(d, n, P2_RED_TPB, 4);
+	if (part_reserve(d, blocks) < 0)
+		return -1;
+	if (d->prec == PHASE2_PREC_FP64)
+		k_cm_inner<<<blocks, P2_RED_TPB, 0, d->stream>>>(
+			(const double2 *)d->state, (const uint64_t *)p[0],
+			(const uint64_t *)p[1], Ma, Mb, w, (const double *)p[3],
+			(const double *)p[4], n_sites, tapered, d->d_part);
+	else
+		k_cm_inner<<<blocks, P2_RED_TPB, 0, d->stream>>>(
+			(const float2 *)d->state, (const uint64_t *)p[0],
+			(const uint64_t *)p[1], Ma, Mb, w, (const double *)p[3],
+			(const double *)p[4], n_sites, tapered, d->d_part);
+	d->launches += 1;
+	return reduce_finish(d, blocks, out);
 }
 
 extern "C" int p2d_norm2(struct p2_dev *d, double *out)

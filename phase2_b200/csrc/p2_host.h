@@ -77,6 +77,13 @@ long p2_qreg_record_gather(struct qreg *reg, const uint64_t *idx, size_t n);
 int p2_qreg_record_end(struct qreg *reg);
 struct p2_dev *p2_qreg_dev(const struct qreg *reg);
 
+/* For work on the device state outside the queues (coefficient-matrix
+ * state prep and overlap): drain the queues, drop the host copy, and
+ * return the device state (NULL on a register error or while recording).
+ * p2_qreg_fail marks the register failed and returns -1. */
+struct p2_dev *p2_qreg_direct(struct qreg *reg);
+int p2_qreg_fail(struct qreg *reg);
+
 /* sum_d a[d] * conj(cf_d) over the circuit's determinants, the expression
  * of circ_measure (a: the determinant amplitudes in order). */
 _Complex double p2_circ_overlap(const struct circ_muldet *md,

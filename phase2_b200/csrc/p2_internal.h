@@ -66,6 +66,22 @@ void p2d_stats_reset(struct p2_dev *d);
 void p2d_set_timing(struct p2_dev *d, int on);
 void *p2d_stream(const struct p2_dev *d);
 
+/*
+ * Coefficient-matrix trial states (state_prep.c).  occ_a (Ma) and occ_b
+ * (Mb) are the alpha and beta occupation masks (beta already shifted by
+ * n_sites); det_a/det_b hold ncomp blocks of Ma/Mb determinants.
+ * expand: for every (i, j), the unpruned w_k det_a_k[i] det_b_k[j] are
+ * added in block order to the amplitude (accumulate) or to a first
+ * assignment (not accumulate); inner: out = sum of w da db * amplitude.
+ */
+int p2d_cm_expand(struct p2_dev *d, uint32_t n_sites, int tapered,
+	int accumulate, const uint64_t *occ_a, size_t Ma, const uint64_t *occ_b,
+	size_t Mb, const double *w, const double *det_a, const double *det_b,
+	size_t ncomp);
+int p2d_cm_inner(struct p2_dev *d, uint32_t n_sites, int tapered,
+	const uint64_t *occ_a, size_t Ma, const uint64_t *occ_b, size_t Mb,
+	double w, const double *det_a, const double *det_b, double out[2]);
+
 /* ---- recorded programs (batched persistent execution) ------------------- */
 
 /*

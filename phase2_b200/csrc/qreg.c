@@ -509,6 +509,24 @@ struct p2_dev *p2_qreg_dev(const struct qreg *reg)
 	return b ? b->dev : NULL;
 }
 
+struct p2_dev *p2_qreg_direct(struct qreg *reg)
+{
+	struct p2_qreg *b = B(reg);
+	if (!b || recording(b, "coefficient-matrix state") ||
+		qreg_flush(reg) < 0)
+		return NULL;
+	b->host_copy_valid = 0;
+	return b->dev;
+}
+
+int p2_qreg_fail(struct qreg *reg)
+{
+	struct p2_qreg *b = B(reg);
+	if (b)
+		b->error = -1;
+	return -1;
+}
+
 int qreg_get_stats(const struct qreg *reg, struct phase2_stats *st)
 {
 	const struct p2_qreg *b = B(reg);

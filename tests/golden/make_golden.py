@@ -98,6 +98,12 @@ def h2o_fixture() -> dict:
             "det_cf": [[det_cf[0], det_cf[1]]], "normalization": norm}
 
 
+def _psi_from_seed(nqb: int, seed: int) -> np.ndarray:
+    """The complex test state of a coefficient-matrix golden case."""
+    g = np.random.Generator(np.random.PCG64(seed))
+    return g.standard_normal(1 << nqb) + 1j * g.standard_normal(1 << nqb)
+
+
 def main() -> None:
     ref = Reference()
     L = ref.L
@@ -290,6 +296,43 @@ def main() -> None:
                                               4, 60, 50, 0.1, 0.02,
                                               0xBEEF)]
     gold["h2o"] = h
+
+    # -- coefficient-matrix trial states: the reference's expansion
+    # (state_prep_coeff_expand_all) and overlap (circ.c measure_coeff)
+    from types import SimpleNamespace
+    crng = np.random.Generator(np.random.PCG64(0xC0EFF))
+    cms = []
+    for ns, na, nb, closed, tap, nc in ((4, 2, 2, True, False, 0),
+                                        (5, 2, 3, False, False, 0),
+                                        (5, 2, 2, True, True, 0),
+                                        (4, 2, 1, False, False, 3),
+                                        (6, 3, 3, False, True, 2),
+                                        (3, 0, 1, False, False, 0)):
+        nblk = max(nc, 1)
+        cm = SimpleNamespace(
+            n_sites=ns, n_alpha=na, n_beta=nb,
+            C_alpha=[crng.standard_normal((ns, na)) for _ in range(nblk)],
+            C_beta=(None if closed else
+                    [crng.standard_normal((ns, nb)) for _ in range(nblk)]),
+            weights=None if nc == 0 else list(crng.standard_normal(nc)),
+            tapered=tap)
+        nqb = 2 * ns - (2 if tap else 0)
+        amp = ref.coeff_expand(nqb, cm)
+        nz = np.nonzero(amp)[0]
+        seed = int(crng.integers(1 << 30))
+        cms.append({
+            "nqb": nqb, "n_sites": ns, "n_alpha": na, "n_beta": nb,
+            "tapered": tap,
+            "C_alpha": [c.tolist() for c in cm.C_alpha],
+            "C_beta": (None if cm.C_beta is None
+                       else [c.tolist() for c in cm.C_beta]),
+            "weights": cm.weights,
+            "expand_idx": nz.tolist(),
+            "expand_val": [float(v.real) for v in amp[nz]],
+            "psi_seed": seed,
+            "inner": cplx(ref.coeff_inner(nqb, cm,
+                                          _psi_from_seed(nqb, seed)))})
+    gold["coeff_matrix"] = cms
 
     (OUT / "golden.json").write_text(json.dumps(gold, indent=0))
 

@@ -130,6 +130,34 @@ def test_h2o_fixture(golden, oracle_lib):
         assert np.all(np.abs(z) <= 1 + 1e-12), kind
 
 
+def coeff_case(c):
+    """A golden coefficient-matrix case as (nqb, state object, psi)."""
+    from types import SimpleNamespace
+    cm = SimpleNamespace(
+        n_sites=c["n_sites"], n_alpha=c["n_alpha"], n_beta=c["n_beta"],
+        C_alpha=[np.array(a) for a in c["C_alpha"]],
+        C_beta=(None if c["C_beta"] is None
+                else [np.array(b) for b in c["C_beta"]]),
+        weights=c["weights"], tapered=c["tapered"])
+    g = np.random.Generator(np.random.PCG64(c["psi_seed"]))
+    n = c["nqb"]
+    psi = g.standard_normal(1 << n) + 1j * g.standard_normal(1 << n)
+    return n, cm, psi
+
+
+def test_coeff_matrix_fixtures(golden, oracle_lib):
+    """The restated Slater-Condon expansion and overlap reproduce the
+    reference's (state_prep_coeff.c) bit for bit."""
+    for c in golden["coeff_matrix"]:
+        n, cm, psi = coeff_case(c)
+        amp = oracle_lib.coeff_expand(n, cm)
+        nz = np.nonzero(amp)[0]
+        assert nz.tolist() == c["expand_idx"]
+        assert np.array_equal(amp[nz].real, np.array(c["expand_val"]))
+        assert not np.any(amp.imag)
+        assert oracle_lib.coeff_inner(n, cm, psi) == _cz(c["inner"])
+
+
 needs_ref = pytest.mark.skipif(not REF_SO.is_file(),
                                reason="oracle/_ref not built here")
 

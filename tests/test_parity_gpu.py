@@ -470,6 +470,85 @@ def test_persistent_batch_empty_and_single():
     assert len(got[1]) == 0
 
 
+# ---- coefficient-matrix trial states ----------------------------------
+
+
+def _coeff_state(c):
+    cm = p2.CoeffMatrix(
+        n_sites=c["n_sites"], n_alpha=c["n_alpha"], n_beta=c["n_beta"],
+        C_alpha=[np.array(a) for a in c["C_alpha"]],
+        C_beta=(None if c["C_beta"] is None
+                else [np.array(b) for b in c["C_beta"]]),
+        weights=c["weights"], tapered=c["tapered"])
+    g = np.random.Generator(np.random.PCG64(c["psi_seed"]))
+    n = c["nqb"]
+    return n, cm, g.standard_normal(1 << n) + 1j * g.standard_normal(1 << n)
+
+
+def test_coeff_matrix_golden(golden, fp32_form):
+    """Device expansion bit-identical to the reference's (FP64) and its
+    device overlap within 1e-12 relative of the reference's sequential sum;
+    FP32 registers within the FP32 tolerance."""
+    for c in golden["coeff_matrix"]:
+        n, cm, psi = _coeff_state(c)
+        want = np.zeros(1 << n, dtype=np.complex128)
+        want[c["expand_idx"]] = c["expand_val"]
+        z_ref = _cz(c["inner"])
+        with Register(n, p2.PREC_FP64) as r:
+            r.coeff_expand(cm)
+            assert np.array_equal(r.get_state(), want)
+            r.set_state(psi)
+            z = r.coeff_inner(cm)
+        assert abs(z - z_ref) <= 1e-12 * max(1.0, abs(z_ref))
+        with Register(n, p2.PREC_FP32) as r:
+            r.coeff_expand(cm)
+            got = r.get_state()
+            assert np.max(np.abs(got - want)) <= 1e-6 * max(
+                1.0, np.max(np.abs(want)))
+
+
+@pytest.mark.parametrize("kind", ["trott", "trott2"])
+def test_coeff_matrix_drivers(kind, oracle_lib):
+    """Drivers with a coefficient-matrix initial state and overlap (the
+    coeff_matrix branch of circ_prepst / circ_measure): equal to the
+    oracle's expand -> sorted rotations -> sequential overlap, to 1e-12."""
+    rng = np.random.Generator(np.random.PCG64(77))
+    ns, na, nb = 5, 2, 2
+    blocks = 2
+    cm = p2.CoeffMatrix(ns, na, nb,
+                        [rng.standard_normal((ns, na)) for _ in range(blocks)],
+                        [rng.standard_normal((ns, nb)) for _ in range(blocks)],
+                        [0.8, -0.6])
+    n = 2 * ns
+    t = workloads.jw_terms(n, 60, seed=78)
+    steps, delta = 3, 0.2
+    z = (p2.trott if kind == "trott" else p2.trott2)(n, t, cm, steps, delta)
+    rec = oracle_lib.sort_lex(t.flip, t.phase, t.cf)
+    amp = oracle_lib.coeff_expand(n, cm)
+    want = []
+    for _ in range(steps):
+        if kind == "trott":
+            amp = oracle_lib.rotate(amp, n, rec["flip"], rec["phase"],
+                                    delta * rec["cf"])
+        else:
+            amp = oracle_lib.rotate(amp, n, rec["flip"], rec["phase"],
+                                    0.5 * delta * rec["cf"])
+            amp = oracle_lib.rotate(amp, n, rec["flip"][::-1],
+                                    rec["phase"][::-1],
+                                    0.5 * delta * rec["cf"][::-1])
+        want.append(oracle_lib.coeff_inner(n, cm, amp))
+    want = np.array(want)
+    assert np.all(np.abs(z - want) <= 1e-12 * np.maximum(1.0, np.abs(want)))
+
+
+def test_coeff_matrix_rejects_small_register():
+    """An expansion needing more qubits than the register is refused."""
+    cm = p2.CoeffMatrix(5, 2, 2, [np.eye(5, 2)], None, None)
+    with Register(8, p2.PREC_FP64) as r:
+        with pytest.raises(RuntimeError):
+            r.coeff_expand(cm)
+
+
 def test_sharded_qdrift_equals_single_run():
     """Replica sharding (phase2_b200.replicas): the blocks of 3 ranks,
     each with its generator advanced to its first sample, concatenate to
