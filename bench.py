@@ -345,7 +345,13 @@ def gpu_arm(args) -> None:
                 extra["fp32_error"][fname] = fp32_error_study()
             finally:
                 p2.set_fp32_form(form0)
-        extra["batched"] = batched_study()
+        studies = set(args.studies.split(",")) if args.studies else set()
+        if "batched" in studies:
+            extra["batched"] = batched_study()
+        if "trott26" in studies:
+            extra["trott26"] = trott26_study()
+        if "cmpsit33" in studies:
+            extra["cmpsit33"] = cmpsit33_study()
     if rank != 0:
         return
     clocks = clk.summary()
@@ -420,6 +426,80 @@ def fp32_error_study(nqb: int = 20, nterms: int = 300, steps: int = 1000,
             "max_abs_err": float(err.max()), "err_at_step": at,
             "final_overlap_fp64": [float(z64[-1].real), float(z64[-1].imag)],
             "seconds": time.perf_counter() - t0}
+
+
+def trott26_study(steps: int = 2) -> dict:
+    """Second-order Trotter at 26 qubits (20,000 JW terms in flip-mask
+    order -- phase2_set_term_order(FLIP), not the reference's lexicographic
+    sort -- 16 determinants of weight 13, delta 0.05), FP64 and FP32 states
+    side by side on the same inputs, `steps` of its 256 steps (bounded
+    run): device rot.amp/s of each (CUDA events around the pass launches)
+    and the FP32 overlap error against the FP64 run."""
+    import numpy as np
+
+    import phase2_b200 as p2
+    from phase2_b200 import workloads
+    cfg = workloads.strang26(steps=steps)
+    t, d = cfg["terms"], cfg["dets"]
+    out = {"workload": ("trott2 26 qubits, 20000 JW terms in flip-mask "
+                        f"order, 16 determinants, delta 0.05, {steps} of "
+                        "256 steps"), "unit": UNIT}
+    zs = {}
+    order = p2.lib().phase2_get_term_order()
+    for name, prec in (("fp64", p2.PREC_FP64), ("fp32", p2.PREC_FP32)):
+        p2.set_precision(prec)
+        p2.set_term_order(2)  # PHASE2_ORDER_FLIP
+        try:
+            z, st = p2.trott2(26, t, d, steps, cfg["delta"], timing=True,
+                              with_stats=True)
+        finally:
+            p2.set_precision(p2.PREC_FP64)
+            p2.set_term_order(order)
+        zs[name] = z
+        rot = st["rotations"]
+        out[name] = {"value": rot * (1 << 26) / (st["pass_ms"] / 1e3),
+                     "rotations": int(rot), "passes": int(st["passes"]),
+                     "rotations_per_pass": rot / max(1, st["passes"]),
+                     "pass_seconds": st["pass_ms"] / 1e3,
+                     "hbm_gbs": st["bytes"] / (st["pass_ms"] / 1e3) / 1e9}
+    out["fp32_vs_fp64"] = out["fp32"]["value"] / out["fp64"]["value"]
+    out["fp32_max_abs_err"] = float(np.max(np.abs(zs["fp32"] - zs["fp64"])))
+    return out
+
+
+def cmpsit33_study(steps: int = 1) -> dict:
+    """The composite driver at 33 qubits (200,000 JW terms, 2,000
+    deterministic, 8,192 draws per half step, 32 determinants), `steps` of
+    its 64 steps, FP32 state (64 GiB) and FP64 state (128 GiB) in turn:
+    device rot.amp/s and the FP32 error (opt-in: several minutes)."""
+    import numpy as np
+
+    import phase2_b200 as p2
+    from phase2_b200 import workloads
+    cfg = workloads.cmpsit33(steps=steps)
+    out = {"workload": (f"cmpsit 33 qubits, {steps} of 64 steps, "
+                        "200000 JW terms, length 2000, depth 8192, "
+                        "32 determinants"), "unit": UNIT}
+    zs = {}
+    for name, prec in (("fp32", p2.PREC_FP32), ("fp64", p2.PREC_FP64)):
+        p2.set_precision(prec)
+        try:
+            z, st = p2.cmpsit(cfg["nqb"], cfg["terms"], cfg["dets"],
+                              cfg["samples"], cfg["steps"], cfg["length"],
+                              cfg["depth"], cfg["angle_det"],
+                              cfg["angle_rand"], cfg["seed"], timing=True,
+                              with_stats=True)
+        finally:
+            p2.set_precision(p2.PREC_FP64)
+        zs[name] = z
+        rot = st["rotations"]
+        out[name] = {"value": rot * (1 << cfg["nqb"]) /
+                     (st["pass_ms"] / 1e3), "rotations": int(rot),
+                     "passes": int(st["passes"]),
+                     "pass_seconds": st["pass_ms"] / 1e3,
+                     "hbm_gbs": st["bytes"] / (st["pass_ms"] / 1e3) / 1e9}
+    out["fp32_max_abs_err"] = float(np.max(np.abs(zs["fp32"] - zs["fp64"])))
+    return out
 
 
 def batched_study(ninst: int = 64, step_cap: int = 4, seed: int = 0xBA7C4):
@@ -523,6 +603,9 @@ def main() -> None:
     ap.add_argument("--cmp-depth", type=int, default=512)
     ap.add_argument("--quick", action="store_true",
                     help="skip the CPU baseline and secondary arms")
+    ap.add_argument("--studies", default="batched,trott26",
+                    help="comma list of studies to append: batched, "
+                         "trott26, cmpsit33 (the last takes minutes)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

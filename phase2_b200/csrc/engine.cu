@@ -908,7 +908,11 @@ __global__ void __launch_bounds__(P2_TPB, p2_lift32_blocks(M))
  * and stores go through L2 only (ld/st .cg), since L1 is not coherent
  * across SMs.
  */
-#define P2_BATCH_COSETS 4 /* cosets per thread in a pass tile */
+/* Cosets per thread in a pass tile: 4 for passes of at least
+ * P2_BATCH_BIG_PASS representatives, 1 below (more tiles for small
+ * registers, whose passes are otherwise too few tiles to spread). */
+#define P2_BATCH_COSETS 4
+#define P2_BATCH_BIG_PASS (UINT64_C(1) << 16)
 #define P2_BATCH_ZERO_TILE (P2_TPB * 128)
 
 struct p2_binst {
@@ -924,10 +928,10 @@ struct p2_bctl {
 };
 
 /* The cosets of one pass tile: thread k takes representatives
- * tile * P2_BATCH_COSETS * P2_TPB + j * P2_TPB + k (coalesced per j). */
+ * tile * cpt * P2_TPB + j * P2_TPB + k, j < cpt (coalesced per j). */
 template <int M>
 __device__ __forceinline__ void p2_batch_pass_tile(float2 *st,
-	const struct phase2_pass &p, uint32_t tile, uint64_t nrep,
+	const struct phase2_pass &p, uint32_t tile, uint64_t nrep, uint32_t cpt,
 	const struct p2_lift32_rec *srec)
 {
 	uint32_t pb[M > 0 ? M : 1];
@@ -935,9 +939,8 @@ __device__ __forceinline__ void p2_batch_pass_tile(float2 *st,
 	for (int k = 0; k < M; ++k)
 		pb[k] = (uint32_t)p.basis[k];
 	const uint32_t negm = p.scale < 0 ? 0x80000000u : 0u;
-	const uint64_t t0 = (uint64_t)tile * (P2_BATCH_COSETS * P2_TPB) +
-		threadIdx.x;
-	for (int j = 0; j < P2_BATCH_COSETS; ++j) {
+	const uint64_t t0 = (uint64_t)tile * cpt * P2_TPB + threadIdx.x;
+	for (uint32_t j = 0; j < cpt; ++j) {
 		const uint64_t t = t0 + (uint64_t)j * P2_TPB;
 		if (t < nrep)
 			p2_lift32_coset<M, uint32_t, true>(st,
@@ -1032,22 +1035,28 @@ __global__ void __launch_bounds__(P2_TPB, 5)
 				const uint64_t nrep = namp >> p.span;
 				switch (p.span) {
 				case 0:
-					p2_batch_pass_tile<0>(st, p, tile, nrep, srec);
+					p2_batch_pass_tile<0>(st, p, tile, nrep,
+						op.b, srec);
 					break;
 				case 1:
-					p2_batch_pass_tile<1>(st, p, tile, nrep, srec);
+					p2_batch_pass_tile<1>(st, p, tile, nrep,
+						op.b, srec);
 					break;
 				case 2:
-					p2_batch_pass_tile<2>(st, p, tile, nrep, srec);
+					p2_batch_pass_tile<2>(st, p, tile, nrep,
+						op.b, srec);
 					break;
 				case 3:
-					p2_batch_pass_tile<3>(st, p, tile, nrep, srec);
+					p2_batch_pass_tile<3>(st, p, tile, nrep,
+						op.b, srec);
 					break;
 				case 4:
-					p2_batch_pass_tile<4>(st, p, tile, nrep, srec);
+					p2_batch_pass_tile<4>(st, p, tile, nrep,
+						op.b, srec);
 					break;
 				default:
-					p2_batch_pass_tile<5>(st, p, tile, nrep, srec);
+					p2_batch_pass_tile<5>(st, p, tile, nrep,
+						op.b, srec);
 					break;
 				}
 			} else if (op.kind == P2_OP_ZERO) {
@@ -2214,7 +2223,9 @@ extern "C" int p2d_batch_run(struct p2_dev *const *devs,
 			case P2_OP_PASS: {
 				op.a += (uint32_t)bp;
 				const uint64_t nrep = d->namp >> hp[op.a].span;
-				const uint64_t per = P2_BATCH_COSETS * P2_TPB;
+				op.b = nrep >= P2_BATCH_BIG_PASS ? P2_BATCH_COSETS
+								  : 1;
+				const uint64_t per = (uint64_t)op.b * P2_TPB;
 				op.ntiles = (uint32_t)((nrep + per - 1) / per);
 				break;
 			}

@@ -92,7 +92,8 @@ int p2d_cm_inner(struct p2_dev *d, uint32_t n_sites, int tapered,
 enum p2_op_kind {
 	P2_OP_ZERO = 0,   /* state <- 0 */
 	P2_OP_WRITE = 1,  /* writes a .. a+b-1 of widx/wval, in order */
-	P2_OP_PASS = 2,   /* pass a of passes */
+	P2_OP_PASS = 2,   /* pass a of passes (b: cosets per thread a tile,
+			   * set by p2d_batch_run) */
 	P2_OP_GATHER = 3, /* amplitudes gidx[a .. a+b-1] -> output a .. a+b-1 */
 };
 
