@@ -1619,8 +1619,9 @@ static struct p2_tune_entry p2_tune[2][PHASE2_MAX_SPAN + 1] = {
 	 * peak for every span at 28 qubits on B200) */
 	{ { 0, 32 }, { 0, 32 }, { 0, 32 }, { 0, 32 }, { 0, 32 }, { 0, 32 } },
 	/* FP32: 32 blocks per SM (k_pass_lift32 at span 5: 95 % of HBM peak
-	 * at 28 and 30 qubits, ahead of 16 and 8) */
-	{ { 0, 32 }, { 0, 32 }, { 0, 32 }, { 0, 32 }, { 0, 32 }, { 0, 32 } },
+	 * at 28 and 30 qubits, ahead of 16 and 8), 16 at span 1
+	 * (phase2_b200/tuning_b200.json, 28 qubits) */
+	{ { 0, 32 }, { 0, 16 }, { 0, 32 }, { 0, 32 }, { 0, 32 }, { 0, 32 } },
 };
 
 extern "C" int phase2_tune_set(int prec, int span, int variant, int per_sm)
