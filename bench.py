@@ -502,6 +502,33 @@ def cmpsit33_study(steps: int = 1) -> dict:
     return out
 
 
+def batch8_study() -> dict:
+    """A small, L2-resident persistent batch (8 trott instances of 18-20
+    qubits, 2,000 JW terms, 2 steps, FP32), run twice: the case the
+    persistent kernel's profile summary captures (its second launch)."""
+    import numpy as np
+
+    import phase2_b200 as p2
+    from phase2_b200 import workloads
+    g = np.random.Generator(np.random.PCG64(5))
+    probs = []
+    for k in range(8):
+        n = int(g.integers(18, 21))
+        probs.append(dict(nqb=n, terms=workloads.jw_terms(n, 2000,
+                                                          seed=100 + k),
+                          dets=workloads.hamming_dets(n, 1, n // 2,
+                                                      seed=200 + k),
+                          steps=2, delta=0.05))
+    p2.set_precision(p2.PREC_FP32)
+    try:
+        for _ in range(2):
+            _, st = p2.batch("trott", probs, with_stats=True)
+    finally:
+        p2.set_precision(p2.PREC_FP64)
+    return {"passes": int(sum(s["passes"] for s in st)),
+            "kernel_ms": float(sum(s["pass_ms"] for s in st))}
+
+
 def batched_study(ninst: int = 64, step_cap: int = 4, seed: int = 0xBA7C4):
     """Independent trott problems of uneven size run together: qubits
     U{18..24}, JW terms log-uniform in [1e3, 5e4], steps U{16..512} capped
@@ -606,7 +633,16 @@ def main() -> None:
     ap.add_argument("--studies", default="batched,trott26",
                     help="comma list of studies to append: batched, "
                          "trott26, cmpsit33 (the last takes minutes)")
+    ap.add_argument("--only-study", default=None,
+                    help="run just this study (batched, trott26, cmpsit33, "
+                         "batch8) and print its JSON")
     args = ap.parse_args()
+    if args.only_study:
+        import phase2_b200 as p2
+        p2.world_ensure()
+        fn = globals()[f"{args.only_study}_study"]
+        print(json.dumps({args.only_study: fn()}), flush=True)
+        return
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
