@@ -100,6 +100,32 @@ void circ_hamil_sort_flip(struct circ_hamil *hm);
 int phase2_set_batch_persistent(int on);
 
 /*
+ * qdrift_simul with device sampling: when the register is FP32 in
+ * PHASE2_FORM_LIFTED_F32 with at most 31 qubits and the trial state is a
+ * MULTIDET, the samples' term draws (CDF inversion of the host generator's
+ * uniforms), their pass plans and their passes all run on the GPU: one
+ * planning kernel per round of samples (a block per sample) writes the
+ * programs that one persistent launch executes, several samples at once
+ * on copies of the state where the register is small.  The host only steps
+ * the generator to each sample's start.  The overlaps, the register's
+ * final state, the generator's end state and the last sample's drawn terms
+ * equal the host loop's bit for bit.
+ *
+ * Modes: OFF (host loop), ON (device whenever the register qualifies),
+ * AUTO (default: device for qualifying registers of at most
+ * PHASE2_DEVICE_SAMPLING_AUTO_QB qubits, where samples run concurrently;
+ * wider registers keep the host loop, whose passes already fill the GPU).
+ * Also PHASE2_DEVICE_SAMPLING=off|on|auto.  Returns -1 on a bad mode.
+ */
+enum phase2_device_sampling {
+	PHASE2_DEVICE_SAMPLING_OFF = 0,
+	PHASE2_DEVICE_SAMPLING_ON = 1,
+	PHASE2_DEVICE_SAMPLING_AUTO = 2,
+};
+#define PHASE2_DEVICE_SAMPLING_AUTO_QB 25
+int phase2_set_device_sampling(int mode);
+
+/*
  * Run n independent, already initialised problems of one kind together.
  * Persistent mode (above): one launch for all instances and all their
  * steps.  Stream mode: each keeps its own register (its own CUDA stream),

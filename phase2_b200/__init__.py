@@ -82,6 +82,19 @@ def set_batch_persistent(on: bool) -> None:
     lib().phase2_set_batch_persistent(1 if on else 0)
 
 
+DEVICE_SAMPLING_OFF, DEVICE_SAMPLING_ON, DEVICE_SAMPLING_AUTO = 0, 1, 2
+
+
+def set_device_sampling(mode) -> None:
+    """qdrift on FP32 registers: draw, plan and run the samples on the GPU
+    (same results as the host loop, bit for bit).  True/False force it on
+    or off; DEVICE_SAMPLING_AUTO (default) uses it for registers of at most
+    25 qubits."""
+    mode = {True: 1, False: 0}.get(mode, mode)
+    if lib().phase2_set_device_sampling(int(mode)) != 0:
+        raise ValueError(f"bad device sampling mode {mode}")
+
+
 def set_fusion(max_span: int, max_rots: int = 0) -> None:
     if lib().phase2_set_fusion(max_span, max_rots) != 0:
         raise ValueError("bad fusion setting")
@@ -426,6 +439,13 @@ def _run_driver(kind: str, nqb: int, terms: Terms, dets, **kw):
         st = _ffi.Stats()
         L.qreg_get_stats(C.byref(obj.ct.reg), C.byref(st))
         stats = {k: getattr(st, k) for k, _ in _ffi.Stats._fields_}
+        if kw.get("with_state"):
+            # the register after the run (small registers)
+            stats["state"] = np.empty(1 << nqb, dtype=np.complex128)
+            if L.qreg_get_state(C.byref(obj.ct.reg),
+                                stats["state"].ctypes.data_as(
+                                    C.POINTER(C.c_double))):
+                raise RuntimeError("qreg_get_state failed")
     finally:
         getattr(L, f"{kind}_free")(C.byref(obj))
     return (vals, stats) if kw.get("with_stats") else vals

@@ -281,6 +281,7 @@ _SIGS = {
     "phase2_get_precision": (C.c_int, []),
     "phase2_set_fp32_form": (C.c_int, [C.c_int]),
     "phase2_set_batch_persistent": (C.c_int, [C.c_int]),
+    "phase2_set_device_sampling": (C.c_int, [C.c_int]),
     "state_prep_coeff_scratch_init": (C.c_int, [C.c_void_p, C.c_uint32,
                                                 C.c_uint32, C.c_uint32]),
     "state_prep_coeff_scratch_free": (None, [C.c_void_p]),

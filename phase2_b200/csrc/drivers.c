@@ -9,6 +9,8 @@
  *   qdrift  per sample: prepst, depth draws from the |c| CDF with
  *           cf = sign(c), circ_step(asin(step_size)), measure
  *                                                          (qdrift.c:95-134)
+ *           (FP32 registers: the same loop with draws, plans and passes
+ *           on the GPU, qdrift_simul_device)
  *   cmpsit  split by |c| (top `length` lex-sorted, rest sampled); per
  *           sample: prepst, per step a forward half of one sample and a
  *           reverse half of a fresh one at omega 0.5; measure
@@ -202,11 +204,128 @@ static void qdrift_draw(struct qdrift *qd)
 	}
 }
 
+static int qdrift_device_ok(const struct qdrift *qd)
+{
+	const struct circ *ct = &qd->ct;
+	const struct p2_qreg *b = ct->reg.backend;
+	if (p2_cfg.device_sampling == PHASE2_DEVICE_SAMPLING_OFF ||
+		(p2_cfg.device_sampling == PHASE2_DEVICE_SAMPLING_AUTO &&
+			ct->reg.qb_lo > PHASE2_DEVICE_SAMPLING_AUTO_QB))
+		return 0;
+	return b && b->rec == NULL &&
+		b->prec == PHASE2_PREC_FP32 &&
+		p2_form_for(PHASE2_PREC_FP32) == PHASE2_FORM_LIFTED_F32 &&
+		p2d_batch_ok(b->dev) && ct->stprep_kind == STPREP_MULTIDET &&
+		ct->md.len > 0 && qd->ranct.cdf.len > 0 &&
+		qd->ranct.hm_ran.len > 0 &&
+		qd->ranct.hm_ran.len <= UINT32_MAX - 3;
+}
+
+/*
+ * qdrift_simul with the draws, plans and passes on the GPU
+ * (p2d_qdrift_device).  The host steps the generator to every sample's
+ * start (depth draws each) and draws the last sample itself, so qd->rng
+ * and the drawn terms end as the host loop leaves them; each overlap is
+ * then the host loop's expression over the gathered amplitudes.
+ */
+static int qdrift_simul_device(struct qdrift *qd)
+{
+	struct circ *ct = &qd->ct;
+	struct circ_values *vals = &ct->vals;
+	struct p2_qreg *b = ct->reg.backend;
+	const size_t ns = vals->len, depth = qd->ranct.hm_ran.len;
+	const size_t nt = qd->ranct.cdf.len, nd = ct->md.len;
+	if (ns == 0)
+		return 0;
+	struct p2_dev *dev = p2_qreg_direct(&ct->reg);
+	if (!dev)
+		return -1;
+	for (size_t d = 0; d < nd; d++)
+		if (ct->md.dets[d].idx >= ct->reg.namp) {
+			log_error("qdrift_simul: determinant %llu out of range",
+				(unsigned long long)ct->md.dets[d].idx);
+			return p2_qreg_fail(&ct->reg);
+		}
+	uint64_t *rng0 = malloc(sizeof *rng0 * 4 * ns);
+	uint64_t *tflip = malloc(sizeof *tflip * nt);
+	uint64_t *tphase = malloc(sizeof *tphase * nt);
+	double *tcf = malloc(sizeof *tcf * nt);
+	uint64_t *didx = malloc(sizeof *didx * nd);
+	double *dval = malloc(sizeof *dval * 2 * nd);
+	_Complex double *g = malloc(sizeof *g * ns * nd);
+	int rc = -1;
+	if (!rng0 || !tflip || !tphase || !tcf || !didx || !dval || !g) {
+		log_error("qdrift_simul: allocation failed");
+		goto out;
+	}
+	for (size_t i = 0; i < ns; i++) {
+		memcpy(&rng0[4 * i], qd->rng.s, sizeof qd->rng.s);
+		if (i + 1 == ns)
+			qdrift_draw(qd);
+		else
+			for (size_t k = 0; k < depth; k++)
+				(void)xoshiro256ss_next(&qd->rng);
+	}
+	for (size_t k = 0; k < nt; k++) {
+		tflip[k] = ct->hm.terms[k].op.pak[0];
+		tphase[k] = ct->hm.terms[k].op.pak[1];
+		tcf[k] = ct->hm.terms[k].cf;
+	}
+	for (size_t d = 0; d < nd; d++) {
+		didx[d] = ct->md.dets[d].idx;
+		dval[2 * d] = creal(ct->md.dets[d].cf);
+		dval[2 * d + 1] = cimag(ct->md.dets[d].cf);
+	}
+	struct p2_qd_job job;
+	memset(&job, 0, sizeof job);
+	job.nqb = ct->reg.qb_lo;
+	job.depth = (uint32_t)depth;
+	job.nterms = nt;
+	job.mask = ct->reg.qb_lo >= 64 ? ~UINT64_C(0)
+				       : (UINT64_C(1) << ct->reg.qb_lo) - 1;
+	job.omega = asin(qd->dt.step_size);
+	/* the angles a host flush would plan: omega * sign_dz(cf) */
+	for (int sg = 0; sg < 3; sg++) {
+		const double phi = job.omega * (double)(sg - 1);
+		job.cs[sg][0] = cos(phi);
+		job.cs[sg][1] = sin(phi);
+	}
+	job.max_span = b->max_span;
+	job.max_rots = b->max_rots;
+	job.form = PHASE2_FORM_LIFTED_F32;
+	job.ndet = (uint32_t)nd;
+	uint64_t npass = 0;
+	if (p2d_qdrift_device(dev, &job, rng0, ns, qd->ranct.cdf.y, tflip,
+		    tphase, tcf, didx, dval, (double *)g, &npass) < 0) {
+		p2_qreg_fail(&ct->reg);
+		goto out;
+	}
+	for (size_t i = 0; i < ns; i++) {
+		vals->z[i] = p2_circ_overlap(&ct->md, g + i * nd);
+		if (emit(qd->sw, i, vals->z[i]) < 0) {
+			log_error("qdrift_simul: sample %zu output failed", i);
+			goto out;
+		}
+	}
+	rc = 0;
+out:
+	free(rng0);
+	free(tflip);
+	free(tphase);
+	free(tcf);
+	free(didx);
+	free(dval);
+	free(g);
+	return rc;
+}
+
 int qdrift_simul(struct qdrift *qd)
 {
 	struct circ *ct = &qd->ct;
 	struct circ_values *vals = &ct->vals;
 	const double omega = asin(qd->dt.step_size);
+	if (qdrift_device_ok(qd))
+		return qdrift_simul_device(qd);
 	for (size_t i = 0; i < vals->len; i++) {
 		if (circ_prepst(ct) < 0)
 			return -1;

@@ -30,6 +30,7 @@
  */
 #include <cuda_runtime.h>
 
+#include <float.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -38,6 +39,7 @@
 #include "log.h"
 
 #include "p2_internal.h"
+#include "plan_core.h"
 
 #define P2_TPB 128
 #define P2_RED_TPB 256
@@ -898,9 +900,12 @@ __global__ void __launch_bounds__(P2_TPB, p2_lift32_blocks(M))
  * tile of an op publishes the next op by resetting the ticket.  Blocks
  * look for work across programs starting from the last one they served,
  * so small programs interleave and the GPU stays busy without a launch per
- * pass.  Waiting is bounded: a block that finds nothing to claim for
- * idle_limit consecutive rounds (about a microsecond each) raises status
- * and returns, so a scheduling fault ends the launch instead of hanging it.
+ * pass.  Waiting is bounded: a block that finds nothing to claim while no
+ * ticket moves for idle_limit consecutive rounds (about a microsecond
+ * each; a ticket moves whenever any tile is claimed or any op is
+ * published) raises status and returns, so a scheduling fault ends the
+ * launch instead of hanging it, while long single-program runs, where most
+ * blocks wait on one op at a time, keep going.
  *
  * Ordering: a tile's stores are made visible (each thread fences, then the
  * block barrier) before its completion count; the finisher fences before
@@ -920,6 +925,23 @@ struct p2_binst {
 	uint64_t namp;
 	uint32_t op_off, nops;
 };
+
+/* Work tiles of an op on a register of namp amplitudes; for a pass of
+ * span `span` also the cosets per thread of a tile (*b). */
+__host__ __device__ __forceinline__ uint32_t p2_op_tiles(uint32_t kind,
+	uint64_t namp, uint32_t span, uint32_t *b)
+{
+	if (kind == P2_OP_PASS) {
+		const uint64_t nrep = namp >> span;
+		*b = nrep >= P2_BATCH_BIG_PASS ? P2_BATCH_COSETS : 1;
+		const uint64_t per = (uint64_t)*b * P2_TPB;
+		return (uint32_t)((nrep + per - 1) / per);
+	}
+	if (kind == P2_OP_ZERO)
+		return (uint32_t)((namp + P2_BATCH_ZERO_TILE - 1) /
+			P2_BATCH_ZERO_TILE);
+	return 1;
+}
 
 struct p2_bctl {
 	unsigned long long ticket;
@@ -967,9 +989,11 @@ __global__ void __launch_bounds__(P2_TPB, 5)
 	uint32_t held = 0xffffffffu;
 	uint32_t cursor = blockIdx.x % ninst;
 	unsigned int idle = 0;
+	unsigned long long seen = 0; /* tickets at the last idle round */
 	for (;;) {
 		if (threadIdx.x == 0) {
 			int what = 2;
+			unsigned long long sig = 0;
 			for (uint32_t k = 0; k < ninst; ++k) {
 				const uint32_t i = cursor + k < ninst
 					? cursor + k
@@ -978,6 +1002,7 @@ __global__ void __launch_bounds__(P2_TPB, 5)
 				const unsigned long long tk =
 					*(volatile unsigned long long *)&ctl[i]
 						 .ticket;
+				sig += tk * (2ull * i + 1ull);
 				if ((uint32_t)(tk >> 32) >= nops)
 					continue; /* program finished */
 				what = 0;
@@ -1000,6 +1025,10 @@ __global__ void __launch_bounds__(P2_TPB, 5)
 				}
 			}
 			if (what == 0) {
+				if (sig != seen) {
+					seen = sig;
+					idle = 0;
+				}
 				if (++idle > idle_limit) {
 					atomicOr(status, 1u);
 					what = 2;
@@ -2221,19 +2250,14 @@ extern "C" int p2d_batch_run(struct p2_dev *const *devs,
 		for (size_t k = 0; k < pg->nops; k++) {
 			struct p2_op op = pg->ops[k];
 			switch (op.kind) {
-			case P2_OP_PASS: {
+			case P2_OP_PASS:
 				op.a += (uint32_t)bp;
-				const uint64_t nrep = d->namp >> hp[op.a].span;
-				op.b = nrep >= P2_BATCH_BIG_PASS ? P2_BATCH_COSETS
-								  : 1;
-				const uint64_t per = (uint64_t)op.b * P2_TPB;
-				op.ntiles = (uint32_t)((nrep + per - 1) / per);
+				op.ntiles = p2_op_tiles(P2_OP_PASS, d->namp,
+					hp[op.a].span, &op.b);
 				break;
-			}
 			case P2_OP_ZERO:
-				op.ntiles = (uint32_t)((d->namp +
-						       P2_BATCH_ZERO_TILE - 1) /
-					P2_BATCH_ZERO_TILE);
+				op.ntiles = p2_op_tiles(P2_OP_ZERO, d->namp, 0,
+					&op.b);
 				break;
 			case P2_OP_WRITE:
 				op.a += (uint32_t)bw;
@@ -2342,6 +2366,351 @@ extern "C" int p2d_batch_run(struct p2_dev *const *devs,
 	d0->timed_passes += npass_run;
 	d0->h2d_bytes += o_pass; /* program tables */
 	return 0;
+}
+
+/* ---- device-side qDRIFT ------------------------------------------------- */
+
+/* xoshiro256** step (lib/xoshiro256ss.c of the reference). */
+__device__ __forceinline__ uint64_t p2_xo_next(uint64_t (&s)[4])
+{
+	const uint64_t x = s[1] * 5;
+	const uint64_t out = ((x << 7) | (x >> 57)) * 9;
+	const uint64_t t = s[1] << 17;
+	s[2] ^= s[0];
+	s[3] ^= s[1];
+	s[1] ^= s[2];
+	s[0] ^= s[3];
+	s[2] ^= t;
+	s[3] = (s[3] << 45) | (s[3] >> 19);
+	return out;
+}
+
+/*
+ * One block per sample: thread 0 runs the sample's generator for `depth`
+ * uniforms (sequential by nature, cheap); all threads then invert the CDF
+ * for them (prob_cdf_inverse: smallest i with y[i] > x, clamped; sign_dz:
+ * |c| < DBL_EPSILON -> 0); thread 0 plans the rotations in chunks of
+ * P2_QUEUE_FLUSH (a host flush plans the same chunks) and writes the
+ * sample's ops (zero, write dets, passes, gather dets) into its segment;
+ * nops[s] gets their count.  Segment capacities: depth passes, depth + 3
+ * ops.  rot/cs are per-sample scratch (cs first holds the uniforms).
+ */
+__global__ void k_qdrift_plan(const struct p2_qd_job job, uint32_t s0,
+	uint64_t namp, const uint64_t *__restrict__ rng0,
+	const double *__restrict__ cdf_y, const uint64_t *__restrict__ tflip,
+	const uint64_t *__restrict__ tphase, const double *__restrict__ tcf,
+	struct phase2_rot_in *rot, double *cs, struct phase2_pass *passes,
+	struct phase2_rot_rec *recs, struct p2_op *ops, uint32_t *nops)
+{
+	const uint32_t s = blockIdx.x;
+	const size_t base = (size_t)s * job.depth;
+	struct phase2_rot_in *r = rot + base;
+	double *c = cs + 2 * base;
+	if (threadIdx.x == 0) {
+		uint64_t st[4];
+		for (int k = 0; k < 4; ++k)
+			st[k] = rng0[4 * (size_t)(s0 + s) + k];
+		for (uint32_t i = 0; i < job.depth; ++i)
+			c[2 * i] = (double)(p2_xo_next(st) >> 11) * 0x1.0p-53;
+	}
+	__syncthreads();
+	for (uint32_t i = threadIdx.x; i < job.depth; i += blockDim.x) {
+		const double x = c[2 * i];
+		uint64_t lo = 0, hi = job.nterms;
+		while (lo < hi) {
+			const uint64_t mid = lo + (hi - lo) / 2;
+			if (cdf_y[mid] <= x)
+				lo = mid + 1;
+			else
+				hi = mid;
+		}
+		const uint64_t k = lo < job.nterms ? lo : job.nterms - 1;
+		const double a = tcf[k], f = fabs(a);
+		const int sg = f < DBL_EPSILON ? 1 : (a < f ? 0 : 2);
+		const double cf = sg == 1 ? 0.0 : (sg == 0 ? -1.0 : 1.0);
+		r[i].flip = tflip[k] & job.mask;
+		r[i].phase = tphase[k] & job.mask;
+		r[i].phi = job.omega * cf;
+		c[2 * i] = job.cs[sg][0];
+		c[2 * i + 1] = job.cs[sg][1];
+	}
+	__syncthreads();
+	if (threadIdx.x != 0)
+		return;
+	struct phase2_pass *ps = passes + base;
+	uint32_t np = 0;
+	for (uint32_t c0 = 0; c0 < job.depth; c0 += P2_QUEUE_FLUSH) {
+		const uint32_t n = job.depth - c0 < P2_QUEUE_FLUSH
+			? job.depth - c0
+			: P2_QUEUE_FLUSH;
+		const long got = p2_plan_core(job.nqb, r + c0, c + 2 * c0, n,
+			job.max_span, job.max_rots, P2_DEFAULT_PAD_SPAN, job.form,
+			ps + np, recs + base + c0);
+		for (long p = 0; p < got; ++p)
+			ps[np + p].rot_off += (uint32_t)(base + c0);
+		np += (uint32_t)(got > 0 ? got : 0);
+	}
+	struct p2_op *o = ops + (size_t)s * (job.depth + 3);
+	uint32_t k = 0;
+	o[k].kind = P2_OP_ZERO;
+	o[k].a = o[k].b = 0;
+	o[k].ntiles = p2_op_tiles(P2_OP_ZERO, namp, 0, &o[k].b);
+	k++;
+	o[k].kind = P2_OP_WRITE;
+	o[k].a = 0;
+	o[k].b = job.ndet;
+	o[k].ntiles = 1;
+	k++;
+	for (uint32_t p = 0; p < np; ++p, ++k) {
+		o[k].kind = P2_OP_PASS;
+		o[k].a = (uint32_t)base + p;
+		o[k].ntiles = p2_op_tiles(P2_OP_PASS, namp, ps[p].span, &o[k].b);
+	}
+	o[k].kind = P2_OP_GATHER;
+	o[k].a = (s0 + s) * job.ndet;
+	o[k].b = job.ndet;
+	o[k].ntiles = 1;
+	k++;
+	nops[s] = k;
+}
+
+/*
+ * Gather the samples' op segments into the registers' programs (one
+ * block): sample s0 + s runs on register (last - s0 - s) % nreg, so the
+ * run's last sample lands on register 0; a register's samples keep their
+ * order.  Thread 0 lays out the programs, all threads copy.
+ */
+__global__ void k_prog_compact(const struct p2_op *__restrict__ seg,
+	const uint32_t *__restrict__ nops, uint32_t samples, uint32_t cap,
+	uint64_t last, uint64_t s0, uint32_t nreg, struct p2_op *__restrict__ out,
+	struct p2_binst *inst)
+{
+	extern __shared__ uint32_t sh[];
+	uint32_t *off = sh;            /* [samples] */
+	uint32_t *fill = sh + samples; /* [nreg] */
+	if (threadIdx.x == 0) {
+		for (uint32_t r = 0; r < nreg; ++r)
+			fill[r] = 0;
+		for (uint32_t s = 0; s < samples; ++s)
+			fill[(uint32_t)((last - s0 - s) % nreg)] += nops[s];
+		uint32_t t = 0;
+		for (uint32_t r = 0; r < nreg; ++r) {
+			inst[r].op_off = t;
+			inst[r].nops = fill[r];
+			t += fill[r];
+			fill[r] = inst[r].op_off;
+		}
+		for (uint32_t s = 0; s < samples; ++s) {
+			const uint32_t r = (uint32_t)((last - s0 - s) % nreg);
+			off[s] = fill[r];
+			fill[r] += nops[s];
+		}
+	}
+	__syncthreads();
+	for (uint32_t s = 0; s < samples; ++s)
+		for (uint32_t k = threadIdx.x; k < nops[s]; k += blockDim.x)
+			out[off[s] + k] = seg[(size_t)s * cap + k];
+}
+
+/* Samples per device round: bounded by the rotations held at once. */
+#define P2_QD_ROUND_ROTS (UINT64_C(1) << 22)
+/* Amplitudes of all the registers of one round together (FP32: 512 MiB);
+ * from 2^26 amplitudes up the register runs alone. */
+#define P2_QD_ROUND_AMPS (UINT64_C(1) << 26)
+
+extern "C" int p2d_qdrift_device(struct p2_dev *d, const struct p2_qd_job *job,
+	const uint64_t *rng0, size_t samples, const double *cdf_y,
+	const uint64_t *tflip, const uint64_t *tphase, const double *tcf,
+	const uint64_t *det_idx, const double *det_val, double *gout,
+	uint64_t *npass_out)
+{
+	*npass_out = 0;
+	if (samples == 0)
+		return 0;
+	if (!p2d_batch_ok(d) || job->nterms == 0 || job->depth == 0 ||
+		samples > UINT32_MAX / (job->ndet ? job->ndet : 1)) {
+		log_error("device qdrift: unsupported register or sizes");
+		return -1;
+	}
+	const size_t depth = job->depth;
+	size_t G = (size_t)(P2_QD_ROUND_ROTS / depth);
+	if (G < 1)
+		G = 1;
+	if (G > samples)
+		G = samples;
+	if (G > 4096)
+		G = 4096;
+	size_t R = (size_t)(P2_QD_ROUND_AMPS / d->namp);
+	if (R > P2_QD_MAX_REGS)
+		R = P2_QD_MAX_REGS;
+	if (R > G)
+		R = G;
+	if (R < 1)
+		R = 1;
+	const size_t nt = job->nterms, nd = job->ndet;
+	const size_t cap = depth + 3;
+	/* device buffer: tables, per-round scratch and program, registers */
+	size_t sz[17], off[17], total = 0;
+	int k = 0;
+	sz[k++] = 4 * samples * sizeof(uint64_t);          /* 0 rng0 */
+	sz[k++] = nt * sizeof(double);                     /* 1 cdf */
+	sz[k++] = nt * sizeof(uint64_t);                   /* 2 flip */
+	sz[k++] = nt * sizeof(uint64_t);                   /* 3 phase */
+	sz[k++] = nt * sizeof(double);                     /* 4 cf */
+	sz[k++] = (nd ? nd : 1) * sizeof(uint64_t);        /* 5 widx */
+	sz[k++] = 2 * (nd ? nd : 1) * sizeof(double);      /* 6 wval */
+	sz[k++] = (samples * nd ? samples * nd : 1) * sizeof(uint64_t); /* 7 */
+	sz[k++] = (samples * nd ? samples * nd : 1) * sizeof(double2);  /* 8 */
+	sz[k++] = G * depth * sizeof(struct phase2_rot_in); /* 9 rot */
+	sz[k++] = 2 * G * depth * sizeof(double);          /* 10 cs */
+	sz[k++] = G * depth * sizeof(struct phase2_pass);  /* 11 passes */
+	sz[k++] = G * depth * sizeof(struct phase2_rot_rec); /* 12 recs */
+	sz[k++] = G * cap * sizeof(struct p2_op);          /* 13 segments */
+	sz[k++] = G * cap * sizeof(struct p2_op);          /* 14 program */
+	sz[k++] = G * sizeof(uint32_t);                    /* 15 nops */
+	sz[k++] = R * (sizeof(struct p2_binst) + sizeof(struct p2_bctl)) +
+		sizeof(unsigned int) +
+		(R - 1) * d->namp * sizeof(float2);        /* 16 regs */
+	for (int i = 0; i < 17; i++) {
+		off[i] = total;
+		total += (sz[i] + 255) & ~(size_t)255;
+	}
+	unsigned char *b = NULL;
+	CUDA_OK(cudaStreamSynchronize(d->stream), "device qdrift: sync");
+	CUDA_OK(cudaMalloc((void **)&b, total), "device qdrift: alloc");
+	uint64_t *gidx = (uint64_t *)malloc(sz[7]);
+	struct p2_binst *hinst = (struct p2_binst *)malloc(
+		R * sizeof(struct p2_binst));
+	int rc = -1;
+	cudaError_t e = gidx && hinst ? cudaSuccess
+				      : cudaErrorMemoryAllocation;
+	/* registers: 256-aligned copies first, then inst, ctl, status */
+	float2 *copies = (float2 *)(b + off[16]);
+	struct p2_binst *inst = (struct p2_binst *)(b + off[16] +
+		(R - 1) * d->namp * sizeof(float2));
+	struct p2_bctl *ctl = (struct p2_bctl *)(inst + R);
+	unsigned int *status = (unsigned int *)(ctl + R);
+	uint32_t *nops = (uint32_t *)(b + off[15]);
+	if (e == cudaSuccess) {
+		for (size_t s = 0; s < samples; s++)
+			for (size_t j = 0; j < nd; j++)
+				gidx[s * nd + j] = det_idx[j];
+		for (size_t r = 0; r < R; r++) {
+			hinst[r].state = r == 0 ? (float2 *)d->state
+						: copies + (r - 1) * d->namp;
+			hinst[r].namp = d->namp;
+			hinst[r].op_off = hinst[r].nops = 0;
+		}
+		const void *src[9] = { rng0, cdf_y, tflip, tphase, tcf, det_idx,
+			det_val, gidx, hinst };
+		void *dst[9] = { b + off[0], b + off[1], b + off[2], b + off[3],
+			b + off[4], b + off[5], b + off[6], b + off[7], inst };
+		const size_t n9[9] = { sz[0], nt * sizeof(double),
+			nt * sizeof(uint64_t), nt * sizeof(uint64_t),
+			nt * sizeof(double), nd * sizeof(uint64_t),
+			2 * nd * sizeof(double), samples * nd * sizeof(uint64_t),
+			R * sizeof(struct p2_binst) };
+		for (int i = 0; i < 9 && e == cudaSuccess; i++)
+			if (n9[i]) {
+				e = cudaMemcpyAsync(dst[i], src[i], n9[i],
+					cudaMemcpyHostToDevice, d->stream);
+				d->h2d_bytes += n9[i];
+			}
+	}
+	int per_sm = 0;
+	if (e == cudaSuccess)
+		e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm,
+			k_batch, P2_TPB, 0);
+	/* no op has more tiles than a span-0 pass or a zero (more blocks
+	 * would only poll) */
+	uint32_t cpt = 0;
+	uint64_t most = p2_op_tiles(P2_OP_PASS, d->namp, 0, &cpt);
+	const uint32_t zt = p2_op_tiles(P2_OP_ZERO, d->namp, 0, &cpt);
+	if (zt > most)
+		most = zt;
+	most *= R;
+	unsigned grid =
+		(unsigned)d->sm_count * (unsigned)(per_sm > 0 ? per_sm : 1);
+	if (most < grid)
+		grid = (unsigned)most;
+	uint64_t nops_run = 0;
+	for (size_t s0 = 0; s0 < samples && e == cudaSuccess; s0 += G) {
+		const uint32_t g = (uint32_t)(samples - s0 < G ? samples - s0 : G);
+		const uint32_t nreg = (uint32_t)(g < R ? g : R);
+		k_qdrift_plan<<<g, P2_TPB, 0, d->stream>>>(*job,
+			(uint32_t)s0, d->namp, (const uint64_t *)(b + off[0]),
+			(const double *)(b + off[1]),
+			(const uint64_t *)(b + off[2]),
+			(const uint64_t *)(b + off[3]),
+			(const double *)(b + off[4]),
+			(struct phase2_rot_in *)(b + off[9]),
+			(double *)(b + off[10]),
+			(struct phase2_pass *)(b + off[11]),
+			(struct phase2_rot_rec *)(b + off[12]),
+			(struct p2_op *)(b + off[13]), nops);
+		e = cudaGetLastError();
+		if (e == cudaSuccess)
+			k_prog_compact<<<1, 256, (g + nreg) * sizeof(uint32_t),
+				d->stream>>>((const struct p2_op *)(b + off[13]),
+				nops, g, (uint32_t)cap, (uint64_t)samples - 1,
+				(uint64_t)s0, nreg,
+				(struct p2_op *)(b + off[14]), inst);
+		if (e == cudaSuccess)
+			e = cudaMemsetAsync(ctl, 0,
+				nreg * sizeof *ctl + sizeof(unsigned int),
+				d->stream);
+		if (e == cudaSuccess)
+			e = cudaMemsetAsync(status, 0, sizeof(unsigned int),
+				d->stream);
+		if (e == cudaSuccess)
+			k_batch<<<grid, P2_TPB, 0, d->stream>>>(inst, nreg,
+				(const struct p2_op *)(b + off[14]),
+				(const struct phase2_pass *)(b + off[11]),
+				(const struct phase2_rot_rec *)(b + off[12]),
+				(const uint64_t *)(b + off[5]),
+				(const double *)(b + off[6]),
+				(const uint64_t *)(b + off[7]),
+				(double2 *)(b + off[8]), ctl, status,
+				P2_BATCH_IDLE_LIMIT);
+		if (e == cudaSuccess)
+			e = cudaGetLastError();
+		d->launches += 3;
+		unsigned int st = 0;
+		if (e == cudaSuccess)
+			e = cudaMemcpyAsync(&st, status, sizeof st,
+				cudaMemcpyDeviceToHost, d->stream);
+		if (e == cudaSuccess)
+			e = cudaMemcpyAsync(hinst, inst,
+				nreg * sizeof(struct p2_binst),
+				cudaMemcpyDeviceToHost, d->stream);
+		if (e == cudaSuccess)
+			e = cudaStreamSynchronize(d->stream);
+		if (e == cudaSuccess && st) {
+			log_error("device qdrift: a block found no work for %u"
+				  " rounds",
+				P2_BATCH_IDLE_LIMIT);
+			e = cudaErrorLaunchFailure;
+		}
+		for (uint32_t r = 0; e == cudaSuccess && r < nreg; r++)
+			nops_run += hinst[r].nops;
+		nops_run -= 3ull * g;
+	}
+	if (e == cudaSuccess && samples * nd)
+		e = cudaMemcpy(gout, b + off[8], samples * nd * sizeof(double2),
+			cudaMemcpyDeviceToHost);
+	if (e == cudaSuccess) {
+		d->d2h_bytes += samples * nd * sizeof(double2);
+		d->passes += nops_run;
+		d->rotations += (uint64_t)samples * depth;
+		*npass_out = nops_run;
+		rc = 0;
+	} else {
+		log_error("device qdrift: %s", cudaGetErrorString(e));
+	}
+	free(gidx);
+	free(hinst);
+	cudaFree(b);
+	return rc;
 }
 
 /* ---- allocation-free norm (phase2_norm2_noalloc) ------------------------ */

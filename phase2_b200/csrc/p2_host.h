@@ -22,6 +22,7 @@ struct p2_settings {
 	int order;
 	int fp32_form; /* enum phase2_form used for FP32 registers */
 	int batch_persistent; /* batched drivers: one persistent launch */
+	int device_sampling; /* qdrift on the GPU: PHASE2_DEVICE_SAMPLING_* */
 };
 extern struct p2_settings p2_cfg;
 void p2_settings_from_env(void);

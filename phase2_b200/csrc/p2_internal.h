@@ -153,6 +153,40 @@ int p2d_batch_run(struct p2_dev *const *devs,
 	const struct p2_prog *const *progs, size_t n, double *gout,
 	double *kernel_ms);
 
+/* ---- device-side qDRIFT (qdrift_simul with device sampling) ------------ */
+
+/*
+ * One qDRIFT run executed on the device: for each sample s (generator
+ * state rng0[s], taken where the host run would be), the device draws
+ * `depth` terms from the |c| CDF (xoshiro256** top 53 bits, smallest i
+ * with y[i] > x, sign with the DBL_EPSILON dead zone), plans them exactly
+ * as a host flush would (chunks of P2_QUEUE_FLUSH, plan_core.h, cos/sin of
+ * omega * {-1, 0, +1} given in cs), and the program zero / write dets /
+ * passes / gather dets of every sample runs in one persistent launch.
+ * Samples are independent (each starts from the trial state), so small
+ * registers run up to P2_QD_MAX_REGS samples at once on copies of the
+ * state; the last sample always runs on the register itself, which ends
+ * holding its state as after the host loop.
+ */
+#define P2_QD_MAX_REGS 256
+struct p2_qd_job {
+	uint32_t nqb, depth;
+	uint64_t nterms, mask;
+	double omega;
+	double cs[3][2]; /* cos, sin of omega * cf, cf = -1, 0, +1 */
+	int max_span, max_rots, form;
+	uint32_t ndet;
+};
+
+/* Samples (rng0: 4 words each) run in groups; gout gets ndet amplitudes
+ * (re, im) per sample, in sample order.  *npass_out: passes executed.
+ * 0 or -1. */
+int p2d_qdrift_device(struct p2_dev *d, const struct p2_qd_job *job,
+	const uint64_t *rng0, size_t samples, const double *cdf_y,
+	const uint64_t *tflip, const uint64_t *tphase, const double *tcf,
+	const uint64_t *det_idx, const double *det_val, double *gout,
+	uint64_t *npass_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -19,6 +19,7 @@ struct p2_settings p2_cfg = {
 	.order = PHASE2_ORDER_LEX,
 	.fp32_form = PHASE2_FORM_LIFTED_F32,
 	.batch_persistent = 1,
+	.device_sampling = PHASE2_DEVICE_SAMPLING_AUTO,
 };
 
 void p2_settings_from_env(void)
@@ -41,6 +42,17 @@ void p2_settings_from_env(void)
 		else
 			log_warn("PHASE2_FP32_FORM=%s not understood", f);
 	}
+	const char *d = getenv("PHASE2_DEVICE_SAMPLING");
+	if (d && *d) {
+		if (!strcmp(d, "0") || !strcmp(d, "off"))
+			p2_cfg.device_sampling = PHASE2_DEVICE_SAMPLING_OFF;
+		else if (!strcmp(d, "1") || !strcmp(d, "on"))
+			p2_cfg.device_sampling = PHASE2_DEVICE_SAMPLING_ON;
+		else if (!strcmp(d, "auto"))
+			p2_cfg.device_sampling = PHASE2_DEVICE_SAMPLING_AUTO;
+		else
+			log_warn("PHASE2_DEVICE_SAMPLING=%s not understood", d);
+	}
 }
 
 int phase2_set_fp32_form(int form)
@@ -59,6 +71,16 @@ int phase2_get_fp32_form(void)
 int phase2_set_batch_persistent(int on)
 {
 	p2_cfg.batch_persistent = on ? 1 : 0;
+	return 0;
+}
+
+int phase2_set_device_sampling(int mode)
+{
+	if (mode != PHASE2_DEVICE_SAMPLING_OFF &&
+		mode != PHASE2_DEVICE_SAMPLING_ON &&
+		mode != PHASE2_DEVICE_SAMPLING_AUTO)
+		return -1;
+	p2_cfg.device_sampling = mode;
 	return 0;
 }
 

@@ -273,6 +273,9 @@ def test_settings_validate():
     assert L.phase2_set_term_order(2) == 0
     assert L.phase2_get_term_order() == 2
     assert L.phase2_set_term_order(0) == 0
+    assert L.phase2_set_device_sampling(3) == -1
+    for mode in (0, 1, 2):
+        assert L.phase2_set_device_sampling(mode) == 0
 
 
 def test_phase2_run_rejects_without_touching_device():

@@ -454,6 +454,60 @@ def test_persistent_batch(kind, oracle_lib):
         assert np.max(np.abs(z - want)) < FP32_TOL, kind
 
 
+def _qdrift_both_ways(nqb, t, d, samples, depth, step, seed):
+    """FP32 qdrift with host sampling, then with device sampling."""
+    p2.set_precision(p2.PREC_FP32)
+    p2.set_device_sampling(False)
+    try:
+        host, hst = p2.qdrift(nqb, t, d, samples, depth, step, seed,
+                              with_stats=True, with_state=True)
+        p2.set_device_sampling(True)
+        dev, st = p2.qdrift(nqb, t, d, samples, depth, step, seed,
+                            with_stats=True, with_state=True)
+    finally:
+        p2.set_device_sampling(p2.DEVICE_SAMPLING_AUTO)
+        p2.set_precision(p2.PREC_FP64)
+    # the register ends holding the last sample's state either way
+    assert np.array_equal(st["state"], hst["state"])
+    return host, dev, st
+
+
+@pytest.mark.parametrize("nqb,nterms,ndet,samples,depth", [
+    (9, 60, 1, 3, 40),        # one determinant, short circuits
+    (11, 500, 5, 5, 300),
+    (12, 200, 3, 2, 9000),    # planned in two chunks of the host queue
+    (8, 30, 2, 4200, 3),      # two planning rounds, the last one short
+    (16, 300, 4, 7, 700),
+])
+def test_qdrift_device_sampling(nqb, nterms, ndet, samples, depth,
+                                oracle_lib):
+    """Device sampling (draws, plans and passes on the GPU; small registers
+    run many samples at once on copies of the state) gives the host loop's
+    overlaps and final register bit for bit, within the FP32 tolerance of
+    the oracle."""
+    t = workloads.jw_terms(nqb, nterms, seed=nqb * 7 + depth)
+    # a term below DBL_EPSILON draws the zero angle
+    t.cf[3] = 1e-17
+    d = workloads.hamming_dets(nqb, ndet, nqb // 2, seed=nqb + ndet)
+    host, dev, st = _qdrift_both_ways(nqb, t, d, samples, depth, 0.02,
+                                      0x5EED + nqb)
+    assert np.array_equal(dev, host)
+    assert st["passes"] > 0 and st["launches"] >= 3
+    if samples * depth <= 20000:
+        want = oracle_lib.qdrift(nqb, t.flip, t.phase, t.cf, d.idx, d.cf,
+                                 samples, depth, 0.02, 0x5EED + nqb)
+        assert np.max(np.abs(dev - want)) < FP32_TOL
+
+
+def test_qdrift_device_sampling_h2o(golden):
+    """The water fixture (real molecular terms) under device sampling."""
+    _, t, d = _h2o(golden)
+    host, dev, _ = _qdrift_both_ways(10, t, d, 6, 300, 0.01, 0xC0FFEE)
+    assert np.array_equal(dev, host)
+    want = np.array([_cz(v) for v in golden["h2o"]["qdrift"]])
+    assert np.max(np.abs(dev - want)) < FP32_TOL
+
+
 def test_persistent_batch_empty_and_single():
     """Edge cases: an empty batch, one instance, an instance with no
     outputs (zero steps) beside others."""
