@@ -204,37 +204,41 @@ static void qdrift_draw(struct qdrift *qd)
 	}
 }
 
-static int qdrift_device_ok(const struct qdrift *qd)
+/* Registers that device sampling (p2d_sampled_device) takes under the
+ * current mode: FP32 in the FP32-arithmetic form, at most 31 qubits,
+ * multi-determinant trial state; AUTO also caps the width. */
+static int device_sampling_ok(const struct circ *ct)
 {
-	const struct circ *ct = &qd->ct;
 	const struct p2_qreg *b = ct->reg.backend;
 	if (p2_cfg.device_sampling == PHASE2_DEVICE_SAMPLING_OFF ||
 		(p2_cfg.device_sampling == PHASE2_DEVICE_SAMPLING_AUTO &&
 			ct->reg.qb_lo > PHASE2_DEVICE_SAMPLING_AUTO_QB))
 		return 0;
-	return b && b->rec == NULL &&
-		b->prec == PHASE2_PREC_FP32 &&
+	return b && b->rec == NULL && b->prec == PHASE2_PREC_FP32 &&
 		p2_form_for(PHASE2_PREC_FP32) == PHASE2_FORM_LIFTED_F32 &&
 		p2d_batch_ok(b->dev) && ct->stprep_kind == STPREP_MULTIDET &&
-		ct->md.len > 0 && qd->ranct.cdf.len > 0 &&
-		qd->ranct.hm_ran.len > 0 &&
-		qd->ranct.hm_ran.len <= UINT32_MAX - 3;
+		ct->md.len > 0;
 }
 
 /*
- * qdrift_simul with the draws, plans and passes on the GPU
- * (p2d_qdrift_device).  The host steps the generator to every sample's
- * start (depth draws each) and draws the last sample itself, so qd->rng
- * and the drawn terms end as the host loop leaves them; each overlap is
- * then the host loop's expression over the gathered amplitudes.
+ * A sampled driver run with the draws, plans and passes on the GPU.  The
+ * caller fills job's depth, length, halves, reverse_odd and rphi; pool and
+ * cdf are the drawable terms, head/hphi the head terms and their angles.
+ * The host steps *rng to the start of every (sample, half) (depth draws
+ * each) and lets last_half(obj) draw the final half itself, so the
+ * generator and the driver's drawn terms end as the host loop leaves them;
+ * each overlap is the host loop's expression over the gathered amplitudes.
  */
-static int qdrift_simul_device(struct qdrift *qd)
+static int sampled_device(struct circ *ct, struct p2_smp_job *job,
+	const struct circ_hamil *pool, const struct prob_cdf *cdf,
+	const struct circ_hamil *head, const double *hphi,
+	struct xoshiro256ss *rng, void (*last_half)(void *), void *obj,
+	struct phase2_step_writer *sw, const char *who)
 {
-	struct circ *ct = &qd->ct;
 	struct circ_values *vals = &ct->vals;
 	struct p2_qreg *b = ct->reg.backend;
-	const size_t ns = vals->len, depth = qd->ranct.hm_ran.len;
-	const size_t nt = qd->ranct.cdf.len, nd = ct->md.len;
+	const size_t ns = vals->len, nh = job->halves;
+	const size_t nt = cdf->len, nd = ct->md.len, nl = job->length;
 	if (ns == 0)
 		return 0;
 	struct p2_dev *dev = p2_qreg_direct(&ct->reg);
@@ -242,81 +246,115 @@ static int qdrift_simul_device(struct qdrift *qd)
 		return -1;
 	for (size_t d = 0; d < nd; d++)
 		if (ct->md.dets[d].idx >= ct->reg.namp) {
-			log_error("qdrift_simul: determinant %llu out of range",
+			log_error("%s: determinant %llu out of range", who,
 				(unsigned long long)ct->md.dets[d].idx);
 			return p2_qreg_fail(&ct->reg);
 		}
-	uint64_t *rng0 = malloc(sizeof *rng0 * 4 * ns);
-	uint64_t *tflip = malloc(sizeof *tflip * nt);
-	uint64_t *tphase = malloc(sizeof *tphase * nt);
-	double *tcf = malloc(sizeof *tcf * nt);
+	uint64_t *rng0 = malloc(sizeof *rng0 * 4 * ns * nh);
+	uint64_t *tfl = malloc(sizeof *tfl * (nt ? nt : 1));
+	uint64_t *tph = malloc(sizeof *tph * (nt ? nt : 1));
+	double *tcf = malloc(sizeof *tcf * (nt ? nt : 1));
+	uint64_t *hfl = malloc(sizeof *hfl * (nl ? nl : 1));
+	uint64_t *hph = malloc(sizeof *hph * (nl ? nl : 1));
+	double *hcs = malloc(sizeof *hcs * 2 * (nl ? nl : 1));
 	uint64_t *didx = malloc(sizeof *didx * nd);
 	double *dval = malloc(sizeof *dval * 2 * nd);
 	_Complex double *g = malloc(sizeof *g * ns * nd);
 	int rc = -1;
-	if (!rng0 || !tflip || !tphase || !tcf || !didx || !dval || !g) {
-		log_error("qdrift_simul: allocation failed");
+	if (!rng0 || !tfl || !tph || !tcf || !hfl || !hph || !hcs || !didx ||
+		!dval || !g) {
+		log_error("%s: allocation failed", who);
 		goto out;
 	}
-	for (size_t i = 0; i < ns; i++) {
-		memcpy(&rng0[4 * i], qd->rng.s, sizeof qd->rng.s);
-		if (i + 1 == ns)
-			qdrift_draw(qd);
+	for (size_t i = 0; i < ns * nh; i++) {
+		memcpy(&rng0[4 * i], rng->s, sizeof rng->s);
+		if (i + 1 == ns * nh)
+			last_half(obj);
 		else
-			for (size_t k = 0; k < depth; k++)
-				(void)xoshiro256ss_next(&qd->rng);
+			for (size_t k = 0; k < job->depth; k++)
+				(void)xoshiro256ss_next(rng);
 	}
 	for (size_t k = 0; k < nt; k++) {
-		tflip[k] = ct->hm.terms[k].op.pak[0];
-		tphase[k] = ct->hm.terms[k].op.pak[1];
-		tcf[k] = ct->hm.terms[k].cf;
+		tfl[k] = pool->terms[k].op.pak[0];
+		tph[k] = pool->terms[k].op.pak[1];
+		tcf[k] = pool->terms[k].cf;
+	}
+	for (size_t k = 0; k < nl; k++) {
+		hfl[k] = head->terms[k].op.pak[0];
+		hph[k] = head->terms[k].op.pak[1];
+		hcs[2 * k] = cos(hphi[k]);
+		hcs[2 * k + 1] = sin(hphi[k]);
 	}
 	for (size_t d = 0; d < nd; d++) {
 		didx[d] = ct->md.dets[d].idx;
 		dval[2 * d] = creal(ct->md.dets[d].cf);
 		dval[2 * d + 1] = cimag(ct->md.dets[d].cf);
 	}
-	struct p2_qd_job job;
-	memset(&job, 0, sizeof job);
-	job.nqb = ct->reg.qb_lo;
-	job.depth = (uint32_t)depth;
-	job.nterms = nt;
-	job.mask = ct->reg.qb_lo >= 64 ? ~UINT64_C(0)
-				       : (UINT64_C(1) << ct->reg.qb_lo) - 1;
-	job.omega = asin(qd->dt.step_size);
-	/* the angles a host flush would plan: omega * sign_dz(cf) */
+	job->nqb = ct->reg.qb_lo;
+	job->ndet = (uint32_t)nd;
+	job->nterms = nt;
+	job->mask = ct->reg.qb_lo >= 64 ? ~UINT64_C(0)
+					: (UINT64_C(1) << ct->reg.qb_lo) - 1;
 	for (int sg = 0; sg < 3; sg++) {
-		const double phi = job.omega * (double)(sg - 1);
-		job.cs[sg][0] = cos(phi);
-		job.cs[sg][1] = sin(phi);
+		job->rcs[sg][0] = cos(job->rphi[sg]);
+		job->rcs[sg][1] = sin(job->rphi[sg]);
 	}
-	job.max_span = b->max_span;
-	job.max_rots = b->max_rots;
-	job.form = PHASE2_FORM_LIFTED_F32;
-	job.ndet = (uint32_t)nd;
+	job->max_span = b->max_span;
+	job->max_rots = b->max_rots;
+	job->form = PHASE2_FORM_LIFTED_F32;
 	uint64_t npass = 0;
-	if (p2d_qdrift_device(dev, &job, rng0, ns, qd->ranct.cdf.y, tflip,
-		    tphase, tcf, didx, dval, (double *)g, &npass) < 0) {
+	if (p2d_sampled_device(dev, job, rng0, ns, cdf->y, tfl, tph, tcf, hfl,
+		    hph, hphi, hcs, didx, dval, (double *)g, &npass) < 0) {
 		p2_qreg_fail(&ct->reg);
 		goto out;
 	}
 	for (size_t i = 0; i < ns; i++) {
 		vals->z[i] = p2_circ_overlap(&ct->md, g + i * nd);
-		if (emit(qd->sw, i, vals->z[i]) < 0) {
-			log_error("qdrift_simul: sample %zu output failed", i);
+		if (emit(sw, i, vals->z[i]) < 0) {
+			log_error("%s: sample %zu output failed", who, i);
 			goto out;
 		}
 	}
 	rc = 0;
 out:
 	free(rng0);
-	free(tflip);
-	free(tphase);
+	free(tfl);
+	free(tph);
 	free(tcf);
+	free(hfl);
+	free(hph);
+	free(hcs);
 	free(didx);
 	free(dval);
 	free(g);
 	return rc;
+}
+
+static void qdrift_last_half(void *obj)
+{
+	qdrift_draw(obj);
+}
+
+/* qdrift_simul on the GPU: one forward half of `depth` draws per sample
+ * at angle asin(step_size) * sign_dz(c), as the host loop applies them. */
+static int qdrift_simul_device(struct qdrift *qd)
+{
+	struct p2_smp_job job;
+	memset(&job, 0, sizeof job);
+	job.depth = (uint32_t)qd->ranct.hm_ran.len;
+	job.halves = 1;
+	const double omega = asin(qd->dt.step_size);
+	for (int sg = 0; sg < 3; sg++)
+		job.rphi[sg] = omega * (double)(sg - 1);
+	return sampled_device(&qd->ct, &job, &qd->ct.hm, &qd->ranct.cdf, NULL,
+		NULL, &qd->rng, qdrift_last_half, qd, qd->sw, "qdrift_simul");
+}
+
+static int qdrift_device_ok(const struct qdrift *qd)
+{
+	return device_sampling_ok(&qd->ct) && qd->ranct.cdf.len > 0 &&
+		qd->ranct.hm_ran.len > 0 &&
+		qd->ranct.hm_ran.len < (UINT64_C(1) << 31);
 }
 
 int qdrift_simul(struct qdrift *qd)
@@ -445,10 +483,56 @@ static int cmpsit_sample(struct cmpsit *cp)
 	return 0;
 }
 
+static void cmpsit_last_half(void *obj)
+{
+	(void)cmpsit_sample(obj);
+}
+
+/* cmpsit_simul on the GPU: per step a forward half (head at
+ * 0.5 * (c * angle_det), then depth draws at 0.5 * (sign_dz(c) * tau))
+ * and a reversed half of fresh draws, as the host loop applies them. */
+static int cmpsit_simul_device(struct cmpsit *cp)
+{
+	struct cmpsit_ranct *rc = &cp->ranct;
+	const size_t nl = cp->dt.length;
+	double *hphi = malloc(sizeof *hphi * (nl ? nl : 1));
+	if (!hphi)
+		return -1;
+	for (size_t k = 0; k < nl; k++)
+		hphi[k] = 0.5 * (rc->hm_det.terms[k].cf * cp->dt.angle_det);
+	struct p2_smp_job job;
+	memset(&job, 0, sizeof job);
+	job.depth = (uint32_t)rc->depth;
+	job.length = (uint32_t)nl;
+	job.halves = (uint32_t)(2 * cp->dt.steps);
+	job.reverse_odd = 1;
+	for (int sg = 0; sg < 3; sg++)
+		job.rphi[sg] = 0.5 * ((double)(sg - 1) * rc->angle_rand);
+	const int r = sampled_device(&cp->ct, &job, &rc->hm_ran, &rc->cdf,
+		&rc->hm_det, hphi, &cp->rng, cmpsit_last_half, cp, cp->sw,
+		"cmpsit_simul");
+	free(hphi);
+	return r;
+}
+
+static int cmpsit_device_ok(const struct cmpsit *cp)
+{
+	const uint64_t T = 2 * (uint64_t)cp->dt.steps *
+		((uint64_t)cp->dt.length + cp->ranct.depth);
+	return device_sampling_ok(&cp->ct) && cp->dt.steps > 0 &&
+		cp->dt.steps < (UINT64_C(1) << 30) &&
+		cp->ranct.depth < (UINT64_C(1) << 31) &&
+		cp->dt.length < (UINT64_C(1) << 31) &&
+		(cp->ranct.depth == 0 || cp->ranct.cdf.len > 0) &&
+		T < (UINT64_C(1) << 31);
+}
+
 int cmpsit_simul(struct cmpsit *cp)
 {
 	struct circ *ct = &cp->ct;
 	struct circ_values *vals = &ct->vals;
+	if (cmpsit_device_ok(cp))
+		return cmpsit_simul_device(cp);
 	for (size_t i = 0; i < vals->len; i++) {
 		if (circ_prepst(ct) < 0)
 			return -1;

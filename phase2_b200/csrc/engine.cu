@@ -32,6 +32,7 @@
 
 #include <float.h>
 #include <stdint.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -2386,211 +2387,327 @@ __device__ __forceinline__ uint64_t p2_xo_next(uint64_t (&s)[4])
 }
 
 /*
- * One block per sample: thread 0 runs the sample's generator for `depth`
- * uniforms (sequential by nature, cheap); all threads then invert the CDF
- * for them (prob_cdf_inverse: smallest i with y[i] > x, clamped; sign_dz:
- * |c| < DBL_EPSILON -> 0); thread 0 plans the rotations in chunks of
- * P2_QUEUE_FLUSH (a host flush plans the same chunks) and writes the
- * sample's ops (zero, write dets, passes, gather dets) into its segment;
- * nops[s] gets their count.  Segment capacities: depth passes, depth + 3
- * ops.  rot/cs are per-sample scratch (cs first holds the uniforms).
+ * Device sampling (p2d_sampled_device).  A sample's rotation stream is
+ * `halves` halves of (length + depth) rotations: a forward half is the
+ * head terms 0..length-1 then the draws 0..depth-1, a reversed half (odd
+ * halves when reverse_odd) the draws depth-1..0 then the head terms
+ * length-1..0.  Buffers of a round of g samples, T rotations each:
+ * x[(s * halves + h) * depth + i] uniforms, rot/cs/passes/recs at
+ * s * T + position, per-chunk pass counts npc[s * C + c].
  */
-__global__ void k_qdrift_plan(const struct p2_qd_job job, uint32_t s0,
-	uint64_t namp, const uint64_t *__restrict__ rng0,
-	const double *__restrict__ cdf_y, const uint64_t *__restrict__ tflip,
-	const uint64_t *__restrict__ tphase, const double *__restrict__ tcf,
-	struct phase2_rot_in *rot, double *cs, struct phase2_pass *passes,
-	struct phase2_rot_rec *recs, struct p2_op *ops, uint32_t *nops)
+
+/* Uniforms of one (sample, half): the half's generator, depth draws. */
+__global__ void k_smp_draw(const struct p2_smp_job job, uint32_t s0,
+	uint32_t n, const uint64_t *__restrict__ rng0, double *__restrict__ x)
 {
-	const uint32_t s = blockIdx.x;
-	const size_t base = (size_t)s * job.depth;
-	struct phase2_rot_in *r = rot + base;
-	double *c = cs + 2 * base;
-	if (threadIdx.x == 0) {
-		uint64_t st[4];
-		for (int k = 0; k < 4; ++k)
-			st[k] = rng0[4 * (size_t)(s0 + s) + k];
-		for (uint32_t i = 0; i < job.depth; ++i)
-			c[2 * i] = (double)(p2_xo_next(st) >> 11) * 0x1.0p-53;
-	}
-	__syncthreads();
-	for (uint32_t i = threadIdx.x; i < job.depth; i += blockDim.x) {
-		const double x = c[2 * i];
-		uint64_t lo = 0, hi = job.nterms;
-		while (lo < hi) {
-			const uint64_t mid = lo + (hi - lo) / 2;
-			if (cdf_y[mid] <= x)
-				lo = mid + 1;
-			else
-				hi = mid;
-		}
-		const uint64_t k = lo < job.nterms ? lo : job.nterms - 1;
-		const double a = tcf[k], f = fabs(a);
-		const int sg = f < DBL_EPSILON ? 1 : (a < f ? 0 : 2);
-		const double cf = sg == 1 ? 0.0 : (sg == 0 ? -1.0 : 1.0);
-		r[i].flip = tflip[k] & job.mask;
-		r[i].phase = tphase[k] & job.mask;
-		r[i].phi = job.omega * cf;
-		c[2 * i] = job.cs[sg][0];
-		c[2 * i + 1] = job.cs[sg][1];
-	}
-	__syncthreads();
-	if (threadIdx.x != 0)
+	const uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
+	if (id >= n)
 		return;
-	struct phase2_pass *ps = passes + base;
-	uint32_t np = 0;
-	for (uint32_t c0 = 0; c0 < job.depth; c0 += P2_QUEUE_FLUSH) {
-		const uint32_t n = job.depth - c0 < P2_QUEUE_FLUSH
-			? job.depth - c0
-			: P2_QUEUE_FLUSH;
-		const long got = p2_plan_core(job.nqb, r + c0, c + 2 * c0, n,
-			job.max_span, job.max_rots, P2_DEFAULT_PAD_SPAN, job.form,
-			ps + np, recs + base + c0);
-		for (long p = 0; p < got; ++p)
-			ps[np + p].rot_off += (uint32_t)(base + c0);
-		np += (uint32_t)(got > 0 ? got : 0);
+	uint64_t st[4];
+	const size_t g = (size_t)s0 * job.halves + id;
+	for (int k = 0; k < 4; ++k)
+		st[k] = rng0[4 * g + k];
+	double *out = x + (size_t)id * job.depth;
+	for (uint32_t i = 0; i < job.depth; ++i)
+		out[i] = (double)(p2_xo_next(st) >> 11) * 0x1.0p-53;
+}
+
+/* The rotation at every stream position: head terms from the head table,
+ * draws by CDF inversion (prob_cdf_inverse: smallest i with y[i] > x,
+ * clamped) with the sign dead zone (|c| < DBL_EPSILON -> 0). */
+__global__ void k_smp_stream(const struct p2_smp_job job, uint64_t total,
+	const double *__restrict__ x, const double *__restrict__ cdf_y,
+	const uint64_t *__restrict__ tflip, const uint64_t *__restrict__ tphase,
+	const double *__restrict__ tcf, const uint64_t *__restrict__ hflip,
+	const uint64_t *__restrict__ hphase, const double *__restrict__ hphi,
+	const double *__restrict__ hcs, struct phase2_rot_in *__restrict__ rot,
+	double *__restrict__ cs)
+{
+	const uint64_t per = (uint64_t)job.length + job.depth;
+	const uint64_t T = per * job.halves;
+	for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+		q < total; q += (uint64_t)gridDim.x * blockDim.x) {
+		const uint64_t s = q / T, p = q - s * T;
+		const uint64_t h = p / per, o = p - h * per;
+		const bool rev = job.reverse_odd && (h & 1);
+		int64_t head = -1, draw = -1;
+		if (!rev) {
+			if (o < job.length)
+				head = (int64_t)o;
+			else
+				draw = (int64_t)(o - job.length);
+		} else {
+			if (o < job.depth)
+				draw = (int64_t)(job.depth - 1 - o);
+			else
+				head = (int64_t)(job.length - 1 - (o - job.depth));
+		}
+		struct phase2_rot_in r;
+		double c, sn;
+		if (head >= 0) {
+			r.flip = hflip[head] & job.mask;
+			r.phase = hphase[head] & job.mask;
+			r.phi = hphi[head];
+			c = hcs[2 * head];
+			sn = hcs[2 * head + 1];
+		} else {
+			const double xv =
+				x[(s * job.halves + h) * job.depth + (uint64_t)draw];
+			uint64_t lo = 0, hi = job.nterms;
+			while (lo < hi) {
+				const uint64_t mid = lo + (hi - lo) / 2;
+				if (cdf_y[mid] <= xv)
+					lo = mid + 1;
+				else
+					hi = mid;
+			}
+			const uint64_t k = lo < job.nterms ? lo : job.nterms - 1;
+			const double a = tcf[k], f = fabs(a);
+			const int sg = f < DBL_EPSILON ? 1 : (a < f ? 0 : 2);
+			r.flip = tflip[k] & job.mask;
+			r.phase = tphase[k] & job.mask;
+			/* selects, not an index (keeps job out of local memory) */
+			r.phi = sg == 0 ? job.rphi[0]
+					: (sg == 1 ? job.rphi[1] : job.rphi[2]);
+			c = sg == 0 ? job.rcs[0][0]
+				    : (sg == 1 ? job.rcs[1][0] : job.rcs[2][0]);
+			sn = sg == 0 ? job.rcs[0][1]
+				     : (sg == 1 ? job.rcs[1][1] : job.rcs[2][1]);
+		}
+		rot[q] = r;
+		cs[2 * q] = c;
+		cs[2 * q + 1] = sn;
 	}
-	struct p2_op *o = ops + (size_t)s * (job.depth + 3);
-	uint32_t k = 0;
-	o[k].kind = P2_OP_ZERO;
-	o[k].a = o[k].b = 0;
-	o[k].ntiles = p2_op_tiles(P2_OP_ZERO, namp, 0, &o[k].b);
-	k++;
-	o[k].kind = P2_OP_WRITE;
-	o[k].a = 0;
-	o[k].b = job.ndet;
-	o[k].ntiles = 1;
-	k++;
-	for (uint32_t p = 0; p < np; ++p, ++k) {
-		o[k].kind = P2_OP_PASS;
-		o[k].a = (uint32_t)base + p;
-		o[k].ntiles = p2_op_tiles(P2_OP_PASS, namp, ps[p].span, &o[k].b);
-	}
-	o[k].kind = P2_OP_GATHER;
-	o[k].a = (s0 + s) * job.ndet;
-	o[k].b = job.ndet;
-	o[k].ntiles = 1;
-	k++;
-	nops[s] = k;
 }
 
 /*
- * Gather the samples' op segments into the registers' programs (one
- * block): sample s0 + s runs on register (last - s0 - s) % nreg, so the
- * run's last sample lands on register 0; a register's samples keep their
- * order.  Thread 0 lays out the programs, all threads copy.
+ * One block per P2_QUEUE_FLUSH chunk of a sample's stream: the passes a
+ * host flush of that chunk plans (plan_core.h), at the chunk's position;
+ * npc gets their count.  The flip masks are staged in shared memory for
+ * the sequential boundary scan (thread 0); the records are then filled by
+ * all threads, and each pass's scale is the parity of its records' signs.
  */
-__global__ void k_prog_compact(const struct p2_op *__restrict__ seg,
-	const uint32_t *__restrict__ nops, uint32_t samples, uint32_t cap,
-	uint64_t last, uint64_t s0, uint32_t nreg, struct p2_op *__restrict__ out,
-	struct p2_binst *inst)
+#define P2_SMP_PLAN_TPB 256
+#define P2_SMP_PLAN_SMEM                                                      \
+	(P2_QUEUE_FLUSH * (sizeof(uint64_t) + sizeof(uint16_t) + 1) +          \
+		P2_QUEUE_FLUSH / 8)
+
+__global__ void __launch_bounds__(P2_SMP_PLAN_TPB)
+	k_smp_plan(const struct p2_smp_job job, uint64_t T, uint32_t C,
+		const struct phase2_rot_in *__restrict__ rot,
+		const double *__restrict__ cs, struct phase2_pass *passes,
+		struct phase2_rot_rec *__restrict__ recs, uint32_t *npc)
 {
-	extern __shared__ uint32_t sh[];
-	uint32_t *off = sh;            /* [samples] */
-	uint32_t *fill = sh + samples; /* [nreg] */
-	if (threadIdx.x == 0) {
-		for (uint32_t r = 0; r < nreg; ++r)
-			fill[r] = 0;
-		for (uint32_t s = 0; s < samples; ++s)
-			fill[(uint32_t)((last - s0 - s) % nreg)] += nops[s];
-		uint32_t t = 0;
-		for (uint32_t r = 0; r < nreg; ++r) {
-			inst[r].op_off = t;
-			inst[r].nops = fill[r];
-			t += fill[r];
-			fill[r] = inst[r].op_off;
-		}
-		for (uint32_t s = 0; s < samples; ++s) {
-			const uint32_t r = (uint32_t)((last - s0 - s) % nreg);
-			off[s] = fill[r];
-			fill[r] += nops[s];
-		}
+	extern __shared__ __align__(16) unsigned char sm[];
+	uint64_t *fl = (uint64_t *)sm;
+	uint16_t *pid = (uint16_t *)(fl + P2_QUEUE_FLUSH);
+	uint8_t *U = (uint8_t *)(pid + P2_QUEUE_FLUSH);
+	uint32_t *neg = (uint32_t *)(U + P2_QUEUE_FLUSH);
+	__shared__ long s_np;
+	const uint64_t s = blockIdx.x / C, c = blockIdx.x - s * C;
+	const uint64_t at = s * T + c * P2_QUEUE_FLUSH;
+	const uint32_t n = (uint32_t)(T - c * P2_QUEUE_FLUSH < P2_QUEUE_FLUSH
+			? T - c * P2_QUEUE_FLUSH
+			: P2_QUEUE_FLUSH);
+	for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
+		fl[i] = rot[at + i].flip;
+	for (uint32_t w = threadIdx.x; w < P2_QUEUE_FLUSH / 32; w += blockDim.x)
+		neg[w] = 0;
+	__syncthreads();
+	if (threadIdx.x == 0)
+		s_np = p2_plan_scan(job.nqb, fl, 1, n, job.max_span,
+			job.max_rots, P2_DEFAULT_PAD_SPAN, job.form, passes + at,
+			U, 1, pid);
+	__syncthreads();
+	const long np = s_np;
+	if (np < 0) {
+		if (threadIdx.x == 0)
+			npc[blockIdx.x] = 0;
+		return;
+	}
+	for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+		const uint32_t p = pid[i];
+		struct phase2_rot_rec r;
+		if (p2_rec_fill(&passes[at + p], fl[i], rot[at + i].phase,
+			    cs[2 * (at + i)], cs[2 * (at + i) + 1], U[i], &r))
+			atomicXor(&neg[p >> 5], 1u << (p & 31));
+		recs[at + i] = r;
 	}
 	__syncthreads();
-	for (uint32_t s = 0; s < samples; ++s)
-		for (uint32_t k = threadIdx.x; k < nops[s]; k += blockDim.x)
-			out[off[s] + k] = seg[(size_t)s * cap + k];
+	for (uint32_t p = threadIdx.x; p < (uint32_t)np; p += blockDim.x) {
+		passes[at + p].scale = (neg[p >> 5] >> (p & 31)) & 1 ? -1.0 : 1.0;
+		passes[at + p].rot_off += (uint32_t)at;
+	}
+	if (threadIdx.x == 0)
+		npc[blockIdx.x] = (uint32_t)np;
 }
 
-/* Samples per device round: bounded by the rotations held at once. */
-#define P2_QD_ROUND_ROTS (UINT64_C(1) << 22)
+/*
+ * Lay out the registers' programs (one thread): sample s0 + s runs on
+ * register (last - s0 - s) % nreg, so the run's last sample lands on
+ * register 0; a register's samples keep their order.  A sample's ops are
+ * zero, write, its chunks' passes in order, gather: poff[s * C + c] is
+ * the op index of chunk c's first pass, soff[s] of the sample's zero.
+ */
+__global__ void k_smp_layout(uint32_t g, uint32_t C,
+	const uint32_t *__restrict__ npc, uint64_t last, uint64_t s0,
+	uint32_t nreg, uint32_t *soff, uint32_t *poff, struct p2_binst *inst)
+{
+	if (blockIdx.x != 0 || threadIdx.x != 0)
+		return;
+	for (uint32_t r = 0; r < nreg; ++r)
+		inst[r].nops = 0;
+	for (uint32_t s = 0; s < g; ++s) {
+		uint32_t n = 3;
+		for (uint32_t c = 0; c < C; ++c)
+			n += npc[s * C + c];
+		inst[(uint32_t)((last - s0 - s) % nreg)].nops += n;
+		soff[s] = n; /* count for now */
+	}
+	uint32_t t = 0;
+	for (uint32_t r = 0; r < nreg; ++r) {
+		inst[r].op_off = t;
+		t += inst[r].nops;
+		inst[r].nops = 0; /* filled below */
+	}
+	for (uint32_t s = 0; s < g; ++s) {
+		const uint32_t r = (uint32_t)((last - s0 - s) % nreg);
+		const uint32_t n = soff[s];
+		soff[s] = inst[r].op_off + inst[r].nops;
+		inst[r].nops += n;
+		uint32_t o = soff[s] + 2;
+		for (uint32_t c = 0; c < C; ++c) {
+			poff[s * C + c] = o;
+			o += npc[s * C + c];
+		}
+	}
+}
+
+/* Fill the ops laid out by k_smp_layout (grid-stride over chunks). */
+__global__ void k_smp_fill(const struct p2_smp_job job, uint32_t g,
+	uint32_t C, uint64_t T, uint64_t namp, uint64_t s0,
+	const uint32_t *__restrict__ npc, const uint32_t *__restrict__ soff,
+	const uint32_t *__restrict__ poff,
+	const struct phase2_pass *__restrict__ passes, struct p2_op *ops)
+{
+	const uint32_t stride = gridDim.x * blockDim.x;
+	const uint32_t id0 = blockIdx.x * blockDim.x + threadIdx.x;
+	for (uint32_t s = id0; s < g; s += stride) {
+		struct p2_op *o = ops + soff[s];
+		o[0].kind = P2_OP_ZERO;
+		o[0].a = o[0].b = 0;
+		o[0].ntiles = p2_op_tiles(P2_OP_ZERO, namp, 0, &o[0].b);
+		o[1].kind = P2_OP_WRITE;
+		o[1].a = 0;
+		o[1].b = job.ndet;
+		o[1].ntiles = 1;
+		uint32_t np = 0;
+		for (uint32_t c = 0; c < C; ++c)
+			np += npc[s * C + c];
+		struct p2_op *gth = o + 2 + np;
+		gth->kind = P2_OP_GATHER;
+		gth->a = (uint32_t)((s0 + s) * job.ndet);
+		gth->b = job.ndet;
+		gth->ntiles = 1;
+	}
+	for (uint32_t e = id0; e < g * C; e += stride) {
+		const uint64_t s = e / C, c = e - s * C;
+		const uint64_t at = s * T + c * P2_QUEUE_FLUSH;
+		struct p2_op *o = ops + poff[e];
+		for (uint32_t p = 0; p < npc[e]; ++p) {
+			o[p].kind = P2_OP_PASS;
+			o[p].a = (uint32_t)(at + p);
+			o[p].ntiles = p2_op_tiles(P2_OP_PASS, namp,
+				passes[at + p].span, &o[p].b);
+		}
+	}
+}
+
+/* Rotations held per device round (rotation scratch, plans, program). */
+#define P2_SMP_ROUND_ROTS (UINT64_C(1) << 21)
 /* Amplitudes of all the registers of one round together (FP32: 512 MiB);
  * from 2^26 amplitudes up the register runs alone. */
-#define P2_QD_ROUND_AMPS (UINT64_C(1) << 26)
+#define P2_SMP_ROUND_AMPS (UINT64_C(1) << 26)
 
-extern "C" int p2d_qdrift_device(struct p2_dev *d, const struct p2_qd_job *job,
-	const uint64_t *rng0, size_t samples, const double *cdf_y,
-	const uint64_t *tflip, const uint64_t *tphase, const double *tcf,
-	const uint64_t *det_idx, const double *det_val, double *gout,
-	uint64_t *npass_out)
+extern "C" int p2d_sampled_device(struct p2_dev *d,
+	const struct p2_smp_job *job, const uint64_t *rng0, size_t samples,
+	const double *cdf_y, const uint64_t *tflip, const uint64_t *tphase,
+	const double *tcf, const uint64_t *hflip, const uint64_t *hphase,
+	const double *hphi, const double *hcs, const uint64_t *det_idx,
+	const double *det_val, double *gout, uint64_t *npass_out)
 {
 	*npass_out = 0;
 	if (samples == 0)
 		return 0;
-	if (!p2d_batch_ok(d) || job->nterms == 0 || job->depth == 0 ||
+	const uint64_t per = (uint64_t)job->length + job->depth;
+	const uint64_t T = per * job->halves;
+	if (!p2d_batch_ok(d) || (job->depth && job->nterms == 0) ||
+		T >= (UINT64_C(1) << 31) || job->halves == 0 ||
 		samples > UINT32_MAX / (job->ndet ? job->ndet : 1)) {
-		log_error("device qdrift: unsupported register or sizes");
+		log_error("device sampling: unsupported register or sizes");
 		return -1;
 	}
-	const size_t depth = job->depth;
-	size_t G = (size_t)(P2_QD_ROUND_ROTS / depth);
+	size_t G = T ? (size_t)(P2_SMP_ROUND_ROTS / T) : 4096;
 	if (G < 1)
 		G = 1;
 	if (G > samples)
 		G = samples;
 	if (G > 4096)
 		G = 4096;
-	size_t R = (size_t)(P2_QD_ROUND_AMPS / d->namp);
+	size_t R = (size_t)(P2_SMP_ROUND_AMPS / d->namp);
 	if (R > P2_QD_MAX_REGS)
 		R = P2_QD_MAX_REGS;
 	if (R > G)
 		R = G;
 	if (R < 1)
 		R = 1;
-	const size_t nt = job->nterms, nd = job->ndet;
-	const size_t cap = depth + 3;
+	const uint32_t C = (uint32_t)((T + P2_QUEUE_FLUSH - 1) / P2_QUEUE_FLUSH);
+	const size_t nt = job->nterms, nd = job->ndet, nh = job->length;
+	const size_t GT = G * T > 0 ? G * T : 1;
 	/* device buffer: tables, per-round scratch and program, registers */
-	size_t sz[17], off[17], total = 0;
-	int k = 0;
-	sz[k++] = 4 * samples * sizeof(uint64_t);          /* 0 rng0 */
-	sz[k++] = nt * sizeof(double);                     /* 1 cdf */
-	sz[k++] = nt * sizeof(uint64_t);                   /* 2 flip */
-	sz[k++] = nt * sizeof(uint64_t);                   /* 3 phase */
-	sz[k++] = nt * sizeof(double);                     /* 4 cf */
-	sz[k++] = (nd ? nd : 1) * sizeof(uint64_t);        /* 5 widx */
-	sz[k++] = 2 * (nd ? nd : 1) * sizeof(double);      /* 6 wval */
-	sz[k++] = (samples * nd ? samples * nd : 1) * sizeof(uint64_t); /* 7 */
-	sz[k++] = (samples * nd ? samples * nd : 1) * sizeof(double2);  /* 8 */
-	sz[k++] = G * depth * sizeof(struct phase2_rot_in); /* 9 rot */
-	sz[k++] = 2 * G * depth * sizeof(double);          /* 10 cs */
-	sz[k++] = G * depth * sizeof(struct phase2_pass);  /* 11 passes */
-	sz[k++] = G * depth * sizeof(struct phase2_rot_rec); /* 12 recs */
-	sz[k++] = G * cap * sizeof(struct p2_op);          /* 13 segments */
-	sz[k++] = G * cap * sizeof(struct p2_op);          /* 14 program */
-	sz[k++] = G * sizeof(uint32_t);                    /* 15 nops */
-	sz[k++] = R * (sizeof(struct p2_binst) + sizeof(struct p2_bctl)) +
-		sizeof(unsigned int) +
-		(R - 1) * d->namp * sizeof(float2);        /* 16 regs */
-	for (int i = 0; i < 17; i++) {
+	enum { RNG, CDF, TFL, TPH, TCF, HFL, HPH, HPHI, HCS, WIDX, WVAL, GIDX,
+		GOUT, X, ROT, CS, PASS, REC, PROG, NPC, SOFF, POFF, REGS, NBUF };
+	size_t sz[NBUF], off[NBUF], total = 0;
+	sz[RNG] = 4 * samples * job->halves * sizeof(uint64_t);
+	sz[CDF] = nt * sizeof(double);
+	sz[TFL] = sz[TPH] = nt * sizeof(uint64_t);
+	sz[TCF] = nt * sizeof(double);
+	sz[HFL] = sz[HPH] = nh * sizeof(uint64_t);
+	sz[HPHI] = nh * sizeof(double);
+	sz[HCS] = 2 * nh * sizeof(double);
+	sz[WIDX] = nd * sizeof(uint64_t);
+	sz[WVAL] = 2 * nd * sizeof(double);
+	sz[GIDX] = samples * nd * sizeof(uint64_t);
+	sz[GOUT] = samples * nd * sizeof(double2);
+	sz[X] = G * job->halves * (size_t)job->depth * sizeof(double);
+	sz[ROT] = GT * sizeof(struct phase2_rot_in);
+	sz[CS] = 2 * GT * sizeof(double);
+	sz[PASS] = GT * sizeof(struct phase2_pass);
+	sz[REC] = GT * sizeof(struct phase2_rot_rec);
+	sz[PROG] = (G * T + 3 * G) * sizeof(struct p2_op);
+	sz[NPC] = sz[POFF] = (G * C ? G * C : 1) * sizeof(uint32_t);
+	sz[SOFF] = G * sizeof(uint32_t);
+	sz[REGS] = R * (sizeof(struct p2_binst) + sizeof(struct p2_bctl)) +
+		sizeof(unsigned int) + (R - 1) * d->namp * sizeof(float2);
+	for (int i = 0; i < NBUF; i++) {
 		off[i] = total;
 		total += (sz[i] + 255) & ~(size_t)255;
 	}
 	unsigned char *b = NULL;
-	CUDA_OK(cudaStreamSynchronize(d->stream), "device qdrift: sync");
-	CUDA_OK(cudaMalloc((void **)&b, total), "device qdrift: alloc");
-	uint64_t *gidx = (uint64_t *)malloc(sz[7]);
+	CUDA_OK(cudaStreamSynchronize(d->stream), "device sampling: sync");
+	CUDA_OK(cudaMalloc((void **)&b, total), "device sampling: alloc");
+	uint64_t *gidx = (uint64_t *)malloc(sz[GIDX] ? sz[GIDX] : 1);
 	struct p2_binst *hinst = (struct p2_binst *)malloc(
 		R * sizeof(struct p2_binst));
 	int rc = -1;
 	cudaError_t e = gidx && hinst ? cudaSuccess
 				      : cudaErrorMemoryAllocation;
-	/* registers: 256-aligned copies first, then inst, ctl, status */
-	float2 *copies = (float2 *)(b + off[16]);
-	struct p2_binst *inst = (struct p2_binst *)(b + off[16] +
+	/* registers: the copies first (256-aligned), then inst, ctl, status */
+	float2 *copies = (float2 *)(b + off[REGS]);
+	struct p2_binst *inst = (struct p2_binst *)(b + off[REGS] +
 		(R - 1) * d->namp * sizeof(float2));
 	struct p2_bctl *ctl = (struct p2_bctl *)(inst + R);
 	unsigned int *status = (unsigned int *)(ctl + R);
-	uint32_t *nops = (uint32_t *)(b + off[15]);
 	if (e == cudaSuccess) {
 		for (size_t s = 0; s < samples; s++)
 			for (size_t j = 0; j < nd; j++)
@@ -2601,26 +2718,30 @@ extern "C" int p2d_qdrift_device(struct p2_dev *d, const struct p2_qd_job *job,
 			hinst[r].namp = d->namp;
 			hinst[r].op_off = hinst[r].nops = 0;
 		}
-		const void *src[9] = { rng0, cdf_y, tflip, tphase, tcf, det_idx,
-			det_val, gidx, hinst };
-		void *dst[9] = { b + off[0], b + off[1], b + off[2], b + off[3],
-			b + off[4], b + off[5], b + off[6], b + off[7], inst };
-		const size_t n9[9] = { sz[0], nt * sizeof(double),
-			nt * sizeof(uint64_t), nt * sizeof(uint64_t),
-			nt * sizeof(double), nd * sizeof(uint64_t),
-			2 * nd * sizeof(double), samples * nd * sizeof(uint64_t),
-			R * sizeof(struct p2_binst) };
-		for (int i = 0; i < 9 && e == cudaSuccess; i++)
-			if (n9[i]) {
-				e = cudaMemcpyAsync(dst[i], src[i], n9[i],
-					cudaMemcpyHostToDevice, d->stream);
-				d->h2d_bytes += n9[i];
+		const void *src[] = { rng0, cdf_y, tflip, tphase, tcf, hflip,
+			hphase, hphi, hcs, det_idx, det_val, gidx };
+		const int at[] = { RNG, CDF, TFL, TPH, TCF, HFL, HPH, HPHI, HCS,
+			WIDX, WVAL, GIDX };
+		for (int i = 0; i < 12 && e == cudaSuccess; i++)
+			if (sz[at[i]]) {
+				e = cudaMemcpyAsync(b + off[at[i]], src[i],
+					sz[at[i]], cudaMemcpyHostToDevice,
+					d->stream);
+				d->h2d_bytes += sz[at[i]];
 			}
+		if (e == cudaSuccess)
+			e = cudaMemcpyAsync(inst, hinst,
+				R * sizeof(struct p2_binst),
+				cudaMemcpyHostToDevice, d->stream);
 	}
 	int per_sm = 0;
 	if (e == cudaSuccess)
 		e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm,
 			k_batch, P2_TPB, 0);
+	if (e == cudaSuccess)
+		e = cudaFuncSetAttribute(k_smp_plan,
+			cudaFuncAttributeMaxDynamicSharedMemorySize,
+			(int)P2_SMP_PLAN_SMEM);
 	/* no op has more tiles than a span-0 pass or a zero (more blocks
 	 * would only poll) */
 	uint32_t cpt = 0;
@@ -2633,48 +2754,85 @@ extern "C" int p2d_qdrift_device(struct p2_dev *d, const struct p2_qd_job *job,
 		(unsigned)d->sm_count * (unsigned)(per_sm > 0 ? per_sm : 1);
 	if (most < grid)
 		grid = (unsigned)most;
+	uint32_t *npc = (uint32_t *)(b + off[NPC]);
+	uint32_t *soff = (uint32_t *)(b + off[SOFF]);
+	uint32_t *poff = (uint32_t *)(b + off[POFF]);
 	uint64_t nops_run = 0;
+	/* PHASE2_SAMPLING_TIMING=1: per-round stage times on stderr */
+	const char *tenv = getenv("PHASE2_SAMPLING_TIMING");
+	const int timing = tenv && *tenv == '1';
+	cudaEvent_t ev[5] = { 0, 0, 0, 0, 0 };
+	for (int i = 0; timing && i < 5; i++)
+		cudaEventCreate(&ev[i]);
 	for (size_t s0 = 0; s0 < samples && e == cudaSuccess; s0 += G) {
 		const uint32_t g = (uint32_t)(samples - s0 < G ? samples - s0 : G);
 		const uint32_t nreg = (uint32_t)(g < R ? g : R);
-		k_qdrift_plan<<<g, P2_TPB, 0, d->stream>>>(*job,
-			(uint32_t)s0, d->namp, (const uint64_t *)(b + off[0]),
-			(const double *)(b + off[1]),
-			(const uint64_t *)(b + off[2]),
-			(const uint64_t *)(b + off[3]),
-			(const double *)(b + off[4]),
-			(struct phase2_rot_in *)(b + off[9]),
-			(double *)(b + off[10]),
-			(struct phase2_pass *)(b + off[11]),
-			(struct phase2_rot_rec *)(b + off[12]),
-			(struct p2_op *)(b + off[13]), nops);
+		const uint32_t nx = g * job->halves;
+		if (timing)
+			cudaEventRecord(ev[0], d->stream);
+		if (job->depth)
+			k_smp_draw<<<(nx + 127) / 128, 128, 0, d->stream>>>(
+				*job, (uint32_t)s0, nx,
+				(const uint64_t *)(b + off[RNG]),
+				(double *)(b + off[X]));
+		const uint64_t tot = (uint64_t)g * T;
+		if (tot)
+			k_smp_stream<<<grid_for(d, tot, P2_TPB, 8), P2_TPB, 0,
+				d->stream>>>(*job, tot,
+				(const double *)(b + off[X]),
+				(const double *)(b + off[CDF]),
+				(const uint64_t *)(b + off[TFL]),
+				(const uint64_t *)(b + off[TPH]),
+				(const double *)(b + off[TCF]),
+				(const uint64_t *)(b + off[HFL]),
+				(const uint64_t *)(b + off[HPH]),
+				(const double *)(b + off[HPHI]),
+				(const double *)(b + off[HCS]),
+				(struct phase2_rot_in *)(b + off[ROT]),
+				(double *)(b + off[CS]));
+		if (timing)
+			cudaEventRecord(ev[1], d->stream);
+		const uint32_t nch = g * C;
+		if (nch)
+			k_smp_plan<<<nch, P2_SMP_PLAN_TPB, P2_SMP_PLAN_SMEM,
+				d->stream>>>(*job, T, C,
+				(const struct phase2_rot_in *)(b + off[ROT]),
+				(const double *)(b + off[CS]),
+				(struct phase2_pass *)(b + off[PASS]),
+				(struct phase2_rot_rec *)(b + off[REC]), npc);
+		if (timing)
+			cudaEventRecord(ev[2], d->stream);
+		k_smp_layout<<<1, 32, 0, d->stream>>>(g, C, npc,
+			(uint64_t)samples - 1, (uint64_t)s0, nreg, soff, poff,
+			inst);
+		k_smp_fill<<<(g * C + g + 127) / 128, 128, 0, d->stream>>>(
+			*job, g, C, T, d->namp, (uint64_t)s0, npc, soff, poff,
+			(const struct phase2_pass *)(b + off[PASS]),
+			(struct p2_op *)(b + off[PROG]));
 		e = cudaGetLastError();
+		if (timing)
+			cudaEventRecord(ev[3], d->stream);
 		if (e == cudaSuccess)
-			k_prog_compact<<<1, 256, (g + nreg) * sizeof(uint32_t),
-				d->stream>>>((const struct p2_op *)(b + off[13]),
-				nops, g, (uint32_t)cap, (uint64_t)samples - 1,
-				(uint64_t)s0, nreg,
-				(struct p2_op *)(b + off[14]), inst);
-		if (e == cudaSuccess)
-			e = cudaMemsetAsync(ctl, 0,
-				nreg * sizeof *ctl + sizeof(unsigned int),
+			e = cudaMemsetAsync(ctl, 0, nreg * sizeof *ctl,
 				d->stream);
 		if (e == cudaSuccess)
 			e = cudaMemsetAsync(status, 0, sizeof(unsigned int),
 				d->stream);
 		if (e == cudaSuccess)
 			k_batch<<<grid, P2_TPB, 0, d->stream>>>(inst, nreg,
-				(const struct p2_op *)(b + off[14]),
-				(const struct phase2_pass *)(b + off[11]),
-				(const struct phase2_rot_rec *)(b + off[12]),
-				(const uint64_t *)(b + off[5]),
-				(const double *)(b + off[6]),
-				(const uint64_t *)(b + off[7]),
-				(double2 *)(b + off[8]), ctl, status,
+				(const struct p2_op *)(b + off[PROG]),
+				(const struct phase2_pass *)(b + off[PASS]),
+				(const struct phase2_rot_rec *)(b + off[REC]),
+				(const uint64_t *)(b + off[WIDX]),
+				(const double *)(b + off[WVAL]),
+				(const uint64_t *)(b + off[GIDX]),
+				(double2 *)(b + off[GOUT]), ctl, status,
 				P2_BATCH_IDLE_LIMIT);
 		if (e == cudaSuccess)
 			e = cudaGetLastError();
-		d->launches += 3;
+		if (timing)
+			cudaEventRecord(ev[4], d->stream);
+		d->launches += 6;
 		unsigned int st = 0;
 		if (e == cudaSuccess)
 			e = cudaMemcpyAsync(&st, status, sizeof st,
@@ -2686,26 +2844,42 @@ extern "C" int p2d_qdrift_device(struct p2_dev *d, const struct p2_qd_job *job,
 		if (e == cudaSuccess)
 			e = cudaStreamSynchronize(d->stream);
 		if (e == cudaSuccess && st) {
-			log_error("device qdrift: a block found no work for %u"
-				  " rounds",
+			log_error("device sampling: a block found no work for"
+				  " %u rounds",
 				P2_BATCH_IDLE_LIMIT);
 			e = cudaErrorLaunchFailure;
 		}
+		uint64_t rops = 0;
 		for (uint32_t r = 0; e == cudaSuccess && r < nreg; r++)
-			nops_run += hinst[r].nops;
-		nops_run -= 3ull * g;
+			rops += hinst[r].nops;
+		nops_run += rops - 3ull * g;
+		if (timing && e == cudaSuccess) {
+			float t[4];
+			for (int i = 0; i < 4; i++)
+				cudaEventElapsedTime(&t[i], ev[i], ev[i + 1]);
+			fprintf(stderr,
+				"device sampling: %u samples x %llu rotations,"
+				" %u registers, %llu ops, grid %u: draw+stream"
+				" %.3f ms, plan %.3f ms, layout %.3f ms, run"
+				" %.3f ms\n",
+				g, (unsigned long long)T, nreg,
+				(unsigned long long)rops, grid, t[0], t[1], t[2],
+				t[3]);
+		}
 	}
-	if (e == cudaSuccess && samples * nd)
-		e = cudaMemcpy(gout, b + off[8], samples * nd * sizeof(double2),
+	for (int i = 0; timing && i < 5; i++)
+		cudaEventDestroy(ev[i]);
+	if (e == cudaSuccess && sz[GOUT])
+		e = cudaMemcpy(gout, b + off[GOUT], sz[GOUT],
 			cudaMemcpyDeviceToHost);
 	if (e == cudaSuccess) {
-		d->d2h_bytes += samples * nd * sizeof(double2);
+		d->d2h_bytes += sz[GOUT];
 		d->passes += nops_run;
-		d->rotations += (uint64_t)samples * depth;
+		d->rotations += (uint64_t)samples * T;
 		*npass_out = nops_run;
 		rc = 0;
 	} else {
-		log_error("device qdrift: %s", cudaGetErrorString(e));
+		log_error("device sampling: %s", cudaGetErrorString(e));
 	}
 	free(gidx);
 	free(hinst);

@@ -153,39 +153,46 @@ int p2d_batch_run(struct p2_dev *const *devs,
 	const struct p2_prog *const *progs, size_t n, double *gout,
 	double *kernel_ms);
 
-/* ---- device-side qDRIFT (qdrift_simul with device sampling) ------------ */
+/* ---- device sampling (qdrift / cmpsit simul on the GPU) --------------- */
 
 /*
- * One qDRIFT run executed on the device: for each sample s (generator
- * state rng0[s], taken where the host run would be), the device draws
- * `depth` terms from the |c| CDF (xoshiro256** top 53 bits, smallest i
- * with y[i] > x, sign with the DBL_EPSILON dead zone), plans them exactly
- * as a host flush would (chunks of P2_QUEUE_FLUSH, plan_core.h, cos/sin of
- * omega * {-1, 0, +1} given in cs), and the program zero / write dets /
- * passes / gather dets of every sample runs in one persistent launch.
- * Samples are independent (each starts from the trial state), so small
- * registers run up to P2_QD_MAX_REGS samples at once on copies of the
- * state; the last sample always runs on the register itself, which ends
- * holding its state as after the host loop.
+ * A sampled run executed on the device.  Sample s's rotation stream is
+ * `halves` halves; a forward half applies the head terms 0..length-1 (a
+ * fixed table with its own angles) and then `depth` drawn terms, a
+ * reversed half (odd halves when reverse_odd) the drawn terms in reverse
+ * then the head in reverse.  Half h of sample s draws from generator state
+ * rng0[s * halves + h] (xoshiro256** top 53 bits; the term is the smallest
+ * i with y[i] > x, its sign with the DBL_EPSILON dead zone picks rphi/rcs).
+ * The stream is planned exactly as host flushes of P2_QUEUE_FLUSH
+ * rotations would plan it (plan_core.h), and the program zero / write
+ * dets / passes / gather dets of every sample runs in one persistent
+ * launch per round of samples.  Samples are independent (each starts from
+ * the trial state), so small registers run up to P2_QD_MAX_REGS samples at
+ * once on copies of the state; the last sample always runs on the register
+ * itself, which ends holding its state as after the host loop.
+ *   qdrift: halves 1, length 0, rphi = asin(step) * {-1, 0, 1}.
+ *   cmpsit: halves 2 * steps, reverse_odd, head = the deterministic terms
+ *           at 0.5 * (c * angle_det), rphi = 0.5 * ({-1, 0, 1} * tau).
  */
 #define P2_QD_MAX_REGS 256
-struct p2_qd_job {
-	uint32_t nqb, depth;
+
+struct p2_smp_job {
+	uint32_t nqb, ndet;
 	uint64_t nterms, mask;
-	double omega;
-	double cs[3][2]; /* cos, sin of omega * cf, cf = -1, 0, +1 */
+	uint32_t depth, length, halves, reverse_odd;
+	double rphi[3];   /* angle of a drawn term, sign -1, 0, +1 */
+	double rcs[3][2]; /* its cos, sin */
 	int max_span, max_rots, form;
-	uint32_t ndet;
 };
 
-/* Samples (rng0: 4 words each) run in groups; gout gets ndet amplitudes
- * (re, im) per sample, in sample order.  *npass_out: passes executed.
- * 0 or -1. */
-int p2d_qdrift_device(struct p2_dev *d, const struct p2_qd_job *job,
+/* gout gets ndet amplitudes (re, im) per sample, in sample order;
+ * *npass_out: passes executed.  0 or -1. */
+int p2d_sampled_device(struct p2_dev *d, const struct p2_smp_job *job,
 	const uint64_t *rng0, size_t samples, const double *cdf_y,
 	const uint64_t *tflip, const uint64_t *tphase, const double *tcf,
-	const uint64_t *det_idx, const double *det_val, double *gout,
-	uint64_t *npass_out);
+	const uint64_t *hflip, const uint64_t *hphase, const double *hphi,
+	const double *hcs, const uint64_t *det_idx, const double *det_val,
+	double *gout, uint64_t *npass_out);
 
 #ifdef __cplusplus
 }

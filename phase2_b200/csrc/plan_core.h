@@ -125,11 +125,11 @@ P2_HD void lift_f32(double c, double s, double *t_out, double *s_out)
 	*t_out = s32 == 0.0f ? 0.0 : s * s / (1.0 + c) / (double)s32;
 }
 
-/* Close the open pass: pad the basis with unit vectors (more amplitudes per
- * thread, contiguous along low qubits), fix pivots, fill slot masks. */
-P2_HD void builder_close(struct pass_builder *b, uint32_t nqb, int pad_to,
-	int form, const struct phase2_rot_in *rots, struct phase2_pass *pass,
-	struct phase2_rot_rec *recs)
+/* Header of the open pass: pad the basis with unit vectors (more
+ * amplitudes per thread, contiguous along low qubits), pivots ascending,
+ * basis, sizes; scale 1 (the records' signs set it, p2_rec_fill). */
+P2_HD void builder_header(struct pass_builder *b, uint32_t nqb, int pad_to,
+	int form, struct phase2_pass *pass)
 {
 	for (uint32_t q = 0; b->m < pad_to && q < nqb; q++) {
 		uint32_t combo;
@@ -145,56 +145,72 @@ P2_HD void builder_close(struct pass_builder *b, uint32_t nqb, int pad_to,
 		pass->piv[k] = (uint8_t)b->ech.piv[b->m - 1 - k];
 		pass->basis[k] = b->basis[k];
 	}
-	const uint32_t nslot = UINT32_C(1) << b->m;
-	double scale = 1.0;
-	for (uint32_t r = 0; r < b->nrot; r++) {
-		struct phase2_rot_rec *rec = &recs[b->first_rec + r];
-		const struct phase2_rot_in *in = &rots[b->first_rec + r];
-		uint32_t W = 0;
-		for (int k = 0; k < b->m; k++)
-			W |= (uint32_t)parity64(b->basis[k] & in->phase) << k;
-		const int kbase =
-			(1 - P2_POPC64(in->flip & in->phase)) & 3;
-		uint32_t smask = 0;
-		for (uint32_t u = 0; u < nslot; u++)
-			smask |= (uint32_t)((P2_POPC32(u & W) & 1) ^
-					(kbase >> 1))
-				<< u;
-		rec->smask = smask;
-		rec->W = (uint8_t)W;
-		rec->odd = (uint8_t)(kbase & 1);
-		rec->form = 0;
-		if (form == PHASE2_FORM_LIFTED ||
-			form == PHASE2_FORM_LIFTED_F32) {
-			/* Three shears per pair (no temporaries, no pass-wide
-			 * factor): t = tan(phi/2) = s / (1 + c), computed with
-			 * c >= 0 so it stays in [-1, 1]; for c < 0 the rotation
-			 * is exp(i(phi -+ pi)P) times -1, and the -1 goes to
-			 * the pass. */
-			double c = rec->c, s = rec->s;
-			if (c < 0) {
-				c = -c;
-				s = -s;
-				scale = -scale;
-			}
-			rec->form = 1;
-			if (form == PHASE2_FORM_LIFTED_F32) {
-				lift_f32(c, s, &rec->c, &rec->s);
-			} else {
-				rec->c = s / (1.0 + c);
-				rec->s = s;
-			}
-		}
-	}
-	pass->scale = scale;
+	pass->scale = 1.0;
 	pass->form = (uint8_t)form;
 }
 
-/* Records are emitted in input order: recs[i] describes rots[i].  cs
- * holds cos(phi), sin(phi) per rotation, or is NULL (computed here). */
-P2_HD long p2_plan_core(uint32_t nqb, const struct phase2_rot_in *rots,
-	const double *cs, size_t n, int max_span, int max_rots, int pad_span,
-	int form, struct phase2_pass *passes, struct phase2_rot_rec *recs)
+/*
+ * The record of one rotation (flip, phase, cos c, sin s, slot combination
+ * U) of a pass: slot masks, W, odd and, in the lifted forms, the lifted
+ * coefficients.  Returns 1 when the record's -1 goes to the pass scale (a
+ * lifted rotation with c < 0), else 0.
+ */
+P2_HD int p2_rec_fill(const struct phase2_pass *pass, uint64_t flip,
+	uint64_t phase, double c, double s, uint32_t U,
+	struct phase2_rot_rec *rec)
+{
+	const int m = (int)pass->span;
+	const uint32_t nslot = UINT32_C(1) << m;
+	uint32_t W = 0;
+	for (int k = 0; k < m; k++)
+		W |= (uint32_t)parity64(pass->basis[k] & phase) << k;
+	const int kbase = (1 - P2_POPC64(flip & phase)) & 3;
+	uint32_t smask = 0;
+	for (uint32_t u = 0; u < nslot; u++)
+		smask |= (uint32_t)((P2_POPC32(u & W) & 1) ^ (kbase >> 1)) << u;
+	rec->z = phase;
+	rec->smask = smask;
+	rec->U = (uint8_t)U;
+	rec->W = (uint8_t)W;
+	rec->odd = (uint8_t)(kbase & 1);
+	rec->form = 0;
+	rec->c = c;
+	rec->s = s;
+	const int form = pass->form;
+	int neg = 0;
+	if (form == PHASE2_FORM_LIFTED || form == PHASE2_FORM_LIFTED_F32) {
+		/* Three shears per pair (no temporaries, no pass-wide factor):
+		 * t = tan(phi/2) = s / (1 + c), computed with c >= 0 so it
+		 * stays in [-1, 1]; for c < 0 the rotation is
+		 * exp(i(phi -+ pi)P) times -1, and the -1 goes to the pass. */
+		if (c < 0) {
+			c = -c;
+			s = -s;
+			neg = 1;
+		}
+		rec->form = 1;
+		if (form == PHASE2_FORM_LIFTED_F32) {
+			lift_f32(c, s, &rec->c, &rec->s);
+		} else {
+			rec->c = s / (1.0 + c);
+			rec->s = s;
+		}
+	}
+	return neg;
+}
+
+/*
+ * Pass boundaries (the sequential half of the planner): greedy passes in
+ * input order, a pass closing when the next flip mask would widen its
+ * span beyond max_span or its rotations reach max_rots.  flip i is
+ * flips[i * fstride]; writes the pass headers, each rotation's slot
+ * combination U to U_out[i * ustride] and, when pidx is not NULL, its pass
+ * index to pidx[i].  Returns the number of passes or -1.
+ */
+P2_HD long p2_plan_scan(uint32_t nqb, const uint64_t *flips, size_t fstride,
+	size_t n, int max_span, int max_rots, int pad_span, int form,
+	struct phase2_pass *passes, uint8_t *U_out, size_t ustride,
+	uint16_t *pidx)
 {
 	if (nqb == 0 || nqb > QREG_MAX_WIDTH)
 		return -1;
@@ -216,7 +232,7 @@ P2_HD long p2_plan_core(uint32_t nqb, const struct phase2_rot_in *rots,
 	struct pass_builder b;
 	builder_reset(&b, 0);
 	for (size_t i = 0; i < n; i++) {
-		const uint64_t f = rots[i].flip;
+		const uint64_t f = flips[i * fstride];
 		uint32_t U = 0;
 		int fits = b.nrot < cap;
 		if (fits && f != 0) {
@@ -230,8 +246,7 @@ P2_HD long p2_plan_core(uint32_t nqb, const struct phase2_rot_in *rots,
 				fits = 0;
 		}
 		if (!fits) {
-			builder_close(&b, nqb, pad_span, form, rots,
-				&passes[npass], recs);
+			builder_header(&b, nqb, pad_span, form, &passes[npass]);
 			npass++;
 			builder_reset(&b, i);
 			if (f != 0)
@@ -239,26 +254,40 @@ P2_HD long p2_plan_core(uint32_t nqb, const struct phase2_rot_in *rots,
 		}
 		if (U == 0xffffffffu)
 			U = builder_add(&b, f);
-		struct phase2_rot_rec *rec = &recs[i];
-		rec->z = rots[i].phase;
-		if (cs) {
-			rec->c = cs[2 * i];
-			rec->s = cs[2 * i + 1];
-		} else {
-			rec->c = cos(rots[i].phi);
-			rec->s = sin(rots[i].phi);
-		}
-		rec->U = (uint8_t)U;
-		rec->W = 0;
-		rec->form = 0;
+		U_out[i * ustride] = (uint8_t)U;
+		if (pidx)
+			pidx[i] = (uint16_t)npass;
 		b.nrot++;
 	}
 	if (b.nrot > 0) {
-		builder_close(&b, nqb, pad_span, form, rots, &passes[npass],
-			recs);
+		builder_header(&b, nqb, pad_span, form, &passes[npass]);
 		npass++;
 	}
 	return npass;
+}
+
+/* Records are emitted in input order: recs[i] describes rots[i].  cs
+ * holds cos(phi), sin(phi) per rotation, or is NULL (computed here). */
+P2_HD long p2_plan_core(uint32_t nqb, const struct phase2_rot_in *rots,
+	const double *cs, size_t n, int max_span, int max_rots, int pad_span,
+	int form, struct phase2_pass *passes, struct phase2_rot_rec *recs)
+{
+	const long np = p2_plan_scan(nqb, &rots[0].flip,
+		sizeof *rots / sizeof(uint64_t), n, max_span, max_rots,
+		pad_span, form, passes, &recs[0].U, sizeof *recs, NULL);
+	for (long p = 0; p < np; p++) {
+		struct phase2_pass *ps = &passes[p];
+		int neg = 0;
+		for (uint32_t r = 0; r < ps->nrot; r++) {
+			const size_t i = ps->rot_off + (size_t)r;
+			const double c = cs ? cs[2 * i] : cos(rots[i].phi);
+			const double s = cs ? cs[2 * i + 1] : sin(rots[i].phi);
+			neg ^= p2_rec_fill(ps, rots[i].flip, rots[i].phase, c, s,
+				recs[i].U, &recs[i]);
+		}
+		ps->scale = neg ? -1.0 : 1.0;
+	}
+	return np;
 }
 
 #endif /* P2_PLAN_CORE_H */

@@ -499,12 +499,61 @@ def test_qdrift_device_sampling(nqb, nterms, ndet, samples, depth,
         assert np.max(np.abs(dev - want)) < FP32_TOL
 
 
-def test_qdrift_device_sampling_h2o(golden):
+def _cmpsit_both_ways(nqb, t, d, samples, steps, length, depth, adet,
+                      arand, seed):
+    """FP32 cmpsit with host sampling, then with device sampling."""
+    args = (nqb, t, d, samples, steps, length, depth, adet, arand, seed)
+    p2.set_precision(p2.PREC_FP32)
+    p2.set_device_sampling(False)
+    try:
+        host, hst = p2.cmpsit(*args, with_stats=True, with_state=True)
+        p2.set_device_sampling(True)
+        dev, st = p2.cmpsit(*args, with_stats=True, with_state=True)
+    finally:
+        p2.set_device_sampling(p2.DEVICE_SAMPLING_AUTO)
+        p2.set_precision(p2.PREC_FP64)
+    assert np.array_equal(st["state"], hst["state"])
+    return host, dev, st
+
+
+@pytest.mark.parametrize("nqb,nterms,ndet,samples,steps,length,depth", [
+    (9, 60, 1, 3, 2, 8, 12),
+    (11, 400, 3, 2, 3, 50, 100),
+    (12, 1500, 2, 2, 2, 1000, 3000),  # halves straddle queue chunks
+    (8, 40, 2, 300, 1, 5, 3),        # many samples on register copies
+    (10, 50, 2, 3, 2, 10, 0),        # head terms only
+    (10, 50, 2, 3, 2, 0, 20),        # draws only
+])
+def test_cmpsit_device_sampling(nqb, nterms, ndet, samples, steps, length,
+                                depth, oracle_lib):
+    """cmpsit with device sampling (forward and reversed halves of head
+    terms and fresh draws on the GPU) gives the host loop's overlaps and
+    final register bit for bit, within the FP32 tolerance of the
+    oracle."""
+    t = workloads.jw_terms(nqb, nterms, seed=nqb * 11 + depth)
+    t.cf[5] = -1e-17  # a drawn term in the sign dead zone
+    d = workloads.hamming_dets(nqb, ndet, nqb // 2, seed=nqb + 2 * ndet)
+    args = (samples, steps, length, depth, 0.05, 0.004, 0xC0DE + nqb)
+    host, dev, st = _cmpsit_both_ways(nqb, t, d, *args)
+    assert np.array_equal(dev, host)
+    assert st["passes"] > 0
+    if samples * steps * (length + depth) <= 20000:
+        want = oracle_lib.cmpsit(nqb, t.flip, t.phase, t.cf, d.idx, d.cf,
+                                 *args)
+        assert np.max(np.abs(dev - want)) < FP32_TOL
+
+
+def test_device_sampling_h2o(golden):
     """The water fixture (real molecular terms) under device sampling."""
     _, t, d = _h2o(golden)
     host, dev, _ = _qdrift_both_ways(10, t, d, 6, 300, 0.01, 0xC0FFEE)
     assert np.array_equal(dev, host)
     want = np.array([_cz(v) for v in golden["h2o"]["qdrift"]])
+    assert np.max(np.abs(dev - want)) < FP32_TOL
+    host, dev, _ = _cmpsit_both_ways(10, t, d, 3, 4, 60, 50, 0.1, 0.02,
+                                     0xBEEF)
+    assert np.array_equal(dev, host)
+    want = np.array([_cz(v) for v in golden["h2o"]["cmpsit"]])
     assert np.max(np.abs(dev - want)) < FP32_TOL
 
 
