@@ -318,7 +318,7 @@ def gpu_arm(args) -> None:
             "value": ws * cmp_depth * namp / (ms / 1e3), "unit": UNIT,
             "rotations": cmp_depth,
             "passes": s["passes"],
-            "kernel_gbs": (s["passes"] * 2 * namp * elem / 1e9) /
+            "kernel_gbs": (s["sweeps"] * 2 * namp * elem / 1e9) /
             (s["pass_ms"] / 1e3) if s["pass_ms"] else None}
     p2.set_precision(p2.PREC_FP64)
     if rank == 0 and not args.quick:
@@ -328,10 +328,13 @@ def gpu_arm(args) -> None:
 
     peaks = _peaks()
     passes_per_step = st["passes"] / args.steps
-    launch_ms = st_t["pass_ms"] / max(1, st_t["timed_passes"])
+    # one state round trip per pass kernel (or per sweep kernel when
+    # sweeps are on): the unit the roofline bytes are counted in
+    trips_per_step = st["sweeps"] / args.steps
+    launch_ms = st_t["pass_ms"] / max(1, st_t["timed_sweeps"])
     bytes_per_launch = 2 * namp * 8
     achieved = bytes_per_launch / (launch_ms / 1e3) / 1e9
-    hbm_gbs_step = passes_per_step * bytes_per_launch / (
+    hbm_gbs_step = trips_per_step * bytes_per_launch / (
         dev_ms / args.steps / 1e3) / 1e9
     cpu = _cpu_baseline() if (rank == 0 and ws == 1 and not args.quick) \
         else None

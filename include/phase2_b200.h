@@ -100,6 +100,26 @@ void circ_hamil_sort_flip(struct circ_hamil *hm);
 int phase2_set_batch_persistent(int on);
 
 /*
+ * Sweeps (FP32 registers in PHASE2_FORM_LIFTED_F32, tile + 3 to 31
+ * qubits): the planner also closes passes at sweep boundaries, a sweep
+ * being a run of passes whose bases, modulo the low `low_qubits` qubits,
+ * span at most tile_qubits - low_qubits dimensions (struct
+ * phase2_pass.sweep marks its first pass), and the executor runs each
+ * sweep as ONE kernel that reads and writes the state once: it walks tiles
+ * of 2^tile_qubits amplitudes closed under those passes, the first pass
+ * reading from HBM, the middle ones in shared memory, the last writing
+ * back.  The FP32 plan therefore depends on the shape; running a plan's
+ * sweeps as one kernel each is bit-identical to one kernel per pass
+ * (phase2_set_sweep_kernel(0)).  tile_qubits 0 turns sweeps off.  Valid:
+ * tile 8..14, low 3..8, tile - low <= 9.  Returns -1 on invalid values.
+ */
+int phase2_set_sweep(int tile_qubits, int low_qubits);
+void phase2_get_sweep(int *tile_qubits, int *low_qubits);
+/* on = 0: keep the sweep grouping of plans but run one kernel per pass
+ * (the same bits, one state round trip per pass; for comparisons). */
+int phase2_set_sweep_kernel(int on);
+
+/*
  * qdrift_simul with device sampling: when the register is FP32 in
  * PHASE2_FORM_LIFTED_F32 with at most 31 qubits and the trial state is a
  * MULTIDET, the samples' term draws (CDF inversion of the host generator's
@@ -177,9 +197,10 @@ int qreg_inner_dense(struct qreg *reg, const double *trial, double out[2]);
 
 struct phase2_stats {
 	uint64_t rotations; /* rotations executed */
-	uint64_t passes;    /* state sweeps (pass kernels) */
+	uint64_t passes;    /* passes (fused rotation groups) executed */
 	uint64_t launches;  /* kernels launched by this library */
-	uint64_t bytes;     /* algorithmic HBM bytes: 2 * namp * elem per pass */
+	uint64_t bytes;     /* algorithmic HBM bytes: 2 * namp * elem per
+			     * state round trip (sweeps) */
 	uint64_t timed_passes;
 	double pass_ms;     /* device time of timed pass launches (CUDA events) */
 	uint64_t h2d_bytes; /* host-to-device bytes copied for this register */
@@ -188,6 +209,9 @@ struct phase2_stats {
 				 * (a plan seen before, e.g. every Trotter
 				 * step after the second; registers of up to
 				 * 24 qubits) */
+	uint64_t sweeps;    /* state round trips: one per pass kernel, one per
+			     * sweep kernel (several passes, phase2_set_sweep) */
+	uint64_t timed_sweeps; /* round trips inside pass_ms */
 };
 
 int qreg_get_stats(const struct qreg *reg, struct phase2_stats *st);
@@ -252,7 +276,10 @@ struct phase2_pass {
 	uint32_t rot_off;  /* first rotation record */
 	uint8_t piv[PHASE2_MAX_SPAN]; /* pivot bits, ascending */
 	uint8_t form;      /* PHASE2_FORM_* of every record of the pass */
-	uint8_t pad[2];
+	uint8_t sweep;     /* 1: the pass starts a sweep (phase2_set_sweep);
+			    * the passes up to the next start share one tile
+			    * shape and may run as one kernel */
+	uint8_t pad;
 	uint64_t basis[PHASE2_MAX_SPAN];
 	double scale;      /* lifted forms: +-1, applied at the store */
 };

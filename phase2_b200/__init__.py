@@ -82,6 +82,27 @@ def set_batch_persistent(on: bool) -> None:
     lib().phase2_set_batch_persistent(1 if on else 0)
 
 
+def set_sweep(tile_qubits: int, low_qubits: int = 5) -> None:
+    """FP32 sweeps: plans group passes that fit a tile of 2^tile_qubits
+    amplitudes (low_qubits of them the lowest qubits), and each group runs
+    as one kernel, one read and one write of the state.  tile_qubits 0
+    turns them off."""
+    if lib().phase2_set_sweep(int(tile_qubits), int(low_qubits)) != 0:
+        raise ValueError(f"bad sweep shape {tile_qubits}, {low_qubits}")
+
+
+def get_sweep() -> tuple:
+    a, b = C.c_int(), C.c_int()
+    lib().phase2_get_sweep(C.byref(a), C.byref(b))
+    return a.value, b.value
+
+
+def set_sweep_kernel(on: bool) -> None:
+    """False: keep the plans' sweep grouping but run one kernel per pass
+    (same bits; for comparisons)."""
+    lib().phase2_set_sweep_kernel(1 if on else 0)
+
+
 DEVICE_SAMPLING_OFF, DEVICE_SAMPLING_ON, DEVICE_SAMPLING_AUTO = 0, 1, 2
 
 
@@ -542,7 +563,7 @@ def plan(nqb: int, flip, phase, phi, max_span: int = 5, max_rots: int = 0,
         raise ValueError("phase2_plan failed")
     out_p = [{"span": p.span, "nrot": p.nrot, "rot_off": p.rot_off,
               "piv": list(p.piv)[:p.span], "basis": list(p.basis)[:p.span],
-              "scale": p.scale, "form": p.form}
+              "scale": p.scale, "form": p.form, "sweep": p.sweep}
              for p in passes[:np_]]
     out_r = [{"z": r.z, "c": r.c, "s": r.s, "smask": r.smask, "U": r.U,
               "odd": r.odd, "form": r.form} for r in recs[:n]]

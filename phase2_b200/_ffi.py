@@ -157,7 +157,8 @@ MAX_SPAN = 5
 class Pass(C.Structure):
     _fields_ = [("span", C.c_uint32), ("nrot", C.c_uint32),
                 ("rot_off", C.c_uint32), ("piv", C.c_uint8 * MAX_SPAN),
-                ("form", C.c_uint8), ("pad", C.c_uint8 * 2),
+                ("form", C.c_uint8), ("sweep", C.c_uint8),
+                ("pad", C.c_uint8),
                 ("basis", C.c_uint64 * MAX_SPAN),
                 ("scale", C.c_double)]
 
@@ -173,7 +174,8 @@ class Stats(C.Structure):
                 ("launches", C.c_uint64), ("bytes", C.c_uint64),
                 ("timed_passes", C.c_uint64), ("pass_ms", C.c_double),
                 ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64),
-                ("graph_replays", C.c_uint64)]
+                ("graph_replays", C.c_uint64), ("sweeps", C.c_uint64),
+                ("timed_sweeps", C.c_uint64)]
 
 
 LAYOUT = {0: Qreg, 1: Circ, 2: Trott, 3: Trott2, 4: Qdrift, 5: Cmpsit,
@@ -282,6 +284,9 @@ _SIGS = {
     "phase2_set_fp32_form": (C.c_int, [C.c_int]),
     "phase2_set_batch_persistent": (C.c_int, [C.c_int]),
     "phase2_set_device_sampling": (C.c_int, [C.c_int]),
+    "phase2_set_sweep": (C.c_int, [C.c_int, C.c_int]),
+    "phase2_get_sweep": (None, [C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "phase2_set_sweep_kernel": (C.c_int, [C.c_int]),
     "state_prep_coeff_scratch_init": (C.c_int, [C.c_void_p, C.c_uint32,
                                                 C.c_uint32, C.c_uint32]),
     "state_prep_coeff_scratch_free": (None, [C.c_void_p]),

@@ -302,6 +302,7 @@ static int sampled_device(struct circ *ct, struct p2_smp_job *job,
 	job->max_span = b->max_span;
 	job->max_rots = b->max_rots;
 	job->form = PHASE2_FORM_LIFTED_F32;
+	p2_sweep_for(job->nqb, job->form, &job->sweep_k, &job->sweep_low);
 	uint64_t npass = 0;
 	if (p2d_sampled_device(dev, job, rng0, ns, cdf->y, tfl, tph, tcf, hfl,
 		    hph, hphi, hcs, didx, dval, (double *)g, &npass) < 0) {

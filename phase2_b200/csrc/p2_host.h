@@ -60,7 +60,7 @@ struct p2_qreg {
 	struct phase2_rot_in *plan_q;
 	size_t plan_qlen, plan_qcap;
 	long plan_np;
-	int plan_span, plan_rots, plan_form;
+	int plan_span, plan_rots, plan_form, plan_sweep;
 };
 
 /* Sticky error of a register (0 ok, -1 failed). */

@@ -23,10 +23,18 @@ extern "C" {
 /* Queued rotations that trigger an automatic flush. */
 #define P2_QUEUE_FLUSH 8192
 
-/* form: enum phase2_form of every pass (and the records it implies). */
+/* form: enum phase2_form of every pass (and the records it implies);
+ * sweep_k, sweep_low: sweep grouping (p2_sweep_for; 0, 0 for none). */
 long p2_plan(uint32_t nqb, const struct phase2_rot_in *rots, size_t n,
-	int max_span, int max_rots, int pad_span, int form,
-	struct phase2_pass *passes, struct phase2_rot_rec *recs);
+	int max_span, int max_rots, int pad_span, int form, int sweep_k,
+	int sweep_low, struct phase2_pass *passes,
+	struct phase2_rot_rec *recs);
+
+/* Sweep grouping the executor uses for a register of nqb qubits whose
+ * passes have form `form`: *k = tile - low qubits and *low under the
+ * process's sweep shape for FP32-arithmetic registers of tile + 3 to 31
+ * qubits, else 0 and 0. */
+void p2_sweep_for(uint32_t nqb, int form, int *k, int *low);
 
 /* Pass form for a state precision: exact for FP64, the process's FP32
  * form (phase2_set_fp32_form) for FP32. */
@@ -145,6 +153,11 @@ long p2_prog_gather(struct p2_prog *pg, const uint64_t *idx, size_t n);
  * the FP32-arithmetic lifted form, at most 31 qubits). */
 int p2d_batch_ok(const struct p2_dev *d);
 
+/* Sweep shape of the FP32 pass executor (phase2_set_sweep). */
+int p2d_set_sweep(int tile_qubits, int low_qubits);
+void p2d_get_sweep(int *tile_qubits, int *low_qubits);
+void p2d_set_sweep_kernel(int on);
+
 /* Run n recorded programs, program i on register devs[i], in one
  * persistent launch; gout receives every program's gathered amplitudes
  * (FP64 re, im) in program order.  *kernel_ms (if non-NULL) gets the
@@ -183,6 +196,7 @@ struct p2_smp_job {
 	double rphi[3];   /* angle of a drawn term, sign -1, 0, +1 */
 	double rcs[3][2]; /* its cos, sin */
 	int max_span, max_rots, form;
+	int sweep_k, sweep_low; /* sweep grouping, as p2_sweep_for */
 };
 
 /* gout gets ndet amplitudes (re, im) per sample, in sample order;

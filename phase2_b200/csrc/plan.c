@@ -38,20 +38,38 @@
 #include "p2_internal.h"
 #include "plan_core.h"
 
+void p2_sweep_for(uint32_t nqb, int form, int *k, int *low)
+{
+	int tile = 0, lw = 0;
+	p2d_get_sweep(&tile, &lw);
+	if (tile > 0 && form == PHASE2_FORM_LIFTED_F32 && nqb <= 31 &&
+		nqb >= (uint32_t)tile + 3) {
+		*k = tile - lw;
+		*low = lw;
+	} else {
+		*k = 0;
+		*low = 0;
+	}
+}
+
 long phase2_plan(uint32_t nqb, const struct phase2_rot_in *rots, size_t n,
 	int max_span, int max_rots, int prec, struct phase2_pass *passes,
 	struct phase2_rot_rec *recs)
 {
 	if (prec != PHASE2_PREC_FP64 && prec != PHASE2_PREC_FP32)
 		return -1;
+	const int form = p2_form_for(prec);
+	int k, low;
+	p2_sweep_for(nqb, form, &k, &low);
 	return p2_plan(nqb, rots, n, max_span, max_rots, P2_DEFAULT_PAD_SPAN,
-		p2_form_for(prec), passes, recs);
+		form, k, low, passes, recs);
 }
 
 long p2_plan(uint32_t nqb, const struct phase2_rot_in *rots, size_t n,
-	int max_span, int max_rots, int pad_span, int form,
-	struct phase2_pass *passes, struct phase2_rot_rec *recs)
+	int max_span, int max_rots, int pad_span, int form, int sweep_k,
+	int sweep_low, struct phase2_pass *passes,
+	struct phase2_rot_rec *recs)
 {
 	return p2_plan_core(nqb, rots, NULL, n, max_span, max_rots, pad_span,
-		form, passes, recs);
+		form, sweep_k, sweep_low, passes, recs);
 }

@@ -127,9 +127,10 @@ P2_HD void lift_f32(double c, double s, double *t_out, double *s_out)
 
 /* Header of the open pass: pad the basis with unit vectors (more
  * amplitudes per thread, contiguous along low qubits), pivots ascending,
- * basis, sizes; scale 1 (the records' signs set it, p2_rec_fill). */
+ * basis, sizes; scale 1 (the records' signs set it, p2_rec_fill); head:
+ * the pass starts a sweep. */
 P2_HD void builder_header(struct pass_builder *b, uint32_t nqb, int pad_to,
-	int form, struct phase2_pass *pass)
+	int form, int head, struct phase2_pass *pass)
 {
 	for (uint32_t q = 0; b->m < pad_to && q < nqb; q++) {
 		uint32_t combo;
@@ -147,6 +148,38 @@ P2_HD void builder_header(struct pass_builder *b, uint32_t nqb, int pad_to,
 	}
 	pass->scale = 1.0;
 	pass->form = (uint8_t)form;
+	pass->sweep = (uint8_t)(head != 0);
+}
+
+/* Echelon of a sweep's flip masks modulo the low qubits (rows with
+ * distinct top bits, kept in descending order). */
+#define P2_SWEEP_ROWS 16
+struct sweep_ech {
+	int rows;
+	uint64_t v[P2_SWEEP_ROWS];
+	int piv[P2_SWEEP_ROWS];
+};
+
+P2_HD uint64_t swe_reduce(const struct sweep_ech *e, uint64_t v)
+{
+	for (int r = 0; r < e->rows; r++)
+		if (v >> e->piv[r] & 1)
+			v ^= e->v[r];
+	return v;
+}
+
+P2_HD void swe_insert(struct sweep_ech *e, uint64_t v)
+{
+	const int p = top_bit(v);
+	int at = e->rows;
+	while (at > 0 && e->piv[at - 1] < p) {
+		e->v[at] = e->v[at - 1];
+		e->piv[at] = e->piv[at - 1];
+		at--;
+	}
+	e->v[at] = v;
+	e->piv[at] = p;
+	e->rows++;
 }
 
 /*
@@ -202,15 +235,19 @@ P2_HD int p2_rec_fill(const struct phase2_pass *pass, uint64_t flip,
 /*
  * Pass boundaries (the sequential half of the planner): greedy passes in
  * input order, a pass closing when the next flip mask would widen its
- * span beyond max_span or its rotations reach max_rots.  flip i is
- * flips[i * fstride]; writes the pass headers, each rotation's slot
- * combination U to U_out[i * ustride] and, when pidx is not NULL, its pass
- * index to pidx[i].  Returns the number of passes or -1.
+ * span beyond max_span or its rotations reach max_rots.  With sweep_k > 0,
+ * passes also group into sweeps: a sweep closes (and with it the pass)
+ * when the next flip mask, taken modulo the low sweep_low qubits, would
+ * widen the sweep's span beyond sweep_k; a pass that starts a sweep has
+ * its sweep flag set.  flip i is flips[i * fstride]; writes the pass
+ * headers, each rotation's slot combination U to U_out[i * ustride] and,
+ * when pidx is not NULL, its pass index to pidx[i].  Returns the number of
+ * passes or -1.
  */
 P2_HD long p2_plan_scan(uint32_t nqb, const uint64_t *flips, size_t fstride,
 	size_t n, int max_span, int max_rots, int pad_span, int form,
-	struct phase2_pass *passes, uint8_t *U_out, size_t ustride,
-	uint16_t *pidx)
+	int sweep_k, int sweep_low, struct phase2_pass *passes,
+	uint8_t *U_out, size_t ustride, uint16_t *pidx)
 {
 	if (nqb == 0 || nqb > QREG_MAX_WIDTH)
 		return -1;
@@ -228,9 +265,16 @@ P2_HD long p2_plan_scan(uint32_t nqb, const uint64_t *flips, size_t fstride,
 		? (uint32_t)max_rots
 		: P2_MAX_ROTS_PER_PASS;
 
+	if (sweep_k < 0 || sweep_k > P2_SWEEP_ROWS || sweep_low < 0 ||
+		sweep_low > 31)
+		return -1;
+	const uint64_t lowm = (UINT64_C(1) << sweep_low) - 1;
 	long npass = 0;
 	struct pass_builder b;
 	builder_reset(&b, 0);
+	struct sweep_ech sw;
+	sw.rows = 0;
+	int head = 1; /* the open pass starts a sweep */
 	for (size_t i = 0; i < n; i++) {
 		const uint64_t f = flips[i * fstride];
 		uint32_t U = 0;
@@ -245,22 +289,35 @@ P2_HD long p2_plan_scan(uint32_t nqb, const uint64_t *flips, size_t fstride,
 			else
 				fits = 0;
 		}
-		if (!fits) {
-			builder_header(&b, nqb, pad_span, form, &passes[npass]);
+		uint64_t vs = 0;
+		int new_sweep = 0;
+		if (sweep_k > 0 && (f & ~lowm) != 0) {
+			vs = swe_reduce(&sw, f & ~lowm);
+			new_sweep = vs != 0 && sw.rows >= sweep_k;
+		}
+		if (!fits || new_sweep) {
+			builder_header(&b, nqb, pad_span, form, head,
+				&passes[npass]);
 			npass++;
 			builder_reset(&b, i);
-			if (f != 0)
-				U = 0xffffffffu;
+			head = new_sweep;
+			if (new_sweep) {
+				sw.rows = 0;
+				vs = f & ~lowm;
+			}
+			U = f != 0 ? 0xffffffffu : 0;
 		}
 		if (U == 0xffffffffu)
 			U = builder_add(&b, f);
+		if (vs != 0)
+			swe_insert(&sw, vs);
 		U_out[i * ustride] = (uint8_t)U;
 		if (pidx)
 			pidx[i] = (uint16_t)npass;
 		b.nrot++;
 	}
 	if (b.nrot > 0) {
-		builder_header(&b, nqb, pad_span, form, &passes[npass]);
+		builder_header(&b, nqb, pad_span, form, head, &passes[npass]);
 		npass++;
 	}
 	return npass;
@@ -270,11 +327,13 @@ P2_HD long p2_plan_scan(uint32_t nqb, const uint64_t *flips, size_t fstride,
  * holds cos(phi), sin(phi) per rotation, or is NULL (computed here). */
 P2_HD long p2_plan_core(uint32_t nqb, const struct phase2_rot_in *rots,
 	const double *cs, size_t n, int max_span, int max_rots, int pad_span,
-	int form, struct phase2_pass *passes, struct phase2_rot_rec *recs)
+	int form, int sweep_k, int sweep_low, struct phase2_pass *passes,
+	struct phase2_rot_rec *recs)
 {
 	const long np = p2_plan_scan(nqb, &rots[0].flip,
 		sizeof *rots / sizeof(uint64_t), n, max_span, max_rots,
-		pad_span, form, passes, &recs[0].U, sizeof *recs, NULL);
+		pad_span, form, sweep_k, sweep_low, passes, &recs[0].U,
+		sizeof *recs, NULL);
 	for (long p = 0; p < np; p++) {
 		struct phase2_pass *ps = &passes[p];
 		int neg = 0;

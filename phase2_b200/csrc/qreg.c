@@ -150,7 +150,7 @@ static int drain_writes(struct p2_qreg *b)
 }
 
 /* Keep a copy of the queue just planned (the plan cache's key). */
-static void remember_plan(struct p2_qreg *b, long np, int form)
+static void remember_plan(struct p2_qreg *b, long np, int form, int sweep)
 {
 	b->plan_qlen = 0;
 	if (np < 0)
@@ -168,6 +168,7 @@ static void remember_plan(struct p2_qreg *b, long np, int form)
 	b->plan_span = b->max_span;
 	b->plan_rots = b->max_rots;
 	b->plan_form = form;
+	b->plan_sweep = sweep;
 }
 
 /* Plan and launch the queued rotations (asynchronously). */
@@ -194,18 +195,21 @@ static int drain_rotations(struct qreg *reg)
 		b->plan_qlen = 0; /* the held plan is gone */
 	}
 	const int form = p2_form_for(b->prec);
+	int swk, swl;
+	p2_sweep_for(reg->qb_lo, form, &swk, &swl);
+	const int sweep = swk << 8 | swl;
 	/* the same queue under the same settings plans to the same passes:
 	 * reuse the plan still held in passes/recs */
 	const int same = b->plan_q && b->plan_qlen == b->qlen &&
 		b->plan_span == b->max_span && b->plan_rots == b->max_rots &&
-		b->plan_form == form &&
+		b->plan_form == form && b->plan_sweep == sweep &&
 		memcmp(b->plan_q, b->q, sizeof *b->q * b->qlen) == 0;
 	long np = b->plan_np;
 	if (!same) {
 		np = p2_plan(reg->qb_lo, b->q, b->qlen, b->max_span,
-			b->max_rots, P2_DEFAULT_PAD_SPAN, form, b->passes,
-			b->recs);
-		remember_plan(b, np, form);
+			b->max_rots, P2_DEFAULT_PAD_SPAN, form, swk, swl,
+			b->passes, b->recs);
+		remember_plan(b, np, form, sweep);
 	}
 	if (np >= 0 && b->rec) {
 		if (p2_prog_plan(b->rec, b->passes, (size_t)np, b->recs,

@@ -74,6 +74,22 @@ int phase2_set_batch_persistent(int on)
 	return 0;
 }
 
+int phase2_set_sweep(int tile_qubits, int low_qubits)
+{
+	return p2d_set_sweep(tile_qubits, low_qubits);
+}
+
+void phase2_get_sweep(int *tile_qubits, int *low_qubits)
+{
+	p2d_get_sweep(tile_qubits, low_qubits);
+}
+
+int phase2_set_sweep_kernel(int on)
+{
+	p2d_set_sweep_kernel(on);
+	return 0;
+}
+
 int phase2_set_device_sampling(int mode)
 {
 	if (mode != PHASE2_DEVICE_SAMPLING_OFF &&

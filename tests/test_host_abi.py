@@ -257,6 +257,66 @@ def test_planner_fuses_jw_runs():
     assert len(one) == len(t)
 
 
+def _rank(vectors):
+    rows = []
+    for v in vectors:
+        v = int(v)
+        for r in rows:
+            v = min(v, v ^ r)
+        if v:
+            rows.append(v)
+    return len(rows)
+
+
+@pytest.mark.parametrize("tile,low", [(13, 5), (12, 4), (11, 3)])
+def test_planner_sweep_grouping(tile, low, oracle_lib):
+    """FP32 plans of registers of tile + 3 qubits or more group passes into
+    sweeps: every sweep's bases, modulo the low qubits, span at most
+    tile - low dimensions; the plan still applies every rotation in order
+    (emulated execution matches the oracle)."""
+    n = 17
+    rng = np.random.Generator(np.random.PCG64(tile * 7 + low))
+    jw = workloads.jw_terms(n, 3000, seed=tile)
+    pick = rng.integers(0, len(jw), 400)  # qDRIFT-like random draws
+    flip, phase = jw.flip[pick], jw.phase[pick]
+    phi = rng.uniform(-np.pi, np.pi, len(pick))
+    old = p2.get_sweep()
+    p2.set_sweep(tile, low)
+    try:
+        passes, recs = plan(n, flip, phase, phi, 5, 0, prec=1)
+        p2.set_sweep(0, 5)
+        plain, _ = plan(n, flip, phase, phi, 5, 0, prec=1)
+    finally:
+        p2.set_sweep(*old)
+    assert passes[0]["sweep"] == 1
+    assert sum(p["sweep"] for p in plain) == 1
+    heads = [i for i, p in enumerate(passes) if p["sweep"]] + [len(passes)]
+    assert len(heads) - 1 < len(plain)  # fewer round trips than passes
+    lowm = (1 << low) - 1
+    for a, b in zip(heads[:-1], heads[1:]):
+        vecs = [int(v) & ~lowm for p in passes[a:b]
+                for v in p["basis"][:p["span"]]]
+        assert _rank(vecs) <= tile - low
+    assert sum(p["nrot"] for p in passes) == len(pick)
+    amp = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+    got = emulate(amp, n, passes, recs)
+    want = oracle_lib.rotate(amp, n, flip, phase, phi)
+    assert np.max(np.abs(got - want)) < 100 * 2.0 ** -24 * np.max(np.abs(want))
+
+
+def test_sweep_setting_validates():
+    old = p2.get_sweep()
+    for bad in ((15, 5), (13, 3), (10, 2), (7, 3)):
+        with pytest.raises(ValueError):
+            p2.set_sweep(*bad)
+    p2.set_sweep(13, 5)
+    assert p2.get_sweep() == (13, 5)
+    p2.set_sweep(0, 5)
+    assert p2.get_sweep()[0] == 0
+    p2.set_sweep(*old)
+    assert p2.get_sweep() == old
+
+
 def test_planner_rejects_bad_width():
     L = lib()
     rin = (_ffi.RotIn * 1)()

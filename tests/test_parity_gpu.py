@@ -220,6 +220,121 @@ def test_stats_count_passes():
     assert st["rotations"] == 256
     assert 0 < st["passes"] < 256
     assert st["bytes"] == st["passes"] * 2 * (1 << 16) * 16
+    assert st["sweeps"] == st["passes"]
+
+
+def _fp32_run(n, amp, flip, phase, phi, shape, kernel=True):
+    """FP32 register through the pass executor under a sweep shape, the
+    planned sweeps run as one kernel each or one kernel per pass."""
+    old = p2.get_sweep()
+    p2.set_sweep(*shape)
+    p2.set_sweep_kernel(kernel)
+    try:
+        with Register(n, p2.PREC_FP32) as r:
+            r.set_state(amp)
+            r.reset_stats()
+            r.paulirot(flip, phase, phi)
+            out = r.get_state()
+            st = r.stats()
+    finally:
+        p2.set_sweep(*old)
+        p2.set_sweep_kernel(True)
+    return out, st
+
+
+@pytest.mark.parametrize("tile,low", [(13, 5), (12, 4), (14, 6), (13, 4),
+                                      (11, 3), (14, 5)])
+@pytest.mark.parametrize("n", [17, 20])
+def test_sweeps_bit_identical(tile, low, n, oracle_lib):
+    """A plan's sweeps run as one kernel each (shared-memory tiles, one
+    state round trip per sweep) give the same bits as one kernel per pass
+    of the same plan, for every tile shape; and fewer round trips."""
+    rng = np.random.Generator(np.random.PCG64(70 * n + tile))
+    amp = _rand_state(rng, n)
+    jw = workloads.jw_terms(n, 3000, seed=n * tile + low)
+    pick = rng.integers(0, len(jw), 700)  # qDRIFT-like random draws
+    flip, phase = jw.flip[pick], jw.phase[pick]
+    phi = rng.uniform(-math.pi, math.pi, len(pick))
+    want, st0 = _fp32_run(n, amp, flip, phase, phi, (tile, low), False)
+    got, st1 = _fp32_run(n, amp, flip, phase, phi, (tile, low))
+    assert np.array_equal(got, want)
+    assert st0["sweeps"] == st0["passes"] == st1["passes"]
+    assert st1["sweeps"] < st1["passes"]
+    assert st1["bytes"] == st1["sweeps"] * 2 * (1 << n) * 8
+    if n <= 17:
+        ref = oracle_lib.rotate(amp, n, flip, phase, phi)
+        assert np.max(np.abs(got - ref)) < FP32_TOL
+    # the sweep-free plan of the same rotations agrees to FP32 rounding
+    plain, _ = _fp32_run(n, amp, flip, phase, phi, (0, 5))
+    assert np.max(np.abs(plain - got)) < FP32_TOL
+
+
+@pytest.mark.parametrize("span,rots", [(5, 0), (3, 0), (2, 7), (1, 1)])
+def test_sweeps_fusion_settings_and_random_strings(span, rots):
+    """Sweep kernels under every fusion setting, with diagonal strings and
+    random (wide) flip masks: bit-identical to one kernel per pass."""
+    n = 18
+    rng = np.random.Generator(np.random.PCG64(span * 10 + rots))
+    amp = _rand_state(rng, n)
+    jw = workloads.jw_terms(n, 300, seed=span)
+    fl, ph, phi = _rand_rots(rng, n, 200, diag_frac=0.3)
+    flip = np.concatenate([jw.flip, fl, jw.flip[:50]])
+    phase = np.concatenate([jw.phase, ph, jw.phase[:50]])
+    ang = np.concatenate([rng.uniform(-3, 3, len(jw)), phi,
+                          rng.uniform(-3, 3, 50)])
+    outs = []
+    old = p2.get_sweep()
+    p2.set_sweep(13, 5)
+    try:
+        for kernel in (False, True):
+            p2.set_sweep_kernel(kernel)
+            with Register(n, p2.PREC_FP32) as r:
+                r.set_fusion(span, rots)
+                r.set_state(amp)
+                r.paulirot(flip, phase, ang)
+                outs.append(r.get_state())
+    finally:
+        p2.set_sweep_kernel(True)
+        p2.set_sweep(*old)
+    assert np.array_equal(outs[0], outs[1])
+
+
+def test_sweeps_drivers_and_graphs(oracle_lib):
+    """Trotter steps replayed from CUDA graphs and qDRIFT samples (host and
+    device sampling) with sweep kernels: the same overlaps as one kernel
+    per pass of the same plans; within FP32 tolerance of the oracle."""
+    t = workloads.jw_terms(18, 500, seed=44)
+    d = workloads.hamming_dets(18, 3, 9, seed=45)
+    res = {}
+    old = p2.get_sweep()
+    p2.set_precision(p2.PREC_FP32)
+    p2.set_sweep(13, 5)
+    try:
+        for kernel in (False, True):
+            p2.set_sweep_kernel(kernel)
+            p2.set_device_sampling(False)
+            z1, st = p2.trott2(18, t, d, 6, 0.1, with_stats=True)
+            z2 = p2.qdrift(18, t, d, 3, 700, 0.02, 0x51)
+            p2.set_device_sampling(True)
+            z3 = p2.qdrift(18, t, d, 3, 700, 0.02, 0x51)
+            res[kernel] = (z1, z2, st, z3)
+    finally:
+        p2.set_sweep_kernel(True)
+        p2.set_sweep(*old)
+        p2.set_device_sampling(p2.DEVICE_SAMPLING_AUTO)
+        p2.set_precision(p2.PREC_FP64)
+    assert np.array_equal(res[False][0], res[True][0])
+    assert np.array_equal(res[False][1], res[True][1])
+    # device sampling plans the same sweeps and runs them pass by pass
+    assert np.array_equal(res[True][3], res[True][1])
+    assert res[True][2]["graph_replays"] >= 3
+    assert res[True][2]["sweeps"] < res[False][2]["sweeps"]
+    want = oracle_lib.trott(18, t.flip, t.phase, t.cf, d.idx, d.cf, 6, 0.1,
+                            order2=True)
+    assert np.max(np.abs(res[True][0] - want)) < FP32_TOL
+    want = oracle_lib.qdrift(18, t.flip, t.phase, t.cf, d.idx, d.cf, 3, 700,
+                             0.02, 0x51)
+    assert np.max(np.abs(res[True][1] - want)) < FP32_TOL
 
 
 # ---- drivers -----------------------------------------------------------
