@@ -355,6 +355,10 @@ def gpu_arm(args) -> None:
             extra["trott26"] = trott26_study()
         if "cmpsit33" in studies:
             extra["cmpsit33"] = cmpsit33_study()
+        if "sampling" in studies:
+            extra["sampling"] = sampling_study()
+        if "sweeps" in studies:
+            extra["sweeps"] = sweeps_study()
     if rank != 0:
         return
     clocks = clk.summary()
@@ -468,6 +472,91 @@ def trott26_study(steps: int = 2) -> dict:
     out["fp32_vs_fp64"] = out["fp32"]["value"] / out["fp64"]["value"]
     out["fp32_max_abs_err"] = float(np.max(np.abs(zs["fp32"] - zs["fp64"])))
     return out
+
+
+def sampling_study() -> dict:
+    """qdrift and cmpsit on FP32 registers of 10-24 qubits (JW-like terms,
+    four determinants), the samples drawn, planned and run by the host loop
+    and then on the device (device sampling): wall time of the driver call
+    each way (after one untimed run of the same shape) and whether the
+    overlaps agree bit for bit."""
+    import time
+
+    import numpy as np
+
+    import phase2_b200 as p2
+    from phase2_b200 import workloads
+    cases = [("qdrift", 10, 251, (64, 300, 0.01, 7)),
+             ("qdrift", 14, 400, (64, 1000, 0.01, 7)),
+             ("qdrift", 20, 800, (16, 2000, 0.01, 7)),
+             ("qdrift", 24, 1000, (8, 2000, 0.01, 7)),
+             ("cmpsit", 10, 251, (16, 8, 60, 50, 0.05, 0.002, 9)),
+             ("cmpsit", 14, 2000, (16, 4, 200, 800, 0.05, 0.002, 9)),
+             ("cmpsit", 20, 2000, (4, 4, 200, 800, 0.05, 0.002, 9))]
+    out = []
+    p2.set_precision(p2.PREC_FP32)
+    try:
+        for kind, n, nt, args in cases:
+            t = workloads.jw_terms(n, nt, seed=n)
+            d = workloads.hamming_dets(n, 4, n // 2, seed=n + 1)
+            fn = getattr(p2, kind)
+            res = {}
+            for mode in (p2.DEVICE_SAMPLING_OFF, p2.DEVICE_SAMPLING_ON):
+                p2.set_device_sampling(mode)
+                fn(n, t, d, *args)
+                t0 = time.perf_counter()
+                z = fn(n, t, d, *args)
+                res[mode] = (time.perf_counter() - t0, z)
+            host, dev = res[p2.DEVICE_SAMPLING_OFF], res[p2.DEVICE_SAMPLING_ON]
+            out.append({"driver": kind, "nqb": n, "terms": nt,
+                        "args": list(args), "host_ms": host[0] * 1e3,
+                        "device_ms": dev[0] * 1e3,
+                        "speedup": host[0] / dev[0],
+                        "bit_identical": bool(np.array_equal(host[1],
+                                                             dev[1]))})
+    finally:
+        p2.set_device_sampling(p2.DEVICE_SAMPLING_AUTO)
+        p2.set_precision(p2.PREC_FP64)
+    return {"workload": "FP32 qdrift/cmpsit, host vs device sampling",
+            "cases": out}
+
+
+def sweeps_study(nqb: int = 26) -> dict:
+    """The bench's qDRIFT draws (100,000 JW terms, 4096 per sample, two
+    samples) at `nqb` qubits, FP32, under several sweep shapes: each plan
+    run with one kernel per sweep and with one kernel per pass, device
+    rot.amp/s (CUDA events) and the HBM GB/s of the state round trips."""
+    import phase2_b200 as p2
+    from phase2_b200 import workloads
+    cfg = workloads.qdrift30(nqb=nqb)
+    t, d = cfg["terms"], cfg["dets"]
+    rows = []
+    old = p2.get_sweep()
+    p2.set_precision(p2.PREC_FP32)
+    p2.set_device_sampling(p2.DEVICE_SAMPLING_OFF)
+    try:
+        for shape in ((0, 5), (13, 5), (13, 4), (12, 4), (14, 5)):
+            for kernel in ((True, False) if shape[0] else (True,)):
+                p2.set_sweep(*shape)
+                p2.set_sweep_kernel(kernel)
+                p2.qdrift(nqb, t, d, 1, cfg["depth"], 1e-3, 11)
+                z, st = p2.qdrift(nqb, t, d, 2, cfg["depth"], 1e-3, 12,
+                                  with_stats=True, timing=True)
+                sec = st["pass_ms"] / 1e3
+                rows.append({"tile": shape[0], "low": shape[1],
+                             "sweep_kernel": kernel,
+                             "passes": int(st["passes"]),
+                             "round_trips": int(st["sweeps"]),
+                             "value": st["rotations"] * (1 << nqb) / sec,
+                             "hbm_gbs": st["bytes"] / sec / 1e9})
+    finally:
+        p2.set_sweep(*old)
+        p2.set_sweep_kernel(True)
+        p2.set_device_sampling(p2.DEVICE_SAMPLING_AUTO)
+        p2.set_precision(p2.PREC_FP64)
+    return {"workload": (f"qdrift {nqb} qubits, 100000 JW terms, 2 samples "
+                         f"x {cfg['depth']} draws, FP32"), "unit": UNIT,
+            "rows": rows}
 
 
 def cmpsit33_study(steps: int = 1) -> dict:
@@ -635,16 +724,24 @@ def main() -> None:
                     help="skip the CPU baseline and secondary arms")
     ap.add_argument("--studies", default="batched,trott26",
                     help="comma list of studies to append: batched, "
-                         "trott26, cmpsit33 (the last takes minutes)")
+                         "trott26, cmpsit33 (takes minutes), sampling, "
+                         "sweeps")
     ap.add_argument("--only-study", default=None,
                     help="run just this study (batched, trott26, cmpsit33, "
-                         "batch8) and print its JSON")
+                         "batch8, sampling, sweeps) and print its JSON; "
+                         "--nqb, when given, sets the sweeps study's width")
     args = ap.parse_args()
     if args.only_study:
+        import inspect
+
         import phase2_b200 as p2
         p2.world_ensure()
         fn = globals()[f"{args.only_study}_study"]
-        print(json.dumps({args.only_study: fn()}), flush=True)
+        kw = {}
+        if "nqb" in inspect.signature(fn).parameters and \
+                "--nqb" in sys.argv:
+            kw["nqb"] = args.nqb
+        print(json.dumps({args.only_study: fn(**kw)}), flush=True)
         return
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
