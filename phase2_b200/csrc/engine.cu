@@ -3062,39 +3062,60 @@ extern "C" int p2d_sampled_device(struct p2_dev *d,
 		R = 1;
 	const uint32_t C = (uint32_t)((T + P2_QUEUE_FLUSH - 1) / P2_QUEUE_FLUSH);
 	const size_t nt = job->nterms, nd = job->ndet, nh = job->length;
-	const size_t GT = G * T > 0 ? G * T : 1;
 	/* device buffer: tables, per-round scratch and program, registers */
 	enum { RNG, CDF, TFL, TPH, TCF, HFL, HPH, HPHI, HCS, WIDX, WVAL, GIDX,
 		GOUT, X, ROT, CS, PASS, REC, PROG, NPC, SOFF, POFF, REGS, NBUF };
 	size_t sz[NBUF], off[NBUF], total = 0;
-	sz[RNG] = 4 * samples * job->halves * sizeof(uint64_t);
-	sz[CDF] = nt * sizeof(double);
-	sz[TFL] = sz[TPH] = nt * sizeof(uint64_t);
-	sz[TCF] = nt * sizeof(double);
-	sz[HFL] = sz[HPH] = nh * sizeof(uint64_t);
-	sz[HPHI] = nh * sizeof(double);
-	sz[HCS] = 2 * nh * sizeof(double);
-	sz[WIDX] = nd * sizeof(uint64_t);
-	sz[WVAL] = 2 * nd * sizeof(double);
-	sz[GIDX] = samples * nd * sizeof(uint64_t);
-	sz[GOUT] = samples * nd * sizeof(double2);
-	sz[X] = G * job->halves * (size_t)job->depth * sizeof(double);
-	sz[ROT] = GT * sizeof(struct phase2_rot_in);
-	sz[CS] = 2 * GT * sizeof(double);
-	sz[PASS] = GT * sizeof(struct phase2_pass);
-	sz[REC] = GT * sizeof(struct phase2_rot_rec);
-	sz[PROG] = (G * T + 3 * G) * sizeof(struct p2_op);
-	sz[NPC] = sz[POFF] = (G * C ? G * C : 1) * sizeof(uint32_t);
-	sz[SOFF] = G * sizeof(uint32_t);
-	sz[REGS] = R * (sizeof(struct p2_binst) + sizeof(struct p2_bctl)) +
-		sizeof(unsigned int) + (R - 1) * d->namp * sizeof(float2);
-	for (int i = 0; i < NBUF; i++) {
-		off[i] = total;
-		total += (sz[i] + 255) & ~(size_t)255;
-	}
+	/* sizes and offsets for rounds of G samples on R registers */
+	auto layout = [&](size_t G, size_t R) {
+		const size_t GT = G * T > 0 ? G * T : 1;
+		sz[RNG] = 4 * samples * job->halves * sizeof(uint64_t);
+		sz[CDF] = nt * sizeof(double);
+		sz[TFL] = sz[TPH] = nt * sizeof(uint64_t);
+		sz[TCF] = nt * sizeof(double);
+		sz[HFL] = sz[HPH] = nh * sizeof(uint64_t);
+		sz[HPHI] = nh * sizeof(double);
+		sz[HCS] = 2 * nh * sizeof(double);
+		sz[WIDX] = nd * sizeof(uint64_t);
+		sz[WVAL] = 2 * nd * sizeof(double);
+		sz[GIDX] = samples * nd * sizeof(uint64_t);
+		sz[GOUT] = samples * nd * sizeof(double2);
+		sz[X] = G * job->halves * (size_t)job->depth * sizeof(double);
+		sz[ROT] = GT * sizeof(struct phase2_rot_in);
+		sz[CS] = 2 * GT * sizeof(double);
+		sz[PASS] = GT * sizeof(struct phase2_pass);
+		sz[REC] = GT * sizeof(struct phase2_rot_rec);
+		sz[PROG] = (G * T + 3 * G) * sizeof(struct p2_op);
+		sz[NPC] = sz[POFF] = (G * C ? G * C : 1) * sizeof(uint32_t);
+		sz[SOFF] = G * sizeof(uint32_t);
+		sz[REGS] = R * (sizeof(struct p2_binst) +
+				       sizeof(struct p2_bctl)) +
+			sizeof(unsigned int) + (R - 1) * d->namp * sizeof(float2);
+		total = 0;
+		for (int i = 0; i < NBUF; i++) {
+			off[i] = total;
+			total += (sz[i] + 255) & ~(size_t)255;
+		}
+	};
 	unsigned char *b = NULL;
 	CUDA_OK(cudaStreamSynchronize(d->stream), "device sampling: sync");
-	CUDA_OK(cudaMalloc((void **)&b, total), "device sampling: alloc");
+	/* on a full device: fewer state copies, then smaller rounds */
+	for (;;) {
+		layout(G, R);
+		if (cudaMalloc((void **)&b, total) == cudaSuccess)
+			break;
+		cudaGetLastError();
+		b = NULL;
+		if (R > 1) {
+			R = 1;
+		} else if (G > 1) {
+			G = (G + 1) / 2;
+		} else {
+			log_error("device sampling: no room for %zu bytes of "
+				  "scratch", total);
+			return -1;
+		}
+	}
 	uint64_t *gidx = (uint64_t *)malloc(sz[GIDX] ? sz[GIDX] : 1);
 	struct p2_binst *hinst = (struct p2_binst *)malloc(
 		R * sizeof(struct p2_binst));

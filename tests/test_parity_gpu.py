@@ -614,6 +614,35 @@ def test_qdrift_device_sampling(nqb, nterms, ndet, samples, depth,
         assert np.max(np.abs(dev - want)) < FP32_TOL
 
 
+def test_device_sampling_on_a_nearly_full_device():
+    """With too little free memory for state copies, device sampling runs
+    its samples on the register alone (smaller rounds if need be) and
+    still gives the host loop's overlaps bit for bit."""
+    torch = pytest.importorskip("torch")
+    n = 24
+    t = workloads.jw_terms(n, 600, seed=24)
+    d = workloads.hamming_dets(n, 2, 12, seed=25)
+    p2.set_precision(p2.PREC_FP32)
+    try:
+        p2.set_device_sampling(False)
+        host = p2.qdrift(n, t, d, 6, 500, 0.01, 0xF011)
+        free, _ = torch.cuda.mem_get_info()
+        # room for the 128 MiB register and a little scratch, not for
+        # the three 128 MiB copies four concurrent samples would need
+        hold = torch.empty(free - (400 << 20), dtype=torch.uint8,
+                           device="cuda")
+        try:
+            p2.set_device_sampling(True)
+            dev = p2.qdrift(n, t, d, 6, 500, 0.01, 0xF011)
+        finally:
+            del hold
+            torch.cuda.empty_cache()
+    finally:
+        p2.set_device_sampling(p2.DEVICE_SAMPLING_AUTO)
+        p2.set_precision(p2.PREC_FP64)
+    assert np.array_equal(dev, host)
+
+
 def _cmpsit_both_ways(nqb, t, d, samples, steps, length, depth, adet,
                       arand, seed):
     """FP32 cmpsit with host sampling, then with device sampling."""
