@@ -743,12 +743,20 @@ __device__ __forceinline__ void p2_rot_lift32(float (&re)[1 << M],
 				re[u] = fmaf(-st, im[w], re[u]);
 				im[u] = fmaf(st, re[w], im[u]);
 			} else {
-				re[u] = fmaf(st, re[w], re[u]);
-				im[u] = fmaf(st, im[w], im[u]);
-				re[w] = fmaf(-ss, re[u], re[w]);
-				im[w] = fmaf(-ss, im[u], im[w]);
-				re[u] = fmaf(st, re[w], re[u]);
-				im[u] = fmaf(st, im[w], im[u]);
+				/* the same three shears as six fmaf, two lanes
+				 * per packed FMA (round-to-nearest per lane: the
+				 * same bits) */
+				const float2 a = make_float2(st, st);
+				const float2 b = make_float2(-ss, -ss);
+				float2 yu = make_float2(re[u], im[u]);
+				float2 yw = make_float2(re[w], im[w]);
+				yu = __ffma2_rn(a, yw, yu);
+				yw = __ffma2_rn(b, yu, yw);
+				yu = __ffma2_rn(a, yw, yu);
+				re[u] = yu.x;
+				im[u] = yu.y;
+				re[w] = yw.x;
+				im[w] = yw.y;
 			}
 		}
 	}
