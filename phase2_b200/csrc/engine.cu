@@ -3260,7 +3260,8 @@ extern "C" int p2d_sampled_device(struct p2_dev *d,
 			e = cudaGetLastError();
 		if (timing)
 			cudaEventRecord(ev[4], d->stream);
-		d->launches += 6;
+		/* draw, stream and plan run only when they have work */
+		d->launches += 3 + (job->depth != 0) + (tot != 0) + (nch != 0);
 		unsigned int st = 0;
 		if (e == cudaSuccess)
 			e = cudaMemcpyAsync(&st, status, sizeof st,
