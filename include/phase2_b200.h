@@ -91,11 +91,13 @@ void circ_hamil_sort_flip(struct circ_hamil *hm);
 
 /*
  * Batched drivers run in one of two ways.  Persistent (default, when every
- * instance is an FP32 register of at most 31 qubits and the FP32 form is
- * PHASE2_FORM_LIFTED_F32): each instance's steps are recorded as a program
- * and all programs run in ONE persistent kernel launch that schedules
- * (instance, op, tile) work over all SMs.  Otherwise, or after
- * phase2_set_batch_persistent(0): per-instance streams as described below.
+ * instance is a register of at most 31 qubits of one precision: FP64, or
+ * FP32 with the FP32 form PHASE2_FORM_LIFTED_F32): each instance's steps
+ * are recorded as a program and all programs run in ONE persistent kernel
+ * launch that schedules (instance, op, tile) work over all SMs; FP64
+ * instances keep the pass kernels' exact arithmetic (bit-identical to the
+ * reference).  Otherwise, or after phase2_set_batch_persistent(0):
+ * per-instance streams as described below.
  */
 int phase2_set_batch_persistent(int on);
 
@@ -120,9 +122,10 @@ void phase2_get_sweep(int *tile_qubits, int *low_qubits);
 int phase2_set_sweep_kernel(int on);
 
 /*
- * qdrift_simul with device sampling: when the register is FP32 in
- * PHASE2_FORM_LIFTED_F32 with at most 31 qubits and the trial state is a
- * MULTIDET, the samples' term draws (CDF inversion of the host generator's
+ * qdrift_simul and cmpsit_simul with device sampling: when the register
+ * runs in the persistent kernel (at most 31 qubits; FP64, or FP32 in
+ * PHASE2_FORM_LIFTED_F32) and the trial state is a MULTIDET, the samples'
+ * term draws (CDF inversion of the host generator's
  * uniforms), their pass plans and their passes all run on the GPU: one
  * planning kernel per round of samples (a block per sample) writes the
  * programs that one persistent launch executes, several samples at once

@@ -204,9 +204,21 @@ static void qdrift_draw(struct qdrift *qd)
 	}
 }
 
+/* A register the persistent kernel runs: FP64 (exact form), or FP32 in
+ * the FP32-arithmetic form; at most 31 qubits. */
+static int persistent_reg_ok(const struct qreg *reg)
+{
+	const struct p2_qreg *b = reg->backend;
+	return b && p2d_batch_ok(b->dev) &&
+		(b->prec == PHASE2_PREC_FP64 ||
+			p2_form_for(PHASE2_PREC_FP32) ==
+				PHASE2_FORM_LIFTED_F32);
+}
+
 /* Registers that device sampling (p2d_sampled_device) takes under the
- * current mode: FP32 in the FP32-arithmetic form, at most 31 qubits,
- * multi-determinant trial state; AUTO also caps the width. */
+ * current mode: those the persistent kernel runs (FP64, or FP32 in the
+ * FP32-arithmetic form; at most 31 qubits) with a multi-determinant trial
+ * state; AUTO also caps the width. */
 static int device_sampling_ok(const struct circ *ct)
 {
 	const struct p2_qreg *b = ct->reg.backend;
@@ -214,10 +226,8 @@ static int device_sampling_ok(const struct circ *ct)
 		(p2_cfg.device_sampling == PHASE2_DEVICE_SAMPLING_AUTO &&
 			ct->reg.qb_lo > PHASE2_DEVICE_SAMPLING_AUTO_QB))
 		return 0;
-	return b && b->rec == NULL && b->prec == PHASE2_PREC_FP32 &&
-		p2_form_for(PHASE2_PREC_FP32) == PHASE2_FORM_LIFTED_F32 &&
-		p2d_batch_ok(b->dev) && ct->stprep_kind == STPREP_MULTIDET &&
-		ct->md.len > 0;
+	return b && b->rec == NULL && persistent_reg_ok(&ct->reg) &&
+		ct->stprep_kind == STPREP_MULTIDET && ct->md.len > 0;
 }
 
 /*
@@ -301,7 +311,7 @@ static int sampled_device(struct circ *ct, struct p2_smp_job *job,
 	}
 	job->max_span = b->max_span;
 	job->max_rots = b->max_rots;
-	job->form = PHASE2_FORM_LIFTED_F32;
+	job->form = p2_form_for(b->prec);
 	p2_sweep_for(job->nqb, job->form, &job->sweep_k, &job->sweep_low);
 	uint64_t npass = 0;
 	if (p2d_sampled_device(dev, job, rng0, ns, cdf->y, tfl, tph, tcf, hfl,
@@ -780,16 +790,21 @@ out:
 	return rc;
 }
 
-/* Whether every instance can run in one persistent launch. */
+/* Whether every instance can run in one persistent launch (registers of
+ * one precision). */
 static int batch_persistent_ok(const struct batch_item *items, size_t n)
 {
-	if (!p2_cfg.batch_persistent ||
-		p2_form_for(PHASE2_PREC_FP32) != PHASE2_FORM_LIFTED_F32)
+	if (!p2_cfg.batch_persistent)
 		return 0;
-	for (size_t i = 0; i < n; i++)
-		if (!p2d_batch_ok(p2_qreg_dev(&items[i].ct->reg)) ||
-			items[i].ct->stprep_kind != STPREP_MULTIDET)
+	for (size_t i = 0; i < n; i++) {
+		const struct qreg *reg = &items[i].ct->reg;
+		if (!persistent_reg_ok(reg) ||
+			items[i].ct->stprep_kind != STPREP_MULTIDET ||
+			((const struct p2_qreg *)reg->backend)->prec !=
+				((const struct p2_qreg *)items[0].ct->reg.backend)
+					->prec)
 			return 0;
+	}
 	return 1;
 }
 

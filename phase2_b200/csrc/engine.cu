@@ -1121,7 +1121,7 @@ __global__ void __launch_bounds__(P2_SW_TPB, 2)
 #define P2_BATCH_ZERO_TILE (P2_TPB * 128)
 
 struct p2_binst {
-	float2 *state;
+	void *state; /* float2 (FP32) or double2 (FP64) amplitudes */
 	uint64_t namp;
 	uint32_t op_off, nops;
 };
@@ -1171,7 +1171,60 @@ __device__ __forceinline__ void p2_batch_pass_tile(float2 *st,
 	}
 }
 
-__global__ void __launch_bounds__(P2_TPB, 5)
+/* The same for an FP64 register: the exact per-coset arithmetic of
+ * k_pass (p2_apply_run), loads and stores at L2 only. */
+template <int M>
+__device__ __forceinline__ void p2_batch_pass_tile64(double2 *st,
+	const struct phase2_pass &p, uint32_t tile, uint64_t nrep, uint32_t cpt,
+	const struct phase2_rot_rec *srec)
+{
+	uint64_t pb[M > 0 ? M : 1];
+#pragma unroll
+	for (int k = 0; k < M; ++k)
+		pb[k] = p.basis[k];
+	const uint64_t t0 = (uint64_t)tile * cpt * P2_TPB + threadIdx.x;
+	for (uint32_t j = 0; j < cpt; ++j) {
+		const uint64_t t = t0 + (uint64_t)j * P2_TPB;
+		if (t >= nrep)
+			continue;
+		const uint64_t x = p2_rep<M>(t, p);
+		double re[1 << M], im[1 << M];
+#pragma unroll
+		for (int u = 0; u < (1 << M); ++u) {
+			const double2 v = __ldcg(st + (x ^ p2_slot_off<M>(u, pb)));
+			re[u] = v.x;
+			im[u] = v.y;
+		}
+		p2_apply_run<M>(re, im, x, srec, p.nrot);
+		const uint64_t xs = p2_opaque(x);
+#pragma unroll
+		for (int u = 0; u < (1 << M); ++u)
+			__stcg(st + (xs ^ p2_slot_off<M>(u, pb)),
+				make_double2(re[u], im[u]));
+	}
+}
+
+/* Records as a batch kernel of state type ST holds them in shared
+ * memory: repacked lifted records (FP32) or the records themselves
+ * (FP64). */
+template <typename ST> struct p2_brec;
+template <> struct p2_brec<float2> {
+	typedef struct p2_lift32_rec type;
+	static __device__ __forceinline__ type of(const phase2_rot_rec &r)
+	{
+		return p2_lift32_of(r);
+	}
+};
+template <> struct p2_brec<double2> {
+	typedef struct phase2_rot_rec type;
+	static __device__ __forceinline__ type of(const phase2_rot_rec &r)
+	{
+		return r;
+	}
+};
+
+template <typename ST>
+__global__ void __launch_bounds__(P2_TPB, sizeof(ST) == 8 ? 5 : 2)
 	k_batch(const struct p2_binst *__restrict__ inst, uint32_t ninst,
 		const struct p2_op *__restrict__ ops,
 		const struct phase2_pass *__restrict__ passes,
@@ -1182,7 +1235,9 @@ __global__ void __launch_bounds__(P2_TPB, 5)
 		struct p2_bctl *ctl, unsigned int *status,
 		unsigned int idle_limit)
 {
-	__shared__ struct p2_lift32_rec srec[P2_MAX_ROTS_PER_PASS];
+	constexpr bool F64 = sizeof(ST) == 16;
+	typedef typename p2_brec<ST>::type RT;
+	__shared__ RT srec[P2_MAX_ROTS_PER_PASS];
 	__shared__ uint32_t s_inst, s_seq, s_tile;
 	__shared__ int s_what; /* 0 nothing claimable yet, 1 work, 2 exit */
 	/* pass whose records srec holds (block-uniform), none at first */
@@ -1246,7 +1301,7 @@ __global__ void __launch_bounds__(P2_TPB, 5)
 			return;
 		if (what == 1) {
 			const uint32_t i = s_inst, seq = s_seq, tile = s_tile;
-			float2 *const st = inst[i].state;
+			ST *const st = (ST *)inst[i].state;
 			const uint64_t namp = inst[i].namp;
 			const struct p2_op op = ops[inst[i].op_off + seq];
 			if (op.kind == P2_OP_PASS) {
@@ -1256,59 +1311,95 @@ __global__ void __launch_bounds__(P2_TPB, 5)
 				if (held != op.a) {
 					for (uint32_t r = threadIdx.x; r < p.nrot;
 						r += blockDim.x)
-						srec[r] = p2_lift32_of(
+						srec[r] = p2_brec<ST>::of(
 							recs[p.rot_off + r]);
 					held = op.a;
 					__syncthreads();
 				}
 				const uint64_t nrep = namp >> p.span;
-				switch (p.span) {
-				case 0:
-					p2_batch_pass_tile<0>(st, p, tile, nrep,
-						op.b, srec);
-					break;
-				case 1:
-					p2_batch_pass_tile<1>(st, p, tile, nrep,
-						op.b, srec);
-					break;
-				case 2:
-					p2_batch_pass_tile<2>(st, p, tile, nrep,
-						op.b, srec);
-					break;
-				case 3:
-					p2_batch_pass_tile<3>(st, p, tile, nrep,
-						op.b, srec);
-					break;
-				case 4:
-					p2_batch_pass_tile<4>(st, p, tile, nrep,
-						op.b, srec);
-					break;
-				default:
-					p2_batch_pass_tile<5>(st, p, tile, nrep,
-						op.b, srec);
-					break;
+				if constexpr (F64) {
+					switch (p.span) {
+					case 0:
+						p2_batch_pass_tile64<0>(st, p, tile,
+							nrep, op.b, srec);
+						break;
+					case 1:
+						p2_batch_pass_tile64<1>(st, p, tile,
+							nrep, op.b, srec);
+						break;
+					case 2:
+						p2_batch_pass_tile64<2>(st, p, tile,
+							nrep, op.b, srec);
+						break;
+					case 3:
+						p2_batch_pass_tile64<3>(st, p, tile,
+							nrep, op.b, srec);
+						break;
+					case 4:
+						p2_batch_pass_tile64<4>(st, p, tile,
+							nrep, op.b, srec);
+						break;
+					default:
+						p2_batch_pass_tile64<5>(st, p, tile,
+							nrep, op.b, srec);
+						break;
+					}
+				} else {
+					switch (p.span) {
+					case 0:
+						p2_batch_pass_tile<0>(st, p, tile,
+							nrep, op.b, srec);
+						break;
+					case 1:
+						p2_batch_pass_tile<1>(st, p, tile,
+							nrep, op.b, srec);
+						break;
+					case 2:
+						p2_batch_pass_tile<2>(st, p, tile,
+							nrep, op.b, srec);
+						break;
+					case 3:
+						p2_batch_pass_tile<3>(st, p, tile,
+							nrep, op.b, srec);
+						break;
+					case 4:
+						p2_batch_pass_tile<4>(st, p, tile,
+							nrep, op.b, srec);
+						break;
+					default:
+						p2_batch_pass_tile<5>(st, p, tile,
+							nrep, op.b, srec);
+						break;
+					}
 				}
 			} else if (op.kind == P2_OP_ZERO) {
 				const uint64_t base =
 					(uint64_t)tile * P2_BATCH_ZERO_TILE;
+				ST zero;
+				zero.x = 0;
+				zero.y = 0;
 				for (uint32_t k = threadIdx.x;
 					k < P2_BATCH_ZERO_TILE; k += blockDim.x)
 					if (base + k < namp)
-						__stcg(st + base + k,
-							make_float2(0.f, 0.f));
+						__stcg(st + base + k, zero);
 			} else if (op.kind == P2_OP_WRITE) {
 				/* in order: later writes win */
 				if (threadIdx.x == 0)
-					for (uint32_t e = op.a; e < op.a + op.b; ++e)
-						__stcg(st + widx[e],
-							make_float2(
-								(float)wval[2 * e],
-								(float)wval[2 * e + 1]));
+					for (uint32_t e = op.a; e < op.a + op.b; ++e) {
+						ST v;
+						if constexpr (F64) {
+							v.x = wval[2 * e];
+							v.y = wval[2 * e + 1];
+						} else {
+							v.x = (float)wval[2 * e];
+							v.y = (float)wval[2 * e + 1];
+						}
+						__stcg(st + widx[e], v);
+					}
 			} else {
 				for (uint32_t d = threadIdx.x; d < op.b;
 					d += blockDim.x) {
-					const float2 v =
-						__ldcg(st + gidx[op.a + d]);
+					const ST v = __ldcg(st + gidx[op.a + d]);
 					gout[op.a + d] = make_double2(v.x, v.y);
 				}
 			}
@@ -2581,7 +2672,9 @@ extern "C" void *p2d_stream(const struct p2_dev *d)
 
 extern "C" int p2d_batch_ok(const struct p2_dev *d)
 {
-	return d && d->prec == PHASE2_PREC_FP32 && d->nqb <= 31;
+	return d && (d->prec == PHASE2_PREC_FP32 ||
+			    d->prec == PHASE2_PREC_FP64) &&
+		d->nqb <= 31;
 }
 
 static size_t p2_align256(size_t v)
@@ -2592,6 +2685,30 @@ static size_t p2_align256(size_t v)
 /* Idle scheduling rounds (each sleeps ~1 us) before a block gives up. */
 #define P2_BATCH_IDLE_LIMIT 2000000u
 
+/* k_batch for FP32 or FP64 registers: its kernel function (occupancy
+ * queries) and its launch. */
+static const void *batch_kernel(bool f64)
+{
+	return f64 ? (const void *)k_batch<double2>
+		   : (const void *)k_batch<float2>;
+}
+
+static void batch_launch(bool f64, unsigned grid, cudaStream_t stream,
+	const struct p2_binst *inst, uint32_t ninst, const struct p2_op *ops,
+	const struct phase2_pass *passes, const struct phase2_rot_rec *recs,
+	const uint64_t *widx, const double *wval, const uint64_t *gidx,
+	double2 *gout, struct p2_bctl *ctl, unsigned int *status)
+{
+	if (f64)
+		k_batch<double2><<<grid, P2_TPB, 0, stream>>>(inst, ninst, ops,
+			passes, recs, widx, wval, gidx, gout, ctl, status,
+			P2_BATCH_IDLE_LIMIT);
+	else
+		k_batch<float2><<<grid, P2_TPB, 0, stream>>>(inst, ninst, ops,
+			passes, recs, widx, wval, gidx, gout, ctl, status,
+			P2_BATCH_IDLE_LIMIT);
+}
+
 extern "C" int p2d_batch_run(struct p2_dev *const *devs,
 	const struct p2_prog *const *progs, size_t n, double *gout,
 	double *kernel_ms)
@@ -2600,7 +2717,8 @@ extern "C" int p2d_batch_run(struct p2_dev *const *devs,
 		return 0;
 	size_t nops = 0, npass = 0, nrec = 0, nw = 0, ng = 0;
 	for (size_t i = 0; i < n; i++) {
-		if (!p2d_batch_ok(devs[i]) || progs[i]->error) {
+		if (!p2d_batch_ok(devs[i]) || progs[i]->error ||
+			devs[i]->prec != devs[0]->prec) {
 			log_error("batch: program %zu cannot run batched", i);
 			return -1;
 		}
@@ -2645,7 +2763,7 @@ extern "C" int p2d_batch_run(struct p2_dev *const *devs,
 	for (size_t i = 0; i < n; i++) {
 		const struct p2_prog *pg = progs[i];
 		struct p2_dev *d = devs[i];
-		hi[i].state = (float2 *)d->state;
+		hi[i].state = d->state;
 		hi[i].namp = d->namp;
 		hi[i].op_off = (uint32_t)bo;
 		hi[i].nops = (uint32_t)pg->nops;
@@ -2704,10 +2822,11 @@ extern "C" int p2d_batch_run(struct p2_dev *const *devs,
 	free(h);
 	if (e == cudaSuccess)
 		e = cudaMemset(dbuf + o_ctl, 0, total - o_ctl);
+	const bool f64 = d0->prec == PHASE2_PREC_FP64;
 	int per_sm = 0;
 	if (e == cudaSuccess)
 		e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm,
-			k_batch, P2_TPB, 0);
+			batch_kernel(f64), P2_TPB, 0);
 	if (e != cudaSuccess) {
 		cudaFree(dbuf);
 		log_error("batch: setup: %s", cudaGetErrorString(e));
@@ -2716,7 +2835,7 @@ extern "C" int p2d_batch_run(struct p2_dev *const *devs,
 	const unsigned grid =
 		(unsigned)d0->sm_count * (unsigned)(per_sm > 0 ? per_sm : 1);
 	cudaEventRecord(d0->t0, d0->stream);
-	k_batch<<<grid, P2_TPB, 0, d0->stream>>>(
+	batch_launch(f64, grid, d0->stream,
 		(const struct p2_binst *)(dbuf + o_inst), (uint32_t)n,
 		(const struct p2_op *)(dbuf + o_ops),
 		(const struct phase2_pass *)(dbuf + o_pass),
@@ -2725,7 +2844,7 @@ extern "C" int p2d_batch_run(struct p2_dev *const *devs,
 		(const double *)(dbuf + o_wval),
 		(const uint64_t *)(dbuf + o_gidx), (double2 *)(dbuf + o_gout),
 		(struct p2_bctl *)(dbuf + o_ctl),
-		(unsigned int *)(dbuf + o_status), P2_BATCH_IDLE_LIMIT);
+		(unsigned int *)(dbuf + o_status));
 	e = cudaGetLastError();
 	cudaEventRecord(d0->t1, d0->stream);
 	unsigned int status = 0;
@@ -3098,7 +3217,7 @@ extern "C" int p2d_sampled_device(struct p2_dev *d,
 		sz[SOFF] = G * sizeof(uint32_t);
 		sz[REGS] = R * (sizeof(struct p2_binst) +
 				       sizeof(struct p2_bctl)) +
-			sizeof(unsigned int) + (R - 1) * d->namp * sizeof(float2);
+			sizeof(unsigned int) + (R - 1) * d->namp * d->elem;
 		total = 0;
 		for (int i = 0; i < NBUF; i++) {
 			off[i] = total;
@@ -3131,9 +3250,9 @@ extern "C" int p2d_sampled_device(struct p2_dev *d,
 	cudaError_t e = gidx && hinst ? cudaSuccess
 				      : cudaErrorMemoryAllocation;
 	/* registers: the copies first (256-aligned), then inst, ctl, status */
-	float2 *copies = (float2 *)(b + off[REGS]);
+	unsigned char *copies = b + off[REGS];
 	struct p2_binst *inst = (struct p2_binst *)(b + off[REGS] +
-		(R - 1) * d->namp * sizeof(float2));
+		(R - 1) * d->namp * d->elem);
 	struct p2_bctl *ctl = (struct p2_bctl *)(inst + R);
 	unsigned int *status = (unsigned int *)(ctl + R);
 	if (e == cudaSuccess) {
@@ -3141,8 +3260,9 @@ extern "C" int p2d_sampled_device(struct p2_dev *d,
 			for (size_t j = 0; j < nd; j++)
 				gidx[s * nd + j] = det_idx[j];
 		for (size_t r = 0; r < R; r++) {
-			hinst[r].state = r == 0 ? (float2 *)d->state
-						: copies + (r - 1) * d->namp;
+			hinst[r].state = r == 0
+				? d->state
+				: (void *)(copies + (r - 1) * d->namp * d->elem);
 			hinst[r].namp = d->namp;
 			hinst[r].op_off = hinst[r].nops = 0;
 		}
@@ -3162,10 +3282,11 @@ extern "C" int p2d_sampled_device(struct p2_dev *d,
 				R * sizeof(struct p2_binst),
 				cudaMemcpyHostToDevice, d->stream);
 	}
+	const bool f64 = d->prec == PHASE2_PREC_FP64;
 	int per_sm = 0;
 	if (e == cudaSuccess)
 		e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm,
-			k_batch, P2_TPB, 0);
+			batch_kernel(f64), P2_TPB, 0);
 	if (e == cudaSuccess)
 		e = cudaFuncSetAttribute(k_smp_plan,
 			cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -3247,15 +3368,14 @@ extern "C" int p2d_sampled_device(struct p2_dev *d,
 			e = cudaMemsetAsync(status, 0, sizeof(unsigned int),
 				d->stream);
 		if (e == cudaSuccess)
-			k_batch<<<grid, P2_TPB, 0, d->stream>>>(inst, nreg,
+			batch_launch(f64, grid, d->stream, inst, nreg,
 				(const struct p2_op *)(b + off[PROG]),
 				(const struct phase2_pass *)(b + off[PASS]),
 				(const struct phase2_rot_rec *)(b + off[REC]),
 				(const uint64_t *)(b + off[WIDX]),
 				(const double *)(b + off[WVAL]),
 				(const uint64_t *)(b + off[GIDX]),
-				(double2 *)(b + off[GOUT]), ctl, status,
-				P2_BATCH_IDLE_LIMIT);
+				(double2 *)(b + off[GOUT]), ctl, status);
 		if (e == cudaSuccess)
 			e = cudaGetLastError();
 		if (timing)

@@ -569,9 +569,10 @@ def test_persistent_batch(kind, oracle_lib):
         assert np.max(np.abs(z - want)) < FP32_TOL, kind
 
 
-def _qdrift_both_ways(nqb, t, d, samples, depth, step, seed):
-    """FP32 qdrift with host sampling, then with device sampling."""
-    p2.set_precision(p2.PREC_FP32)
+def _qdrift_both_ways(nqb, t, d, samples, depth, step, seed,
+                      prec=p2.PREC_FP32):
+    """qdrift with host sampling, then with device sampling."""
+    p2.set_precision(prec)
     p2.set_device_sampling(False)
     try:
         host, hst = p2.qdrift(nqb, t, d, samples, depth, step, seed,
@@ -587,6 +588,8 @@ def _qdrift_both_ways(nqb, t, d, samples, depth, step, seed):
     return host, dev, st
 
 
+@pytest.mark.parametrize("prec", [p2.PREC_FP32, p2.PREC_FP64],
+                         ids=["fp32", "fp64"])
 @pytest.mark.parametrize("nqb,nterms,ndet,samples,depth", [
     (9, 60, 1, 3, 40),        # one determinant, short circuits
     (11, 500, 5, 5, 300),
@@ -594,24 +597,27 @@ def _qdrift_both_ways(nqb, t, d, samples, depth, step, seed):
     (8, 30, 2, 4200, 3),      # two planning rounds, the last one short
     (16, 300, 4, 7, 700),
 ])
-def test_qdrift_device_sampling(nqb, nterms, ndet, samples, depth,
+def test_qdrift_device_sampling(nqb, nterms, ndet, samples, depth, prec,
                                 oracle_lib):
     """Device sampling (draws, plans and passes on the GPU; small registers
     run many samples at once on copies of the state) gives the host loop's
-    overlaps and final register bit for bit, within the FP32 tolerance of
-    the oracle."""
+    overlaps and final register bit for bit; FP64 registers also match the
+    oracle bit for bit, FP32 ones within the FP32 tolerance."""
     t = workloads.jw_terms(nqb, nterms, seed=nqb * 7 + depth)
     # a term below DBL_EPSILON draws the zero angle
     t.cf[3] = 1e-17
     d = workloads.hamming_dets(nqb, ndet, nqb // 2, seed=nqb + ndet)
     host, dev, st = _qdrift_both_ways(nqb, t, d, samples, depth, 0.02,
-                                      0x5EED + nqb)
+                                      0x5EED + nqb, prec)
     assert np.array_equal(dev, host)
     assert st["passes"] > 0 and st["launches"] >= 3
-    if samples * depth <= 20000:
+    if samples * depth <= 20000 or prec == p2.PREC_FP64 and nqb <= 12:
         want = oracle_lib.qdrift(nqb, t.flip, t.phase, t.cf, d.idx, d.cf,
                                  samples, depth, 0.02, 0x5EED + nqb)
-        assert np.max(np.abs(dev - want)) < FP32_TOL
+        if prec == p2.PREC_FP64:
+            assert np.array_equal(dev, want)
+        else:
+            assert np.max(np.abs(dev - want)) < FP32_TOL
 
 
 def test_device_sampling_on_a_nearly_full_device():
@@ -644,10 +650,10 @@ def test_device_sampling_on_a_nearly_full_device():
 
 
 def _cmpsit_both_ways(nqb, t, d, samples, steps, length, depth, adet,
-                      arand, seed):
-    """FP32 cmpsit with host sampling, then with device sampling."""
+                      arand, seed, prec=p2.PREC_FP32):
+    """cmpsit with host sampling, then with device sampling."""
     args = (nqb, t, d, samples, steps, length, depth, adet, arand, seed)
-    p2.set_precision(p2.PREC_FP32)
+    p2.set_precision(prec)
     p2.set_device_sampling(False)
     try:
         host, hst = p2.cmpsit(*args, with_stats=True, with_state=True)
@@ -668,23 +674,28 @@ def _cmpsit_both_ways(nqb, t, d, samples, steps, length, depth, adet,
     (10, 50, 2, 3, 2, 10, 0),        # head terms only
     (10, 50, 2, 3, 2, 0, 20),        # draws only
 ])
+@pytest.mark.parametrize("prec", [p2.PREC_FP32, p2.PREC_FP64],
+                         ids=["fp32", "fp64"])
 def test_cmpsit_device_sampling(nqb, nterms, ndet, samples, steps, length,
-                                depth, oracle_lib):
+                                depth, prec, oracle_lib):
     """cmpsit with device sampling (forward and reversed halves of head
     terms and fresh draws on the GPU) gives the host loop's overlaps and
-    final register bit for bit, within the FP32 tolerance of the
-    oracle."""
+    final register bit for bit; FP64 also the oracle's bits, FP32 within
+    the FP32 tolerance."""
     t = workloads.jw_terms(nqb, nterms, seed=nqb * 11 + depth)
     t.cf[5] = -1e-17  # a drawn term in the sign dead zone
     d = workloads.hamming_dets(nqb, ndet, nqb // 2, seed=nqb + 2 * ndet)
     args = (samples, steps, length, depth, 0.05, 0.004, 0xC0DE + nqb)
-    host, dev, st = _cmpsit_both_ways(nqb, t, d, *args)
+    host, dev, st = _cmpsit_both_ways(nqb, t, d, *args, prec=prec)
     assert np.array_equal(dev, host)
     assert st["passes"] > 0
     if samples * steps * (length + depth) <= 20000:
         want = oracle_lib.cmpsit(nqb, t.flip, t.phase, t.cf, d.idx, d.cf,
                                  *args)
-        assert np.max(np.abs(dev - want)) < FP32_TOL
+        if prec == p2.PREC_FP64:
+            assert np.array_equal(dev, want)
+        else:
+            assert np.max(np.abs(dev - want)) < FP32_TOL
 
 
 def test_device_sampling_h2o(golden):
@@ -699,6 +710,41 @@ def test_device_sampling_h2o(golden):
     assert np.array_equal(dev, host)
     want = np.array([_cz(v) for v in golden["h2o"]["cmpsit"]])
     assert np.max(np.abs(dev - want)) < FP32_TOL
+
+
+@pytest.mark.parametrize("kind", ["trott", "trott2", "qdrift", "cmpsit"])
+def test_persistent_batch_fp64(kind, oracle_lib):
+    """FP64 batches in one persistent launch (the exact per-coset
+    arithmetic of the pass kernel): every result bit-identical to the
+    oracle and to the per-instance stream mode, one kernel launch."""
+    probs = _uneven_problems()[:5]
+    if kind == "cmpsit":
+        probs = [dict(p, samples=2, steps=2, depth=12) for p in probs]
+    try:
+        p2.set_batch_persistent(True)
+        got, stats = p2.batch(kind, probs, with_stats=True)
+        p2.set_batch_persistent(False)
+        ref = p2.batch(kind, probs)
+    finally:
+        p2.set_batch_persistent(True)
+    assert sum(s["launches"] for s in stats) == 1
+    for p, z, r in zip(probs, got, ref):
+        assert np.array_equal(z, r), kind
+        t, d = p["terms"], p["dets"]
+        if kind in ("trott", "trott2"):
+            want = oracle_lib.trott(p["nqb"], t.flip, t.phase, t.cf, d.idx,
+                                    d.cf, p["steps"], p["delta"],
+                                    order2=kind == "trott2")
+        elif kind == "qdrift":
+            want = oracle_lib.qdrift(p["nqb"], t.flip, t.phase, t.cf, d.idx,
+                                     d.cf, p["samples"], p["depth"],
+                                     p["step_size"], p["seed"])
+        else:
+            want = oracle_lib.cmpsit(p["nqb"], t.flip, t.phase, t.cf, d.idx,
+                                     d.cf, 2, 2, p["length"], 12,
+                                     p["angle_det"], p["angle_rand"],
+                                     p["seed"])
+        assert np.array_equal(z, want), kind
 
 
 def test_persistent_batch_empty_and_single():
