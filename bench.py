@@ -475,11 +475,11 @@ def trott26_study(steps: int = 2) -> dict:
 
 
 def sampling_study() -> dict:
-    """qdrift and cmpsit on FP32 registers of 10-24 qubits (JW-like terms,
-    four determinants), the samples drawn, planned and run by the host loop
-    and then on the device (device sampling): wall time of the driver call
-    each way (after one untimed run of the same shape) and whether the
-    overlaps agree bit for bit."""
+    """qdrift and cmpsit on FP32 and FP64 registers of 10-24 qubits
+    (JW-like terms, four determinants), the samples drawn, planned and run
+    by the host loop and then on the device (device sampling): wall time of
+    the driver call each way (after one untimed run of the same shape) and
+    whether the overlaps agree bit for bit."""
     import time
 
     import numpy as np
@@ -494,9 +494,11 @@ def sampling_study() -> dict:
              ("cmpsit", 14, 2000, (16, 4, 200, 800, 0.05, 0.002, 9)),
              ("cmpsit", 20, 2000, (4, 4, 200, 800, 0.05, 0.002, 9))]
     out = []
-    p2.set_precision(p2.PREC_FP32)
     try:
-        for kind, n, nt, args in cases:
+        for (kind, n, nt, args), prec in [(c, p) for p in (p2.PREC_FP32,
+                                                            p2.PREC_FP64)
+                                           for c in cases]:
+            p2.set_precision(prec)
             t = workloads.jw_terms(n, nt, seed=n)
             d = workloads.hamming_dets(n, 4, n // 2, seed=n + 1)
             fn = getattr(p2, kind)
@@ -509,6 +511,8 @@ def sampling_study() -> dict:
                 res[mode] = (time.perf_counter() - t0, z)
             host, dev = res[p2.DEVICE_SAMPLING_OFF], res[p2.DEVICE_SAMPLING_ON]
             out.append({"driver": kind, "nqb": n, "terms": nt,
+                        "precision": "fp64" if prec == p2.PREC_FP64
+                        else "fp32",
                         "args": list(args), "host_ms": host[0] * 1e3,
                         "device_ms": dev[0] * 1e3,
                         "speedup": host[0] / dev[0],
@@ -517,7 +521,7 @@ def sampling_study() -> dict:
     finally:
         p2.set_device_sampling(p2.DEVICE_SAMPLING_AUTO)
         p2.set_precision(p2.PREC_FP64)
-    return {"workload": "FP32 qdrift/cmpsit, host vs device sampling",
+    return {"workload": "qdrift/cmpsit, host vs device sampling",
             "cases": out}
 
 
