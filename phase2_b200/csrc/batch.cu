@@ -1,0 +1,515 @@
+/*
+ * batch.cu -- the persistent kernel (k_batch): recorded programs of many
+ * registers (zero, determinant writes, passes, gathers) scheduled as
+ * (register, op, tile) work over all SMs in one launch, FP32 or FP64 state;
+ * the batched drivers' executor (p2d_batch_run).  Device sampling
+ * (sampling.cu) runs its programs through the same kernel.
+ */
+#include <cuda_runtime.h>
+
+#include <float.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define LOG_SUBSYS "engine"
+#include "log.h"
+
+#include "p2_kernels.cuh"
+
+/* The cosets of one pass tile: thread k takes representatives
+ * tile * cpt * P2_TPB + j * P2_TPB + k, j < cpt (coalesced per j). */
+template <int M>
+__device__ __forceinline__ void p2_batch_pass_tile(float2 *st,
+	const struct phase2_pass &p, uint32_t tile, uint64_t nrep, uint32_t cpt,
+	const struct p2_lift32_rec *srec)
+{
+	uint32_t pb[M > 0 ? M : 1];
+#pragma unroll
+	for (int k = 0; k < M; ++k)
+		pb[k] = (uint32_t)p.basis[k];
+	const uint32_t negm = p.scale < 0 ? 0x80000000u : 0u;
+	const uint64_t t0 = (uint64_t)tile * cpt * P2_TPB + threadIdx.x;
+	for (uint32_t j = 0; j < cpt; ++j) {
+		const uint64_t t = t0 + (uint64_t)j * P2_TPB;
+		if (t < nrep)
+			p2_lift32_coset<M, uint32_t, true>(st,
+				p2_rep_t<M, uint32_t>((uint32_t)t, p), pb, srec,
+				p.nrot, negm);
+	}
+}
+
+/* The same for an FP64 register: the exact per-coset arithmetic of
+ * k_pass (p2_apply_run), loads and stores at L2 only. */
+template <int M>
+__device__ __forceinline__ void p2_batch_pass_tile64(double2 *st,
+	const struct phase2_pass &p, uint32_t tile, uint64_t nrep, uint32_t cpt,
+	const struct phase2_rot_rec *srec)
+{
+	uint64_t pb[M > 0 ? M : 1];
+#pragma unroll
+	for (int k = 0; k < M; ++k)
+		pb[k] = p.basis[k];
+	const uint64_t t0 = (uint64_t)tile * cpt * P2_TPB + threadIdx.x;
+	for (uint32_t j = 0; j < cpt; ++j) {
+		const uint64_t t = t0 + (uint64_t)j * P2_TPB;
+		if (t >= nrep)
+			continue;
+		const uint64_t x = p2_rep<M>(t, p);
+		double re[1 << M], im[1 << M];
+#pragma unroll
+		for (int u = 0; u < (1 << M); ++u) {
+			const double2 v = __ldcg(st + (x ^ p2_slot_off<M>(u, pb)));
+			re[u] = v.x;
+			im[u] = v.y;
+		}
+		p2_apply_run<M>(re, im, x, srec, p.nrot);
+		const uint64_t xs = p2_opaque(x);
+#pragma unroll
+		for (int u = 0; u < (1 << M); ++u)
+			__stcg(st + (xs ^ p2_slot_off<M>(u, pb)),
+				make_double2(re[u], im[u]));
+	}
+}
+
+/* Records as a batch kernel of state type ST holds them in shared
+ * memory: repacked lifted records (FP32) or the records themselves
+ * (FP64). */
+template <typename ST> struct p2_brec;
+template <> struct p2_brec<float2> {
+	typedef struct p2_lift32_rec type;
+	static __device__ __forceinline__ type of(const phase2_rot_rec &r)
+	{
+		return p2_lift32_of(r);
+	}
+};
+template <> struct p2_brec<double2> {
+	typedef struct phase2_rot_rec type;
+	static __device__ __forceinline__ type of(const phase2_rot_rec &r)
+	{
+		return r;
+	}
+};
+
+template <typename ST>
+__global__ void __launch_bounds__(P2_TPB, sizeof(ST) == 8 ? 5 : 2)
+	k_batch(const struct p2_binst *__restrict__ inst, uint32_t ninst,
+		const struct p2_op *__restrict__ ops,
+		const struct phase2_pass *__restrict__ passes,
+		const struct phase2_rot_rec *__restrict__ recs,
+		const uint64_t *__restrict__ widx,
+		const double *__restrict__ wval,
+		const uint64_t *__restrict__ gidx, double2 *__restrict__ gout,
+		struct p2_bctl *ctl, unsigned int *status,
+		unsigned int idle_limit)
+{
+	constexpr bool F64 = sizeof(ST) == 16;
+	typedef typename p2_brec<ST>::type RT;
+	__shared__ RT srec[P2_MAX_ROTS_PER_PASS];
+	__shared__ uint32_t s_inst, s_seq, s_tile;
+	__shared__ int s_what; /* 0 nothing claimable yet, 1 work, 2 exit */
+	/* pass whose records srec holds (block-uniform), none at first */
+	uint32_t held = 0xffffffffu;
+	uint32_t cursor = blockIdx.x % ninst;
+	unsigned int idle = 0;
+	unsigned long long seen = 0; /* tickets at the last idle round */
+	for (;;) {
+		if (threadIdx.x == 0) {
+			int what = 2;
+			unsigned long long sig = 0;
+			for (uint32_t k = 0; k < ninst; ++k) {
+				const uint32_t i = cursor + k < ninst
+					? cursor + k
+					: cursor + k - ninst;
+				const uint32_t nops = inst[i].nops;
+				const unsigned long long tk =
+					*(volatile unsigned long long *)&ctl[i]
+						 .ticket;
+				sig += tk * (2ull * i + 1ull);
+				if ((uint32_t)(tk >> 32) >= nops)
+					continue; /* program finished */
+				what = 0;
+				const uint32_t off = inst[i].op_off;
+				if ((uint32_t)tk >=
+					ops[off + (uint32_t)(tk >> 32)].ntiles)
+					continue; /* all tiles taken */
+				const unsigned long long got =
+					atomicAdd(&ctl[i].ticket, 1ull);
+				const uint32_t seq = (uint32_t)(got >> 32);
+				const uint32_t tile = (uint32_t)got;
+				if (seq < nops && tile < ops[off + seq].ntiles) {
+					__threadfence();
+					s_inst = i;
+					s_seq = seq;
+					s_tile = tile;
+					cursor = i;
+					what = 1;
+					break;
+				}
+			}
+			if (what == 0) {
+				if (sig != seen) {
+					seen = sig;
+					idle = 0;
+				}
+				if (++idle > idle_limit) {
+					atomicOr(status, 1u);
+					what = 2;
+				} else {
+					__nanosleep(1000);
+				}
+			} else if (what == 1) {
+				idle = 0;
+			}
+			s_what = what;
+		}
+		__syncthreads();
+		const int what = s_what;
+		if (what == 2)
+			return;
+		if (what == 1) {
+			const uint32_t i = s_inst, seq = s_seq, tile = s_tile;
+			ST *const st = (ST *)inst[i].state;
+			const uint64_t namp = inst[i].namp;
+			const struct p2_op op = ops[inst[i].op_off + seq];
+			if (op.kind == P2_OP_PASS) {
+				const struct phase2_pass p = passes[op.a];
+				/* consecutive tiles of one pass (a Trotter step
+				 * replays the same passes) keep their records */
+				if (held != op.a) {
+					for (uint32_t r = threadIdx.x; r < p.nrot;
+						r += blockDim.x)
+						srec[r] = p2_brec<ST>::of(
+							recs[p.rot_off + r]);
+					held = op.a;
+					__syncthreads();
+				}
+				const uint64_t nrep = namp >> p.span;
+				if constexpr (F64) {
+					switch (p.span) {
+					case 0:
+						p2_batch_pass_tile64<0>(st, p, tile,
+							nrep, op.b, srec);
+						break;
+					case 1:
+						p2_batch_pass_tile64<1>(st, p, tile,
+							nrep, op.b, srec);
+						break;
+					case 2:
+						p2_batch_pass_tile64<2>(st, p, tile,
+							nrep, op.b, srec);
+						break;
+					case 3:
+						p2_batch_pass_tile64<3>(st, p, tile,
+							nrep, op.b, srec);
+						break;
+					case 4:
+						p2_batch_pass_tile64<4>(st, p, tile,
+							nrep, op.b, srec);
+						break;
+					default:
+						p2_batch_pass_tile64<5>(st, p, tile,
+							nrep, op.b, srec);
+						break;
+					}
+				} else {
+					switch (p.span) {
+					case 0:
+						p2_batch_pass_tile<0>(st, p, tile,
+							nrep, op.b, srec);
+						break;
+					case 1:
+						p2_batch_pass_tile<1>(st, p, tile,
+							nrep, op.b, srec);
+						break;
+					case 2:
+						p2_batch_pass_tile<2>(st, p, tile,
+							nrep, op.b, srec);
+						break;
+					case 3:
+						p2_batch_pass_tile<3>(st, p, tile,
+							nrep, op.b, srec);
+						break;
+					case 4:
+						p2_batch_pass_tile<4>(st, p, tile,
+							nrep, op.b, srec);
+						break;
+					default:
+						p2_batch_pass_tile<5>(st, p, tile,
+							nrep, op.b, srec);
+						break;
+					}
+				}
+			} else if (op.kind == P2_OP_ZERO) {
+				const uint64_t base =
+					(uint64_t)tile * P2_BATCH_ZERO_TILE;
+				ST zero;
+				zero.x = 0;
+				zero.y = 0;
+				for (uint32_t k = threadIdx.x;
+					k < P2_BATCH_ZERO_TILE; k += blockDim.x)
+					if (base + k < namp)
+						__stcg(st + base + k, zero);
+			} else if (op.kind == P2_OP_WRITE) {
+				/* in order: later writes win */
+				if (threadIdx.x == 0)
+					for (uint32_t e = op.a; e < op.a + op.b; ++e) {
+						ST v;
+						if constexpr (F64) {
+							v.x = wval[2 * e];
+							v.y = wval[2 * e + 1];
+						} else {
+							v.x = (float)wval[2 * e];
+							v.y = (float)wval[2 * e + 1];
+						}
+						__stcg(st + widx[e], v);
+					}
+			} else {
+				for (uint32_t d = threadIdx.x; d < op.b;
+					d += blockDim.x) {
+					const ST v = __ldcg(st + gidx[op.a + d]);
+					gout[op.a + d] = make_double2(v.x, v.y);
+				}
+			}
+			__threadfence();
+			__syncthreads();
+			if (threadIdx.x == 0) {
+				const unsigned int d =
+					atomicAdd(&ctl[i].done, 1u) + 1u;
+				if (d == op.ntiles) {
+					atomicExch(&ctl[i].done, 0u);
+					__threadfence();
+					atomicExch(&ctl[i].ticket,
+						(unsigned long long)(seq + 1) << 32);
+				}
+			}
+		}
+		__syncthreads();
+	}
+}
+
+/* ---- batched persistent execution --------------------------------------- */
+
+extern "C" int p2d_batch_ok(const struct p2_dev *d)
+{
+	return d && (d->prec == PHASE2_PREC_FP32 ||
+			    d->prec == PHASE2_PREC_FP64) &&
+		d->nqb <= 31;
+}
+
+static size_t p2_align256(size_t v)
+{
+	return (v + 255) & ~(size_t)255;
+}
+
+/* k_batch for FP32 or FP64 registers: its kernel function (occupancy
+ * queries) and its launch. */
+const void *p2_batch_kernel(bool f64)
+{
+	return f64 ? (const void *)k_batch<double2>
+		   : (const void *)k_batch<float2>;
+}
+
+void p2_batch_launch(bool f64, unsigned grid, cudaStream_t stream,
+	const struct p2_binst *inst, uint32_t ninst, const struct p2_op *ops,
+	const struct phase2_pass *passes, const struct phase2_rot_rec *recs,
+	const uint64_t *widx, const double *wval, const uint64_t *gidx,
+	double2 *gout, struct p2_bctl *ctl, unsigned int *status)
+{
+	if (f64)
+		k_batch<double2><<<grid, P2_TPB, 0, stream>>>(inst, ninst, ops,
+			passes, recs, widx, wval, gidx, gout, ctl, status,
+			P2_BATCH_IDLE_LIMIT);
+	else
+		k_batch<float2><<<grid, P2_TPB, 0, stream>>>(inst, ninst, ops,
+			passes, recs, widx, wval, gidx, gout, ctl, status,
+			P2_BATCH_IDLE_LIMIT);
+}
+
+extern "C" int p2d_batch_run(struct p2_dev *const *devs,
+	const struct p2_prog *const *progs, size_t n, double *gout,
+	double *kernel_ms)
+{
+	if (n == 0)
+		return 0;
+	size_t nops = 0, npass = 0, nrec = 0, nw = 0, ng = 0;
+	for (size_t i = 0; i < n; i++) {
+		if (!p2d_batch_ok(devs[i]) || progs[i]->error ||
+			devs[i]->prec != devs[0]->prec) {
+			log_error("batch: program %zu cannot run batched", i);
+			return -1;
+		}
+		nops += progs[i]->nops;
+		npass += progs[i]->npass;
+		nrec += progs[i]->nrec;
+		nw += progs[i]->nw;
+		ng += progs[i]->ng;
+	}
+	if (n > UINT32_MAX || nops > UINT32_MAX || npass > UINT32_MAX ||
+		nrec > UINT32_MAX || nw > UINT32_MAX || ng > UINT32_MAX) {
+		log_error("batch: program too large");
+		return -1;
+	}
+	/* one device buffer: uploaded part, then outputs and control */
+	const size_t o_inst = 0;
+	const size_t o_ops = p2_align256(o_inst + n * sizeof(struct p2_binst));
+	const size_t o_pass = p2_align256(o_ops + nops * sizeof(struct p2_op));
+	const size_t o_rec =
+		p2_align256(o_pass + npass * sizeof(struct phase2_pass));
+	const size_t o_widx =
+		p2_align256(o_rec + nrec * sizeof(struct phase2_rot_rec));
+	const size_t o_wval = p2_align256(o_widx + nw * sizeof(uint64_t));
+	const size_t o_gidx = p2_align256(o_wval + 2 * nw * sizeof(double));
+	const size_t up = p2_align256(o_gidx + ng * sizeof(uint64_t));
+	const size_t o_gout = up;
+	const size_t o_ctl = p2_align256(o_gout + ng * sizeof(double2));
+	const size_t o_status = p2_align256(o_ctl + n * sizeof(struct p2_bctl));
+	const size_t total = o_status + 256;
+
+	unsigned char *h = (unsigned char *)malloc(up);
+	if (!h)
+		return -1;
+	struct p2_binst *hi = (struct p2_binst *)(h + o_inst);
+	struct p2_op *ho = (struct p2_op *)(h + o_ops);
+	struct phase2_pass *hp = (struct phase2_pass *)(h + o_pass);
+	struct phase2_rot_rec *hr = (struct phase2_rot_rec *)(h + o_rec);
+	uint64_t *hwi = (uint64_t *)(h + o_widx);
+	double *hwv = (double *)(h + o_wval);
+	uint64_t *hgi = (uint64_t *)(h + o_gidx);
+	size_t bo = 0, bp = 0, br = 0, bw = 0, bg = 0;
+	for (size_t i = 0; i < n; i++) {
+		const struct p2_prog *pg = progs[i];
+		struct p2_dev *d = devs[i];
+		hi[i].state = d->state;
+		hi[i].namp = d->namp;
+		hi[i].op_off = (uint32_t)bo;
+		hi[i].nops = (uint32_t)pg->nops;
+		for (size_t k = 0; k < pg->npass; k++) {
+			hp[bp + k] = pg->passes[k];
+			hp[bp + k].rot_off += (uint32_t)br;
+		}
+		for (size_t k = 0; k < pg->nops; k++) {
+			struct p2_op op = pg->ops[k];
+			switch (op.kind) {
+			case P2_OP_PASS:
+				op.a += (uint32_t)bp;
+				op.ntiles = p2_op_tiles(P2_OP_PASS, d->namp,
+					hp[op.a].span, &op.b);
+				break;
+			case P2_OP_ZERO:
+				op.ntiles = p2_op_tiles(P2_OP_ZERO, d->namp, 0,
+					&op.b);
+				break;
+			case P2_OP_WRITE:
+				op.a += (uint32_t)bw;
+				op.ntiles = 1;
+				break;
+			default:
+				op.a += (uint32_t)bg;
+				op.ntiles = 1;
+				break;
+			}
+			ho[bo + k] = op;
+		}
+		if (pg->nrec)
+			memcpy(hr + br, pg->recs, pg->nrec * sizeof *hr);
+		if (pg->nw) {
+			memcpy(hwi + bw, pg->widx, pg->nw * sizeof *hwi);
+			memcpy(hwv + 2 * bw, pg->wval,
+				2 * pg->nw * sizeof *hwv);
+		}
+		if (pg->ng)
+			memcpy(hgi + bg, pg->gidx, pg->ng * sizeof *hgi);
+		bo += pg->nops;
+		bp += pg->npass;
+		br += pg->nrec;
+		bw += pg->nw;
+		bg += pg->ng;
+	}
+
+	struct p2_dev *d0 = devs[0];
+	unsigned char *dbuf = NULL;
+	cudaError_t e = cudaSuccess;
+	for (size_t i = 0; i < n && e == cudaSuccess; i++)
+		e = cudaStreamSynchronize(devs[i]->stream);
+	if (e == cudaSuccess)
+		e = cudaMalloc((void **)&dbuf, total);
+	if (e == cudaSuccess)
+		e = cudaMemcpy(dbuf, h, up, cudaMemcpyHostToDevice);
+	free(h);
+	if (e == cudaSuccess)
+		e = cudaMemset(dbuf + o_ctl, 0, total - o_ctl);
+	const bool f64 = d0->prec == PHASE2_PREC_FP64;
+	int per_sm = 0;
+	if (e == cudaSuccess)
+		e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm,
+			p2_batch_kernel(f64), P2_TPB, 0);
+	if (e != cudaSuccess) {
+		cudaFree(dbuf);
+		log_error("batch: setup: %s", cudaGetErrorString(e));
+		return -1;
+	}
+	const unsigned grid =
+		(unsigned)d0->sm_count * (unsigned)(per_sm > 0 ? per_sm : 1);
+	cudaEventRecord(d0->t0, d0->stream);
+	p2_batch_launch(f64, grid, d0->stream,
+		(const struct p2_binst *)(dbuf + o_inst), (uint32_t)n,
+		(const struct p2_op *)(dbuf + o_ops),
+		(const struct phase2_pass *)(dbuf + o_pass),
+		(const struct phase2_rot_rec *)(dbuf + o_rec),
+		(const uint64_t *)(dbuf + o_widx),
+		(const double *)(dbuf + o_wval),
+		(const uint64_t *)(dbuf + o_gidx), (double2 *)(dbuf + o_gout),
+		(struct p2_bctl *)(dbuf + o_ctl),
+		(unsigned int *)(dbuf + o_status));
+	e = cudaGetLastError();
+	cudaEventRecord(d0->t1, d0->stream);
+	unsigned int status = 0;
+	if (e == cudaSuccess)
+		e = cudaStreamSynchronize(d0->stream);
+	if (e == cudaSuccess)
+		e = cudaMemcpy(&status, dbuf + o_status, sizeof status,
+			cudaMemcpyDeviceToHost);
+	if (e == cudaSuccess && ng)
+		e = cudaMemcpy(gout, dbuf + o_gout, ng * sizeof(double2),
+			cudaMemcpyDeviceToHost);
+	float ms = 0.0f;
+	if (e == cudaSuccess)
+		e = cudaEventElapsedTime(&ms, d0->t0, d0->t1);
+	cudaFree(dbuf);
+	if (e != cudaSuccess) {
+		log_error("batch: %s", cudaGetErrorString(e));
+		return -1;
+	}
+	if (status) {
+		log_error("batch: a block found no work for %u rounds",
+			P2_BATCH_IDLE_LIMIT);
+		return -1;
+	}
+	if (kernel_ms)
+		*kernel_ms = ms;
+	uint64_t npass_run = 0;
+	for (size_t i = 0; i < n; i++) {
+		struct p2_dev *d = devs[i];
+		const struct p2_prog *pg = progs[i];
+		uint64_t np = 0;
+		for (size_t k = 0; k < pg->nops; k++)
+			np += pg->ops[k].kind == P2_OP_PASS;
+		npass_run += np;
+		d->passes += np;
+		d->sweeps += np;
+		d->rotations += pg->rotations;
+		d->h2d_bytes += pg->nrec * sizeof(struct phase2_rot_rec) +
+			pg->nw * (sizeof(uint64_t) + 2 * sizeof(double));
+		d->d2h_bytes += pg->ng * sizeof(double2);
+	}
+	/* the one launch, timed with events, counts as the first program's */
+	d0->launches += 1;
+	d0->pass_ms += ms;
+	d0->timed_passes += npass_run;
+	d0->timed_sweeps += npass_run;
+	d0->h2d_bytes += o_pass; /* program tables */
+	return 0;
+}
+

@@ -27,6 +27,10 @@
  * and a two-stage FP64 sum of squares / inner product (warp-shuffle tree
  * per block, then one block combining the per-block partials with
  * Neumaier compensated summation).
+ *
+ * The device helpers these kernels share live in p2_kernels.cuh; the
+ * persistent kernel is in batch.cu, device sampling in sampling.cu and
+ * sweeps in sweep.cu.
  */
 #include <cuda_runtime.h>
 
@@ -39,326 +43,7 @@
 #define LOG_SUBSYS "engine"
 #include "log.h"
 
-#include "p2_internal.h"
-#include "plan_core.h"
-
-#define P2_TPB 128
-#define P2_RED_TPB 256
-
-/* Replay of repeated flushes: registers up to this width keep a small LRU
- * of captured pass sequences (launch overhead matters only there). */
-#define P2_GRAPH_SLOTS 8
-#define P2_GRAPH_MAX_QB 24
-
-struct p2_graph {
-	uint64_t hash;
-	size_t npass, nrec;
-	struct phase2_pass *passes;    /* host copies: exact comparison */
-	struct phase2_rot_rec *recs;
-	struct phase2_rot_rec *d_recs; /* records read by the graph */
-	cudaGraphExec_t exec;
-	size_t nlaunch; /* kernel launches in the graph */
-	uint64_t used;
-};
-
-struct p2_dev {
-	uint32_t nqb;
-	int prec;
-	size_t elem;
-	uint64_t namp;
-	void *state;
-	cudaStream_t stream;
-	int sm_count;
-
-	struct phase2_rot_rec *d_recs;
-	size_t d_recs_cap;
-	struct phase2_rot_rec *h_recs[2];
-	size_t h_recs_cap[2];
-	cudaEvent_t h_ev[2];
-	int h_ev_live[2];
-	int ring;
-
-	uint64_t *d_idx;
-	double *d_val;
-	uint64_t *h_idx;
-	double *h_val;
-	size_t io_cap;
-
-	double *d_part;
-	size_t part_cap;
-
-	unsigned char *d_cm; /* coefficient-matrix tables */
-	size_t cm_cap;
-
-	int timing;
-	cudaEvent_t t0, t1;
-
-	uint64_t rotations, passes, launches, timed_passes;
-	uint64_t sweeps, timed_sweeps; /* state round trips (pass or sweep
-					* kernels) */
-	uint64_t h2d_bytes, d2h_bytes;
-	double pass_ms;
-
-	struct p2_graph graphs[P2_GRAPH_SLOTS];
-	uint64_t graph_clock;
-	uint64_t graph_replays;
-	int graphs_on;
-};
-
-#define CUDA_OK(call, what)                                                    \
-	do {                                                                   \
-		cudaError_t e_ = (call);                                       \
-		if (e_ != cudaSuccess) {                                       \
-			log_error("%s: %s", (what), cudaGetErrorString(e_));  \
-			return -1;                                             \
-		}                                                              \
-	} while (0)
-
-/* ---- arithmetic --------------------------------------------------------- */
-
-/* Products and sums rounded separately (no FMA contraction), as the
- * reference's CPU build computes them. */
-__device__ __forceinline__ double p2_mul(double a, double b)
-{
-	return __dmul_rn(a, b);
-}
-
-/* c*x + t with two roundings. */
-__device__ __forceinline__ double p2_cxt(double c, double x, double t)
-{
-	return __dadd_rn(__dmul_rn(c, x), t);
-}
-
-__host__ __device__ constexpr int p2_hibit(int v)
-{
-	return v <= 1 ? 0 : 1 + p2_hibit(v >> 1);
-}
-
-/* k with a zero bit inserted at position h (pair index -> lower slot). */
-__host__ __device__ constexpr int p2_ins0(int g, int h)
-{
-	return ((g >> h) << (h + 1)) | (g & ((1 << h) - 1));
-}
-
-/* Bit u of sm moved to the sign position (u is a compile-time constant
- * after unrolling: one shift and one mask, independent per slot). */
-__device__ __forceinline__ uint32_t p2_bitmask(uint32_t sm, int u)
-{
-	return (sm << (31 - u)) & 0x80000000u;
-}
-
-/* v with the sign mask (0 or 1 << 31) XORed into its high word. */
-__device__ __forceinline__ double p2_sgn(double v, uint32_t mask)
-{
-	return __hiloint2double(__double2hiint(v) ^ (int)mask,
-		__double2loint(v));
-}
-
-/*
- * One rotation on the 2^M slots of a coset (FP64 state, exact rounding).
- * The sign of slot u is bit u of sm (the thread's parity already folded
- * in); each slot's sign is extracted independently so the per-slot work
- * has no serial dependency.
- */
-template <int M, int U, int ODD>
-__device__ __forceinline__ void p2_rot(double (&re)[1 << M],
-	double (&im)[1 << M], double c, double s, uint32_t sm, uint32_t W)
-{
-	(void)W;
-	if constexpr (U == 0) {
-#pragma unroll
-		for (int u = 0; u < (1 << M); ++u) {
-			const double su = p2_sgn(s, p2_bitmask(sm, u));
-			double tr, ti;
-			if constexpr (ODD) {
-				tr = p2_mul(-su, im[u]);
-				ti = p2_mul(su, re[u]);
-			} else {
-				tr = p2_mul(su, re[u]);
-				ti = p2_mul(su, im[u]);
-			}
-			re[u] = p2_cxt(c, re[u], tr);
-			im[u] = p2_cxt(c, im[u], ti);
-		}
-	} else {
-		constexpr int H = p2_hibit(U);
-#pragma unroll
-		for (int k = 0; k < (1 << (M - 1)); ++k) {
-			const int u = p2_ins0(k, H);
-			const int w = u ^ U;
-			const double su = p2_sgn(s, p2_bitmask(sm, u));
-			const double sw = p2_sgn(s, p2_bitmask(sm, w));
-			double tur, tui, twr, twi;
-			if constexpr (ODD) {
-				tur = p2_mul(-su, im[w]);
-				tui = p2_mul(su, re[w]);
-				twr = p2_mul(-sw, im[u]);
-				twi = p2_mul(sw, re[u]);
-			} else {
-				tur = p2_mul(su, re[w]);
-				tui = p2_mul(su, im[w]);
-				twr = p2_mul(sw, re[u]);
-				twi = p2_mul(sw, im[u]);
-			}
-			const double nur = p2_cxt(c, re[u], tur);
-			const double nui = p2_cxt(c, im[u], tui);
-			const double nwr = p2_cxt(c, re[w], twr);
-			const double nwi = p2_cxt(c, im[w], twi);
-			re[u] = nur;
-			im[u] = nui;
-			re[w] = nwr;
-			im[w] = nwi;
-		}
-	}
-}
-
-#define P2_CASE(K)                                                             \
-	case K:                                                                \
-		if constexpr ((K) < (2 << M))                                  \
-			p2_rot<M, ((K) >> 1), ((K)&1)>(re, im, c, s, sm, W);   \
-		break;
-
-/* key = U << 1 | odd; a jump table over the (U, odd) variants. */
-template <int M>
-__device__ __forceinline__ void p2_apply(uint32_t key, double (&re)[1 << M],
-	double (&im)[1 << M], double c, double s, uint32_t sm, uint32_t W)
-{
-	switch (key) {
-		P2_CASE(0) P2_CASE(1) P2_CASE(2) P2_CASE(3) P2_CASE(4)
-		P2_CASE(5) P2_CASE(6) P2_CASE(7) P2_CASE(8) P2_CASE(9)
-		P2_CASE(10) P2_CASE(11) P2_CASE(12) P2_CASE(13) P2_CASE(14)
-		P2_CASE(15) P2_CASE(16) P2_CASE(17) P2_CASE(18) P2_CASE(19)
-		P2_CASE(20) P2_CASE(21) P2_CASE(22) P2_CASE(23) P2_CASE(24)
-		P2_CASE(25) P2_CASE(26) P2_CASE(27) P2_CASE(28) P2_CASE(29)
-		P2_CASE(30) P2_CASE(31) P2_CASE(32) P2_CASE(33) P2_CASE(34)
-		P2_CASE(35) P2_CASE(36) P2_CASE(37) P2_CASE(38) P2_CASE(39)
-		P2_CASE(40) P2_CASE(41) P2_CASE(42) P2_CASE(43) P2_CASE(44)
-		P2_CASE(45) P2_CASE(46) P2_CASE(47) P2_CASE(48) P2_CASE(49)
-		P2_CASE(50) P2_CASE(51) P2_CASE(52) P2_CASE(53) P2_CASE(54)
-		P2_CASE(55) P2_CASE(56) P2_CASE(57) P2_CASE(58) P2_CASE(59)
-		P2_CASE(60) P2_CASE(61) P2_CASE(62) P2_CASE(63)
-	default:
-		break;
-	}
-}
-#undef P2_CASE
-
-/* ---- storage ------------------------------------------------------------ */
-
-__device__ __forceinline__ void p2_ld(const double2 *st, uint64_t g,
-	double &re, double &im)
-{
-	const double2 v = st[g];
-	re = v.x;
-	im = v.y;
-}
-
-__device__ __forceinline__ void p2_ld(const float2 *st, uint64_t g,
-	double &re, double &im)
-{
-	const float2 v = st[g];
-	re = (double)v.x;
-	im = (double)v.y;
-}
-
-__device__ __forceinline__ void p2_st(double2 *st, uint64_t g, double re,
-	double im)
-{
-	st[g] = make_double2(re, im);
-}
-
-__device__ __forceinline__ void p2_st(float2 *st, uint64_t g, double re,
-	double im)
-{
-	st[g] = make_float2(__double2float_rn(re), __double2float_rn(im));
-}
-
-template <int M>
-__device__ __forceinline__ uint64_t p2_slot_off(int u, const uint64_t *basis)
-{
-	uint64_t off = 0;
-#pragma unroll
-	for (int k = 0; k < M; ++k)
-		if (u >> k & 1)
-			off ^= basis[k];
-	return off;
-}
-
-/* ---- the pass kernel ---------------------------------------------------- */
-
-/* Threads per block of the FP64 prefetch kernel: 128, or 64 with 32 slots
- * per thread (three blocks of two stages then fit in shared memory). */
-__host__ __device__ constexpr int p2_tpb(int m)
-{
-	return m >= 5 ? 64 : P2_TPB;
-}
-
-/* Resident blocks per SM the register allocation should allow: 2^M FP64
- * complex values need 4 * 2^M registers per thread. */
-__host__ __device__ constexpr int p2_min_blocks(int m)
-{
-	return m >= 5 ? 1 : (m == 4 ? 4 : (m == 3 ? 6 : 8));
-}
-
-/* Representative number t -> index x: zeros inserted at the pivots. */
-template <int M>
-__device__ __forceinline__ uint64_t p2_rep(uint64_t t,
-	const struct phase2_pass &p)
-{
-	uint64_t x = t;
-#pragma unroll
-	for (int k = 0; k < M; ++k) {
-		const uint32_t q = p.piv[k];
-		x = ((x >> q) << (q + 1)) | (x & ((UINT64_C(1) << q) - 1));
-	}
-	return x;
-}
-
-/* Asynchronous global -> shared copy of one amplitude. */
-__device__ __forceinline__ void p2_cp_async(double2 *smem, const double2 *g)
-{
-	const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s),
-		"l"(g)
-		: "memory");
-}
-
-__device__ __forceinline__ void p2_cp_commit()
-{
-	asm volatile("cp.async.commit_group;\n" ::: "memory");
-}
-
-template <int N> __device__ __forceinline__ void p2_cp_wait()
-{
-	asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
-/* The run of rotations of one pass on one coset held in registers. */
-template <int M>
-__device__ __forceinline__ void p2_apply_run(double (&re)[1 << M],
-	double (&im)[1 << M], uint64_t x, const struct phase2_rot_rec *srec,
-	uint32_t nrot)
-{
-	for (uint32_t r = 0; r < nrot; ++r) {
-		const uint64_t z = srec[r].z;
-		const uint32_t px = (uint32_t)(__popcll(x & z) & 1);
-		const uint32_t sm = srec[r].smask ^ (0u - px);
-		const uint32_t key = ((uint32_t)srec[r].U << 1) | srec[r].odd;
-		p2_apply<M>(key, re, im, srec[r].c, srec[r].s, sm, srec[r].W);
-	}
-}
-
-/* Stage layout [slot][thread]: a warp's accesses to one slot are 32
- * consecutive elements, conflict-free. */
-template <int M>
-__device__ __forceinline__ void p2_prefetch(double2 *stage, const double2 *st,
-	uint64_t x, const uint64_t (&pb)[M > 0 ? M : 1])
-{
-#pragma unroll
-	for (int u = 0; u < (1 << M); ++u)
-		p2_cp_async(&stage[u * blockDim.x + threadIdx.x],
-			st + (x ^ p2_slot_off<M>(u, pb)));
-}
+#include "p2_kernels.cuh"
 
 /*
  * One pass.  Persistent grid: each thread walks representatives
@@ -470,152 +155,6 @@ __global__ void __launch_bounds__(P2_TPB, p2_min_blocks(M))
 	}
 }
 
-/* ---- lifted pass kernel (FP32 storage) ---------------------------------- */
-
-/*
- * One lifted rotation on the 2^M slots of a coset.  A pair (u, w = u ^ U)
- * with sign sigma (bit u of sm) is rotated by three in-place shears,
- *   y_u += t q_u y_w;  y_w += s q_w y_u;  y_u += t q_u y_w,
- * q_u = sigma (odd ? i : 1), q_w = -conj(q_u), t = tan(phi/2): every update
- * writes the register it reads, so a case needs no temporaries and leaves
- * no moves behind.  The partner is held as sigma * y_w during the shears
- * (its sign bits flipped in place), which makes all six FMAs sign-free.
- * U = 0 (the string is diagonal on the coset, and then odd = 1) is the
- * phase c + i sigma s, applied to (re, sigma im) by the same three shears.
- */
-template <int M, int U, int ODD>
-__device__ __forceinline__ void p2_rot_lift(double (&re)[1 << M],
-	double (&im)[1 << M], double t, double s, uint32_t sm)
-{
-	if constexpr (U == 0) {
-#pragma unroll
-		for (int u = 0; u < (1 << M); ++u) {
-			const uint32_t g = p2_bitmask(sm, u);
-			if constexpr (ODD) {
-				double v = p2_sgn(im[u], g);
-				re[u] = fma(-t, v, re[u]);
-				v = fma(s, re[u], v);
-				re[u] = fma(-t, v, re[u]);
-				im[u] = p2_sgn(v, g);
-			} else {
-				/* (c +- s) y with c = 1 - t s; a Hermitian string
-				 * that is diagonal on the coset never has it */
-				const double k = p2_sgn(s, g) + fma(-t, s, 1.0);
-				re[u] *= k;
-				im[u] *= k;
-			}
-		}
-	} else {
-		constexpr int H = p2_hibit(U);
-#pragma unroll
-		for (int k = 0; k < (1 << (M - 1)); ++k) {
-			const int u = p2_ins0(k, H);
-			const int w = u ^ U;
-			const uint32_t g = p2_bitmask(sm, u);
-			double wr = p2_sgn(re[w], g), wi = p2_sgn(im[w], g);
-			if constexpr (ODD) {
-				re[u] = fma(-t, wi, re[u]);
-				im[u] = fma(t, wr, im[u]);
-				wr = fma(-s, im[u], wr);
-				wi = fma(s, re[u], wi);
-				re[u] = fma(-t, wi, re[u]);
-				im[u] = fma(t, wr, im[u]);
-			} else {
-				re[u] = fma(t, wr, re[u]);
-				im[u] = fma(t, wi, im[u]);
-				wr = fma(-s, re[u], wr);
-				wi = fma(-s, im[u], wi);
-				re[u] = fma(t, wr, re[u]);
-				im[u] = fma(t, wi, im[u]);
-			}
-			re[w] = p2_sgn(wr, g);
-			im[w] = p2_sgn(wi, g);
-		}
-	}
-}
-
-#define P2_CASE_L(K)                                                           \
-	case K:                                                                \
-		if constexpr ((K) < (2 << M))                                  \
-			p2_rot_lift<M, ((K) >> 1), ((K)&1)>(re, im, t, s, sm); \
-		break;
-
-/* key = U << 1 | odd */
-template <int M>
-__device__ __forceinline__ void p2_apply_lift(uint32_t key,
-	double (&re)[1 << M], double (&im)[1 << M], double t, double s,
-	uint32_t sm)
-{
-	switch (key) {
-		P2_CASE_L(0) P2_CASE_L(1) P2_CASE_L(2) P2_CASE_L(3)
-		P2_CASE_L(4) P2_CASE_L(5) P2_CASE_L(6) P2_CASE_L(7)
-		P2_CASE_L(8) P2_CASE_L(9) P2_CASE_L(10) P2_CASE_L(11)
-		P2_CASE_L(12) P2_CASE_L(13) P2_CASE_L(14) P2_CASE_L(15)
-		P2_CASE_L(16) P2_CASE_L(17) P2_CASE_L(18) P2_CASE_L(19)
-		P2_CASE_L(20) P2_CASE_L(21) P2_CASE_L(22) P2_CASE_L(23)
-		P2_CASE_L(24) P2_CASE_L(25) P2_CASE_L(26) P2_CASE_L(27)
-		P2_CASE_L(28) P2_CASE_L(29) P2_CASE_L(30) P2_CASE_L(31)
-		P2_CASE_L(32) P2_CASE_L(33) P2_CASE_L(34) P2_CASE_L(35)
-		P2_CASE_L(36) P2_CASE_L(37) P2_CASE_L(38) P2_CASE_L(39)
-		P2_CASE_L(40) P2_CASE_L(41) P2_CASE_L(42) P2_CASE_L(43)
-		P2_CASE_L(44) P2_CASE_L(45) P2_CASE_L(46) P2_CASE_L(47)
-		P2_CASE_L(48) P2_CASE_L(49) P2_CASE_L(50) P2_CASE_L(51)
-		P2_CASE_L(52) P2_CASE_L(53) P2_CASE_L(54) P2_CASE_L(55)
-		P2_CASE_L(56) P2_CASE_L(57) P2_CASE_L(58) P2_CASE_L(59)
-		P2_CASE_L(60) P2_CASE_L(61) P2_CASE_L(62) P2_CASE_L(63)
-	default:
-		break;
-	}
-}
-#undef P2_CASE_L
-
-/* A lifted record as the kernel reads it from shared memory. */
-struct p2_lift_rec {
-	double t, s;
-	uint64_t z;
-	uint32_t sm;  /* smask */
-	uint32_t key; /* U << 1 | odd */
-};
-
-__device__ __forceinline__ uint32_t p2_parity(uint32_t v)
-{
-	return (uint32_t)__popc(v) & 1u;
-}
-
-__device__ __forceinline__ uint32_t p2_parity(uint64_t v)
-{
-	return (uint32_t)__popcll(v) & 1u;
-}
-
-/* x, with its value hidden from the optimiser: store addresses recomputed
- * from it are not merged with the load addresses, which would otherwise
- * stay live (2^M 64-bit pointers) across the whole run of rotations. */
-__device__ __forceinline__ uint32_t p2_opaque(uint32_t x)
-{
-	asm volatile("" : "+r"(x));
-	return x;
-}
-
-__device__ __forceinline__ uint64_t p2_opaque(uint64_t x)
-{
-	asm volatile("" : "+l"(x));
-	return x;
-}
-
-/* Representative number t -> index x in index type IT (32-bit when the
- * register has at most 31 qubits, so that no shift reaches 32). */
-template <int M, typename IT>
-__device__ __forceinline__ IT p2_rep_t(IT t, const struct phase2_pass &p)
-{
-	IT x = t;
-#pragma unroll
-	for (int k = 0; k < M; ++k) {
-		const uint32_t q = p.piv[k];
-		x = ((x >> q) << (q + 1)) | (x & (((IT)1 << q) - 1));
-	}
-	return x;
-}
-
 /*
  * One FP32 pass in the lifted form: each thread loads its coset straight
  * from HBM (2^M independent 8-byte loads, coalesced across the warp),
@@ -691,185 +230,6 @@ __global__ void __launch_bounds__(P2_TPB, M >= 5 ? 3 : p2_min_blocks(M))
 	}
 }
 
-/* ---- lifted pass kernel, FP32 arithmetic -------------------------------- */
-
-__device__ __forceinline__ float p2_fsgn(float v, uint32_t mask)
-{
-	return __int_as_float(__float_as_int(v) ^ (int)mask);
-}
-
-/*
- * The lifted rotation of p2_rot_lift with the amplitudes in FP32 registers
- * and FP32 FMAs.  s reaches the kernel as an FP32 value and t = (1 - cos
- * phi) / s in FP64 (plan.c); the angle of the three shears is fixed by the
- * product t s (their trace is 2 (1 - t s)), so rounding t to FP32 leaves a
- * relative angle error of at most 2^-25.  The signs go onto the
- * coefficients (one XOR each on a 32-bit register).
- */
-template <int M, int U, int ODD>
-__device__ __forceinline__ void p2_rot_lift32(float (&re)[1 << M],
-	float (&im)[1 << M], float t, float s, uint32_t sm)
-{
-	if constexpr (U == 0) {
-#pragma unroll
-		for (int u = 0; u < (1 << M); ++u) {
-			const uint32_t g = p2_bitmask(sm, u);
-			const float st = p2_fsgn(t, g), ss = p2_fsgn(s, g);
-			if constexpr (ODD) {
-				re[u] = fmaf(-st, im[u], re[u]);
-				im[u] = fmaf(ss, re[u], im[u]);
-				re[u] = fmaf(-st, im[u], re[u]);
-			} else {
-				/* (c +- s) y with c = 1 - t s; a Hermitian string
-				 * that is diagonal on the coset never has it */
-				const float k = ss + fmaf(-t, s, 1.f);
-				re[u] *= k;
-				im[u] *= k;
-			}
-		}
-	} else {
-		constexpr int H = p2_hibit(U);
-#pragma unroll
-		for (int k = 0; k < (1 << (M - 1)); ++k) {
-			const int u = p2_ins0(k, H);
-			const int w = u ^ U;
-			const uint32_t g = p2_bitmask(sm, u);
-			const float st = p2_fsgn(t, g), ss = p2_fsgn(s, g);
-			if constexpr (ODD) {
-				re[u] = fmaf(-st, im[w], re[u]);
-				im[u] = fmaf(st, re[w], im[u]);
-				re[w] = fmaf(-ss, im[u], re[w]);
-				im[w] = fmaf(ss, re[u], im[w]);
-				re[u] = fmaf(-st, im[w], re[u]);
-				im[u] = fmaf(st, re[w], im[u]);
-			} else {
-				/* the same three shears as six fmaf, two lanes
-				 * per packed FMA (round-to-nearest per lane: the
-				 * same bits) */
-				const float2 a = make_float2(st, st);
-				const float2 b = make_float2(-ss, -ss);
-				float2 yu = make_float2(re[u], im[u]);
-				float2 yw = make_float2(re[w], im[w]);
-				yu = __ffma2_rn(a, yw, yu);
-				yw = __ffma2_rn(b, yu, yw);
-				yu = __ffma2_rn(a, yw, yu);
-				re[u] = yu.x;
-				im[u] = yu.y;
-				re[w] = yw.x;
-				im[w] = yw.y;
-			}
-		}
-	}
-}
-
-/* A lifted record as the FP32 kernel reads it. */
-struct p2_lift32_rec {
-	float t, s;
-	uint64_t z;
-	uint32_t sm;  /* smask */
-	uint32_t key; /* U << 1 | odd */
-};
-
-#define P2_CASE_L32(K)                                                         \
-	case K:                                                                \
-		if constexpr ((K) < (2 << M))                                  \
-			p2_rot_lift32<M, ((K) >> 1), ((K)&1)>(re, im, q.t,     \
-				q.s, sm);                                      \
-		break;
-
-template <int M>
-__device__ __forceinline__ void p2_apply_lift32(const struct p2_lift32_rec &q,
-	float (&re)[1 << M], float (&im)[1 << M], uint32_t sm)
-{
-	switch (q.key) {
-		P2_CASE_L32(0) P2_CASE_L32(1) P2_CASE_L32(2) P2_CASE_L32(3)
-		P2_CASE_L32(4) P2_CASE_L32(5) P2_CASE_L32(6) P2_CASE_L32(7)
-		P2_CASE_L32(8) P2_CASE_L32(9) P2_CASE_L32(10) P2_CASE_L32(11)
-		P2_CASE_L32(12) P2_CASE_L32(13) P2_CASE_L32(14) P2_CASE_L32(15)
-		P2_CASE_L32(16) P2_CASE_L32(17) P2_CASE_L32(18) P2_CASE_L32(19)
-		P2_CASE_L32(20) P2_CASE_L32(21) P2_CASE_L32(22) P2_CASE_L32(23)
-		P2_CASE_L32(24) P2_CASE_L32(25) P2_CASE_L32(26) P2_CASE_L32(27)
-		P2_CASE_L32(28) P2_CASE_L32(29) P2_CASE_L32(30) P2_CASE_L32(31)
-		P2_CASE_L32(32) P2_CASE_L32(33) P2_CASE_L32(34) P2_CASE_L32(35)
-		P2_CASE_L32(36) P2_CASE_L32(37) P2_CASE_L32(38) P2_CASE_L32(39)
-		P2_CASE_L32(40) P2_CASE_L32(41) P2_CASE_L32(42) P2_CASE_L32(43)
-		P2_CASE_L32(44) P2_CASE_L32(45) P2_CASE_L32(46) P2_CASE_L32(47)
-		P2_CASE_L32(48) P2_CASE_L32(49) P2_CASE_L32(50) P2_CASE_L32(51)
-		P2_CASE_L32(52) P2_CASE_L32(53) P2_CASE_L32(54) P2_CASE_L32(55)
-		P2_CASE_L32(56) P2_CASE_L32(57) P2_CASE_L32(58) P2_CASE_L32(59)
-		P2_CASE_L32(60) P2_CASE_L32(61) P2_CASE_L32(62) P2_CASE_L32(63)
-	default:
-		break;
-	}
-}
-#undef P2_CASE_L32
-
-/* Resident blocks per SM the FP32-arithmetic kernel is built for
- * (2^M FP32 complex values take 2^(M+1) registers per thread). */
-__host__ __device__ constexpr int p2_lift32_blocks(int m)
-{
-	return m >= 5 ? 5 : (m == 4 ? 6 : 8);
-}
-
-/* A lifted record repacked for the FP32 kernels' shared memory. */
-__device__ __forceinline__ struct p2_lift32_rec p2_lift32_of(
-	const struct phase2_rot_rec &in)
-{
-	struct p2_lift32_rec o;
-	o.t = (float)in.c;
-	o.s = (float)in.s; /* an FP32 value: exact */
-	o.z = in.z;
-	o.sm = in.smask;
-	o.key = ((uint32_t)in.U << 1) | in.odd;
-	return o;
-}
-
-/*
- * One coset of a lifted FP32 pass: load the 2^M amplitudes x ^ off(u)
- * into FP32 registers, apply the run of rotations, store them (negated
- * when negm has the sign bit).  CG: loads and stores at L2 only (the
- * persistent batch kernel, whose blocks read what other blocks of the same
- * launch wrote).
- */
-template <int M, typename IT, bool CG>
-__device__ __forceinline__ void p2_lift32_coset(float2 *__restrict__ st, IT x,
-	const IT (&pb)[M > 0 ? M : 1], const struct p2_lift32_rec *srec,
-	uint32_t nrot, uint32_t negm)
-{
-	float re[1 << M], im[1 << M];
-#pragma unroll
-	for (int u = 0; u < (1 << M); ++u) {
-		IT off = 0;
-#pragma unroll
-		for (int k = 0; k < M; ++k)
-			if (u >> k & 1)
-				off ^= pb[k];
-		const float2 v = CG ? __ldcg(st + (x ^ off)) : st[x ^ off];
-		re[u] = v.x;
-		im[u] = v.y;
-	}
-	for (uint32_t r = 0; r < nrot; ++r) {
-		const struct p2_lift32_rec q = srec[r];
-		const uint32_t sm = q.sm ^ (0u - p2_parity(x & (IT)q.z));
-		p2_apply_lift32<M>(q, re, im, sm);
-	}
-	const IT xs = p2_opaque(x);
-#pragma unroll
-	for (int u = 0; u < (1 << M); ++u) {
-		IT off = 0;
-#pragma unroll
-		for (int k = 0; k < M; ++k)
-			if (u >> k & 1)
-				off ^= pb[k];
-		const float2 v = make_float2(p2_fsgn(re[u], negm),
-			p2_fsgn(im[u], negm));
-		if (CG)
-			__stcg(st + (xs ^ off), v);
-		else
-			st[xs ^ off] = v;
-	}
-}
-
 /*
  * One FP32 pass in the lifted form with FP32 arithmetic: loads go straight
  * into FP32 registers, the run is applied with FP32 FMAs, stores write the
@@ -898,526 +258,6 @@ __global__ void __launch_bounds__(P2_TPB, p2_lift32_blocks(M))
 		t < nrep; t += stride)
 		p2_lift32_coset<M, IT, false>(st, p2_rep_t<M, IT>((IT)t, p),
 			pb, srec, nrot, negm);
-}
-
-/* ---- sweeps: several FP32 passes per HBM round trip ---------------------- */
-
-/*
- * A sweep is a run of consecutive passes of one plan whose bases, taken
- * modulo the low L qubits, span a subspace S of rank k with k + L <= the
- * tile width (the planner marks its first pass).  The register splits into
- * tiles R + S + low: 2^k chunks of 2^L contiguous amplitudes, closed under
- * every pass of the sweep.  One block takes a tile at a time: the first
- * pass reads its cosets from HBM, the middle passes work in a
- * shared-memory copy of the tile, the last pass writes back, so the sweep
- * costs one read and one write of the state instead of one per pass.
- *
- * Tile coordinates: amplitude R ^ S(j) ^ l has coordinate (j << L) | l
- * and sits at tile[p2_swz(coordinate)], S(j) the xor of the (reduced,
- * pivots ascending) basis vectors of S selected by j.  For b in S + low,
- * vidx(b) = (b & lowmask) | (bit spiv_i of b) << (L + i) is linear, so a
- * coset x ^ span(pb) of a pass sits at vidx(x ^ R) ^ span(vb) with
- * vb = vidx(pb).  Each pass enumerates its cosets of the tile by virtual
- * representatives (zeros at the virtual pivots vpiv), then moves to the
- * coset's canonical representative, the one with zeros at the physical
- * pivots (row-reduced basis e, virtual images ve), which is the
- * representative the one-pass kernel gives the coset.  Loads, rotations,
- * signs and stores of a coset are then exactly those of k_pass_lift32, so
- * the results are bit-identical to one kernel per pass.
- */
-#define P2_SW_MAXPASS 12
-#define P2_SW_MAXK 9
-#define P2_SW_MAXREC 1024
-#define P2_SW_TPB 256
-#define P2_SW_MAXTILE 14
-
-struct p2_spass {
-	uint32_t span, nrot, rec_off, negm;
-	uint32_t pb[PHASE2_MAX_SPAN]; /* physical basis (slot order) */
-	uint32_t vb[PHASE2_MAX_SPAN]; /* its tile coordinates */
-	uint32_t e[PHASE2_MAX_SPAN];  /* row-reduced basis, pivots piv */
-	uint32_t ve[PHASE2_MAX_SPAN]; /* its tile coordinates */
-	uint8_t piv[PHASE2_MAX_SPAN], vpiv[PHASE2_MAX_SPAN], pad[2];
-};
-
-struct p2_sweep {
-	uint32_t np, k, L, rec0, nrec;
-	uint32_t sb[P2_SW_MAXK]; /* basis of S: reduced, pivots ascending */
-	uint8_t spiv[P2_SW_MAXK], pad[3];
-	struct p2_spass p[P2_SW_MAXPASS];
-};
-
-/* Shared-memory position of tile coordinate v: bits 0-3 xor the other
- * nibbles, so lanes whose coordinates differ in four distinct nibble
- * positions hit distinct bank pairs (8-byte elements).  Linear and
- * invertible on [0, 2^tile), so offsets can be swizzled on their own. */
-__host__ __device__ __forceinline__ uint32_t p2_swz(uint32_t v)
-{
-	return v ^ (((v >> 4) ^ (v >> 8) ^ (v >> 12)) & 15u);
-}
-
-template <int M>
-__device__ __forceinline__ void p2_sweep_pass(float2 *__restrict__ st,
-	float2 *tile, const struct p2_spass &P, uint32_t R,
-	const uint32_t *Stab, uint32_t L, uint32_t tl,
-	const struct p2_lift32_rec *srec, bool from_g, bool to_g)
-{
-	uint32_t pb[M > 0 ? M : 1], vb[M > 0 ? M : 1];
-#pragma unroll
-	for (int k = 0; k < M; ++k) {
-		pb[k] = P.pb[k];
-		vb[k] = p2_swz(P.vb[k]);
-	}
-	const uint32_t lowm = (1u << L) - 1;
-	const uint32_t nc = 1u << (tl - M);
-	const uint32_t nrot = P.nrot;
-	for (uint32_t c = threadIdx.x; c < nc; c += blockDim.x) {
-		uint32_t vx = c;
-#pragma unroll
-		for (int k = 0; k < M; ++k) {
-			const uint32_t q = P.vpiv[k];
-			vx = ((vx >> q) << (q + 1)) | (vx & ((1u << q) - 1));
-		}
-		const uint32_t xv = R ^ Stab[vx >> L] ^ (vx & lowm);
-		uint32_t x = xv;
-#pragma unroll
-		for (int k = 0; k < M; ++k)
-			if (xv >> P.piv[k] & 1) {
-				x ^= P.e[k];
-				vx ^= P.ve[k];
-			}
-		const uint32_t sx = p2_swz(vx);
-		float re[1 << M], im[1 << M];
-#pragma unroll
-		for (int u = 0; u < (1 << M); ++u) {
-			uint32_t off = 0, voff = 0;
-#pragma unroll
-			for (int k = 0; k < M; ++k)
-				if (u >> k & 1) {
-					off ^= pb[k];
-					voff ^= vb[k];
-				}
-			const float2 v = from_g ? st[x ^ off] : tile[sx ^ voff];
-			re[u] = v.x;
-			im[u] = v.y;
-		}
-		for (uint32_t r = 0; r < nrot; ++r) {
-			const struct p2_lift32_rec q = srec[P.rec_off + r];
-			const uint32_t sm = q.sm ^ (0u - p2_parity(x & (uint32_t)q.z));
-			p2_apply_lift32<M>(q, re, im, sm);
-		}
-		const uint32_t xs = (uint32_t)p2_opaque(x);
-		const uint32_t sxs = (uint32_t)p2_opaque(sx);
-#pragma unroll
-		for (int u = 0; u < (1 << M); ++u) {
-			uint32_t off = 0, voff = 0;
-#pragma unroll
-			for (int k = 0; k < M; ++k)
-				if (u >> k & 1) {
-					off ^= pb[k];
-					voff ^= vb[k];
-				}
-			const float2 v = make_float2(p2_fsgn(re[u], P.negm),
-				p2_fsgn(im[u], P.negm));
-			if (to_g)
-				st[xs ^ off] = v;
-			else
-				tile[sxs ^ voff] = v;
-		}
-	}
-}
-
-__global__ void __launch_bounds__(P2_SW_TPB, 2)
-	k_sweep32(float2 *__restrict__ st,
-		const __grid_constant__ struct p2_sweep sw,
-		const struct phase2_rot_rec *__restrict__ recs, uint32_t ntiles)
-{
-	extern __shared__ __align__(16) unsigned char sm[];
-	const uint32_t L = sw.L, tl = sw.k + sw.L;
-	float2 *tile = (float2 *)sm;
-	struct p2_lift32_rec *srec =
-		(struct p2_lift32_rec *)(tile + ((size_t)1 << tl));
-	uint32_t *Stab = (uint32_t *)(srec + sw.nrec);
-	for (uint32_t r = threadIdx.x; r < sw.nrec; r += blockDim.x)
-		srec[r] = p2_lift32_of(recs[sw.rec0 + r]);
-	for (uint32_t j = threadIdx.x; j < (1u << sw.k); j += blockDim.x) {
-		uint32_t v = 0;
-		for (uint32_t i = 0; i < sw.k; ++i)
-			if (j >> i & 1)
-				v ^= sw.sb[i];
-		Stab[j] = v;
-	}
-	__syncthreads();
-	for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-		uint32_t R = t << L;
-		for (uint32_t i = 0; i < sw.k; ++i) {
-			const uint32_t q = sw.spiv[i];
-			R = ((R >> q) << (q + 1)) | (R & ((1u << q) - 1));
-		}
-		for (uint32_t q = 0; q < sw.np; ++q) {
-			const struct p2_spass &P = sw.p[q];
-			const bool from_g = q == 0, to_g = q + 1 == sw.np;
-			switch (P.span) {
-			case 0:
-				p2_sweep_pass<0>(st, tile, P, R, Stab, L, tl, srec,
-					from_g, to_g);
-				break;
-			case 1:
-				p2_sweep_pass<1>(st, tile, P, R, Stab, L, tl, srec,
-					from_g, to_g);
-				break;
-			case 2:
-				p2_sweep_pass<2>(st, tile, P, R, Stab, L, tl, srec,
-					from_g, to_g);
-				break;
-			case 3:
-				p2_sweep_pass<3>(st, tile, P, R, Stab, L, tl, srec,
-					from_g, to_g);
-				break;
-			case 4:
-				p2_sweep_pass<4>(st, tile, P, R, Stab, L, tl, srec,
-					from_g, to_g);
-				break;
-			default:
-				p2_sweep_pass<5>(st, tile, P, R, Stab, L, tl, srec,
-					from_g, to_g);
-				break;
-			}
-			__syncthreads();
-		}
-	}
-}
-
-/* ---- persistent batch kernel -------------------------------------------- */
-
-/*
- * Many registers' recorded programs (p2_internal.h) in one launch.  Every
- * op of a program is cut into tiles (a pass: 128 cosets, one per thread;
- * a zero: 4096 amplitudes; a write or gather: one tile); op k+1 of a
- * program starts only when every tile of op k is done, programs are
- * independent.  Each program has a ticket, (op << 32) | next tile: a block
- * claims a tile with one atomicAdd, and the block that completes the last
- * tile of an op publishes the next op by resetting the ticket.  Blocks
- * look for work across programs starting from the last one they served,
- * so small programs interleave and the GPU stays busy without a launch per
- * pass.  Waiting is bounded: a block that finds nothing to claim while no
- * ticket moves for idle_limit consecutive rounds (about a microsecond
- * each; a ticket moves whenever any tile is claimed or any op is
- * published) raises status and returns, so a scheduling fault ends the
- * launch instead of hanging it, while long single-program runs, where most
- * blocks wait on one op at a time, keep going.
- *
- * Ordering: a tile's stores are made visible (each thread fences, then the
- * block barrier) before its completion count; the finisher fences before
- * publishing the next op; a claimer fences after its claim.  State loads
- * and stores go through L2 only (ld/st .cg), since L1 is not coherent
- * across SMs.
- */
-/* Cosets per thread in a pass tile: 4 for passes of at least
- * P2_BATCH_BIG_PASS representatives, 1 below (more tiles for small
- * registers, whose passes are otherwise too few tiles to spread). */
-#define P2_BATCH_COSETS 4
-#define P2_BATCH_BIG_PASS (UINT64_C(1) << 16)
-#define P2_BATCH_ZERO_TILE (P2_TPB * 128)
-
-struct p2_binst {
-	void *state; /* float2 (FP32) or double2 (FP64) amplitudes */
-	uint64_t namp;
-	uint32_t op_off, nops;
-};
-
-/* Work tiles of an op on a register of namp amplitudes; for a pass of
- * span `span` also the cosets per thread of a tile (*b). */
-__host__ __device__ __forceinline__ uint32_t p2_op_tiles(uint32_t kind,
-	uint64_t namp, uint32_t span, uint32_t *b)
-{
-	if (kind == P2_OP_PASS) {
-		const uint64_t nrep = namp >> span;
-		*b = nrep >= P2_BATCH_BIG_PASS ? P2_BATCH_COSETS : 1;
-		const uint64_t per = (uint64_t)*b * P2_TPB;
-		return (uint32_t)((nrep + per - 1) / per);
-	}
-	if (kind == P2_OP_ZERO)
-		return (uint32_t)((namp + P2_BATCH_ZERO_TILE - 1) /
-			P2_BATCH_ZERO_TILE);
-	return 1;
-}
-
-struct p2_bctl {
-	unsigned long long ticket;
-	unsigned int done;
-	unsigned int pad;
-};
-
-/* The cosets of one pass tile: thread k takes representatives
- * tile * cpt * P2_TPB + j * P2_TPB + k, j < cpt (coalesced per j). */
-template <int M>
-__device__ __forceinline__ void p2_batch_pass_tile(float2 *st,
-	const struct phase2_pass &p, uint32_t tile, uint64_t nrep, uint32_t cpt,
-	const struct p2_lift32_rec *srec)
-{
-	uint32_t pb[M > 0 ? M : 1];
-#pragma unroll
-	for (int k = 0; k < M; ++k)
-		pb[k] = (uint32_t)p.basis[k];
-	const uint32_t negm = p.scale < 0 ? 0x80000000u : 0u;
-	const uint64_t t0 = (uint64_t)tile * cpt * P2_TPB + threadIdx.x;
-	for (uint32_t j = 0; j < cpt; ++j) {
-		const uint64_t t = t0 + (uint64_t)j * P2_TPB;
-		if (t < nrep)
-			p2_lift32_coset<M, uint32_t, true>(st,
-				p2_rep_t<M, uint32_t>((uint32_t)t, p), pb, srec,
-				p.nrot, negm);
-	}
-}
-
-/* The same for an FP64 register: the exact per-coset arithmetic of
- * k_pass (p2_apply_run), loads and stores at L2 only. */
-template <int M>
-__device__ __forceinline__ void p2_batch_pass_tile64(double2 *st,
-	const struct phase2_pass &p, uint32_t tile, uint64_t nrep, uint32_t cpt,
-	const struct phase2_rot_rec *srec)
-{
-	uint64_t pb[M > 0 ? M : 1];
-#pragma unroll
-	for (int k = 0; k < M; ++k)
-		pb[k] = p.basis[k];
-	const uint64_t t0 = (uint64_t)tile * cpt * P2_TPB + threadIdx.x;
-	for (uint32_t j = 0; j < cpt; ++j) {
-		const uint64_t t = t0 + (uint64_t)j * P2_TPB;
-		if (t >= nrep)
-			continue;
-		const uint64_t x = p2_rep<M>(t, p);
-		double re[1 << M], im[1 << M];
-#pragma unroll
-		for (int u = 0; u < (1 << M); ++u) {
-			const double2 v = __ldcg(st + (x ^ p2_slot_off<M>(u, pb)));
-			re[u] = v.x;
-			im[u] = v.y;
-		}
-		p2_apply_run<M>(re, im, x, srec, p.nrot);
-		const uint64_t xs = p2_opaque(x);
-#pragma unroll
-		for (int u = 0; u < (1 << M); ++u)
-			__stcg(st + (xs ^ p2_slot_off<M>(u, pb)),
-				make_double2(re[u], im[u]));
-	}
-}
-
-/* Records as a batch kernel of state type ST holds them in shared
- * memory: repacked lifted records (FP32) or the records themselves
- * (FP64). */
-template <typename ST> struct p2_brec;
-template <> struct p2_brec<float2> {
-	typedef struct p2_lift32_rec type;
-	static __device__ __forceinline__ type of(const phase2_rot_rec &r)
-	{
-		return p2_lift32_of(r);
-	}
-};
-template <> struct p2_brec<double2> {
-	typedef struct phase2_rot_rec type;
-	static __device__ __forceinline__ type of(const phase2_rot_rec &r)
-	{
-		return r;
-	}
-};
-
-template <typename ST>
-__global__ void __launch_bounds__(P2_TPB, sizeof(ST) == 8 ? 5 : 2)
-	k_batch(const struct p2_binst *__restrict__ inst, uint32_t ninst,
-		const struct p2_op *__restrict__ ops,
-		const struct phase2_pass *__restrict__ passes,
-		const struct phase2_rot_rec *__restrict__ recs,
-		const uint64_t *__restrict__ widx,
-		const double *__restrict__ wval,
-		const uint64_t *__restrict__ gidx, double2 *__restrict__ gout,
-		struct p2_bctl *ctl, unsigned int *status,
-		unsigned int idle_limit)
-{
-	constexpr bool F64 = sizeof(ST) == 16;
-	typedef typename p2_brec<ST>::type RT;
-	__shared__ RT srec[P2_MAX_ROTS_PER_PASS];
-	__shared__ uint32_t s_inst, s_seq, s_tile;
-	__shared__ int s_what; /* 0 nothing claimable yet, 1 work, 2 exit */
-	/* pass whose records srec holds (block-uniform), none at first */
-	uint32_t held = 0xffffffffu;
-	uint32_t cursor = blockIdx.x % ninst;
-	unsigned int idle = 0;
-	unsigned long long seen = 0; /* tickets at the last idle round */
-	for (;;) {
-		if (threadIdx.x == 0) {
-			int what = 2;
-			unsigned long long sig = 0;
-			for (uint32_t k = 0; k < ninst; ++k) {
-				const uint32_t i = cursor + k < ninst
-					? cursor + k
-					: cursor + k - ninst;
-				const uint32_t nops = inst[i].nops;
-				const unsigned long long tk =
-					*(volatile unsigned long long *)&ctl[i]
-						 .ticket;
-				sig += tk * (2ull * i + 1ull);
-				if ((uint32_t)(tk >> 32) >= nops)
-					continue; /* program finished */
-				what = 0;
-				const uint32_t off = inst[i].op_off;
-				if ((uint32_t)tk >=
-					ops[off + (uint32_t)(tk >> 32)].ntiles)
-					continue; /* all tiles taken */
-				const unsigned long long got =
-					atomicAdd(&ctl[i].ticket, 1ull);
-				const uint32_t seq = (uint32_t)(got >> 32);
-				const uint32_t tile = (uint32_t)got;
-				if (seq < nops && tile < ops[off + seq].ntiles) {
-					__threadfence();
-					s_inst = i;
-					s_seq = seq;
-					s_tile = tile;
-					cursor = i;
-					what = 1;
-					break;
-				}
-			}
-			if (what == 0) {
-				if (sig != seen) {
-					seen = sig;
-					idle = 0;
-				}
-				if (++idle > idle_limit) {
-					atomicOr(status, 1u);
-					what = 2;
-				} else {
-					__nanosleep(1000);
-				}
-			} else if (what == 1) {
-				idle = 0;
-			}
-			s_what = what;
-		}
-		__syncthreads();
-		const int what = s_what;
-		if (what == 2)
-			return;
-		if (what == 1) {
-			const uint32_t i = s_inst, seq = s_seq, tile = s_tile;
-			ST *const st = (ST *)inst[i].state;
-			const uint64_t namp = inst[i].namp;
-			const struct p2_op op = ops[inst[i].op_off + seq];
-			if (op.kind == P2_OP_PASS) {
-				const struct phase2_pass p = passes[op.a];
-				/* consecutive tiles of one pass (a Trotter step
-				 * replays the same passes) keep their records */
-				if (held != op.a) {
-					for (uint32_t r = threadIdx.x; r < p.nrot;
-						r += blockDim.x)
-						srec[r] = p2_brec<ST>::of(
-							recs[p.rot_off + r]);
-					held = op.a;
-					__syncthreads();
-				}
-				const uint64_t nrep = namp >> p.span;
-				if constexpr (F64) {
-					switch (p.span) {
-					case 0:
-						p2_batch_pass_tile64<0>(st, p, tile,
-							nrep, op.b, srec);
-						break;
-					case 1:
-						p2_batch_pass_tile64<1>(st, p, tile,
-							nrep, op.b, srec);
-						break;
-					case 2:
-						p2_batch_pass_tile64<2>(st, p, tile,
-							nrep, op.b, srec);
-						break;
-					case 3:
-						p2_batch_pass_tile64<3>(st, p, tile,
-							nrep, op.b, srec);
-						break;
-					case 4:
-						p2_batch_pass_tile64<4>(st, p, tile,
-							nrep, op.b, srec);
-						break;
-					default:
-						p2_batch_pass_tile64<5>(st, p, tile,
-							nrep, op.b, srec);
-						break;
-					}
-				} else {
-					switch (p.span) {
-					case 0:
-						p2_batch_pass_tile<0>(st, p, tile,
-							nrep, op.b, srec);
-						break;
-					case 1:
-						p2_batch_pass_tile<1>(st, p, tile,
-							nrep, op.b, srec);
-						break;
-					case 2:
-						p2_batch_pass_tile<2>(st, p, tile,
-							nrep, op.b, srec);
-						break;
-					case 3:
-						p2_batch_pass_tile<3>(st, p, tile,
-							nrep, op.b, srec);
-						break;
-					case 4:
-						p2_batch_pass_tile<4>(st, p, tile,
-							nrep, op.b, srec);
-						break;
-					default:
-						p2_batch_pass_tile<5>(st, p, tile,
-							nrep, op.b, srec);
-						break;
-					}
-				}
-			} else if (op.kind == P2_OP_ZERO) {
-				const uint64_t base =
-					(uint64_t)tile * P2_BATCH_ZERO_TILE;
-				ST zero;
-				zero.x = 0;
-				zero.y = 0;
-				for (uint32_t k = threadIdx.x;
-					k < P2_BATCH_ZERO_TILE; k += blockDim.x)
-					if (base + k < namp)
-						__stcg(st + base + k, zero);
-			} else if (op.kind == P2_OP_WRITE) {
-				/* in order: later writes win */
-				if (threadIdx.x == 0)
-					for (uint32_t e = op.a; e < op.a + op.b; ++e) {
-						ST v;
-						if constexpr (F64) {
-							v.x = wval[2 * e];
-							v.y = wval[2 * e + 1];
-						} else {
-							v.x = (float)wval[2 * e];
-							v.y = (float)wval[2 * e + 1];
-						}
-						__stcg(st + widx[e], v);
-					}
-			} else {
-				for (uint32_t d = threadIdx.x; d < op.b;
-					d += blockDim.x) {
-					const ST v = __ldcg(st + gidx[op.a + d]);
-					gout[op.a + d] = make_double2(v.x, v.y);
-				}
-			}
-			__threadfence();
-			__syncthreads();
-			if (threadIdx.x == 0) {
-				const unsigned int d =
-					atomicAdd(&ctl[i].done, 1u) + 1u;
-				if (d == op.ntiles) {
-					atomicExch(&ctl[i].done, 0u);
-					__threadfence();
-					atomicExch(&ctl[i].ticket,
-						(unsigned long long)(seq + 1) << 32);
-				}
-			}
-		}
-		__syncthreads();
-	}
 }
 
 /* ---- small kernels ------------------------------------------------------ */
@@ -1853,16 +693,6 @@ extern "C" int p2d_get(struct p2_dev *d, const uint64_t *idx, double *z,
 	return 0;
 }
 
-static unsigned grid_for(const struct p2_dev *d, uint64_t work, unsigned tpb,
-	unsigned per_sm)
-{
-	uint64_t b = (work + tpb - 1) / tpb;
-	const uint64_t cap = (uint64_t)d->sm_count * per_sm;
-	if (b > cap)
-		b = cap;
-	return b ? (unsigned)b : 1u;
-}
-
 extern "C" int p2d_get_state(struct p2_dev *d, double *out)
 {
 	const size_t bytes = d->namp * sizeof(double2);
@@ -2110,210 +940,25 @@ static int recs_reserve(struct p2_dev *d, size_t n)
 	return 0;
 }
 
-/* Sweep shape (phase2_set_sweep): tile width and low qubits; 0 = off.
- * p2_sweep_kernel 0: planned sweeps run one kernel per pass. */
-static int p2_sweep_tile = 0, p2_sweep_low = 5, p2_sweep_kernel = 1;
-
-extern "C" int p2d_set_sweep(int tile_qubits, int low_qubits)
-{
-	if (tile_qubits == 0) {
-		p2_sweep_tile = 0;
-		if (low_qubits >= 3 && low_qubits <= 8)
-			p2_sweep_low = low_qubits;
-		return 0;
-	}
-	if (tile_qubits < 8 || tile_qubits > P2_SW_MAXTILE || low_qubits < 3 ||
-		low_qubits > 8 || tile_qubits - low_qubits > P2_SW_MAXK)
-		return -1;
-	p2_sweep_tile = tile_qubits;
-	p2_sweep_low = low_qubits;
-	return 0;
-}
-
-extern "C" void p2d_get_sweep(int *tile_qubits, int *low_qubits)
-{
-	*tile_qubits = p2_sweep_tile;
-	*low_qubits = p2_sweep_low;
-}
-
-extern "C" void p2d_set_sweep_kernel(int on)
-{
-	p2_sweep_kernel = on != 0;
-}
-
-/* Row-reduced basis: rows[] with pivots piv[] (each pivot bit set in its
- * row only).  Adds v when independent; returns the rank. */
-static int rref_add(uint32_t *rows, int *piv, int n, uint32_t v)
-{
-	for (int r = 0; r < n; r++)
-		if (v >> piv[r] & 1)
-			v ^= rows[r];
-	if (!v)
-		return n;
-	const int p = 31 - __builtin_clz(v);
-	for (int r = 0; r < n; r++)
-		if (rows[r] >> p & 1)
-			rows[r] ^= v;
-	rows[n] = v;
-	piv[n] = p;
-	return n + 1;
-}
-
-/* Sort rows by pivot, ascending. */
-static void rref_sort(uint32_t *rows, int *piv, int n)
-{
-	for (int a = 1; a < n; a++)
-		for (int b = a; b > 0 && piv[b - 1] > piv[b]; b--) {
-			const uint32_t t = rows[b];
-			rows[b] = rows[b - 1];
-			rows[b - 1] = t;
-			const int q = piv[b];
-			piv[b] = piv[b - 1];
-			piv[b - 1] = q;
-		}
-}
-
-static uint32_t sweep_vidx(const struct p2_sweep &sw, uint32_t b)
-{
-	uint32_t v = b & ((1u << sw.L) - 1);
-	for (uint32_t i = 0; i < sw.k; i++)
-		v |= (b >> sw.spiv[i] & 1) << (sw.L + i);
-	return v;
-}
-
-static uint32_t sweep_phys(const struct p2_sweep &sw, uint32_t v)
-{
-	uint32_t b = v & ((1u << sw.L) - 1);
-	for (uint32_t i = 0; i < sw.k; i++)
-		if (v >> (sw.L + i) & 1)
-			b ^= sw.sb[i];
-	return b;
-}
-
-/*
- * The sweep starting at passes[i]: the passes up to the next one that
- * starts a sweep (the planner's grouping, struct phase2_pass.sweep), cut
- * at P2_SW_MAXPASS passes and P2_SW_MAXREC records, and checked to fit
- * the current tile shape.  Fills *sw and returns the number of passes (1:
- * run the pass alone).
- */
-static size_t sweep_from(const struct phase2_pass *passes, size_t npass,
-	size_t i, struct p2_sweep *sw)
-{
-	const int tl = p2_sweep_tile, L = p2_sweep_low;
-	const uint32_t lowm = (1u << L) - 1;
-	uint32_t rows[32];
-	int piv[32], n = 0;
-	uint32_t nrec = 0;
-	size_t j = i;
-	for (; j < npass && j - i < P2_SW_MAXPASS; j++) {
-		const struct phase2_pass &p = passes[j];
-		if ((j > i && p.sweep) || p.form != PHASE2_FORM_LIFTED_F32 ||
-			nrec + p.nrot > P2_SW_MAXREC ||
-			(j > i && p.rot_off != passes[j - 1].rot_off +
-					passes[j - 1].nrot))
-			break;
-		for (uint32_t k = 0; k < p.span && n <= tl - L; k++)
-			n = rref_add(rows, piv, n, (uint32_t)p.basis[k] & ~lowm);
-		if (n > tl - L)
-			return 1;
-		nrec += p.nrot;
-	}
-	const size_t np = j - i;
-	if (np < 2)
-		return 1;
-	rref_sort(rows, piv, n);
-	memset(sw, 0, sizeof *sw);
-	sw->np = (uint32_t)np;
-	sw->k = (uint32_t)n;
-	sw->L = (uint32_t)L;
-	sw->rec0 = passes[i].rot_off;
-	sw->nrec = nrec;
-	for (int r = 0; r < n; r++) {
-		sw->sb[r] = rows[r];
-		sw->spiv[r] = (uint8_t)piv[r];
-	}
-	for (size_t q = 0; q < np; q++) {
-		const struct phase2_pass &p = passes[i + q];
-		struct p2_spass &P = sw->p[q];
-		P.span = p.span;
-		P.nrot = p.nrot;
-		P.rec_off = p.rot_off - sw->rec0;
-		P.negm = p.scale < 0 ? 0x80000000u : 0u;
-		uint32_t er[PHASE2_MAX_SPAN], vr[PHASE2_MAX_SPAN];
-		int ep[PHASE2_MAX_SPAN], vp[PHASE2_MAX_SPAN], ne = 0, nv = 0;
-		for (uint32_t k = 0; k < p.span; k++) {
-			P.pb[k] = (uint32_t)p.basis[k];
-			P.vb[k] = sweep_vidx(*sw, P.pb[k]);
-			/* every basis vector must lie in S + low */
-			if (sweep_phys(*sw, P.vb[k]) != P.pb[k])
-				return 1;
-			ne = rref_add(er, ep, ne, P.pb[k]);
-			nv = rref_add(vr, vp, nv, P.vb[k]);
-		}
-		if (ne != (int)p.span || nv != (int)p.span)
-			return 1;
-		rref_sort(er, ep, ne);
-		rref_sort(vr, vp, nv);
-		for (uint32_t k = 0; k < p.span; k++) {
-			/* the pivots of the one-pass kernel's representatives */
-			if ((int)p.piv[k] != ep[k])
-				return 1;
-			P.e[k] = er[k];
-			P.piv[k] = (uint8_t)ep[k];
-			P.ve[k] = sweep_vidx(*sw, er[k]);
-			P.vpiv[k] = (uint8_t)vp[k];
-		}
-	}
-	return np;
-}
-
-static int launch_sweep(struct p2_dev *d, const struct p2_sweep &sw,
-	const struct phase2_rot_rec *d_recs)
-{
-	const uint32_t tl = sw.k + sw.L;
-	const size_t smem = ((size_t)8 << tl) +
-		(size_t)sw.nrec * sizeof(struct p2_lift32_rec) +
-		((size_t)4 << sw.k);
-	static int smem_set;
-	if (!smem_set) {
-		CUDA_OK(cudaFuncSetAttribute(k_sweep32,
-				cudaFuncAttributeMaxDynamicSharedMemorySize,
-				(int)(((size_t)8 << P2_SW_MAXTILE) +
-					P2_SW_MAXREC * sizeof(struct p2_lift32_rec) +
-					((size_t)4 << P2_SW_MAXK))),
-			"sweep kernel shared memory");
-		smem_set = 1;
-	}
-	const uint32_t ntiles = (uint32_t)(d->namp >> tl);
-	uint32_t grid = (uint32_t)d->sm_count * 2;
-	if (grid > ntiles)
-		grid = ntiles;
-	k_sweep32<<<grid, P2_SW_TPB, smem, d->stream>>>((float2 *)d->state, sw,
-		d_recs, ntiles);
-	return 0;
-}
-
-/* Launch a plan: planned sweeps as one kernel each (FP32 registers of
- * tile + 3 to 31 qubits), other passes one kernel each.  Returns the
- * kernels launched (state round trips) or -1. */
+/* Launch a plan: planned sweeps as one kernel each (sweep.cu), other
+ * passes one kernel each.  Returns the kernels launched (state round
+ * trips) or -1. */
 static long launch_all(struct p2_dev *d, const struct phase2_pass *passes,
 	size_t npass, const struct phase2_rot_rec *d_recs)
 {
-	const bool sweeps = p2_sweep_tile > 0 && p2_sweep_kernel &&
-		d->prec == PHASE2_PREC_FP32 && d->nqb <= 31 &&
-		d->nqb >= (uint32_t)p2_sweep_tile + 3;
-	struct p2_sweep sw;
+	const bool sweeps = p2_sweeps_on(d);
 	long launches = 0;
 	for (size_t i = 0; i < npass; launches++) {
-		const size_t n = sweeps ? sweep_from(passes, npass, i, &sw) : 1;
-		if (n >= 2) {
-			if (launch_sweep(d, sw, d_recs) < 0)
-				return -1;
-		} else if (launch_pass(d, passes[i], d_recs) < 0) {
+		long n = sweeps ? p2_sweep_launch(d, passes, npass, i, d_recs)
+				: 1;
+		if (n < 0)
 			return -1;
+		if (n < 2) {
+			if (launch_pass(d, passes[i], d_recs) < 0)
+				return -1;
+			n = 1;
 		}
-		i += n;
+		i += (size_t)n;
 	}
 	return launches;
 }
@@ -2666,775 +1311,6 @@ extern "C" void p2d_set_timing(struct p2_dev *d, int on)
 extern "C" void *p2d_stream(const struct p2_dev *d)
 {
 	return (void *)d->stream;
-}
-
-/* ---- batched persistent execution --------------------------------------- */
-
-extern "C" int p2d_batch_ok(const struct p2_dev *d)
-{
-	return d && (d->prec == PHASE2_PREC_FP32 ||
-			    d->prec == PHASE2_PREC_FP64) &&
-		d->nqb <= 31;
-}
-
-static size_t p2_align256(size_t v)
-{
-	return (v + 255) & ~(size_t)255;
-}
-
-/* Idle scheduling rounds (each sleeps ~1 us) before a block gives up. */
-#define P2_BATCH_IDLE_LIMIT 2000000u
-
-/* k_batch for FP32 or FP64 registers: its kernel function (occupancy
- * queries) and its launch. */
-static const void *batch_kernel(bool f64)
-{
-	return f64 ? (const void *)k_batch<double2>
-		   : (const void *)k_batch<float2>;
-}
-
-static void batch_launch(bool f64, unsigned grid, cudaStream_t stream,
-	const struct p2_binst *inst, uint32_t ninst, const struct p2_op *ops,
-	const struct phase2_pass *passes, const struct phase2_rot_rec *recs,
-	const uint64_t *widx, const double *wval, const uint64_t *gidx,
-	double2 *gout, struct p2_bctl *ctl, unsigned int *status)
-{
-	if (f64)
-		k_batch<double2><<<grid, P2_TPB, 0, stream>>>(inst, ninst, ops,
-			passes, recs, widx, wval, gidx, gout, ctl, status,
-			P2_BATCH_IDLE_LIMIT);
-	else
-		k_batch<float2><<<grid, P2_TPB, 0, stream>>>(inst, ninst, ops,
-			passes, recs, widx, wval, gidx, gout, ctl, status,
-			P2_BATCH_IDLE_LIMIT);
-}
-
-extern "C" int p2d_batch_run(struct p2_dev *const *devs,
-	const struct p2_prog *const *progs, size_t n, double *gout,
-	double *kernel_ms)
-{
-	if (n == 0)
-		return 0;
-	size_t nops = 0, npass = 0, nrec = 0, nw = 0, ng = 0;
-	for (size_t i = 0; i < n; i++) {
-		if (!p2d_batch_ok(devs[i]) || progs[i]->error ||
-			devs[i]->prec != devs[0]->prec) {
-			log_error("batch: program %zu cannot run batched", i);
-			return -1;
-		}
-		nops += progs[i]->nops;
-		npass += progs[i]->npass;
-		nrec += progs[i]->nrec;
-		nw += progs[i]->nw;
-		ng += progs[i]->ng;
-	}
-	if (n > UINT32_MAX || nops > UINT32_MAX || npass > UINT32_MAX ||
-		nrec > UINT32_MAX || nw > UINT32_MAX || ng > UINT32_MAX) {
-		log_error("batch: program too large");
-		return -1;
-	}
-	/* one device buffer: uploaded part, then outputs and control */
-	const size_t o_inst = 0;
-	const size_t o_ops = p2_align256(o_inst + n * sizeof(struct p2_binst));
-	const size_t o_pass = p2_align256(o_ops + nops * sizeof(struct p2_op));
-	const size_t o_rec =
-		p2_align256(o_pass + npass * sizeof(struct phase2_pass));
-	const size_t o_widx =
-		p2_align256(o_rec + nrec * sizeof(struct phase2_rot_rec));
-	const size_t o_wval = p2_align256(o_widx + nw * sizeof(uint64_t));
-	const size_t o_gidx = p2_align256(o_wval + 2 * nw * sizeof(double));
-	const size_t up = p2_align256(o_gidx + ng * sizeof(uint64_t));
-	const size_t o_gout = up;
-	const size_t o_ctl = p2_align256(o_gout + ng * sizeof(double2));
-	const size_t o_status = p2_align256(o_ctl + n * sizeof(struct p2_bctl));
-	const size_t total = o_status + 256;
-
-	unsigned char *h = (unsigned char *)malloc(up);
-	if (!h)
-		return -1;
-	struct p2_binst *hi = (struct p2_binst *)(h + o_inst);
-	struct p2_op *ho = (struct p2_op *)(h + o_ops);
-	struct phase2_pass *hp = (struct phase2_pass *)(h + o_pass);
-	struct phase2_rot_rec *hr = (struct phase2_rot_rec *)(h + o_rec);
-	uint64_t *hwi = (uint64_t *)(h + o_widx);
-	double *hwv = (double *)(h + o_wval);
-	uint64_t *hgi = (uint64_t *)(h + o_gidx);
-	size_t bo = 0, bp = 0, br = 0, bw = 0, bg = 0;
-	for (size_t i = 0; i < n; i++) {
-		const struct p2_prog *pg = progs[i];
-		struct p2_dev *d = devs[i];
-		hi[i].state = d->state;
-		hi[i].namp = d->namp;
-		hi[i].op_off = (uint32_t)bo;
-		hi[i].nops = (uint32_t)pg->nops;
-		for (size_t k = 0; k < pg->npass; k++) {
-			hp[bp + k] = pg->passes[k];
-			hp[bp + k].rot_off += (uint32_t)br;
-		}
-		for (size_t k = 0; k < pg->nops; k++) {
-			struct p2_op op = pg->ops[k];
-			switch (op.kind) {
-			case P2_OP_PASS:
-				op.a += (uint32_t)bp;
-				op.ntiles = p2_op_tiles(P2_OP_PASS, d->namp,
-					hp[op.a].span, &op.b);
-				break;
-			case P2_OP_ZERO:
-				op.ntiles = p2_op_tiles(P2_OP_ZERO, d->namp, 0,
-					&op.b);
-				break;
-			case P2_OP_WRITE:
-				op.a += (uint32_t)bw;
-				op.ntiles = 1;
-				break;
-			default:
-				op.a += (uint32_t)bg;
-				op.ntiles = 1;
-				break;
-			}
-			ho[bo + k] = op;
-		}
-		if (pg->nrec)
-			memcpy(hr + br, pg->recs, pg->nrec * sizeof *hr);
-		if (pg->nw) {
-			memcpy(hwi + bw, pg->widx, pg->nw * sizeof *hwi);
-			memcpy(hwv + 2 * bw, pg->wval,
-				2 * pg->nw * sizeof *hwv);
-		}
-		if (pg->ng)
-			memcpy(hgi + bg, pg->gidx, pg->ng * sizeof *hgi);
-		bo += pg->nops;
-		bp += pg->npass;
-		br += pg->nrec;
-		bw += pg->nw;
-		bg += pg->ng;
-	}
-
-	struct p2_dev *d0 = devs[0];
-	unsigned char *dbuf = NULL;
-	cudaError_t e = cudaSuccess;
-	for (size_t i = 0; i < n && e == cudaSuccess; i++)
-		e = cudaStreamSynchronize(devs[i]->stream);
-	if (e == cudaSuccess)
-		e = cudaMalloc((void **)&dbuf, total);
-	if (e == cudaSuccess)
-		e = cudaMemcpy(dbuf, h, up, cudaMemcpyHostToDevice);
-	free(h);
-	if (e == cudaSuccess)
-		e = cudaMemset(dbuf + o_ctl, 0, total - o_ctl);
-	const bool f64 = d0->prec == PHASE2_PREC_FP64;
-	int per_sm = 0;
-	if (e == cudaSuccess)
-		e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm,
-			batch_kernel(f64), P2_TPB, 0);
-	if (e != cudaSuccess) {
-		cudaFree(dbuf);
-		log_error("batch: setup: %s", cudaGetErrorString(e));
-		return -1;
-	}
-	const unsigned grid =
-		(unsigned)d0->sm_count * (unsigned)(per_sm > 0 ? per_sm : 1);
-	cudaEventRecord(d0->t0, d0->stream);
-	batch_launch(f64, grid, d0->stream,
-		(const struct p2_binst *)(dbuf + o_inst), (uint32_t)n,
-		(const struct p2_op *)(dbuf + o_ops),
-		(const struct phase2_pass *)(dbuf + o_pass),
-		(const struct phase2_rot_rec *)(dbuf + o_rec),
-		(const uint64_t *)(dbuf + o_widx),
-		(const double *)(dbuf + o_wval),
-		(const uint64_t *)(dbuf + o_gidx), (double2 *)(dbuf + o_gout),
-		(struct p2_bctl *)(dbuf + o_ctl),
-		(unsigned int *)(dbuf + o_status));
-	e = cudaGetLastError();
-	cudaEventRecord(d0->t1, d0->stream);
-	unsigned int status = 0;
-	if (e == cudaSuccess)
-		e = cudaStreamSynchronize(d0->stream);
-	if (e == cudaSuccess)
-		e = cudaMemcpy(&status, dbuf + o_status, sizeof status,
-			cudaMemcpyDeviceToHost);
-	if (e == cudaSuccess && ng)
-		e = cudaMemcpy(gout, dbuf + o_gout, ng * sizeof(double2),
-			cudaMemcpyDeviceToHost);
-	float ms = 0.0f;
-	if (e == cudaSuccess)
-		e = cudaEventElapsedTime(&ms, d0->t0, d0->t1);
-	cudaFree(dbuf);
-	if (e != cudaSuccess) {
-		log_error("batch: %s", cudaGetErrorString(e));
-		return -1;
-	}
-	if (status) {
-		log_error("batch: a block found no work for %u rounds",
-			P2_BATCH_IDLE_LIMIT);
-		return -1;
-	}
-	if (kernel_ms)
-		*kernel_ms = ms;
-	uint64_t npass_run = 0;
-	for (size_t i = 0; i < n; i++) {
-		struct p2_dev *d = devs[i];
-		const struct p2_prog *pg = progs[i];
-		uint64_t np = 0;
-		for (size_t k = 0; k < pg->nops; k++)
-			np += pg->ops[k].kind == P2_OP_PASS;
-		npass_run += np;
-		d->passes += np;
-		d->sweeps += np;
-		d->rotations += pg->rotations;
-		d->h2d_bytes += pg->nrec * sizeof(struct phase2_rot_rec) +
-			pg->nw * (sizeof(uint64_t) + 2 * sizeof(double));
-		d->d2h_bytes += pg->ng * sizeof(double2);
-	}
-	/* the one launch, timed with events, counts as the first program's */
-	d0->launches += 1;
-	d0->pass_ms += ms;
-	d0->timed_passes += npass_run;
-	d0->timed_sweeps += npass_run;
-	d0->h2d_bytes += o_pass; /* program tables */
-	return 0;
-}
-
-/* ---- device-side qDRIFT ------------------------------------------------- */
-
-/* xoshiro256** step (lib/xoshiro256ss.c of the reference). */
-__device__ __forceinline__ uint64_t p2_xo_next(uint64_t (&s)[4])
-{
-	const uint64_t x = s[1] * 5;
-	const uint64_t out = ((x << 7) | (x >> 57)) * 9;
-	const uint64_t t = s[1] << 17;
-	s[2] ^= s[0];
-	s[3] ^= s[1];
-	s[1] ^= s[2];
-	s[0] ^= s[3];
-	s[2] ^= t;
-	s[3] = (s[3] << 45) | (s[3] >> 19);
-	return out;
-}
-
-/*
- * Device sampling (p2d_sampled_device).  A sample's rotation stream is
- * `halves` halves of (length + depth) rotations: a forward half is the
- * head terms 0..length-1 then the draws 0..depth-1, a reversed half (odd
- * halves when reverse_odd) the draws depth-1..0 then the head terms
- * length-1..0.  Buffers of a round of g samples, T rotations each:
- * x[(s * halves + h) * depth + i] uniforms, rot/cs/passes/recs at
- * s * T + position, per-chunk pass counts npc[s * C + c].
- */
-
-/* Uniforms of one (sample, half): the half's generator, depth draws. */
-__global__ void k_smp_draw(const struct p2_smp_job job, uint32_t s0,
-	uint32_t n, const uint64_t *__restrict__ rng0, double *__restrict__ x)
-{
-	const uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
-	if (id >= n)
-		return;
-	uint64_t st[4];
-	const size_t g = (size_t)s0 * job.halves + id;
-	for (int k = 0; k < 4; ++k)
-		st[k] = rng0[4 * g + k];
-	double *out = x + (size_t)id * job.depth;
-	for (uint32_t i = 0; i < job.depth; ++i)
-		out[i] = (double)(p2_xo_next(st) >> 11) * 0x1.0p-53;
-}
-
-/* The rotation at every stream position: head terms from the head table,
- * draws by CDF inversion (prob_cdf_inverse: smallest i with y[i] > x,
- * clamped) with the sign dead zone (|c| < DBL_EPSILON -> 0). */
-__global__ void k_smp_stream(const struct p2_smp_job job, uint64_t total,
-	const double *__restrict__ x, const double *__restrict__ cdf_y,
-	const uint64_t *__restrict__ tflip, const uint64_t *__restrict__ tphase,
-	const double *__restrict__ tcf, const uint64_t *__restrict__ hflip,
-	const uint64_t *__restrict__ hphase, const double *__restrict__ hphi,
-	const double *__restrict__ hcs, struct phase2_rot_in *__restrict__ rot,
-	double *__restrict__ cs)
-{
-	const uint64_t per = (uint64_t)job.length + job.depth;
-	const uint64_t T = per * job.halves;
-	for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-		q < total; q += (uint64_t)gridDim.x * blockDim.x) {
-		const uint64_t s = q / T, p = q - s * T;
-		const uint64_t h = p / per, o = p - h * per;
-		const bool rev = job.reverse_odd && (h & 1);
-		int64_t head = -1, draw = -1;
-		if (!rev) {
-			if (o < job.length)
-				head = (int64_t)o;
-			else
-				draw = (int64_t)(o - job.length);
-		} else {
-			if (o < job.depth)
-				draw = (int64_t)(job.depth - 1 - o);
-			else
-				head = (int64_t)(job.length - 1 - (o - job.depth));
-		}
-		struct phase2_rot_in r;
-		double c, sn;
-		if (head >= 0) {
-			r.flip = hflip[head] & job.mask;
-			r.phase = hphase[head] & job.mask;
-			r.phi = hphi[head];
-			c = hcs[2 * head];
-			sn = hcs[2 * head + 1];
-		} else {
-			const double xv =
-				x[(s * job.halves + h) * job.depth + (uint64_t)draw];
-			uint64_t lo = 0, hi = job.nterms;
-			while (lo < hi) {
-				const uint64_t mid = lo + (hi - lo) / 2;
-				if (cdf_y[mid] <= xv)
-					lo = mid + 1;
-				else
-					hi = mid;
-			}
-			const uint64_t k = lo < job.nterms ? lo : job.nterms - 1;
-			const double a = tcf[k], f = fabs(a);
-			const int sg = f < DBL_EPSILON ? 1 : (a < f ? 0 : 2);
-			r.flip = tflip[k] & job.mask;
-			r.phase = tphase[k] & job.mask;
-			/* selects, not an index (keeps job out of local memory) */
-			r.phi = sg == 0 ? job.rphi[0]
-					: (sg == 1 ? job.rphi[1] : job.rphi[2]);
-			c = sg == 0 ? job.rcs[0][0]
-				    : (sg == 1 ? job.rcs[1][0] : job.rcs[2][0]);
-			sn = sg == 0 ? job.rcs[0][1]
-				     : (sg == 1 ? job.rcs[1][1] : job.rcs[2][1]);
-		}
-		rot[q] = r;
-		cs[2 * q] = c;
-		cs[2 * q + 1] = sn;
-	}
-}
-
-/*
- * One block per P2_QUEUE_FLUSH chunk of a sample's stream: the passes a
- * host flush of that chunk plans (plan_core.h), at the chunk's position;
- * npc gets their count.  The flip masks are staged in shared memory for
- * the sequential boundary scan (thread 0); the records are then filled by
- * all threads, and each pass's scale is the parity of its records' signs.
- */
-#define P2_SMP_PLAN_TPB 256
-#define P2_SMP_PLAN_SMEM                                                      \
-	(P2_QUEUE_FLUSH * (sizeof(uint64_t) + sizeof(uint16_t) + 1) +          \
-		P2_QUEUE_FLUSH / 8)
-
-__global__ void __launch_bounds__(P2_SMP_PLAN_TPB)
-	k_smp_plan(const struct p2_smp_job job, uint64_t T, uint32_t C,
-		const struct phase2_rot_in *__restrict__ rot,
-		const double *__restrict__ cs, struct phase2_pass *passes,
-		struct phase2_rot_rec *__restrict__ recs, uint32_t *npc)
-{
-	extern __shared__ __align__(16) unsigned char sm[];
-	uint64_t *fl = (uint64_t *)sm;
-	uint16_t *pid = (uint16_t *)(fl + P2_QUEUE_FLUSH);
-	uint8_t *U = (uint8_t *)(pid + P2_QUEUE_FLUSH);
-	uint32_t *neg = (uint32_t *)(U + P2_QUEUE_FLUSH);
-	__shared__ long s_np;
-	const uint64_t s = blockIdx.x / C, c = blockIdx.x - s * C;
-	const uint64_t at = s * T + c * P2_QUEUE_FLUSH;
-	const uint32_t n = (uint32_t)(T - c * P2_QUEUE_FLUSH < P2_QUEUE_FLUSH
-			? T - c * P2_QUEUE_FLUSH
-			: P2_QUEUE_FLUSH);
-	for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
-		fl[i] = rot[at + i].flip;
-	for (uint32_t w = threadIdx.x; w < P2_QUEUE_FLUSH / 32; w += blockDim.x)
-		neg[w] = 0;
-	__syncthreads();
-	if (threadIdx.x == 0)
-		s_np = p2_plan_scan(job.nqb, fl, 1, n, job.max_span,
-			job.max_rots, P2_DEFAULT_PAD_SPAN, job.form, job.sweep_k,
-			job.sweep_low, passes + at, U, 1, pid);
-	__syncthreads();
-	const long np = s_np;
-	if (np < 0) {
-		if (threadIdx.x == 0)
-			npc[blockIdx.x] = 0;
-		return;
-	}
-	for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-		const uint32_t p = pid[i];
-		struct phase2_rot_rec r;
-		if (p2_rec_fill(&passes[at + p], fl[i], rot[at + i].phase,
-			    cs[2 * (at + i)], cs[2 * (at + i) + 1], U[i], &r))
-			atomicXor(&neg[p >> 5], 1u << (p & 31));
-		recs[at + i] = r;
-	}
-	__syncthreads();
-	for (uint32_t p = threadIdx.x; p < (uint32_t)np; p += blockDim.x) {
-		passes[at + p].scale = (neg[p >> 5] >> (p & 31)) & 1 ? -1.0 : 1.0;
-		passes[at + p].rot_off += (uint32_t)at;
-	}
-	if (threadIdx.x == 0)
-		npc[blockIdx.x] = (uint32_t)np;
-}
-
-/*
- * Lay out the registers' programs (one thread): sample s0 + s runs on
- * register (last - s0 - s) % nreg, so the run's last sample lands on
- * register 0; a register's samples keep their order.  A sample's ops are
- * zero, write, its chunks' passes in order, gather: poff[s * C + c] is
- * the op index of chunk c's first pass, soff[s] of the sample's zero.
- */
-__global__ void k_smp_layout(uint32_t g, uint32_t C,
-	const uint32_t *__restrict__ npc, uint64_t last, uint64_t s0,
-	uint32_t nreg, uint32_t *soff, uint32_t *poff, struct p2_binst *inst)
-{
-	if (blockIdx.x != 0 || threadIdx.x != 0)
-		return;
-	for (uint32_t r = 0; r < nreg; ++r)
-		inst[r].nops = 0;
-	for (uint32_t s = 0; s < g; ++s) {
-		uint32_t n = 3;
-		for (uint32_t c = 0; c < C; ++c)
-			n += npc[s * C + c];
-		inst[(uint32_t)((last - s0 - s) % nreg)].nops += n;
-		soff[s] = n; /* count for now */
-	}
-	uint32_t t = 0;
-	for (uint32_t r = 0; r < nreg; ++r) {
-		inst[r].op_off = t;
-		t += inst[r].nops;
-		inst[r].nops = 0; /* filled below */
-	}
-	for (uint32_t s = 0; s < g; ++s) {
-		const uint32_t r = (uint32_t)((last - s0 - s) % nreg);
-		const uint32_t n = soff[s];
-		soff[s] = inst[r].op_off + inst[r].nops;
-		inst[r].nops += n;
-		uint32_t o = soff[s] + 2;
-		for (uint32_t c = 0; c < C; ++c) {
-			poff[s * C + c] = o;
-			o += npc[s * C + c];
-		}
-	}
-}
-
-/* Fill the ops laid out by k_smp_layout (grid-stride over chunks). */
-__global__ void k_smp_fill(const struct p2_smp_job job, uint32_t g,
-	uint32_t C, uint64_t T, uint64_t namp, uint64_t s0,
-	const uint32_t *__restrict__ npc, const uint32_t *__restrict__ soff,
-	const uint32_t *__restrict__ poff,
-	const struct phase2_pass *__restrict__ passes, struct p2_op *ops)
-{
-	const uint32_t stride = gridDim.x * blockDim.x;
-	const uint32_t id0 = blockIdx.x * blockDim.x + threadIdx.x;
-	for (uint32_t s = id0; s < g; s += stride) {
-		struct p2_op *o = ops + soff[s];
-		o[0].kind = P2_OP_ZERO;
-		o[0].a = o[0].b = 0;
-		o[0].ntiles = p2_op_tiles(P2_OP_ZERO, namp, 0, &o[0].b);
-		o[1].kind = P2_OP_WRITE;
-		o[1].a = 0;
-		o[1].b = job.ndet;
-		o[1].ntiles = 1;
-		uint32_t np = 0;
-		for (uint32_t c = 0; c < C; ++c)
-			np += npc[s * C + c];
-		struct p2_op *gth = o + 2 + np;
-		gth->kind = P2_OP_GATHER;
-		gth->a = (uint32_t)((s0 + s) * job.ndet);
-		gth->b = job.ndet;
-		gth->ntiles = 1;
-	}
-	for (uint32_t e = id0; e < g * C; e += stride) {
-		const uint64_t s = e / C, c = e - s * C;
-		const uint64_t at = s * T + c * P2_QUEUE_FLUSH;
-		struct p2_op *o = ops + poff[e];
-		for (uint32_t p = 0; p < npc[e]; ++p) {
-			o[p].kind = P2_OP_PASS;
-			o[p].a = (uint32_t)(at + p);
-			o[p].ntiles = p2_op_tiles(P2_OP_PASS, namp,
-				passes[at + p].span, &o[p].b);
-		}
-	}
-}
-
-/* Rotations held per device round (rotation scratch, plans, program). */
-#define P2_SMP_ROUND_ROTS (UINT64_C(1) << 21)
-/* Amplitudes of all the registers of one round together (FP32: 512 MiB);
- * from 2^26 amplitudes up the register runs alone. */
-#define P2_SMP_ROUND_AMPS (UINT64_C(1) << 26)
-
-extern "C" int p2d_sampled_device(struct p2_dev *d,
-	const struct p2_smp_job *job, const uint64_t *rng0, size_t samples,
-	const double *cdf_y, const uint64_t *tflip, const uint64_t *tphase,
-	const double *tcf, const uint64_t *hflip, const uint64_t *hphase,
-	const double *hphi, const double *hcs, const uint64_t *det_idx,
-	const double *det_val, double *gout, uint64_t *npass_out)
-{
-	*npass_out = 0;
-	if (samples == 0)
-		return 0;
-	const uint64_t per = (uint64_t)job->length + job->depth;
-	const uint64_t T = per * job->halves;
-	if (!p2d_batch_ok(d) || (job->depth && job->nterms == 0) ||
-		T >= (UINT64_C(1) << 31) || job->halves == 0 ||
-		samples > UINT32_MAX / (job->ndet ? job->ndet : 1)) {
-		log_error("device sampling: unsupported register or sizes");
-		return -1;
-	}
-	size_t G = T ? (size_t)(P2_SMP_ROUND_ROTS / T) : 4096;
-	if (G < 1)
-		G = 1;
-	if (G > samples)
-		G = samples;
-	if (G > 4096)
-		G = 4096;
-	size_t R = (size_t)(P2_SMP_ROUND_AMPS / d->namp);
-	if (R > P2_QD_MAX_REGS)
-		R = P2_QD_MAX_REGS;
-	if (R > G)
-		R = G;
-	if (R < 1)
-		R = 1;
-	const uint32_t C = (uint32_t)((T + P2_QUEUE_FLUSH - 1) / P2_QUEUE_FLUSH);
-	const size_t nt = job->nterms, nd = job->ndet, nh = job->length;
-	/* device buffer: tables, per-round scratch and program, registers */
-	enum { RNG, CDF, TFL, TPH, TCF, HFL, HPH, HPHI, HCS, WIDX, WVAL, GIDX,
-		GOUT, X, ROT, CS, PASS, REC, PROG, NPC, SOFF, POFF, REGS, NBUF };
-	size_t sz[NBUF], off[NBUF], total = 0;
-	/* sizes and offsets for rounds of G samples on R registers */
-	auto layout = [&](size_t G, size_t R) {
-		const size_t GT = G * T > 0 ? G * T : 1;
-		sz[RNG] = 4 * samples * job->halves * sizeof(uint64_t);
-		sz[CDF] = nt * sizeof(double);
-		sz[TFL] = sz[TPH] = nt * sizeof(uint64_t);
-		sz[TCF] = nt * sizeof(double);
-		sz[HFL] = sz[HPH] = nh * sizeof(uint64_t);
-		sz[HPHI] = nh * sizeof(double);
-		sz[HCS] = 2 * nh * sizeof(double);
-		sz[WIDX] = nd * sizeof(uint64_t);
-		sz[WVAL] = 2 * nd * sizeof(double);
-		sz[GIDX] = samples * nd * sizeof(uint64_t);
-		sz[GOUT] = samples * nd * sizeof(double2);
-		sz[X] = G * job->halves * (size_t)job->depth * sizeof(double);
-		sz[ROT] = GT * sizeof(struct phase2_rot_in);
-		sz[CS] = 2 * GT * sizeof(double);
-		sz[PASS] = GT * sizeof(struct phase2_pass);
-		sz[REC] = GT * sizeof(struct phase2_rot_rec);
-		sz[PROG] = (G * T + 3 * G) * sizeof(struct p2_op);
-		sz[NPC] = sz[POFF] = (G * C ? G * C : 1) * sizeof(uint32_t);
-		sz[SOFF] = G * sizeof(uint32_t);
-		sz[REGS] = R * (sizeof(struct p2_binst) +
-				       sizeof(struct p2_bctl)) +
-			sizeof(unsigned int) + (R - 1) * d->namp * d->elem;
-		total = 0;
-		for (int i = 0; i < NBUF; i++) {
-			off[i] = total;
-			total += (sz[i] + 255) & ~(size_t)255;
-		}
-	};
-	unsigned char *b = NULL;
-	CUDA_OK(cudaStreamSynchronize(d->stream), "device sampling: sync");
-	/* on a full device: fewer state copies, then smaller rounds */
-	for (;;) {
-		layout(G, R);
-		if (cudaMalloc((void **)&b, total) == cudaSuccess)
-			break;
-		cudaGetLastError();
-		b = NULL;
-		if (R > 1) {
-			R = 1;
-		} else if (G > 1) {
-			G = (G + 1) / 2;
-		} else {
-			log_error("device sampling: no room for %zu bytes of "
-				  "scratch", total);
-			return -1;
-		}
-	}
-	uint64_t *gidx = (uint64_t *)malloc(sz[GIDX] ? sz[GIDX] : 1);
-	struct p2_binst *hinst = (struct p2_binst *)malloc(
-		R * sizeof(struct p2_binst));
-	int rc = -1;
-	cudaError_t e = gidx && hinst ? cudaSuccess
-				      : cudaErrorMemoryAllocation;
-	/* registers: the copies first (256-aligned), then inst, ctl, status */
-	unsigned char *copies = b + off[REGS];
-	struct p2_binst *inst = (struct p2_binst *)(b + off[REGS] +
-		(R - 1) * d->namp * d->elem);
-	struct p2_bctl *ctl = (struct p2_bctl *)(inst + R);
-	unsigned int *status = (unsigned int *)(ctl + R);
-	if (e == cudaSuccess) {
-		for (size_t s = 0; s < samples; s++)
-			for (size_t j = 0; j < nd; j++)
-				gidx[s * nd + j] = det_idx[j];
-		for (size_t r = 0; r < R; r++) {
-			hinst[r].state = r == 0
-				? d->state
-				: (void *)(copies + (r - 1) * d->namp * d->elem);
-			hinst[r].namp = d->namp;
-			hinst[r].op_off = hinst[r].nops = 0;
-		}
-		const void *src[] = { rng0, cdf_y, tflip, tphase, tcf, hflip,
-			hphase, hphi, hcs, det_idx, det_val, gidx };
-		const int at[] = { RNG, CDF, TFL, TPH, TCF, HFL, HPH, HPHI, HCS,
-			WIDX, WVAL, GIDX };
-		for (int i = 0; i < 12 && e == cudaSuccess; i++)
-			if (sz[at[i]]) {
-				e = cudaMemcpyAsync(b + off[at[i]], src[i],
-					sz[at[i]], cudaMemcpyHostToDevice,
-					d->stream);
-				d->h2d_bytes += sz[at[i]];
-			}
-		if (e == cudaSuccess)
-			e = cudaMemcpyAsync(inst, hinst,
-				R * sizeof(struct p2_binst),
-				cudaMemcpyHostToDevice, d->stream);
-	}
-	const bool f64 = d->prec == PHASE2_PREC_FP64;
-	int per_sm = 0;
-	if (e == cudaSuccess)
-		e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm,
-			batch_kernel(f64), P2_TPB, 0);
-	if (e == cudaSuccess)
-		e = cudaFuncSetAttribute(k_smp_plan,
-			cudaFuncAttributeMaxDynamicSharedMemorySize,
-			(int)P2_SMP_PLAN_SMEM);
-	/* no op has more tiles than a span-0 pass or a zero (more blocks
-	 * would only poll) */
-	uint32_t cpt = 0;
-	uint64_t most = p2_op_tiles(P2_OP_PASS, d->namp, 0, &cpt);
-	const uint32_t zt = p2_op_tiles(P2_OP_ZERO, d->namp, 0, &cpt);
-	if (zt > most)
-		most = zt;
-	most *= R;
-	unsigned grid =
-		(unsigned)d->sm_count * (unsigned)(per_sm > 0 ? per_sm : 1);
-	if (most < grid)
-		grid = (unsigned)most;
-	uint32_t *npc = (uint32_t *)(b + off[NPC]);
-	uint32_t *soff = (uint32_t *)(b + off[SOFF]);
-	uint32_t *poff = (uint32_t *)(b + off[POFF]);
-	uint64_t nops_run = 0;
-	/* PHASE2_SAMPLING_TIMING=1: per-round stage times on stderr */
-	const char *tenv = getenv("PHASE2_SAMPLING_TIMING");
-	const int timing = tenv && *tenv == '1';
-	cudaEvent_t ev[5] = { 0, 0, 0, 0, 0 };
-	for (int i = 0; timing && i < 5; i++)
-		cudaEventCreate(&ev[i]);
-	for (size_t s0 = 0; s0 < samples && e == cudaSuccess; s0 += G) {
-		const uint32_t g = (uint32_t)(samples - s0 < G ? samples - s0 : G);
-		const uint32_t nreg = (uint32_t)(g < R ? g : R);
-		const uint32_t nx = g * job->halves;
-		if (timing)
-			cudaEventRecord(ev[0], d->stream);
-		if (job->depth)
-			k_smp_draw<<<(nx + 127) / 128, 128, 0, d->stream>>>(
-				*job, (uint32_t)s0, nx,
-				(const uint64_t *)(b + off[RNG]),
-				(double *)(b + off[X]));
-		const uint64_t tot = (uint64_t)g * T;
-		if (tot)
-			k_smp_stream<<<grid_for(d, tot, P2_TPB, 8), P2_TPB, 0,
-				d->stream>>>(*job, tot,
-				(const double *)(b + off[X]),
-				(const double *)(b + off[CDF]),
-				(const uint64_t *)(b + off[TFL]),
-				(const uint64_t *)(b + off[TPH]),
-				(const double *)(b + off[TCF]),
-				(const uint64_t *)(b + off[HFL]),
-				(const uint64_t *)(b + off[HPH]),
-				(const double *)(b + off[HPHI]),
-				(const double *)(b + off[HCS]),
-				(struct phase2_rot_in *)(b + off[ROT]),
-				(double *)(b + off[CS]));
-		if (timing)
-			cudaEventRecord(ev[1], d->stream);
-		const uint32_t nch = g * C;
-		if (nch)
-			k_smp_plan<<<nch, P2_SMP_PLAN_TPB, P2_SMP_PLAN_SMEM,
-				d->stream>>>(*job, T, C,
-				(const struct phase2_rot_in *)(b + off[ROT]),
-				(const double *)(b + off[CS]),
-				(struct phase2_pass *)(b + off[PASS]),
-				(struct phase2_rot_rec *)(b + off[REC]), npc);
-		if (timing)
-			cudaEventRecord(ev[2], d->stream);
-		k_smp_layout<<<1, 32, 0, d->stream>>>(g, C, npc,
-			(uint64_t)samples - 1, (uint64_t)s0, nreg, soff, poff,
-			inst);
-		k_smp_fill<<<(g * C + g + 127) / 128, 128, 0, d->stream>>>(
-			*job, g, C, T, d->namp, (uint64_t)s0, npc, soff, poff,
-			(const struct phase2_pass *)(b + off[PASS]),
-			(struct p2_op *)(b + off[PROG]));
-		e = cudaGetLastError();
-		if (timing)
-			cudaEventRecord(ev[3], d->stream);
-		if (e == cudaSuccess)
-			e = cudaMemsetAsync(ctl, 0, nreg * sizeof *ctl,
-				d->stream);
-		if (e == cudaSuccess)
-			e = cudaMemsetAsync(status, 0, sizeof(unsigned int),
-				d->stream);
-		if (e == cudaSuccess)
-			batch_launch(f64, grid, d->stream, inst, nreg,
-				(const struct p2_op *)(b + off[PROG]),
-				(const struct phase2_pass *)(b + off[PASS]),
-				(const struct phase2_rot_rec *)(b + off[REC]),
-				(const uint64_t *)(b + off[WIDX]),
-				(const double *)(b + off[WVAL]),
-				(const uint64_t *)(b + off[GIDX]),
-				(double2 *)(b + off[GOUT]), ctl, status);
-		if (e == cudaSuccess)
-			e = cudaGetLastError();
-		if (timing)
-			cudaEventRecord(ev[4], d->stream);
-		/* draw, stream and plan run only when they have work */
-		d->launches += 3 + (job->depth != 0) + (tot != 0) + (nch != 0);
-		unsigned int st = 0;
-		if (e == cudaSuccess)
-			e = cudaMemcpyAsync(&st, status, sizeof st,
-				cudaMemcpyDeviceToHost, d->stream);
-		if (e == cudaSuccess)
-			e = cudaMemcpyAsync(hinst, inst,
-				nreg * sizeof(struct p2_binst),
-				cudaMemcpyDeviceToHost, d->stream);
-		if (e == cudaSuccess)
-			e = cudaStreamSynchronize(d->stream);
-		if (e == cudaSuccess && st) {
-			log_error("device sampling: a block found no work for"
-				  " %u rounds",
-				P2_BATCH_IDLE_LIMIT);
-			e = cudaErrorLaunchFailure;
-		}
-		uint64_t rops = 0;
-		for (uint32_t r = 0; e == cudaSuccess && r < nreg; r++)
-			rops += hinst[r].nops;
-		nops_run += rops - 3ull * g;
-		if (timing && e == cudaSuccess) {
-			float t[4];
-			for (int i = 0; i < 4; i++)
-				cudaEventElapsedTime(&t[i], ev[i], ev[i + 1]);
-			fprintf(stderr,
-				"device sampling: %u samples x %llu rotations,"
-				" %u registers, %llu ops, grid %u: draw+stream"
-				" %.3f ms, plan %.3f ms, layout %.3f ms, run"
-				" %.3f ms\n",
-				g, (unsigned long long)T, nreg,
-				(unsigned long long)rops, grid, t[0], t[1], t[2],
-				t[3]);
-		}
-	}
-	for (int i = 0; timing && i < 5; i++)
-		cudaEventDestroy(ev[i]);
-	if (e == cudaSuccess && sz[GOUT])
-		e = cudaMemcpy(gout, b + off[GOUT], sz[GOUT],
-			cudaMemcpyDeviceToHost);
-	if (e == cudaSuccess) {
-		d->d2h_bytes += sz[GOUT];
-		d->passes += nops_run;
-		d->sweeps += nops_run;
-		d->rotations += (uint64_t)samples * T;
-		*npass_out = nops_run;
-		rc = 0;
-	} else {
-		log_error("device sampling: %s", cudaGetErrorString(e));
-	}
-	free(gidx);
-	free(hinst);
-	cudaFree(b);
-	return rc;
 }
 
 /* ---- allocation-free norm (phase2_norm2_noalloc) ------------------------ */
