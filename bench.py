@@ -651,8 +651,15 @@ def batched_study(ninst: int = 64, step_cap: int = 4, seed: int = 0xBA7C4):
                         f"JW terms, {step_cap} steps each, FP32 state"),
            "rot_amp": work, "unit": UNIT}
     p2.set_precision(p2.PREC_FP32)
+    order = p2.lib().phase2_get_term_order()
     try:
-        for mode, persistent in (("persistent", True), ("streams", False)):
+        # the reference's lexicographic term order in both modes, then the
+        # flip-mask order (a different, equally valid product order that
+        # fuses more rotations per pass) in the persistent mode
+        for mode, persistent, ordr in (
+                ("persistent", True, 0), ("streams", False, 0),
+                ("persistent_flip_order", True, 2)):
+            p2.set_term_order(ordr)
             p2.set_batch_persistent(persistent)
             p2.batch("trott", probs[:2])  # warm the kernels
             t0 = time.perf_counter()
@@ -672,6 +679,7 @@ def batched_study(ninst: int = 64, step_cap: int = 4, seed: int = 0xBA7C4):
                                          for s in stats))}
     finally:
         p2.set_batch_persistent(True)
+        p2.set_term_order(order)
         p2.set_precision(p2.PREC_FP64)
     out["value"] = out["persistent"]["value"]
     return out
