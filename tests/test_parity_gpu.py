@@ -620,6 +620,39 @@ def test_qdrift_device_sampling(nqb, nterms, ndet, samples, depth, prec,
             assert np.max(np.abs(dev - want)) < FP32_TOL
 
 
+@pytest.mark.parametrize("prec", [p2.PREC_FP32, p2.PREC_FP64],
+                         ids=["fp32", "fp64"])
+def test_device_sampling_edges(prec, oracle_lib):
+    """Edges under forced device sampling, as the host loop has them: a
+    determinant outside the register is refused; zero samples give no
+    output; cmpsit with zero steps (prepst and measure only) and qdrift
+    with depth 1 match the oracle."""
+    n = 10
+    t = workloads.jw_terms(n, 80, seed=3)
+    d = workloads.hamming_dets(n, 2, 5, seed=4)
+    bad = Dets(np.array([3, 1 << n], dtype=np.uint64),
+               np.array([0.6 + 0j, 0.8 + 0j]))
+    p2.set_precision(prec)
+    tol = 0.0 if prec == p2.PREC_FP64 else FP32_TOL
+    try:
+        for mode in (False, True):
+            p2.set_device_sampling(mode)
+            with pytest.raises(RuntimeError):
+                p2.qdrift(n, t, bad, 2, 10, 0.01, 5)
+            assert len(p2.qdrift(n, t, d, 0, 10, 0.01, 5)) == 0
+            z = p2.cmpsit(n, t, d, 2, 0, 5, 8, 0.05, 0.01, 7)
+            want = oracle_lib.cmpsit(n, t.flip, t.phase, t.cf, d.idx, d.cf,
+                                     2, 0, 5, 8, 0.05, 0.01, 7)
+            assert np.max(np.abs(z - want)) <= tol
+            z = p2.qdrift(n, t, d, 3, 1, 0.01, 6)
+            want = oracle_lib.qdrift(n, t.flip, t.phase, t.cf, d.idx, d.cf,
+                                     3, 1, 0.01, 6)
+            assert np.max(np.abs(z - want)) <= tol
+    finally:
+        p2.set_device_sampling(p2.DEVICE_SAMPLING_AUTO)
+        p2.set_precision(p2.PREC_FP64)
+
+
 def test_device_sampling_on_a_nearly_full_device():
     """With too little free memory for state copies, device sampling runs
     its samples on the register alone (smaller rounds if need be) and
