@@ -598,7 +598,7 @@ def cmpsit33_study(steps: int = 1) -> dict:
     return out
 
 
-def batch8_study() -> dict:
+def batch8_study(prec: int = 1) -> dict:
     """A small, L2-resident persistent batch (8 trott instances of 18-20
     qubits, 2,000 JW terms, 2 steps, FP32), run twice: the case the
     persistent kernel's profile summary captures (its second launch)."""
@@ -615,7 +615,7 @@ def batch8_study() -> dict:
                           dets=workloads.hamming_dets(n, 1, n // 2,
                                                       seed=200 + k),
                           steps=2, delta=0.05))
-    p2.set_precision(p2.PREC_FP32)
+    p2.set_precision(prec)
     try:
         for _ in range(2):
             _, st = p2.batch("trott", probs, with_stats=True)
@@ -623,6 +623,12 @@ def batch8_study() -> dict:
         p2.set_precision(p2.PREC_FP64)
     return {"passes": int(sum(s["passes"] for s in st)),
             "kernel_ms": float(sum(s["pass_ms"] for s in st))}
+
+
+def batch8fp64_study() -> dict:
+    """batch8 with FP64 registers: the FP64 instance of the persistent
+    kernel (exact pass arithmetic), for its profile summary."""
+    return batch8_study(prec=0)
 
 
 def batched_study(ninst: int = 64, step_cap: int = 4, seed: int = 0xBA7C4):
@@ -740,7 +746,8 @@ def main() -> None:
                          "sweeps")
     ap.add_argument("--only-study", default=None,
                     help="run just this study (batched, trott26, cmpsit33, "
-                         "batch8, sampling, sweeps) and print its JSON; "
+                         "batch8, batch8fp64, sampling, sweeps) and print "
+                         "its JSON; "
                          "--nqb, when given, sets the sweeps study's width")
     args = ap.parse_args()
     if args.only_study:
