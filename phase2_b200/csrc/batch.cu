@@ -12,6 +12,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 
 #define LOG_SUBSYS "engine"
 #include "log.h"
@@ -327,6 +328,14 @@ void p2_batch_launch(bool f64, unsigned grid, cudaStream_t stream,
 			P2_BATCH_IDLE_LIMIT);
 }
 
+/* Host seconds (PHASE2_BATCH_TIMING breakdown). */
+static double p2_now(void)
+{
+	struct timespec ts;
+	clock_gettime(CLOCK_MONOTONIC, &ts);
+	return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
 extern "C" int p2d_batch_run(struct p2_dev *const *devs,
 	const struct p2_prog *const *progs, size_t n, double *gout,
 	double *kernel_ms)
@@ -367,6 +376,7 @@ extern "C" int p2d_batch_run(struct p2_dev *const *devs,
 	const size_t o_status = p2_align256(o_ctl + n * sizeof(struct p2_bctl));
 	const size_t total = o_status + 256;
 
+	const double tb0 = p2_now();
 	unsigned char *h = (unsigned char *)malloc(up);
 	if (!h)
 		return -1;
@@ -431,22 +441,28 @@ extern "C" int p2d_batch_run(struct p2_dev *const *devs,
 	struct p2_dev *d0 = devs[0];
 	unsigned char *dbuf = NULL;
 	cudaError_t e = cudaSuccess;
+	const double tb1 = p2_now();
 	for (size_t i = 0; i < n && e == cudaSuccess; i++)
 		e = cudaStreamSynchronize(devs[i]->stream);
+	const double tb2 = p2_now();
 	if (e == cudaSuccess)
-		e = cudaMalloc((void **)&dbuf, total);
+		e = p2_scratch_alloc((void **)&dbuf, total, d0->stream);
+	/* on the stream that owns the pool allocation (a pageable upload is
+	 * staged before the call returns, so h may be freed after it) */
 	if (e == cudaSuccess)
-		e = cudaMemcpy(dbuf, h, up, cudaMemcpyHostToDevice);
+		e = cudaMemcpyAsync(dbuf, h, up, cudaMemcpyHostToDevice,
+			d0->stream);
 	free(h);
+	const double tb3 = p2_now();
 	if (e == cudaSuccess)
-		e = cudaMemset(dbuf + o_ctl, 0, total - o_ctl);
+		e = cudaMemsetAsync(dbuf + o_ctl, 0, total - o_ctl, d0->stream);
 	const bool f64 = d0->prec == PHASE2_PREC_FP64;
 	int per_sm = 0;
 	if (e == cudaSuccess)
 		e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm,
 			p2_batch_kernel(f64), P2_TPB, 0);
 	if (e != cudaSuccess) {
-		cudaFree(dbuf);
+		p2_scratch_free(dbuf, d0->stream);
 		log_error("batch: setup: %s", cudaGetErrorString(e));
 		return -1;
 	}
@@ -477,7 +493,13 @@ extern "C" int p2d_batch_run(struct p2_dev *const *devs,
 	float ms = 0.0f;
 	if (e == cudaSuccess)
 		e = cudaEventElapsedTime(&ms, d0->t0, d0->t1);
-	cudaFree(dbuf);
+	const double tb4 = p2_now();
+	p2_scratch_free(dbuf, d0->stream);
+	if (getenv("PHASE2_BATCH_TIMING"))
+		log_info("batch run: build %.3f s, stream sync %.3f s, alloc+upload"
+			 " %.3f s (%zu bytes), kernel+download %.3f s, free %.3f s",
+			tb1 - tb0, tb2 - tb1, tb3 - tb2, up, tb4 - tb3,
+			p2_now() - tb4);
 	if (e != cudaSuccess) {
 		log_error("batch: %s", cudaGetErrorString(e));
 		return -1;

@@ -547,8 +547,20 @@ extern "C" struct p2_dev *p2d_create(uint32_t nqb, int prec)
 	d->graphs_on = nqb <= P2_GRAPH_MAX_QB;
 
 	size_t free_b = 0, total_b = 0;
+	/* memory the pool holds but does not use can serve the state too */
+	size_t pooled = 0;
+	cudaMemPool_t pool;
+	uint64_t reserved = 0, used = 0;
+	if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess &&
+		cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent,
+			&reserved) == cudaSuccess &&
+		cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent,
+			&used) == cudaSuccess &&
+		reserved > used)
+		pooled = (size_t)(reserved - used);
+	cudaGetLastError();
 	if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess &&
-		bytes > free_b) {
+		bytes > free_b + pooled) {
 		log_error("p2d_create: state of %zu bytes exceeds free device"
 			  " memory (%zu bytes)",
 			bytes, free_b);
@@ -558,8 +570,12 @@ extern "C" struct p2_dev *p2d_create(uint32_t nqb, int prec)
 	if (cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) !=
 		cudaSuccess)
 		goto fail;
-	if (cudaMalloc(&d->state, bytes) != cudaSuccess) {
-		log_error("p2d_create: cudaMalloc(%zu) failed", bytes);
+	/* stream-ordered from the default pool (p2_scratch_alloc): creating
+	 * and destroying many registers (batches) reuses memory instead of
+	 * mapping and unmapping it each time */
+	if (p2_scratch_alloc(&d->state, bytes, d->stream) != cudaSuccess) {
+		d->state = NULL;
+		log_error("p2d_create: allocation of %zu bytes failed", bytes);
 		goto fail;
 	}
 	for (int k = 0; k < 2; k++)
@@ -570,6 +586,9 @@ extern "C" struct p2_dev *p2d_create(uint32_t nqb, int prec)
 		cudaEventCreate(&d->t1) != cudaSuccess)
 		goto fail;
 	if (cudaMemsetAsync(d->state, 0, bytes, d->stream) != cudaSuccess)
+		goto fail;
+	/* the state is ready for any stream from here on */
+	if (cudaStreamSynchronize(d->stream) != cudaSuccess)
 		goto fail;
 	return d;
 fail:
@@ -584,7 +603,8 @@ extern "C" void p2d_destroy(struct p2_dev *d)
 		return;
 	if (d->stream)
 		cudaStreamSynchronize(d->stream);
-	cudaFree(d->state);
+	if (d->state)
+		p2_scratch_free(d->state, d->stream);
 	cudaFree(d->d_recs);
 	for (int k = 0; k < 2; k++) {
 		cudaFreeHost(d->h_recs[k]);
@@ -1311,6 +1331,32 @@ extern "C" void p2d_set_timing(struct p2_dev *d, int on)
 extern "C" void *p2d_stream(const struct p2_dev *d)
 {
 	return (void *)d->stream;
+}
+
+/* ---- transient buffers --------------------------------------------------- */
+
+cudaError_t p2_scratch_alloc(void **p, size_t bytes, cudaStream_t stream)
+{
+	static int pool_ready;
+	if (!pool_ready) {
+		int dev = 0;
+		cudaMemPool_t pool;
+		if (cudaGetDevice(&dev) == cudaSuccess &&
+			cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+			uint64_t keep = UINT64_C(1) << 30;
+			cudaMemPoolSetAttribute(pool,
+				cudaMemPoolAttrReleaseThreshold, &keep);
+		}
+		cudaGetLastError();
+		pool_ready = 1;
+	}
+	return cudaMallocAsync(p, bytes, stream);
+}
+
+void p2_scratch_free(void *p, cudaStream_t stream)
+{
+	if (p)
+		cudaFreeAsync(p, stream);
 }
 
 /* ---- allocation-free norm (phase2_norm2_noalloc) ------------------------ */

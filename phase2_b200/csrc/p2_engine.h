@@ -99,6 +99,15 @@ static inline unsigned grid_for(const struct p2_dev *d, uint64_t work, unsigned 
 
 /* ---- cross-file entry points -------------------------------------------- */
 
+/* engine.cu: transient device buffers of one call (a batch program, the
+ * scratch of device sampling), stream-ordered from the device's default
+ * memory pool, which keeps up to 1 GiB of freed memory for the next call
+ * instead of unmapping it at every synchronisation (a cudaFree of such a
+ * buffer could take hundreds of milliseconds).  The pool is configured on
+ * the first call, for the current device (one device per process). */
+cudaError_t p2_scratch_alloc(void **p, size_t bytes, cudaStream_t stream);
+void p2_scratch_free(void *p, cudaStream_t stream);
+
 struct p2_binst;
 struct p2_bctl;
 

@@ -353,7 +353,8 @@ extern "C" int p2d_sampled_device(struct p2_dev *d,
 	/* on a full device: fewer state copies, then smaller rounds */
 	for (;;) {
 		layout(G, R);
-		if (cudaMalloc((void **)&b, total) == cudaSuccess)
+		if (p2_scratch_alloc((void **)&b, total, d->stream) ==
+			cudaSuccess)
 			break;
 		cudaGetLastError();
 		b = NULL;
@@ -557,7 +558,7 @@ extern "C" int p2d_sampled_device(struct p2_dev *d,
 	}
 	free(gidx);
 	free(hinst);
-	cudaFree(b);
+	p2_scratch_free(b, d->stream);
 	return rc;
 }
 
