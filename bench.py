@@ -563,6 +563,92 @@ def sweeps_study(nqb: int = 26) -> dict:
             "rows": rows}
 
 
+def sharded_study(nqb: int = 30, worlds=(2, 4, 8)) -> dict:
+    """A register split by its high qubits over 2, 4, 8 ranks held by this
+    process on one GPU (phase2_b200.sharded: qubit swaps through
+    qreg_slab_get / qreg_slab_put), against one register, on 4096 qDRIFT
+    draws from the bench's 100,000 JW terms (|c|-weighted numpy draws,
+    angle asin(1e-3) sign(c)), FP32.  Wall clock per sample with the
+    device synchronised (the sharded register's host waits for each
+    exchange), swaps per sample, and the half-slab gather bandwidth
+    (CUDA events on the register's stream; 2 x 8 B per amplitude)."""
+    import numpy as np
+    import torch
+
+    import phase2_b200 as p2
+    from phase2_b200 import sharded, workloads
+    cfg = workloads.qdrift30(nqb=nqb)
+    t, d = cfg["terms"], cfg["dets"]
+    rng = np.random.Generator(np.random.PCG64(0x5A4D))
+    w = np.abs(t.cf)
+    om = math.asin(1e-3)
+
+    def draws():
+        k = rng.choice(len(t), size=cfg["depth"], p=w / w.sum())
+        return t.flip[k], t.phase[k], om * np.sign(t.cf[k])
+
+    samples = [draws() for _ in range(3)]
+
+    def timed(reg, prep):
+        out = []
+        for f, ph, phi in samples:
+            prep()
+            reg.synchronize()
+            t0 = time.perf_counter()
+            reg.paulirot(f, ph, phi)
+            reg.synchronize()
+            out.append(time.perf_counter() - t0)
+        return out[1:]  # the first sample warms plans and buffers
+
+    p2.set_device_sampling(p2.DEVICE_SAMPLING_OFF)
+    res = {"workload": (f"{nqb} qubits FP32, 3 samples x {cfg['depth']} "
+                        "qDRIFT draws of 100000 JW terms, first sample "
+                        "untimed"), "unit": UNIT}
+    try:
+        with p2.Register(nqb, p2.PREC_FP32) as one:
+            def prep1():
+                one.zero()
+                one.setamps(d.idx, d.cf)
+            sec = timed(one, prep1)
+        res["one_register"] = {
+            "sec_per_sample": float(np.mean(sec)),
+            "value": cfg["depth"] * (1 << nqb) / float(np.mean(sec))}
+        rows = []
+        for world in worlds:
+            torch.cuda.empty_cache()
+            with sharded.ShardedRegister.on_one_gpu(nqb, world,
+                                                    p2.PREC_FP32) as reg:
+                s0 = reg.swaps
+                sec = timed(reg, lambda: reg.prepst(d))
+                swaps = (reg.swaps - s0) / len(samples)
+                slab = reg.slabs[0]
+                cnt = min(1 << (reg.nlocal - 1), sharded.CHUNK)
+                buf = slab.buffer(cnt)
+                stream = torch.cuda.ExternalStream(
+                    p2.lib().qreg_stream(C.byref(slab.reg.reg)))
+                ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+                gbs = {}
+                for bit in (reg.nlocal - 1, 5, 0):
+                    ev[0].record(stream)
+                    slab.slab_get(bit, 1, 0, cnt, buf)
+                    ev[1].record(stream)
+                    ev[1].synchronize()
+                    gbs[f"bit{bit}"] = (2 * 8 * cnt /
+                                        (ev[0].elapsed_time(ev[1]) * 1e-3)
+                                        / 1e9)
+                del buf
+            rows.append({
+                "world": world, "local_qubits": reg.nlocal,
+                "sec_per_sample": float(np.mean(sec)),
+                "value": cfg["depth"] * (1 << nqb) / float(np.mean(sec)),
+                "swaps_per_sample": swaps,
+                "gather_gbs": gbs, "gather_amplitudes": cnt})
+        res["sharded"] = rows
+    finally:
+        p2.set_device_sampling(p2.DEVICE_SAMPLING_AUTO)
+    return res
+
+
 def cmpsit33_study(steps: int = 1) -> dict:
     """The composite driver at 33 qubits (200,000 JW terms, 2,000
     deterministic, 8,192 draws per half step, 32 determinants), `steps` of
@@ -746,9 +832,9 @@ def main() -> None:
                          "sweeps")
     ap.add_argument("--only-study", default=None,
                     help="run just this study (batched, trott26, cmpsit33, "
-                         "batch8, batch8fp64, sampling, sweeps) and print "
-                         "its JSON; "
-                         "--nqb, when given, sets the sweeps study's width")
+                         "batch8, batch8fp64, sampling, sweeps, sharded) "
+                         "and print its JSON; --nqb, when given, sets the "
+                         "sweeps or sharded study's width")
     args = ap.parse_args()
     if args.only_study:
         import inspect

@@ -196,6 +196,33 @@ int qreg_norm2(struct qreg *reg, double *out);
  * (2 * namp doubles), reduced on the device like qreg_norm2. */
 int qreg_inner_dense(struct qreg *reg, const double *trial, double out[2]);
 
+/* ---- half slabs (registers sharded by high qubits) ---------------------- */
+
+/*
+ * Copy elements [first, first + count) of the half {i : bit `bit` of i ==
+ * val} of the register's amplitudes (namp / 2 of them, in increasing index
+ * order) to (get) or from (put) the contiguous device buffer d_buf, which
+ * holds them at the register's precision (complex128 for FP64 registers,
+ * complex64 for FP32).  The copy has finished when the call returns.
+ *
+ * These replace the reference's slab exchange buffers (phase2/qreg.c:
+ * 124-142, the backend hooks qreg_backend_exch_init/_waitall of
+ * phase2/qreg.h:14-33): a register sharded over 2^g ranks by its g high
+ * qubits swaps a high qubit with a local qubit l by exchanging, with the
+ * partner rank, the half whose bit l differs from its own rank bit
+ * (phase2_b200/sharded.py); get/put move that half, chunk by chunk,
+ * through exchange buffers the caller owns (for NCCL, torch tensors).
+ *
+ * d_buf must be device memory of the register's device, aligned to the
+ * element size, with count elements inside one allocation; anything else
+ * returns -1 with an error and copies nothing, as do bit >= nqb, val > 1
+ * and a range past namp / 2.  0 on success.
+ */
+int qreg_slab_get(struct qreg *reg, uint32_t bit, uint32_t val,
+	uint64_t first, uint64_t count, void *d_buf);
+int qreg_slab_put(struct qreg *reg, uint32_t bit, uint32_t val,
+	uint64_t first, uint64_t count, const void *d_buf);
+
 /* ---- counters ----------------------------------------------------------- */
 
 struct phase2_stats {

@@ -226,6 +226,10 @@ _SIGS = {
     "qreg_get_state": (C.c_int, [_P(Qreg), _P(C.c_double)]),
     "qreg_set_state": (C.c_int, [_P(Qreg), _P(C.c_double)]),
     "qreg_norm2": (C.c_int, [_P(Qreg), _P(C.c_double)]),
+    "qreg_slab_get": (C.c_int, [_P(Qreg), C.c_uint32, C.c_uint32,
+                                C.c_uint64, C.c_uint64, C.c_void_p]),
+    "qreg_slab_put": (C.c_int, [_P(Qreg), C.c_uint32, C.c_uint32,
+                                C.c_uint64, C.c_uint64, C.c_void_p]),
     "qreg_inner_dense": (C.c_int, [_P(Qreg), _P(C.c_double),
                                    _P(C.c_double)]),
     "qreg_get_stats": (C.c_int, [_P(Qreg), _P(Stats)]),

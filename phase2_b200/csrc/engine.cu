@@ -1281,12 +1281,12 @@ extern "C" int p2d_inner_dense(struct p2_dev *d, const double *trial,
 {
 	double2 *t = NULL;
 	const size_t bytes = d->namp * sizeof(double2);
-	CUDA_OK(cudaMalloc((void **)&t, bytes), "alloc trial");
+	CUDA_OK(p2_scratch_alloc((void **)&t, bytes, d->stream), "alloc trial");
 	cudaError_t e = cudaMemcpyAsync(t, trial, bytes, cudaMemcpyHostToDevice,
 		d->stream);
 	int rc = e == cudaSuccess ? reduce(d, t, out) : -1;
+	p2_scratch_free(t, d->stream);
 	cudaStreamSynchronize(d->stream);
-	cudaFree(t);
 	if (e != cudaSuccess)
 		log_error("upload trial: %s", cudaGetErrorString(e));
 	return rc;

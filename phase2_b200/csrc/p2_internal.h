@@ -66,6 +66,13 @@ int p2d_run(struct p2_dev *d, const struct phase2_pass *passes, size_t npass,
 int p2d_norm2(struct p2_dev *d, double *out);
 int p2d_inner_dense(struct p2_dev *d, const double *trial, double out[2]);
 
+/* Copy elements [first, first + count) of the half {i : bit `bit` of i ==
+ * val} of the state to (put = 0) or from (put = 1) the device buffer buf,
+ * which holds them contiguously at the register's precision; waits for the
+ * copy.  0 or -1 (logged). */
+int p2d_slab_copy(struct p2_dev *d, uint32_t bit, uint32_t val,
+	uint64_t first, uint64_t count, void *buf, int put);
+
 /* Wait for the stream; -1 if any CUDA error is pending. */
 int p2d_sync(struct p2_dev *d);
 

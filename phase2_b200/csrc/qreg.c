@@ -468,6 +468,30 @@ int qreg_inner_dense(struct qreg *reg, const double *trial, double out[2])
 	return p2d_inner_dense(b->dev, trial, out);
 }
 
+static int slab_copy(struct qreg *reg, uint32_t bit, uint32_t val,
+	uint64_t first, uint64_t count, void *buf, int put)
+{
+	struct p2_qreg *b = B(reg);
+	if (!b || recording(b, put ? "qreg_slab_put" : "qreg_slab_get") ||
+		qreg_flush(reg) < 0)
+		return -1;
+	if (put)
+		b->host_copy_valid = 0;
+	return p2d_slab_copy(b->dev, bit, val, first, count, buf, put);
+}
+
+int qreg_slab_get(struct qreg *reg, uint32_t bit, uint32_t val,
+	uint64_t first, uint64_t count, void *d_buf)
+{
+	return slab_copy(reg, bit, val, first, count, d_buf, 0);
+}
+
+int qreg_slab_put(struct qreg *reg, uint32_t bit, uint32_t val,
+	uint64_t first, uint64_t count, const void *d_buf)
+{
+	return slab_copy(reg, bit, val, first, count, (void *)d_buf, 1);
+}
+
 int p2_qreg_record(struct qreg *reg, struct p2_prog *pg)
 {
 	struct p2_qreg *b = B(reg);
