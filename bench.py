@@ -570,8 +570,11 @@ def sharded_study(nqb: int = 30, worlds=(2, 4, 8)) -> dict:
     draws from the bench's 100,000 JW terms (|c|-weighted numpy draws,
     angle asin(1e-3) sign(c)), FP32.  Wall clock per sample with the
     device synchronised (the sharded register's host waits for each
-    exchange), swaps per sample, and the half-slab gather bandwidth
-    (CUDA events on the register's stream; 2 x 8 B per amplitude)."""
+    exchange), swaps per sample (pairs in this process trade halves in
+    place, qreg_slab_swap), the bandwidth of one in-place swap (4 x 8 B
+    per half amplitude) and of the half-slab gather that exchanges between
+    processes use (2 x 8 B per amplitude), from CUDA events on the
+    register's stream."""
     import numpy as np
     import torch
 
@@ -637,11 +640,20 @@ def sharded_study(nqb: int = 30, worlds=(2, 4, 8)) -> dict:
                                         (ev[0].elapsed_time(ev[1]) * 1e-3)
                                         / 1e9)
                 del buf
+                # one in-place pair swap: both halves read and written
+                nhalf = 1 << (reg.nlocal - 1)
+                ev[0].record(stream)
+                slab.swap_halves(reg.slabs[1], reg.nlocal - 1, 1, 0)
+                ev[1].record(stream)
+                ev[1].synchronize()
+                swap_gbs = (4 * 8 * nhalf /
+                            (ev[0].elapsed_time(ev[1]) * 1e-3) / 1e9)
             rows.append({
                 "world": world, "local_qubits": reg.nlocal,
                 "sec_per_sample": float(np.mean(sec)),
                 "value": cfg["depth"] * (1 << nqb) / float(np.mean(sec)),
-                "swaps_per_sample": swaps,
+                "swaps_per_sample": swaps, "in_place": reg.in_place,
+                "swap_gbs": swap_gbs,
                 "gather_gbs": gbs, "gather_amplitudes": cnt})
         res["sharded"] = rows
     finally:

@@ -223,6 +223,18 @@ int qreg_slab_get(struct qreg *reg, uint32_t bit, uint32_t val,
 int qreg_slab_put(struct qreg *reg, uint32_t bit, uint32_t val,
 	uint64_t first, uint64_t count, const void *d_buf);
 
+/*
+ * The same exchange between two registers on one device, in place: the
+ * half {i : bit `bit` of i == val_a} of a trades places, element for
+ * element in index order, with the half {i : bit of i == val_b} of b.  One
+ * kernel reads and writes both halves once (no buffers); it runs the
+ * exchange of paired ranks that one process holds on one GPU.  a and b
+ * must be distinct registers of one size and precision on one device.
+ * Finished when the call returns; 0 or -1.
+ */
+int qreg_slab_swap(struct qreg *a, struct qreg *b, uint32_t bit,
+	uint32_t val_a, uint32_t val_b);
+
 /* ---- counters ----------------------------------------------------------- */
 
 struct phase2_stats {

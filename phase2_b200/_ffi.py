@@ -230,6 +230,8 @@ _SIGS = {
                                 C.c_uint64, C.c_uint64, C.c_void_p]),
     "qreg_slab_put": (C.c_int, [_P(Qreg), C.c_uint32, C.c_uint32,
                                 C.c_uint64, C.c_uint64, C.c_void_p]),
+    "qreg_slab_swap": (C.c_int, [_P(Qreg), _P(Qreg), C.c_uint32,
+                                 C.c_uint32, C.c_uint32]),
     "qreg_inner_dense": (C.c_int, [_P(Qreg), _P(C.c_double),
                                    _P(C.c_double)]),
     "qreg_get_stats": (C.c_int, [_P(Qreg), _P(Stats)]),

@@ -73,6 +73,11 @@ int p2d_inner_dense(struct p2_dev *d, const double *trial, double out[2]);
 int p2d_slab_copy(struct p2_dev *d, uint32_t bit, uint32_t val,
 	uint64_t first, uint64_t count, void *buf, int put);
 
+/* Exchange half (bit, va) of a with half (bit, vb) of b in place (two
+ * registers of one size and precision on one device); waits for it. */
+int p2d_slab_swap(struct p2_dev *a, struct p2_dev *b, uint32_t bit,
+	uint32_t va, uint32_t vb);
+
 /* Wait for the stream; -1 if any CUDA error is pending. */
 int p2d_sync(struct p2_dev *d);
 

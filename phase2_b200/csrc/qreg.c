@@ -492,6 +492,19 @@ int qreg_slab_put(struct qreg *reg, uint32_t bit, uint32_t val,
 	return slab_copy(reg, bit, val, first, count, (void *)d_buf, 1);
 }
 
+int qreg_slab_swap(struct qreg *a, struct qreg *b, uint32_t bit,
+	uint32_t val_a, uint32_t val_b)
+{
+	struct p2_qreg *ba = B(a), *bb = B(b);
+	if (!ba || !bb || recording(ba, "qreg_slab_swap") ||
+		recording(bb, "qreg_slab_swap") || qreg_flush(a) < 0 ||
+		qreg_flush(b) < 0)
+		return -1;
+	ba->host_copy_valid = 0;
+	bb->host_copy_valid = 0;
+	return p2d_slab_swap(ba->dev, bb->dev, bit, val_a, val_b);
+}
+
 int p2_qreg_record(struct qreg *reg, struct p2_prog *pg)
 {
 	struct p2_qreg *b = B(reg);

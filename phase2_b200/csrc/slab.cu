@@ -35,19 +35,72 @@ __device__ __forceinline__ uint64_t p2_half_index(uint64_t j, uint32_t bit,
 	return ((j ^ low) << 1) | (val << bit) | low;
 }
 
+/*
+ * T is one state element (float2, double2) or, for FP32 halves with bit >=
+ * 1, a pair of them (float4): elements 2m and 2m + 1 of such a half are
+ * neighbours in the state, so indices below count in units of T.
+ */
+/* Items per thread and loop trip, all loaded before any is stored: with
+ * one 16-byte item in flight per thread the copy stalls on memory latency
+ * (ncu: long-scoreboard stalls, DRAM well below its peak). */
+#define P2_SLAB_UNROLL 4
+
 template <typename T, bool PUT>
 __global__ void __launch_bounds__(256) k_slab_copy(T *__restrict__ st,
 	T *__restrict__ buf, uint32_t bit, uint64_t val, uint64_t first,
 	uint64_t count)
 {
-	const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-	for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-		k < count; k += stride) {
-		const uint64_t i = p2_half_index(first + k, bit, val);
-		if (PUT)
-			st[i] = buf[k];
-		else
-			buf[k] = st[i];
+	const uint64_t nt = (uint64_t)gridDim.x * blockDim.x;
+	for (uint64_t k0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+		k0 < count; k0 += nt * P2_SLAB_UNROLL) {
+		T v[P2_SLAB_UNROLL];
+#pragma unroll
+		for (int u = 0; u < P2_SLAB_UNROLL; ++u) {
+			const uint64_t k = k0 + u * nt;
+			if (k < count)
+				v[u] = PUT ? buf[k]
+					   : st[p2_half_index(first + k, bit, val)];
+		}
+#pragma unroll
+		for (int u = 0; u < P2_SLAB_UNROLL; ++u) {
+			const uint64_t k = k0 + u * nt;
+			if (k < count) {
+				if (PUT)
+					st[p2_half_index(first + k, bit, val)] = v[u];
+				else
+					buf[k] = v[u];
+			}
+		}
+	}
+}
+
+/* Exchange element j of half (bit, va) of a with element j of half (bit,
+ * vb) of b, for j < count (units of T as in k_slab_copy). */
+template <typename T>
+__global__ void __launch_bounds__(256) k_slab_swap(T *__restrict__ a,
+	T *__restrict__ b, uint32_t bit, uint64_t va, uint64_t vb,
+	uint64_t count)
+{
+	const uint64_t nt = (uint64_t)gridDim.x * blockDim.x;
+	for (uint64_t j0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+		j0 < count; j0 += nt * P2_SLAB_UNROLL) {
+		T x[P2_SLAB_UNROLL], y[P2_SLAB_UNROLL];
+#pragma unroll
+		for (int u = 0; u < P2_SLAB_UNROLL; ++u) {
+			const uint64_t j = j0 + u * nt;
+			if (j < count) {
+				x[u] = a[p2_half_index(j, bit, va)];
+				y[u] = b[p2_half_index(j, bit, vb)];
+			}
+		}
+#pragma unroll
+		for (int u = 0; u < P2_SLAB_UNROLL; ++u) {
+			const uint64_t j = j0 + u * nt;
+			if (j < count) {
+				a[p2_half_index(j, bit, va)] = y[u];
+				b[p2_half_index(j, bit, vb)] = x[u];
+			}
+		}
 	}
 }
 
@@ -138,6 +191,18 @@ extern "C" int p2d_slab_copy(struct p2_dev *d, uint32_t bit, uint32_t val,
 		else
 			k_slab_copy<double2, false><<<grid, 256, 0, d->stream>>>(
 				st, b, bit, val, first, count);
+	} else if (bit >= 1 && first % 2 == 0 && count % 2 == 0 &&
+		(uintptr_t)buf % 16 == 0) {
+		/* pairs of FP32 amplitudes: 16-byte accesses; bit - 1 is the
+		 * bit's position in pair units */
+		float4 *st = (float4 *)d->state, *b = (float4 *)buf;
+		const unsigned g2 = grid_for(d, count / 2, 256, 8);
+		if (put)
+			k_slab_copy<float4, true><<<g2, 256, 0, d->stream>>>(
+				st, b, bit - 1, val, first / 2, count / 2);
+		else
+			k_slab_copy<float4, false><<<g2, 256, 0, d->stream>>>(
+				st, b, bit - 1, val, first / 2, count / 2);
 	} else {
 		float2 *st = (float2 *)d->state, *b = (float2 *)buf;
 		if (put)
@@ -150,5 +215,48 @@ extern "C" int p2d_slab_copy(struct p2_dev *d, uint32_t bit, uint32_t val,
 	CUDA_OK(cudaGetLastError(), "slab copy launch");
 	d->launches++;
 	CUDA_OK(cudaStreamSynchronize(d->stream), "slab copy");
+	return 0;
+}
+
+extern "C" int p2d_slab_swap(struct p2_dev *a, struct p2_dev *b,
+	uint32_t bit, uint32_t va, uint32_t vb)
+{
+	if (a == b || a->nqb != b->nqb || a->prec != b->prec) {
+		log_error("qreg_slab_swap: needs two registers of one size and"
+			  " precision");
+		return -1;
+	}
+	if (bit >= a->nqb || va > 1 || vb > 1) {
+		log_error("qreg_slab_swap: bit %u / values %u %u outside a"
+			  " %u-qubit register", bit, va, vb, a->nqb);
+		return -1;
+	}
+	cudaPointerAttributes pa, pb;
+	CUDA_OK(cudaPointerGetAttributes(&pa, a->state), "slab swap: state a");
+	CUDA_OK(cudaPointerGetAttributes(&pb, b->state), "slab swap: state b");
+	if (pa.device != pb.device) {
+		log_error("qreg_slab_swap: registers on devices %d and %d",
+			pa.device, pb.device);
+		return -1;
+	}
+	/* b's queued work first; the swap itself runs on a's stream */
+	CUDA_OK(cudaStreamSynchronize(b->stream), "slab swap: stream b");
+	const uint64_t nhalf = a->namp >> 1;
+	if (a->prec == PHASE2_PREC_FP64) {
+		k_slab_swap<double2><<<grid_for(a, nhalf, 256, 8), 256, 0,
+			a->stream>>>((double2 *)a->state, (double2 *)b->state,
+			bit, va, vb, nhalf);
+	} else if (bit >= 1) {
+		k_slab_swap<float4><<<grid_for(a, nhalf / 2, 256, 8), 256, 0,
+			a->stream>>>((float4 *)a->state, (float4 *)b->state,
+			bit - 1, va, vb, nhalf / 2);
+	} else {
+		k_slab_swap<float2><<<grid_for(a, nhalf, 256, 8), 256, 0,
+			a->stream>>>((float2 *)a->state, (float2 *)b->state,
+			bit, va, vb, nhalf);
+	}
+	CUDA_OK(cudaGetLastError(), "slab swap launch");
+	a->launches++;
+	CUDA_OK(cudaStreamSynchronize(a->stream), "slab swap");
 	return 0;
 }

@@ -40,7 +40,9 @@ send/recv through torch.distributed between GPUs; gloo on CPU), and
 qreg_slab_put scatters the received chunk into the same places.  Two send
 buffers alternate: chunk k+1 is gathered while chunk k is in flight, and
 chunk k is scattered after that, so between GPUs the HBM gather and
-scatter hide behind the NVLink transfer.  One
+scatter hide behind the NVLink transfer.  When both ranks of a pair live
+in this process on one GPU, qreg_slab_swap trades the two halves in place
+instead (one read and one write of each, no buffers).  One
 process may also hold several ranks (LocalTransport): their exchange is a
 hand-over of buffers, which runs a sharded register on one GPU.
 """
@@ -162,6 +164,12 @@ class CudaSlab:
                                  count, C.c_void_p(buf.data_ptr())):
             raise RuntimeError("qreg_slab_put failed")
 
+    def swap_halves(self, other: "CudaSlab", bit, val, other_val) -> None:
+        if self._L.qreg_slab_swap(C.byref(self.reg.reg),
+                                  C.byref(other.reg.reg), bit, val,
+                                  other_val):
+            raise RuntimeError("qreg_slab_swap failed")
+
 
 # ---- transports: how paired ranks trade their halves ------------------
 
@@ -232,7 +240,7 @@ class ShardedRegister:
     take global qubit indices."""
 
     def __init__(self, nqb: int, world: int, slabs: dict, transport,
-                 chunk: int = CHUNK):
+                 chunk: int = CHUNK, in_place: bool = True):
         g = _log2_exact(world)
         if not slabs or any(not 0 <= r < world for r in slabs):
             raise ValueError("slab ranks outside the world")
@@ -246,6 +254,10 @@ class ShardedRegister:
             raise ValueError("chunk must be positive")
         self.nqb, self.world, self.nlocal = nqb, world, nqb - g
         self.slabs, self.transport, self.chunk = dict(slabs), transport, chunk
+        # pairs held by this process trade halves in place
+        self.in_place = (in_place and isinstance(transport, LocalTransport)
+                         and all(hasattr(s, "swap_halves")
+                                 for s in self.slabs.values()))
         self.layout = Layout(nqb, self.nlocal)
         self.swaps = 0           # qubit swaps performed
         self.exchanged = 0       # amplitudes this process sent
@@ -253,12 +265,13 @@ class ShardedRegister:
     # -- construction
     @classmethod
     def on_one_gpu(cls, nqb: int, world: int, prec: int | None = None,
-                   chunk: int = CHUNK) -> "ShardedRegister":
+                   chunk: int = CHUNK,
+                   in_place: bool = True) -> "ShardedRegister":
         """All `world` ranks in this process, on the current GPU."""
         world_ensure()
         g = _log2_exact(world)
         slabs = {r: CudaSlab(nqb - g, prec) for r in range(world)}
-        return cls(nqb, world, slabs, LocalTransport(), chunk)
+        return cls(nqb, world, slabs, LocalTransport(), chunk, in_place)
 
     @classmethod
     def distributed(cls, nqb: int, prec: int | None = None, group=None,
@@ -352,6 +365,15 @@ class ShardedRegister:
         mask = 1 << b
         nhalf = 1 << (self.nlocal - 1)
         val = {r: 1 - (r >> b & 1) for r in self.slabs}
+        if self.in_place:
+            for r, slab in self.slabs.items():
+                if r < r ^ mask:
+                    slab.swap_halves(self.slabs[r ^ mask], l, val[r],
+                                     val[r ^ mask])
+            self.exchanged += nhalf * len(self.slabs)
+            self.layout.swap(h, l)
+            self.swaps += 1
+            return
         count0 = min(self.chunk, nhalf)
         bufs = [{r: s.buffer(count0) for r, s in self.slabs.items()}, None]
         pending = None

@@ -4,9 +4,10 @@ Each rank's slab here is a numpy array rotated by the oracle (test
 infrastructure), so these tests check the host logic of the sharding: the
 qubit layout, the choice and execution of qubit swaps, the per-rank sign
 of Z on high qubits, chunked half-slab exchange, state preparation and
-overlaps.  Virtual ranks in one process and two gloo ranks must reproduce
-the oracle's full-register results bit for bit.  The CUDA slabs are
-checked in test_parity_gpu.py.
+overlaps.  Virtual ranks in one process (in-place pair swaps and chunked
+buffers) and two or four gloo ranks must reproduce the oracle's
+full-register results bit for bit.  The CUDA slabs are checked in
+test_sharded_gpu.py.
 """
 
 import os
@@ -63,12 +64,20 @@ class OracleSlab:
         flat[first:first + count] = buf.numpy().view(np.complex128)
         v[...] = flat.reshape(v.shape)
 
+    def swap_halves(self, other, bit, val, other_val):
+        x = self.a.reshape(-1, 2, 1 << bit)[:, val, :]
+        y = other.a.reshape(-1, 2, 1 << bit)[:, other_val, :]
+        t = x.copy()
+        x[...] = y
+        y[...] = t
 
-def _local_reg(nqb, world, oracle, chunk=sharded.CHUNK):
+
+def _local_reg(nqb, world, oracle, chunk=sharded.CHUNK, in_place=True):
     g = world.bit_length() - 1
     slabs = {r: OracleSlab(nqb - g, oracle) for r in range(world)}
     return sharded.ShardedRegister(nqb, world, slabs,
-                                   sharded.LocalTransport(), chunk)
+                                   sharded.LocalTransport(), chunk,
+                                   in_place)
 
 
 def _narrow_terms(nqb, n, max_flip, seed):
@@ -109,13 +118,15 @@ def test_layout_maps_are_inverse():
     assert all(lay.at[lay.pos[q]] == q for q in range(9))
 
 
+@pytest.mark.parametrize("in_place", [True, False])
 @pytest.mark.parametrize("world", [1, 2, 4, 8])
-def test_rotations_bitwise_equal_full_register(oracle_lib, world):
+def test_rotations_bitwise_equal_full_register(oracle_lib, world, in_place):
     nqb = 9
     flip, phase, phi = _narrow_terms(nqb, 120, 3, seed=11)
     amp = _start_state(nqb, 5)
     want = oracle_lib.rotate(amp, nqb, flip, phase, phi)
-    reg = _local_reg(nqb, world, oracle_lib)
+    reg = _local_reg(nqb, world, oracle_lib, in_place=in_place)
+    assert reg.in_place == in_place
     _load(reg, amp)
     reg.paulirot(flip, phase, phi)
     got = reg.get_state()
@@ -131,7 +142,7 @@ def test_chunked_exchange_same_bits(oracle_lib, chunk):
     flip, phase, phi = _narrow_terms(nqb, 60, 4, seed=12)
     amp = _start_state(nqb, 6)
     want = oracle_lib.rotate(amp, nqb, flip, phase, phi)
-    reg = _local_reg(nqb, world, oracle_lib, chunk=chunk)
+    reg = _local_reg(nqb, world, oracle_lib, chunk=chunk, in_place=False)
     _load(reg, amp)
     reg.paulirot(flip, phase, phi)
     assert np.array_equal(reg.get_state(), want)

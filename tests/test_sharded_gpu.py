@@ -43,14 +43,17 @@ def _load(reg, amp):
     reg.prepst(Dets(np.arange(len(amp), dtype=np.uint64), amp))
 
 
+@pytest.mark.parametrize("in_place", [True, False])
 @pytest.mark.parametrize("world", [2, 4, 8])
-def test_fp64_rotations_bitwise(oracle_lib, world):
+def test_fp64_rotations_bitwise(oracle_lib, world, in_place):
     nqb = 13
     flip, phase, phi = _narrow_terms(nqb, 300, 4, seed=41)
     amp = _start_state(nqb, 42)
     want = oracle_lib.rotate(amp, nqb, flip, phase, phi)
     with sharded.ShardedRegister.on_one_gpu(nqb, world, p2.PREC_FP64,
-                                            chunk=1000) as reg:
+                                            chunk=1000,
+                                            in_place=in_place) as reg:
+        assert reg.in_place == in_place
         _load(reg, amp)
         reg.paulirot(flip, phase, phi)
         got = reg.get_state()
@@ -75,12 +78,15 @@ def test_fp64_trott_equals_unsharded_engine(oracle_lib, order2):
     assert np.array_equal(got.view(np.float64), ref.view(np.float64))
 
 
-def test_fp32_within_tolerance(oracle_lib):
+@pytest.mark.parametrize("in_place", [True, False])
+def test_fp32_within_tolerance(oracle_lib, in_place):
     nqb = 16
     flip, phase, phi = _narrow_terms(nqb, 200, 4, seed=45)
     amp = _start_state(nqb, 46)
     want = oracle_lib.rotate(amp, nqb, flip, phase, phi)
-    with sharded.ShardedRegister.on_one_gpu(nqb, 4, p2.PREC_FP32) as reg:
+    with sharded.ShardedRegister.on_one_gpu(nqb, 4, p2.PREC_FP32,
+                                            chunk=777,
+                                            in_place=in_place) as reg:
         _load(reg, amp)
         reg.paulirot(flip, phase, phi)
         got = reg.get_state()
@@ -98,23 +104,27 @@ def test_slab_get_put_roundtrip(prec):
         dt = torch.float64 if fp64 else torch.float32
         cdt = np.complex128 if fp64 else np.complex64
         cur = amp.astype(cdt)
-        for bit in (0, 3, nqb - 1):
+        # even offsets and counts take the 16-byte path of FP32 halves
+        # with bit >= 1; odd ones and bit 0 the per-amplitude path
+        for bit in (0, 1, 3, nqb - 1):
             for val in (0, 1):
-                half = cur.reshape(-1, 2, 1 << bit)[:, val, :].reshape(-1)
-                buf = torch.empty(2 * 300, dtype=dt, device="cuda")
-                assert L.qreg_slab_get(C.byref(r.reg), bit, val, 100, 300,
-                                       C.c_void_p(buf.data_ptr())) == 0
-                got = buf.cpu().numpy().view(cdt)
-                assert np.array_equal(got, half[100:400])
-                new = (got * 1j).astype(cdt)
-                buf.copy_(torch.from_numpy(new.view(
-                    np.float64 if fp64 else np.float32)).cuda())
-                assert L.qreg_slab_put(C.byref(r.reg), bit, val, 100, 300,
-                                       C.c_void_p(buf.data_ptr())) == 0
-                v = cur.reshape(-1, 2, 1 << bit)[:, val, :]
-                flat = v.reshape(-1).copy()
-                flat[100:400] = new
-                v[...] = flat.reshape(v.shape)
+                for a, n in ((100, 300), (101, 299)):
+                    half = cur.reshape(-1, 2, 1 << bit)[:, val, :]
+                    half = half.reshape(-1)
+                    buf = torch.empty(2 * n, dtype=dt, device="cuda")
+                    assert L.qreg_slab_get(C.byref(r.reg), bit, val, a, n,
+                                           C.c_void_p(buf.data_ptr())) == 0
+                    got = buf.cpu().numpy().view(cdt)
+                    assert np.array_equal(got, half[a:a + n])
+                    new = (got * 1j).astype(cdt)
+                    buf.copy_(torch.from_numpy(new.view(
+                        np.float64 if fp64 else np.float32)).cuda())
+                    assert L.qreg_slab_put(C.byref(r.reg), bit, val, a, n,
+                                           C.c_void_p(buf.data_ptr())) == 0
+                    v = cur.reshape(-1, 2, 1 << bit)[:, val, :]
+                    flat = v.reshape(-1).copy()
+                    flat[a:a + n] = new
+                    v[...] = flat.reshape(v.shape)
                 st = r.get_state()
                 assert np.array_equal(st.astype(cdt), cur)
 
@@ -142,3 +152,38 @@ def test_slab_errors_copy_nothing():
         assert r.norm2() == 0.0
         torch.cuda.synchronize()
         assert torch.count_nonzero(small).item() == 0
+
+
+@pytest.mark.parametrize("prec", [p2.PREC_FP64, p2.PREC_FP32])
+def test_slab_swap_in_place(prec):
+    nqb = 10
+    x, y = _start_state(nqb, 48), _start_state(nqb, 49)
+    L = lib()
+    with Register(nqb, prec) as a, Register(nqb, prec) as b:
+        cdt = np.complex128 if a.precision == p2.PREC_FP64 else np.complex64
+        xa, yb = x.astype(cdt), y.astype(cdt)
+        a.set_state(x)
+        b.set_state(y)
+        for bit, va, vb in ((0, 1, 0), (1, 0, 1), (4, 1, 1), (nqb - 1, 0, 0)):
+            assert L.qreg_slab_swap(C.byref(a.reg), C.byref(b.reg), bit,
+                                    va, vb) == 0
+            hx = xa.reshape(-1, 2, 1 << bit)[:, va, :]
+            hy = yb.reshape(-1, 2, 1 << bit)[:, vb, :]
+            t = hx.copy()
+            hx[...] = hy
+            hy[...] = t
+            assert np.array_equal(a.get_state().astype(cdt), xa)
+            assert np.array_equal(b.get_state().astype(cdt), yb)
+
+
+def test_slab_swap_errors():
+    L = lib()
+    with Register(8, p2.PREC_FP64) as a, Register(9, p2.PREC_FP64) as b, \
+            Register(8, p2.PREC_FP32) as c:
+        a.set_state(_start_state(8, 50))
+        before = a.get_state()
+        assert L.qreg_slab_swap(C.byref(a.reg), C.byref(a.reg), 0, 0, 1) == -1
+        assert L.qreg_slab_swap(C.byref(a.reg), C.byref(b.reg), 0, 0, 1) == -1
+        assert L.qreg_slab_swap(C.byref(a.reg), C.byref(c.reg), 0, 0, 1) == -1
+        assert L.qreg_slab_swap(C.byref(a.reg), C.byref(a.reg), 8, 0, 1) == -1
+        assert np.array_equal(a.get_state(), before)
