@@ -50,10 +50,11 @@ hand-over of buffers, which runs a sharded register on one GPU.
 from __future__ import annotations
 
 import ctypes as C
+import math
 
 import numpy as np
 
-from . import PREC_FP64, Dets, Register, Terms, _hamil, world_ensure
+from . import PREC_FP64, Dets, Register, Terms, _ffi, _hamil, world_ensure
 from ._ffi import lib
 
 #: default exchange chunk, in amplitudes (1 GiB of FP64 per buffer)
@@ -492,4 +493,51 @@ def trott(reg: ShardedRegister, terms: Terms, dets: Dets, steps: int,
         if order2:
             reg.paulirot(*rev)
         out[s] = reg.measure(dets)
+    return out
+
+
+def _sign_dz(a: np.ndarray) -> np.ndarray:
+    """|a| < DBL_EPSILON -> 0, else -1 or +1 (circ/internal.h:26-32)."""
+    f = np.abs(a)
+    return np.where(f < np.finfo(np.float64).eps, 0.0,
+                    np.where(a < f, -1.0, 1.0))
+
+
+def qdrift(reg: ShardedRegister, terms: Terms, dets: Dets, samples: int,
+           depth: int, step_size: float, seed: int) -> np.ndarray:
+    """qdrift_simul on a sharded register (circ/qdrift.c:95-134): per
+    sample, state preparation, `depth` draws from the |c| CDF with the
+    library's prob_cdf and xoshiro256** (the draws of qdrift_simul for the
+    same seed), rotations at asin(step_size) sign_dz(c), one overlap.
+    Every rank draws the same sequence.  seed must be non-zero: the
+    library's qdrift replaces 0 by the last non-zero seed it was given,
+    which is process state."""
+    if seed == 0:
+        raise ValueError("seed must be non-zero")
+    if len(terms) == 0 or depth < 0 or samples < 0:
+        raise ValueError("no terms, or a negative depth or sample count")
+    L = lib()
+    cf = np.ascontiguousarray(terms.cf, dtype=np.float64)
+    cdf = _ffi.ProbCdf()
+    if L.prob_cdf_init(C.byref(cdf), len(cf)) != 0:
+        raise MemoryError("prob_cdf_init")
+    out = np.zeros(samples, dtype=np.complex128)
+    try:
+        L.prob_cdf_from_array_strided(
+            C.byref(cdf), cf.ctypes.data_as(C.POINTER(C.c_double)), 8,
+            None)
+        rng = _ffi.Xoshiro()
+        L.xoshiro256ss_init(C.byref(rng), seed)
+        omega = math.asin(step_size)
+        k = np.empty(depth, dtype=np.int64)
+        for s in range(samples):
+            reg.prepst(dets)
+            for i in range(depth):
+                x = (L.xoshiro256ss_next(C.byref(rng)) >> 11) * 2.0 ** -53
+                k[i] = L.prob_cdf_inverse(C.byref(cdf), x)
+            reg.paulirot(terms.flip[k], terms.phase[k],
+                         omega * _sign_dz(cf[k]))
+            out[s] = reg.measure(dets)
+    finally:
+        L.prob_cdf_free(C.byref(cdf))
     return out

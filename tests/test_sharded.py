@@ -189,6 +189,25 @@ def test_trott_overlaps_bitwise(oracle_lib, order2):
     assert np.array_equal(got.view(np.float64), want.view(np.float64))
 
 
+@pytest.mark.parametrize("world", [2, 4])
+def test_qdrift_overlaps_bitwise(oracle_lib, world):
+    nqb = 10
+    terms = workloads.jw_terms(nqb, 80, seed=23)
+    dets = workloads.hamming_dets(nqb, 2, 5, seed=24)
+    want = oracle_lib.qdrift(nqb, terms.flip, terms.phase, terms.cf,
+                             dets.idx, dets.cf, 3, 40, 0.01, 0xD41F7)
+    reg = _local_reg(nqb, world, oracle_lib)
+    got = sharded.qdrift(reg, terms, dets, 3, 40, 0.01, 0xD41F7)
+    assert np.array_equal(got.view(np.float64), want.view(np.float64))
+    assert reg.swaps > 0
+    with pytest.raises(ValueError):
+        sharded.qdrift(reg, terms, dets, 1, 4, 0.01, 0)
+    eps = np.finfo(np.float64).eps
+    assert list(sharded._sign_dz(np.array(
+        [eps, eps / 2, -eps / 2, -eps, 0.0, -0.0, 3.0, -2.0]))) == \
+        [1.0, 0.0, 0.0, -1.0, 0.0, 0.0, 1.0, -1.0]
+
+
 def test_errors(oracle_lib):
     with pytest.raises(ValueError):
         _local_reg(4, 3, oracle_lib)  # not a power of two

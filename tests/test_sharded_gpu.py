@@ -78,6 +78,22 @@ def test_fp64_trott_equals_unsharded_engine(oracle_lib, order2):
     assert np.array_equal(got.view(np.float64), ref.view(np.float64))
 
 
+def test_fp64_qdrift_equals_unsharded_engine(oracle_lib):
+    nqb = 14
+    terms = workloads.jw_terms(nqb, 500, seed=51)
+    dets = workloads.hamming_dets(nqb, 1, 7, seed=52)
+    p2.set_precision(p2.PREC_FP64)
+    want = p2.qdrift(nqb, terms, dets, 2, 300, 1e-2, 0x5EED51)
+    ref = oracle_lib.qdrift(nqb, terms.flip, terms.phase, terms.cf,
+                            dets.idx, dets.cf, 2, 300, 1e-2, 0x5EED51)
+    with sharded.ShardedRegister.on_one_gpu(nqb, 4, p2.PREC_FP64) as reg:
+        got = sharded.qdrift(reg, terms, dets, 2, 300, 1e-2, 0x5EED51)
+        assert reg.swaps > 0
+    assert np.array_equal(np.asarray(want).view(np.float64),
+                          ref.view(np.float64))
+    assert np.array_equal(got.view(np.float64), ref.view(np.float64))
+
+
 @pytest.mark.parametrize("in_place", [True, False])
 def test_fp32_within_tolerance(oracle_lib, in_place):
     nqb = 16
