@@ -164,10 +164,26 @@ struct trott;
 struct trott2;
 struct qdrift;
 struct cmpsit;
+struct cmpsit_data;
+struct cmpsit_ranct;
 int trott_simul_batch(struct trott *const *tts, size_t n);
 int trott2_simul_batch(struct trott2 *const *t2s, size_t n);
 int qdrift_simul_batch(struct qdrift *const *qds, size_t n);
 int cmpsit_simul_batch(struct cmpsit *const *cps, size_t n);
+
+/*
+ * The composite driver's term split alone, without a circuit or register:
+ * the first dt->length terms by |c| descending (then in the term order of
+ * phase2_set_term_order) into rc->hm_det, the rest into rc->hm_ran with
+ * its |c| CDF in rc->cdf and lambda_r (circ/cmpsit.c:65-111), exactly as
+ * cmpsit_init splits them.  For drivers above the C surface that apply the
+ * same rotations to a register of their own (sharded registers).  Needs
+ * dt->length < hm->len; 0 or -1.  cmpsit_ranct_free releases it
+ * (idempotent).
+ */
+int cmpsit_ranct_init(struct cmpsit_ranct *rc, const struct circ_hamil *hm,
+	const struct cmpsit_data *dt);
+void cmpsit_ranct_free(struct cmpsit_ranct *rc);
 
 /* ---- execution control and bulk access ---------------------------------- */
 

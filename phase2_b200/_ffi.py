@@ -269,6 +269,9 @@ _SIGS = {
                               C.c_int, C.c_void_p, C.c_void_p]),
     "cmpsit_free": (None, [_P(Cmpsit)]),
     "cmpsit_simul": (C.c_int, [_P(Cmpsit)]),
+    "cmpsit_ranct_init": (C.c_int, [_P(CmpsitRanct), _P(CircHamil),
+                                    _P(CmpsitData)]),
+    "cmpsit_ranct_free": (None, [_P(CmpsitRanct)]),
     "prob_cdf_init": (C.c_int, [_P(ProbCdf), C.c_size_t]),
     "prob_cdf_free": (None, [_P(ProbCdf)]),
     "prob_cdf_from_array_strided": (C.c_int, [_P(ProbCdf), _P(C.c_double),

@@ -439,6 +439,25 @@ fail_tmp:
 	return -1;
 }
 
+int cmpsit_ranct_init(struct cmpsit_ranct *rc, const struct circ_hamil *hm,
+	const struct cmpsit_data *dt)
+{
+	memset(rc, 0, sizeof *rc);
+	if (!hm || !dt || !hm->terms || dt->length >= hm->len) {
+		log_error("cmpsit_ranct_init: needs more terms than length");
+		return -1;
+	}
+	return cmpsit_split(rc, hm, dt);
+}
+
+void cmpsit_ranct_free(struct cmpsit_ranct *rc)
+{
+	circ_hamil_free(&rc->hm_smpl);
+	circ_hamil_free(&rc->hm_ran);
+	circ_hamil_free(&rc->hm_det);
+	prob_cdf_free(&rc->cdf);
+}
+
 int cmpsit_init(struct cmpsit *cp, const struct cmpsit_data *dt,
 	struct circ_hamil hm, enum stprep_kind sp_kind, const void *sp_data,
 	struct phase2_step_writer *sw)

@@ -541,3 +541,63 @@ def qdrift(reg: ShardedRegister, terms: Terms, dets: Dets, samples: int,
     finally:
         L.prob_cdf_free(C.byref(cdf))
     return out
+
+
+def _hamil_terms(hm) -> Terms:
+    n = int(hm.len)
+    rec = np.zeros(n, dtype=[("cf", "<f8"), ("flip", "<u8"),
+                             ("phase", "<u8")])
+    if n:
+        C.memmove(rec.ctypes.data, hm.terms, rec.nbytes)
+    return Terms(rec["flip"].copy(), rec["phase"].copy(), rec["cf"].copy())
+
+
+def cmpsit(reg: ShardedRegister, terms: Terms, dets: Dets, samples: int,
+           steps: int, length: int, depth: int, angle_det: float,
+           angle_rand: float, seed: int) -> np.ndarray:
+    """cmpsit_simul on a sharded register (circ/cmpsit.c:151-235): the
+    library's own split (cmpsit_ranct_init: the `length` largest |c| as
+    the deterministic head at c angle_det, the rest sampled through its
+    |c| CDF at sign_dz(c) angle_rand); per sample, state preparation, then
+    per step a fresh sample applied forward at 0.5 and another applied in
+    reverse at 0.5; one overlap per sample.  seed must be non-zero (see
+    qdrift)."""
+    if seed == 0:
+        raise ValueError("seed must be non-zero")
+    L = lib()
+    hm = _hamil(reg.nqb, terms)
+    rc = _ffi.CmpsitRanct()
+    dt = _ffi.CmpsitData(samples, steps, length, depth, angle_det,
+                         angle_rand, seed)
+    out = np.zeros(samples, dtype=np.complex128)
+    try:
+        if L.cmpsit_ranct_init(C.byref(rc), C.byref(hm), C.byref(dt)):
+            raise ValueError("cmpsit split failed (length >= terms?)")
+        det = _hamil_terms(rc.hm_det)
+        ran = _hamil_terms(rc.hm_ran)
+        det_phi = det.cf * angle_det
+        rng = _ffi.Xoshiro()
+        L.xoshiro256ss_init(C.byref(rng), seed)
+        k = np.empty(depth, dtype=np.int64)
+
+        def sample():
+            for i in range(depth):
+                x = (L.xoshiro256ss_next(C.byref(rng)) >> 11) * 2.0 ** -53
+                k[i] = L.prob_cdf_inverse(C.byref(rc.cdf), x)
+            return (np.concatenate([det.flip, ran.flip[k]]),
+                    np.concatenate([det.phase, ran.phase[k]]),
+                    np.concatenate([det_phi,
+                                    _sign_dz(ran.cf[k]) * angle_rand]))
+
+        for s in range(samples):
+            reg.prepst(dets)
+            for _ in range(steps):
+                f, p, c = sample()
+                reg.paulirot(f, p, 0.5 * c)
+                f, p, c = sample()
+                reg.paulirot(f[::-1], p[::-1], 0.5 * c[::-1])
+            out[s] = reg.measure(dets)
+    finally:
+        L.cmpsit_ranct_free(C.byref(rc))
+        L.circ_hamil_free(C.byref(hm))
+    return out

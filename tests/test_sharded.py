@@ -208,6 +208,21 @@ def test_qdrift_overlaps_bitwise(oracle_lib, world):
         [1.0, 0.0, 0.0, -1.0, 0.0, 0.0, 1.0, -1.0]
 
 
+@pytest.mark.parametrize("world", [2, 4])
+def test_cmpsit_overlaps_bitwise(oracle_lib, world):
+    nqb = 10
+    terms = workloads.jw_terms(nqb, 90, seed=25)
+    dets = workloads.hamming_dets(nqb, 3, 5, seed=26)
+    args = (2, 2, 12, 20, 0.05, 0.003, 0xC0317)
+    want = oracle_lib.cmpsit(nqb, terms.flip, terms.phase, terms.cf,
+                             dets.idx, dets.cf, *args)
+    reg = _local_reg(nqb, world, oracle_lib)
+    got = sharded.cmpsit(reg, terms, dets, *args)
+    assert np.array_equal(got.view(np.float64), want.view(np.float64))
+    with pytest.raises(ValueError):
+        sharded.cmpsit(reg, terms, dets, 1, 1, 90, 4, 0.05, 0.003, 7)
+
+
 def test_errors(oracle_lib):
     with pytest.raises(ValueError):
         _local_reg(4, 3, oracle_lib)  # not a power of two

@@ -94,6 +94,22 @@ def test_fp64_qdrift_equals_unsharded_engine(oracle_lib):
     assert np.array_equal(got.view(np.float64), ref.view(np.float64))
 
 
+def test_fp64_cmpsit_equals_unsharded_engine(oracle_lib):
+    nqb = 13
+    terms = workloads.jw_terms(nqb, 400, seed=53)
+    dets = workloads.hamming_dets(nqb, 4, 6, seed=54)
+    args = (2, 2, 40, 60, 0.05, 0.002, 0xC3317)
+    p2.set_precision(p2.PREC_FP64)
+    want = p2.cmpsit(nqb, terms, dets, *args)
+    ref = oracle_lib.cmpsit(nqb, terms.flip, terms.phase, terms.cf,
+                            dets.idx, dets.cf, *args)
+    with sharded.ShardedRegister.on_one_gpu(nqb, 2, p2.PREC_FP64) as reg:
+        got = sharded.cmpsit(reg, terms, dets, *args)
+    assert np.array_equal(np.asarray(want).view(np.float64),
+                          ref.view(np.float64))
+    assert np.array_equal(got.view(np.float64), ref.view(np.float64))
+
+
 @pytest.mark.parametrize("in_place", [True, False])
 def test_fp32_within_tolerance(oracle_lib, in_place):
     nqb = 16
