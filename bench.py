@@ -359,6 +359,8 @@ def gpu_arm(args) -> None:
             extra["sampling"] = sampling_study()
         if "sweeps" in studies:
             extra["sweeps"] = sweeps_study()
+        if "sharded" in studies:
+            extra["sharded"] = sharded_study()
     if rank != 0:
         return
     clocks = clk.summary()
@@ -838,10 +840,10 @@ def main() -> None:
     ap.add_argument("--cmp-depth", type=int, default=512)
     ap.add_argument("--quick", action="store_true",
                     help="skip the CPU baseline and secondary arms")
-    ap.add_argument("--studies", default="batched,trott26",
+    ap.add_argument("--studies", default="batched,trott26,sharded",
                     help="comma list of studies to append: batched, "
-                         "trott26, cmpsit33 (takes minutes), sampling, "
-                         "sweeps")
+                         "trott26, sharded, cmpsit33 (takes minutes), "
+                         "sampling, sweeps")
     ap.add_argument("--only-study", default=None,
                     help="run just this study (batched, trott26, cmpsit33, "
                          "batch8, batch8fp64, sampling, sweeps, sharded) "
