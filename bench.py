@@ -348,19 +348,17 @@ def gpu_arm(args) -> None:
                 extra["fp32_error"][fname] = fp32_error_study()
             finally:
                 p2.set_fp32_form(form0)
-        studies = set(args.studies.split(",")) if args.studies else set()
-        if "batched" in studies:
-            extra["batched"] = batched_study()
-        if "trott26" in studies:
-            extra["trott26"] = trott26_study()
-        if "cmpsit33" in studies:
-            extra["cmpsit33"] = cmpsit33_study()
-        if "sampling" in studies:
-            extra["sampling"] = sampling_study()
-        if "sweeps" in studies:
-            extra["sweeps"] = sweeps_study()
-        if "sharded" in studies:
-            extra["sharded"] = sharded_study()
+        studies = args.studies.split(",") if args.studies else []
+        for name in ("batched", "trott26", "cmpsit33", "sampling", "sweeps",
+                     "sharded"):
+            if name not in studies:
+                continue
+            # a study that fails is reported in its slot; the bench line
+            # itself still prints
+            try:
+                extra[name] = globals()[f"{name}_study"]()
+            except Exception as e:  # noqa: BLE001
+                extra[name] = {"error": f"{type(e).__name__}: {e}"}
     if rank != 0:
         return
     clocks = clk.summary()
