@@ -1337,18 +1337,20 @@ extern "C" void *p2d_stream(const struct p2_dev *d)
 
 cudaError_t p2_scratch_alloc(void **p, size_t bytes, cudaStream_t stream)
 {
-	static int pool_ready;
-	if (!pool_ready) {
-		int dev = 0;
+	/* once per device (devices 0..63): keep up to 1 GiB of freed memory
+	 * in the device's default pool */
+	static uint64_t pool_ready;
+	int dev = 0;
+	if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 64 &&
+		!(pool_ready >> dev & 1)) {
 		cudaMemPool_t pool;
-		if (cudaGetDevice(&dev) == cudaSuccess &&
-			cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+		if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
 			uint64_t keep = UINT64_C(1) << 30;
 			cudaMemPoolSetAttribute(pool,
 				cudaMemPoolAttrReleaseThreshold, &keep);
 		}
-		cudaGetLastError();
-		pool_ready = 1;
+		cudaGetLastError(); /* a pool call's failure is not the caller's */
+		pool_ready |= UINT64_C(1) << dev;
 	}
 	return cudaMallocAsync(p, bytes, stream);
 }
