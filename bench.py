@@ -736,7 +736,9 @@ def batched_study(ninst: int = 64, step_cap: int = 4, seed: int = 0xBA7C4):
     Aggregate rot.amp/s over the batch (wall clock around the batch call,
     recording/planning and result download included), once in one
     persistent launch and once on per-instance streams; HBM GB/s counts
-    2 * 2^n * 8 bytes per pass (small instances are partly L2-resident)."""
+    2 * 2^n * 8 bytes per pass, and l2_fit_byte_share is the part of
+    those bytes that belongs to instances whose state fits in L2 (n <= 23),
+    which the L2 can serve instead of HBM."""
     import numpy as np
 
     import phase2_b200 as p2
@@ -771,6 +773,10 @@ def batched_study(ninst: int = 64, step_cap: int = 4, seed: int = 0xBA7C4):
             wall = time.perf_counter() - t0
             hbm = sum(s["bytes"] for s in stats)
             kms = sum(s["pass_ms"] for s in stats)
+            # bytes of instances whose FP32 state fits the 126 MB L2
+            # (n <= 23: 64 MiB); their passes can be served from L2
+            l2 = sum(s["bytes"] for s, pr in zip(stats, probs)
+                     if (1 << pr["nqb"]) * 8 <= 126 * 10 ** 6)
             out[mode] = {
                 "seconds": wall, "value": work / wall,
                 "hbm_gbs_wall": hbm / wall / 1e9,
@@ -780,7 +786,8 @@ def batched_study(ninst: int = 64, step_cap: int = 4, seed: int = 0xBA7C4):
                 "launches": int(sum(s["launches"] for s in stats)),
                 "passes": int(sum(s["passes"] for s in stats)),
                 "graph_replays": int(sum(s["graph_replays"]
-                                         for s in stats))}
+                                         for s in stats)),
+                "l2_fit_byte_share": l2 / hbm if hbm else None}
     finally:
         p2.set_batch_persistent(True)
         p2.set_term_order(order)
