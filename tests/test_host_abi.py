@@ -189,6 +189,41 @@ def test_sort_flip_is_stable():
     L.circ_hamil_free(C.byref(hm))
 
 
+def test_cmpsit_split_matches_oracle(oracle_lib):
+    """cmpsit_ranct_init: the `length` largest |c| lexicographically
+    sorted, the rest in |c|-descending order with their CDF and lambda
+    (circ/cmpsit.c:65-111), the split cmpsit_init makes."""
+    L = lib()
+    t = workloads.jw_terms(12, 300, seed=17)
+    order0 = L.phase2_get_term_order()
+    L.phase2_set_term_order(0)
+    hm = _hamil(12, t)
+    rc = _ffi.CmpsitRanct()
+    dt = _ffi.CmpsitData(1, 1, 40, 8, 0.05, 0.01, 5)
+    try:
+        assert L.cmpsit_ranct_init(C.byref(rc), C.byref(hm),
+                                   C.byref(dt)) == 0
+        idx = np.argsort(-np.abs(t.cf), kind="stable")
+        assert len(np.unique(np.abs(t.cf))) == len(t)  # no ties here
+        head = oracle_lib.sort_lex(t.flip[idx[:40]], t.phase[idx[:40]],
+                                   t.cf[idx[:40]])
+        assert _terms_of(rc.hm_det).tobytes() == head.tobytes()
+        tail = _terms_of(rc.hm_ran)
+        assert np.array_equal(tail["cf"], t.cf[idx[40:]])
+        assert np.array_equal(tail["flip"], t.flip[idx[40:]])
+        _, y, lam = oracle_lib.cdf(t.cf[idx[40:]])
+        got = np.ctypeslib.as_array(rc.cdf.y, shape=(int(rc.cdf.len),))
+        assert np.array_equal(got, y) and rc.lambda_r == lam
+    finally:
+        L.cmpsit_ranct_free(C.byref(rc))
+        L.cmpsit_ranct_free(C.byref(rc))  # idempotent
+        L.phase2_set_term_order(order0)
+    bad = _ffi.CmpsitData(1, 1, 300, 8, 0.05, 0.01, 5)
+    assert L.cmpsit_ranct_init(C.byref(rc), C.byref(hm), C.byref(bad)) == -1
+    L.cmpsit_ranct_free(C.byref(rc))
+    L.circ_hamil_free(C.byref(hm))
+
+
 def _rand_rotations(rng, n, k, diag_frac=0.2):
     t = workloads.random_terms(n, k, seed=int(rng.integers(1 << 30)))
     mask = rng.random(k) < diag_frac
