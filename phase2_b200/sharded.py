@@ -75,6 +75,13 @@ def _popcount(a: np.ndarray) -> np.ndarray:
     return np.bitwise_count(a)
 
 
+def _swap_bits(m: np.ndarray, a: int, b: int) -> None:
+    """Exchange bit positions a and b of every mask in m, in place."""
+    one = np.uint64(1)
+    x = ((m >> np.uint64(a)) ^ (m >> np.uint64(b))) & one
+    m ^= (x << np.uint64(a)) | (x << np.uint64(b))
+
+
 class Layout:
     """Global qubit <-> physical position map of a sharded register."""
 
@@ -316,18 +323,26 @@ class ShardedRegister:
         L = np.uint64(self.nlocal)
         n, k = len(phi), 0
         while k < n:
-            end = min(n, k + _WINDOW)
-            pf = self.layout.phys(flip[k:end])
-            pp = self.layout.phys(phase[k:end])
-            far = np.flatnonzero(pf >> L)
-            stop = end if len(far) == 0 else k + int(far[0])
-            if stop > k:
-                m = stop - k
-                self._apply_local(pf[:m], pp[:m], phi[k:stop])
-            if stop < end:
-                ahead = flip[stop + 1:stop + 1 + _LOOKAHEAD]
-                self._make_local(int(pf[stop - k]), self.layout.phys(ahead))
-            k = stop
+            # map a window plus its look-ahead once; a swap then only
+            # exchanges two bit positions of the mapped masks
+            limit = min(n, k + _WINDOW) - k
+            span = min(n, k + _WINDOW + _LOOKAHEAD)
+            pf = self.layout.phys(flip[k:span])
+            pp = self.layout.phys(phase[k:span])
+            off = 0
+            while off < limit:
+                far = np.flatnonzero(pf[off:limit] >> L)
+                stop = limit if len(far) == 0 else off + int(far[0])
+                if stop > off:
+                    self._apply_local(pf[off:stop], pp[off:stop],
+                                      phi[k + off:k + stop])
+                if stop < limit:
+                    ahead = pf[stop + 1:stop + 1 + _LOOKAHEAD]
+                    for h, l in self._make_local(int(pf[stop]), ahead):
+                        _swap_bits(pf[stop:], h, l)
+                        _swap_bits(pp[stop:], h, l)
+                off = stop
+            k += limit
 
     def _apply_local(self, pf, pp, phi) -> None:
         L = np.uint64(self.nlocal)
@@ -337,17 +352,29 @@ class ShardedRegister:
             odd = _popcount(z_hi & np.uint64(r)) & 1
             slab.paulirot(pf, pp & lo, np.where(odd == 1, -phi, phi))
 
-    def _make_local(self, pflip: int, ahead: np.ndarray) -> None:
+    def _make_local(self, pflip: int, ahead: np.ndarray) -> list:
         """Swap every high position of pflip with a local one outside it;
-        `ahead` holds the physical flips of the rotations that follow."""
+        `ahead` holds the physical flips of the rotations that follow.
+        Returns the (high, local) position pairs swapped, in order."""
         L = self.nlocal
         need = [h for h in range(L, self.nqb) if pflip >> h & 1]
         taken = {p for p in range(L) if pflip >> p & 1}
-        nxt = {}
-        for p in range(L):
-            if p not in taken:
-                hit = np.flatnonzero((ahead >> np.uint64(p)) & np.uint64(1))
-                nxt[p] = int(hit[0]) if len(hit) else len(ahead)
+        # first use of each position ahead: where the running OR of the
+        # flips gains that bit
+        first = {}
+        if len(ahead):
+            cum = np.bitwise_or.accumulate(ahead)
+            gain = cum.copy()
+            gain[1:] ^= cum[:-1]
+            for i in np.flatnonzero(gain):
+                g = int(gain[i])
+                while g:
+                    p = (g & -g).bit_length() - 1
+                    first[p] = int(i)
+                    g &= g - 1
+        nxt = {p: first.get(p, len(ahead)) for p in range(L)
+               if p not in taken}
+        done = []
         for h in need:
             free = [p for p in nxt if p not in taken]
             if not free:
@@ -357,6 +384,8 @@ class ShardedRegister:
             l = max(free, key=lambda p: (nxt[p], p))
             self._swap(h, l)
             taken.add(l)
+            done.append((h, l))
+        return done
 
     def _swap(self, h: int, l: int) -> None:
         """Trade the qubits at high position h and local position l: every
