@@ -295,3 +295,52 @@ def test_gloo_ranks_match_oracle(oracle_lib, world):
         assert np.array_equal(vals, want)
         assert np.array_equal(state, amp)
         assert swaps == res[0][3] and swaps > 0
+
+
+def _subgroup_main(rank, world, port, q):
+    """Four gloo ranks as two sharded registers of two ranks each: ranks
+    {0, 2} and {1, 3}, so a group rank differs from the global one."""
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from oracle import Oracle
+        o = Oracle()
+        groups = [dist.new_group([0, 2]), dist.new_group([1, 3])]
+        grp = groups[rank % 2]
+        grank = dist.get_rank(grp)
+        nqb = 8
+        reg = sharded.ShardedRegister(
+            nqb, 2, {grank: OracleSlab(nqb - 1, o)},
+            sharded.DistTransport(group=grp), chunk=7)
+        terms = workloads.jw_terms(nqb, 30, seed=33 + rank % 2)
+        dets = workloads.hamming_dets(nqb, 2, 3, seed=34)
+        vals = sharded.trott(reg, terms, dets, 2, 0.06)
+        q.put((rank, vals, reg.swaps))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_subgroups_match_oracle(oracle_lib):
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_subgroup_main, args=(r, 4, port, q))
+             for r in range(4)]
+    for p in procs:
+        p.start()
+    res = {r: (v, sw) for r, v, sw in (q.get(timeout=240) for _ in range(4))}
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    nqb = 8
+    dets = workloads.hamming_dets(nqb, 2, 3, seed=34)
+    for parity in (0, 1):
+        terms = workloads.jw_terms(nqb, 30, seed=33 + parity)
+        want = oracle_lib.trott(nqb, terms.flip, terms.phase, terms.cf,
+                                dets.idx, dets.cf, 2, 0.06)
+        for r in (parity, parity + 2):
+            assert np.array_equal(res[r][0], want)
+            assert res[r][1] > 0
