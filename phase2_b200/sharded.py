@@ -159,6 +159,9 @@ class CudaSlab:
     def get_state(self) -> np.ndarray:
         return self.reg.get_state()
 
+    def norm2(self) -> float:
+        return self.reg.norm2()
+
     def synchronize(self) -> None:
         self.reg.synchronize()
 
@@ -477,6 +480,18 @@ class ShardedRegister:
             phys = (np.uint64(r) << np.uint64(self.nlocal)) | k
             full[self.layout.glob(phys)] = slab.get_state()
         return self.transport.sum_over_ranks(full)
+
+    def norm2(self) -> float:
+        """sum |a_i|^2 over all ranks: each rank's device reduction
+        (qreg_norm2), then the ranks' sums added in rank order."""
+        part = np.zeros(self.world, dtype=np.complex128)
+        for r, slab in self.slabs.items():
+            part[r] = slab.norm2()
+        part = self.transport.sum_over_ranks(part)
+        tot = 0.0
+        for v in part.real:
+            tot += float(v)
+        return tot
 
     def synchronize(self) -> None:
         for s in self.slabs.values():

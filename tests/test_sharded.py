@@ -48,6 +48,9 @@ class OracleSlab:
     def get_state(self):
         return self.a.copy()
 
+    def norm2(self):
+        return float(np.sum(np.abs(self.a) ** 2))
+
     def synchronize(self):
         pass
 
@@ -165,6 +168,16 @@ def test_high_z_and_y_only_signs(oracle_lib):
     reg.paulirot(flip[1:], phase[1:], phi[1:])
     assert reg.swaps == 2
     assert np.array_equal(reg.get_state(), want)
+
+
+def test_norm2_over_ranks(oracle_lib):
+    nqb = 9
+    flip, phase, phi = _narrow_terms(nqb, 50, 3, seed=13)
+    amp = 0.7 * _start_state(nqb, 14)
+    reg = _local_reg(nqb, 4, oracle_lib)
+    _load(reg, amp)
+    reg.paulirot(flip, phase, phi)
+    assert abs(reg.norm2() - 0.49) < 1e-13
 
 
 def test_swapped_qubit_stays_local(oracle_lib):

@@ -122,6 +122,7 @@ def test_fp32_within_tolerance(oracle_lib, in_place):
         _load(reg, amp)
         reg.paulirot(flip, phase, phi)
         got = reg.get_state()
+        assert abs(reg.norm2() - 1.0) < 1e-5
     assert np.max(np.abs(got - want)) < 1e-5
 
 
