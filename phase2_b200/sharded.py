@@ -320,9 +320,10 @@ class ShardedRegister:
         phi = np.ascontiguousarray(phi, dtype=np.float64)
         if not len(flip) == len(phase) == len(phi):
             raise ValueError("flip, phase and phi differ in length")
-        top = np.uint64(self.nqb)
-        if len(flip) and ((flip >> top).any() or (phase >> top).any()):
-            raise ValueError("Pauli string acts beyond the register")
+        if self.nqb < 64 and len(flip):
+            top = np.uint64(self.nqb)
+            if (flip >> top).any() or (phase >> top).any():
+                raise ValueError("Pauli string acts beyond the register")
         L = np.uint64(self.nlocal)
         n, k = len(phi), 0
         while k < n:
