@@ -872,7 +872,13 @@ def main() -> None:
     if args.impl == "reference":
         reference_arm(args)
     else:
-        gpu_arm(args)
+        try:
+            gpu_arm(args)
+        finally:
+            # every rank has left its last collective when gpu_arm returns
+            import torch.distributed as dist
+            if dist.is_available() and dist.is_initialized():
+                dist.destroy_process_group()
 
 
 if __name__ == "__main__":
