@@ -385,3 +385,19 @@ def test_phase2_run_rejects_without_touching_device():
                         C.byref(im_)) == -1
     assert L.phase2_run(arr, cf, 1, 0.1, b"0" * 31, C.byref(re_),
                         C.byref(im_)) == -1
+
+
+def test_slab_calls_reject_uninitialised_registers():
+    """qreg_slab_get/put/swap on a register that was never initialised
+    return -1 before touching any device (no GPU needed)."""
+    L = lib()
+    a, b = _ffi.Qreg(), _ffi.Qreg()
+    buf = C.c_void_p(0)
+    assert L.qreg_slab_get(C.byref(a), 0, 0, 0, 1, buf) == -1
+    assert L.qreg_slab_put(C.byref(a), 0, 0, 0, 1, buf) == -1
+    assert L.qreg_slab_swap(C.byref(a), C.byref(b), 0, 0, 1) == -1
+    rc = _ffi.CmpsitRanct()
+    empty = _ffi.CircHamil()
+    dt = _ffi.CmpsitData(1, 1, 0, 4, 0.05, 0.01, 5)
+    assert L.cmpsit_ranct_init(C.byref(rc), C.byref(empty), C.byref(dt)) == -1
+    L.cmpsit_ranct_free(C.byref(rc))
