@@ -21,6 +21,8 @@ from __future__ import annotations
 import ctypes as C
 import json
 import math
+import os
+import subprocess
 import sys
 from pathlib import Path
 
@@ -51,7 +53,18 @@ def cplx(z) -> list:
     return [float(np.real(z)), float(np.imag(z))]
 
 
-H2O_DUMP = Path("/root/reference/test/data/H2O_CAS56.h5dump")
+def _reference_tree() -> Path:
+    """$PHASE2_REF, else the oracle recipes' default (oracle/Makefile REF)."""
+    env = os.environ.get("PHASE2_REF")
+    if env:
+        return Path(env)
+    root = Path(__file__).resolve().parents[2]
+    return Path(subprocess.run(["make", "-s", "-C", "oracle", "print-ref"],
+                               cwd=root, check=True, capture_output=True,
+                               text=True).stdout.strip())
+
+
+H2O_DUMP = _reference_tree() / "test" / "data" / "H2O_CAS56.h5dump"
 
 
 def _dataset_values(text: str, name: str) -> list[float]:
@@ -144,6 +157,15 @@ def main() -> None:
         (["W0"], [1.0], 0.1, "0"), (["X5"], [1.0], 0.1, "0"),
         (["Z0"], [1.0], 0.1, "2"), (["Z0"], [1.0], 0.1, ""),
         (["X"], [1.0], 0.1, "0"), (["X0x"], [1.0], 0.1, "0"),
+        # token edges of the index grammar (strtoul inside a token)
+        (["X+1"], [1.0], 0.3, "01"), (["X-0"], [1.0], 0.3, "0"),
+        (["X-1"], [1.0], 0.3, "01"), (["X\r1"], [1.0], 0.3, "01"),
+        (["X00 Z01"], [1.0], 0.3, "01"), (["X0 I0"], [1.0], 0.3, "0"),
+        (["Y1 X1 Z0"], [0.7], 0.3, "01"), (["\tZ0\n Y1 "], [1.0], 0.3, "01"),
+        (["X 0"], [1.0], 0.1, "0"), (["x0"], [1.0], 0.1, "0"),
+        (["X+"], [1.0], 0.1, "0"), (["X1"], [1.0], 0.1, "0"),
+        (["Z0", "W1"], [1.0, 1.0], 0.1, "00"),
+        ([" ", ""], [1.0, 2.0], 0.1, "1"),
     ]
     xz = []
     for k in range(10):
