@@ -297,17 +297,23 @@ void *qreg_stream(const struct qreg *reg);
  * sum but allocates its partials buffer on first use.
  *
  *   d_state  device pointer to namp amplitudes: complex128 (prec =
- *            PHASE2_PREC_FP64) or complex64 (PHASE2_PREC_FP32)
+ *            PHASE2_PREC_FP64) or complex64 (PHASE2_PREC_FP32), memory of
+ *            the current device with all namp amplitudes inside one
+ *            allocation; a host pointer, another device's memory or a
+ *            shorter buffer returns -1 before anything is launched
  *   namp     1 .. 2^34 (the fixed scratch holds 8192 partial sums of up
  *            to 2^21 amplitudes each); larger sizes return -1 with an error
- *   d_out    device pointer to 2 doubles; receives {sum, 0}
+ *   d_out    device pointer to 2 doubles (16-byte aligned, checked like
+ *            d_state); receives {sum, 0}
  *   stream   cudaStream_t (NULL = legacy default stream); the call is
  *            asynchronous on it
  *
  * The per-block partial sums live in a static device array (about
  * 128 KiB) that every GPU loading the library holds until the process
  * exits.  The first call on a device looks up that array's address and
- * caches it; make that first call before starting any stream capture.
+ * caches it; make that first call before starting any stream capture.  A
+ * cudaDeviceReset invalidates the cached address: do not call this entry
+ * point on a device after resetting it in the same process.
  * All calls share the array: two calls whose kernels overlap on the GPU
  * (different streams, no ordering between them) race on it and may
  * return wrong sums.  Calls ordered on one stream are safe; nothing in the

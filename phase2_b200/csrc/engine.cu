@@ -585,6 +585,14 @@ extern "C" struct p2_dev *p2d_create(uint32_t nqb, int prec)
 	if (cudaEventCreate(&d->t0) != cudaSuccess ||
 		cudaEventCreate(&d->t1) != cudaSuccess)
 		goto fail;
+	if (cudaMalloc((void **)&d->d_status, sizeof *d->d_status) !=
+			cudaSuccess ||
+		cudaMallocHost((void **)&d->h_status, sizeof *d->h_status) !=
+			cudaSuccess ||
+		cudaMemsetAsync(d->d_status, 0, sizeof *d->d_status,
+			d->stream) != cudaSuccess)
+		goto fail;
+	*d->h_status = 0;
 	if (cudaMemsetAsync(d->state, 0, bytes, d->stream) != cudaSuccess)
 		goto fail;
 	/* the state is ready for any stream from here on */
@@ -617,6 +625,8 @@ extern "C" void p2d_destroy(struct p2_dev *d)
 	cudaFreeHost(d->h_val);
 	cudaFree(d->d_part);
 	cudaFree(d->d_cm);
+	cudaFree(d->d_status);
+	cudaFreeHost(d->h_status);
 	for (int k = 0; k < P2_GRAPH_SLOTS; k++) {
 		struct p2_graph *g = &d->graphs[k];
 		if (g->exec)
@@ -632,6 +642,29 @@ extern "C" void p2d_destroy(struct p2_dev *d)
 	if (d->stream)
 		cudaStreamDestroy(d->stream);
 	free(d);
+}
+
+int p2_status_check(struct p2_dev *d)
+{
+	if (!d->status_pending)
+		return 0;
+	CUDA_OK(cudaMemcpyAsync(d->h_status, d->d_status, sizeof *d->h_status,
+			cudaMemcpyDeviceToHost, d->stream),
+		"read kernel status");
+	CUDA_OK(cudaStreamSynchronize(d->stream), "kernel status");
+	d->d2h_bytes += sizeof *d->h_status;
+	d->status_pending = 0;
+	if (*d->h_status) {
+		log_error("a pass kernel gave up waiting for its staged loads "
+			  "(status %u): the state is not valid",
+			*d->h_status);
+		*d->h_status = 0;
+		CUDA_OK(cudaMemsetAsync(d->d_status, 0, sizeof *d->d_status,
+				d->stream),
+			"clear kernel status");
+		return -1;
+	}
+	return 0;
 }
 
 extern "C" int p2d_zero(struct p2_dev *d)
@@ -710,12 +743,14 @@ extern "C" int p2d_get(struct p2_dev *d, const uint64_t *idx, double *z,
 	d->d2h_bytes += n * 2 * sizeof(double);
 	CUDA_OK(cudaStreamSynchronize(d->stream), "gather");
 	memcpy(z, d->h_val, n * 2 * sizeof(double));
-	return 0;
+	return p2_status_check(d);
 }
 
 extern "C" int p2d_get_state(struct p2_dev *d, double *out)
 {
 	const size_t bytes = d->namp * sizeof(double2);
+	if (p2_status_check(d) < 0)
+		return -1;
 	if (d->prec == PHASE2_PREC_FP64) {
 		CUDA_OK(cudaMemcpyAsync(out, d->state, bytes,
 				cudaMemcpyDeviceToHost, d->stream),
@@ -776,9 +811,13 @@ extern "C" int p2d_set_state(struct p2_dev *d, const double *in)
  * Launch table: per precision and span, which pass kernel runs and how many
  * blocks per SM the grid holds.  FP64: variant 0 direct loads, 1 shared-
  * memory prefetch (per_sm 0: 16 for the direct kernel, the occupancy for
- * the prefetch kernel).  FP32: the lifted kernels, variant 0 only (per_sm
- * 0: 16).  Set by phase2_tune_set (the autotuner) or left at these
- * defaults.
+ * the prefetch kernel).  FP32: the lifted kernels; for passes of the
+ * FP64-arithmetic form, variants 1 and 2 run the kernels whose next
+ * cosets are staged in shared memory by bulk copies or by cp.async
+ * (lift_bulk.cu; per_sm caps their occupancy) where the pass qualifies,
+ * variant 0 the direct kernel (per_sm 0: 16).  The
+ * FP32-arithmetic form has one kernel.  Set by phase2_tune_set (the
+ * autotuner) or left at these defaults.
  */
 struct p2_tune_entry {
 	int variant;
@@ -798,7 +837,7 @@ extern "C" int phase2_tune_set(int prec, int span, int variant, int per_sm)
 {
 	if ((prec != PHASE2_PREC_FP64 && prec != PHASE2_PREC_FP32) || span < 0 ||
 		span > PHASE2_MAX_SPAN || variant < 0 ||
-		variant > (prec == PHASE2_PREC_FP64 ? 1 : 0) || per_sm < 0 ||
+		variant > (prec == PHASE2_PREC_FP64 ? 1 : 2) || per_sm < 0 ||
 		per_sm > 64)
 		return -1;
 	p2_tune[prec][span].variant = variant;
@@ -883,6 +922,15 @@ static int launch_lift_t(struct p2_dev *d, const struct phase2_pass &p,
 			k_pass_lift32<M, uint64_t>
 				<<<grid, P2_TPB, 0, d->stream>>>(sv, nrep, p, recs);
 	} else if (p.form == PHASE2_FORM_LIFTED) {
+		/* variants 1 and 2: the next cosets staged in shared memory by
+		 * bulk copies or cp.async (lift_bulk.cu), where the pass
+		 * qualifies */
+		if (te.variant != 0) {
+			const int rc = p2_lift_staged_launch(d, &p, recs,
+				te.variant, (unsigned)te.per_sm);
+			if (rc != 0)
+				return rc < 0 ? -1 : 0;
+		}
 		if (narrow)
 			k_pass_lift<M, uint32_t>
 				<<<grid, P2_TPB, 0, d->stream>>>(sv, nrep, p, recs);
@@ -1032,7 +1080,11 @@ static struct p2_graph *graph_for(struct p2_dev *d,
 				    cudaStreamCaptureModeThreadLocal) !=
 				cudaSuccess)
 				return NULL;
+			const int pending = d->status_pending;
+			d->status_pending = 0;
 			const long rc = launch_all(d, passes, npass, g->d_recs);
+			g->status = d->status_pending;
+			d->status_pending |= pending;
 			const cudaError_t e = cudaStreamEndCapture(d->stream,
 				&graph);
 			g->nlaunch = rc > 0 ? (size_t)rc : 0;
@@ -1106,6 +1158,7 @@ extern "C" int p2d_run(struct p2_dev *d, const struct phase2_pass *passes,
 	if (g) {
 		CUDA_OK(cudaGraphLaunch(g->exec, d->stream), "graph launch");
 		d->graph_replays++;
+		d->status_pending |= g->status;
 		launches = (long)g->nlaunch;
 	} else if ((launches = launch_all(d, passes, npass, d->d_recs)) < 0) {
 		return -1;
@@ -1158,7 +1211,7 @@ static int reduce_finish(struct p2_dev *d, unsigned blocks, double out[2])
 	d->d2h_bytes += sizeof h;
 	out[0] = h[0];
 	out[1] = h[1];
-	return 0;
+	return p2_status_check(d);
 }
 
 static int reduce(struct p2_dev *d, const double2 *trial, double out[2])
@@ -1296,7 +1349,7 @@ extern "C" int p2d_sync(struct p2_dev *d)
 {
 	CUDA_OK(cudaStreamSynchronize(d->stream), "stream sync");
 	CUDA_OK(cudaGetLastError(), "pending error");
-	return 0;
+	return p2_status_check(d);
 }
 
 extern "C" void p2d_stats(const struct p2_dev *d, struct phase2_stats *st)
@@ -1379,6 +1432,8 @@ void p2_scratch_free(void *p, cudaStream_t stream)
 static __device__ __align__(256) double
 	p2_noalloc_scratch[2 * P2_NOALLOC_MAX_BLOCKS];
 
+/* Address of the array on each device, looked up by the first call there
+ * (written once with the same value by any thread that races on it). */
 static double *p2_noalloc_addr[P2_NOALLOC_MAX_DEVICES];
 
 extern "C" int phase2_norm2_noalloc(const void *d_state, int prec,
@@ -1402,6 +1457,22 @@ extern "C" int phase2_norm2_noalloc(const void *d_state, int prec,
 			(unsigned long long)P2_NOALLOC_CHUNK);
 		return -1;
 	}
+	const size_t elem =
+		prec == PHASE2_PREC_FP64 ? sizeof(double2) : sizeof(float2);
+	if ((uintptr_t)d_state % elem != 0 || (uintptr_t)d_out % 16 != 0) {
+		log_error("phase2_norm2_noalloc: state not aligned to %zu bytes"
+			  " or output not aligned to 16 bytes",
+			elem);
+		return -1;
+	}
+	/* both pointers must be memory of the current device, with the whole
+	 * range inside one allocation: a host pointer or a short buffer is
+	 * refused here instead of faulting in the kernel */
+	if (p2_check_device_range(d_state, (size_t)namp * elem,
+		    "phase2_norm2_noalloc: state") < 0 ||
+		p2_check_device_range(d_out, 2 * sizeof(double),
+			"phase2_norm2_noalloc: output") < 0)
+		return -1;
 	int dev = 0;
 	CUDA_OK(cudaGetDevice(&dev), "phase2_norm2_noalloc: current device");
 	if (dev < 0 || dev >= P2_NOALLOC_MAX_DEVICES) {
@@ -1409,26 +1480,42 @@ extern "C" int phase2_norm2_noalloc(const void *d_state, int prec,
 			  " supported", dev, P2_NOALLOC_MAX_DEVICES);
 		return -1;
 	}
-	if (!p2_noalloc_addr[dev]) {
+	double *part = __atomic_load_n(&p2_noalloc_addr[dev], __ATOMIC_ACQUIRE);
+	if (!part) {
 		/* first call on this device: resolve the array's address */
-		double *ptr = NULL;
-		CUDA_OK(cudaGetSymbolAddress((void **)&ptr, p2_noalloc_scratch),
+		CUDA_OK(cudaGetSymbolAddress((void **)&part, p2_noalloc_scratch),
 			"phase2_norm2_noalloc: scratch address");
-		p2_noalloc_addr[dev] = ptr;
+		__atomic_store_n(&p2_noalloc_addr[dev], part, __ATOMIC_RELEASE);
 	}
-	double *part = p2_noalloc_addr[dev];
+	int sms = 0;
+	if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
+			cudaSuccess ||
+		sms <= 0) {
+		cudaGetLastError();
+		sms = 148;
+	}
 	const cudaStream_t s = (cudaStream_t)stream;
-	/* Each block writes its own two slots before the final kernel reads
-	 * them (stream order), so the array needs no clearing. */
-	const unsigned blocks =
-		(unsigned)((namp + P2_NOALLOC_CHUNK - 1) / P2_NOALLOC_CHUNK);
+	/* Enough blocks to stream at full bandwidth (four per SM), at least
+	 * one per 2^21 amplitudes so that the array always suffices, at most
+	 * one per 256 amplitudes; k_reduce_partial is a grid-stride loop, so
+	 * any count gives the same sum terms.  Each block writes its own two
+	 * slots before the final kernel reads them (stream order), so the
+	 * array needs no clearing. */
+	uint64_t blocks = (namp + P2_NOALLOC_CHUNK - 1) / P2_NOALLOC_CHUNK;
+	if (blocks < (uint64_t)sms * 4)
+		blocks = (uint64_t)sms * 4;
+	const uint64_t per256 = (namp + P2_RED_TPB - 1) / P2_RED_TPB;
+	if (blocks > per256)
+		blocks = per256;
+	if (blocks > P2_NOALLOC_MAX_BLOCKS)
+		blocks = P2_NOALLOC_MAX_BLOCKS;
 	if (prec == PHASE2_PREC_FP64)
-		k_reduce_partial<<<blocks, P2_RED_TPB, 0, s>>>(
+		k_reduce_partial<<<(unsigned)blocks, P2_RED_TPB, 0, s>>>(
 			(const double2 *)d_state, NULL, namp, part);
 	else
-		k_reduce_partial<<<blocks, P2_RED_TPB, 0, s>>>(
+		k_reduce_partial<<<(unsigned)blocks, P2_RED_TPB, 0, s>>>(
 			(const float2 *)d_state, NULL, namp, part);
-	k_reduce_final<<<1, P2_RED_TPB, 0, s>>>(part, blocks, d_out);
+	k_reduce_final<<<1, P2_RED_TPB, 0, s>>>(part, (unsigned)blocks, d_out);
 	CUDA_OK(cudaGetLastError(), "phase2_norm2_noalloc: launch");
 	return 0;
 }

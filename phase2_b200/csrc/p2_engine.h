@@ -30,6 +30,7 @@ struct p2_graph {
 	struct phase2_rot_rec *d_recs; /* records read by the graph */
 	cudaGraphExec_t exec;
 	size_t nlaunch; /* kernel launches in the graph */
+	int status;     /* the graph holds kernels that write d_status */
 	uint64_t used;
 };
 
@@ -49,6 +50,12 @@ struct p2_dev {
 	cudaEvent_t h_ev[2];
 	int h_ev_live[2];
 	int ring;
+
+	/* error word of kernels with bounded waits (lift_bulk.cu): set on
+	 * the device, read at the next synchronisation (p2_status_check) */
+	unsigned int *d_status;
+	unsigned int *h_status;
+	int status_pending;
 
 	uint64_t *d_idx;
 	double *d_val;
@@ -124,6 +131,25 @@ void p2_batch_launch(bool f64, unsigned grid, cudaStream_t stream,
 	const struct phase2_pass *passes, const struct phase2_rot_rec *recs,
 	const uint64_t *widx, const double *wval, const uint64_t *gidx,
 	double2 *gout, struct p2_bctl *ctl, unsigned int *status);
+
+/* lift_bulk.cu: one FP32 pass of the FP64-arithmetic form on a kernel
+ * whose next cosets are staged in shared memory, by bulk copies (variant
+ * 1) or cp.async (variant 2); returns 1 when launched, 0 when the pass
+ * does not qualify (the caller runs the direct kernel), -1 on error.
+ * per_sm_cap: resident blocks per SM at most (0: occupancy). */
+extern "C" int p2_lift_staged_launch(struct p2_dev *d,
+	const struct phase2_pass *p, const struct phase2_rot_rec *recs,
+	int variant, unsigned per_sm_cap);
+
+/* engine.cu: read the error word of kernels with bounded waits if one ran
+ * since the last check (synchronises the register's stream); -1 and a
+ * logged error when a wait gave up. */
+int p2_status_check(struct p2_dev *d);
+
+/* slab.cu: 0 if [p, p + bytes) is device memory of the current device
+ * inside one allocation; -1 (logged, prefixed by `what`) otherwise, also
+ * when the allocation cannot be looked up.  Allocates nothing. */
+int p2_check_device_range(const void *p, size_t bytes, const char *what);
 
 /* sweep.cu: whether planned sweeps run as one kernel each on this
  * register, and the launch of the sweep starting at passes[i] (returns the

@@ -109,7 +109,7 @@ typedef CUresult (*p2_addr_range_fn)(CUdeviceptr *, size_t *, CUdeviceptr);
 /* 0 if [p, p + bytes) is device memory of the current device inside one
  * allocation; -1 (logged) otherwise, also when the allocation cannot be
  * looked up (no copy runs unchecked). */
-static int check_device_range(const void *p, size_t bytes, const char *what)
+int p2_check_device_range(const void *p, size_t bytes, const char *what)
 {
 	int dev = 0;
 	cudaPointerAttributes a;
@@ -180,7 +180,7 @@ extern "C" int p2d_slab_copy(struct p2_dev *d, uint32_t bit, uint32_t val,
 		log_error("%s: buffer not aligned to %zu bytes", what, d->elem);
 		return -1;
 	}
-	if (check_device_range(buf, count * d->elem, what) < 0)
+	if (p2_check_device_range(buf, count * d->elem, what) < 0)
 		return -1;
 	const unsigned grid = grid_for(d, count, 256, 8);
 	if (d->prec == PHASE2_PREC_FP64) {
