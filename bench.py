@@ -267,6 +267,15 @@ def gpu_arm(args) -> None:
     import phase2_b200 as p2
     from phase2_b200 import workloads
     p2.world_ensure()
+    if args.fp32_form:
+        p2.set_fp32_form({"f32": p2.FORM_LIFTED_F32,
+                          "f64": p2.FORM_LIFTED}[args.fp32_form])
+    if args.lift_kernel:
+        # FP64-arithmetic passes of span 3-5: direct loads, or the next
+        # cosets staged by bulk copies or by cp.async
+        v = {"direct": 0, "bulk": 1, "staged": 2}[args.lift_kernel]
+        for span in (3, 4, 5):
+            p2.lib().phase2_tune_set(p2.PREC_FP32, span, v, 32)
     cfg = workloads.qdrift30(nqb=args.nqb, depth=args.depth)
     nqb, depth = cfg["nqb"], cfg["depth"]
     namp = 1 << nqb
@@ -843,6 +852,15 @@ def main() -> None:
     ap.add_argument("--nqb", type=int, default=30)
     ap.add_argument("--depth", type=int, default=4096)
     ap.add_argument("--cmp-depth", type=int, default=512)
+    ap.add_argument("--fp32-form", default=None, choices=["f32", "f64"],
+                    help="arithmetic of FP32 passes for the run: f32 (FP32 "
+                         "FMAs) or f64 (FP64 arithmetic, one rounding to "
+                         "FP32 per pass); default: the library's")
+    ap.add_argument("--lift-kernel", default=None,
+                    choices=["direct", "bulk", "staged"],
+                    help="kernel of FP64-arithmetic FP32 passes: direct "
+                         "loads, or the next cosets staged by bulk copies "
+                         "or by cp.async")
     ap.add_argument("--quick", action="store_true",
                     help="skip the CPU baseline and secondary arms")
     ap.add_argument("--studies", default="batched,trott26,sharded",
@@ -872,13 +890,13 @@ def main() -> None:
     if args.impl == "reference":
         reference_arm(args)
     else:
-        try:
-            gpu_arm(args)
-        finally:
-            # every rank has left its last collective when gpu_arm returns
-            import torch.distributed as dist
-            if dist.is_available() and dist.is_initialized():
-                dist.destroy_process_group()
+        gpu_arm(args)
+        # every rank has left its last collective when gpu_arm returns;
+        # after an exception a peer may still be inside one, so the group
+        # is left to process exit instead of a blocking teardown
+        import torch.distributed as dist
+        if dist.is_available() and dist.is_initialized():
+            dist.destroy_process_group()
 
 
 if __name__ == "__main__":
