@@ -264,10 +264,12 @@ __device__ __forceinline__ void p2_prefetch(double2 *stage, const double2 *st,
  *   y_u += t q_u y_w;  y_w += s q_w y_u;  y_u += t q_u y_w,
  * q_u = sigma (odd ? i : 1), q_w = -conj(q_u), t = tan(phi/2): every update
  * writes the register it reads, so a case needs no temporaries and leaves
- * no moves behind.  The partner is held as sigma * y_w during the shears
- * (its sign bits flipped in place), which makes all six FMAs sign-free.
+ * no moves behind.  The sign goes onto the two coefficients (one XOR on the
+ * high word of each, sigma t and sigma s); the FMAs then take them with
+ * free operand negations.  Rounding is symmetric under negation, so this
+ * gives the same bits as flipping the partner's sign around the shears.
  * U = 0 (the string is diagonal on the coset, and then odd = 1) is the
- * phase c + i sigma s, applied to (re, sigma im) by the same three shears.
+ * phase c + i sigma s, applied to (re, im) by the same three shears.
  */
 template <int M, int U, int ODD>
 __device__ __forceinline__ void p2_rot_lift(double (&re)[1 << M],
@@ -278,11 +280,10 @@ __device__ __forceinline__ void p2_rot_lift(double (&re)[1 << M],
 		for (int u = 0; u < (1 << M); ++u) {
 			const uint32_t g = p2_bitmask(sm, u);
 			if constexpr (ODD) {
-				double v = p2_sgn(im[u], g);
-				re[u] = fma(-t, v, re[u]);
-				v = fma(s, re[u], v);
-				re[u] = fma(-t, v, re[u]);
-				im[u] = p2_sgn(v, g);
+				const double st = p2_sgn(t, g), ss = p2_sgn(s, g);
+				re[u] = fma(-st, im[u], re[u]);
+				im[u] = fma(ss, re[u], im[u]);
+				re[u] = fma(-st, im[u], re[u]);
 			} else {
 				/* (c +- s) y with c = 1 - t s; a Hermitian string
 				 * that is diagonal on the coset never has it */
@@ -298,24 +299,22 @@ __device__ __forceinline__ void p2_rot_lift(double (&re)[1 << M],
 			const int u = p2_ins0(k, H);
 			const int w = u ^ U;
 			const uint32_t g = p2_bitmask(sm, u);
-			double wr = p2_sgn(re[w], g), wi = p2_sgn(im[w], g);
+			const double st = p2_sgn(t, g), ss = p2_sgn(s, g);
 			if constexpr (ODD) {
-				re[u] = fma(-t, wi, re[u]);
-				im[u] = fma(t, wr, im[u]);
-				wr = fma(-s, im[u], wr);
-				wi = fma(s, re[u], wi);
-				re[u] = fma(-t, wi, re[u]);
-				im[u] = fma(t, wr, im[u]);
+				re[u] = fma(-st, im[w], re[u]);
+				im[u] = fma(st, re[w], im[u]);
+				re[w] = fma(-ss, im[u], re[w]);
+				im[w] = fma(ss, re[u], im[w]);
+				re[u] = fma(-st, im[w], re[u]);
+				im[u] = fma(st, re[w], im[u]);
 			} else {
-				re[u] = fma(t, wr, re[u]);
-				im[u] = fma(t, wi, im[u]);
-				wr = fma(-s, re[u], wr);
-				wi = fma(-s, im[u], wi);
-				re[u] = fma(t, wr, re[u]);
-				im[u] = fma(t, wi, im[u]);
+				re[u] = fma(st, re[w], re[u]);
+				im[u] = fma(st, im[w], im[u]);
+				re[w] = fma(-ss, re[u], re[w]);
+				im[w] = fma(-ss, im[u], im[w]);
+				re[u] = fma(st, re[w], re[u]);
+				im[u] = fma(st, im[w], im[u]);
 			}
-			re[w] = p2_sgn(wr, g);
-			im[w] = p2_sgn(wi, g);
 		}
 	}
 }

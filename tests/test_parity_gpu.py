@@ -94,23 +94,25 @@ def test_random_rotations_bit_exact(n, fusion, oracle_lib):
     assert np.array_equal(got, want)
 
 
-@pytest.mark.parametrize("variant,per_sm", [(0, 0), (1, 0), (0, 4)])
+@pytest.mark.parametrize("v64,v32,per_sm", [(0, 0, 0), (1, 1, 0), (0, 2, 0),
+                                             (0, 0, 4), (1, 2, 2)])
 @pytest.mark.parametrize("n", [5, 11, 17])
-def test_launch_variants(variant, per_sm, n, fp32_form, oracle_lib):
+def test_launch_variants(v64, v32, per_sm, n, fp32_form, oracle_lib):
     """The direct-load and shared-memory-prefetch FP64 kernels give the
     same bits for every span, at several grid densities; the FP32 lifted
-    kernels (one variant) stay within tolerance at the same densities."""
+    kernels (FP64-arithmetic form: direct, bulk-staged or cp.async-staged)
+    stay within tolerance at the same densities."""
     from phase2_b200._ffi import lib
     L = lib()
     saved = []
-    for prec in (0, 1):
+    for prec, variant in ((0, v64), (1, v32)):
         for m in range(6):
             v, s = C.c_int(), C.c_int()
             L.phase2_tune_get(prec, m, C.byref(v), C.byref(s))
             saved.append((prec, m, v.value, s.value))
-            assert L.phase2_tune_set(prec, m, variant if prec == 0 else 0,
-                                     per_sm) == 0
-        assert L.phase2_tune_set(1, 5, 1, 0) == -1
+            assert L.phase2_tune_set(prec, m, variant, per_sm) == 0
+    assert L.phase2_tune_set(0, 5, 2, 0) == -1
+    assert L.phase2_tune_set(1, 5, 3, 0) == -1
     try:
         rng = np.random.Generator(np.random.PCG64(300 + n))
         amp = _rand_state(rng, n)
