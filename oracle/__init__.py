@@ -257,6 +257,10 @@ class Reference:
         L.phase2_run.argtypes = [_P(C.c_char_p), _D, C.c_size_t, C.c_double,
                                  C.c_char_p, _D, _D]
         L.phase2_run.restype = C.c_int
+        L.refh_capture.argtypes = [C.c_uint64, C.c_size_t, _U, _D]
+        L.refh_capture.restype = C.c_int
+        L.refh_captured.argtypes = []
+        L.refh_captured.restype = C.c_size_t
         cm_args = [C.c_uint32] * 4 + [C.c_int, C.c_size_t, _D, _D, _D]
         L.refh_coeff_expand_all.argtypes = cm_args + [_D]
         L.refh_coeff_expand_all.restype = C.c_int
@@ -286,6 +290,20 @@ class Reference:
                 _dptr(a.view(np.float64)), _dptr(out)):
             raise RuntimeError("reference coeff_inner failed")
         return complex(out[0], out[1])
+
+    def capture(self, stride: int, cap: int):
+        """Arm the amplitude capture of the next driver run; returns a
+        function giving (indices, amplitudes) after the run (stride 0:
+        the non-zero amplitudes in index order)."""
+        idx = np.zeros(cap, dtype=np.uint64)
+        amp = np.zeros(cap, dtype=np.complex128)
+        self.L.refh_capture(stride, cap, _uptr(idx),
+                            _dptr(amp.view(np.float64)))
+
+        def taken():
+            n = self.L.refh_captured()
+            return idx[:n].copy(), amp[:n].copy()
+        return taken
 
     def paulirot(self, amp, nqb, flip, phase, phi):
         a = np.ascontiguousarray(amp, dtype=np.complex128).copy()
@@ -340,3 +358,57 @@ class Reference:
         rc = self.L.phase2_run(arr, cf, n, delta, psi.encode(), C.byref(re),
                                C.byref(im))
         return rc, complex(re.value, im.value)
+
+
+# ---- the reference as R ranks on the host cores (oracle/_ref/ref_mpi) ----
+
+REF_MPI = HERE / "_ref" / "ref_mpi"
+_REF_IN_HDR = np.dtype([("magic", "S8"), ("mode", "<u4"), ("nqb", "<u4"),
+                        ("nterms", "<u8"), ("ndets", "<u8"),
+                        ("count", "<u8"), ("angle", "<f8"), ("seed", "<u8")])
+_REF_IN_DET = np.dtype([("idx", "<u8"), ("re", "<f8"), ("im", "<f8")])
+
+
+def write_ref_input(path, mode: str, nqb: int, flip, phase, cf, det_idx,
+                    det_cf, count: int, angle: float, seed: int = 0) -> None:
+    """Input file of ref_mpi: mode "qdrift" (count = depth, angle =
+    step_size, one sample per run) or "trott2" (count = steps, angle =
+    delta)."""
+    h = np.zeros(1, dtype=_REF_IN_HDR)
+    h["magic"], h["mode"], h["nqb"] = b"P2REFIN1", \
+        {"qdrift": 0, "trott2": 1}[mode], nqb
+    h["nterms"], h["ndets"], h["count"] = len(cf), len(det_idx), count
+    h["angle"], h["seed"] = angle, seed
+    d = np.zeros(len(det_idx), dtype=_REF_IN_DET)
+    dc = np.asarray(det_cf, dtype=np.complex128)
+    d["idx"], d["re"], d["im"] = det_idx, dc.real, dc.imag
+    with open(path, "wb") as f:
+        f.write(h.tobytes())
+        f.write(term_records(flip, phase, cf).tobytes())
+        f.write(d.tobytes())
+
+
+def run_ref_mpi(ranks: int, path, reps: int, timeout: float = 1800,
+                env: dict | None = None, warmup: int = 0) -> dict:
+    """Run ref_mpi: the reference's driver as `ranks` ranks of one job,
+    `warmup` untimed runs then the minimum over `reps` timed ones; returns
+    its timing line as a dict."""
+    import os
+    import subprocess
+    if not REF_MPI.is_file():
+        raise RuntimeError(f"{REF_MPI} missing: run `make -C oracle ref-mpi`")
+    e = dict(os.environ)
+    e.update(env or {})
+    out = subprocess.run([str(REF_MPI), str(ranks), str(path), str(reps),
+                          str(warmup)],
+                         capture_output=True, text=True, timeout=timeout,
+                         env=e)
+    if out.returncode != 0:
+        raise RuntimeError(f"ref_mpi failed ({out.returncode}): "
+                           f"{out.stderr.strip()[-400:]}")
+    # the reference logs to stdout too: the timing line is the last one
+    f = out.stdout.strip().splitlines()[-1].split()
+    return {"ranks": int(f[0]), "rotations": int(f[1]),
+            "seconds": float(f[2]), "rot_amp_s": float(f[3]),
+            "mailbox": bool(int(f[4])), "z": complex(float(f[5]),
+                                                    float(f[6]))}
