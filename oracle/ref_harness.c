@@ -40,6 +40,56 @@ static int ensure_world(void)
 									 : -1;
 }
 
+/*
+ * Amplitude capture: refh_capture arms it, and the next driver run
+ * (refh_trott, refh_qdrift, refh_cmpsit) samples its register's final
+ * state before freeing it, into caller buffers of `cap` entries:
+ * stride > 0 takes indices 0, stride, 2 stride, ...; stride == 0 takes the
+ * non-zero amplitudes in index order.  refh_captured returns the entries
+ * written.  The reference keeps the whole state on one rank here.
+ */
+static struct {
+	int on;
+	uint64_t stride;
+	size_t cap, got;
+	uint64_t *idx;
+	double *amp;
+} CAP;
+
+int refh_capture(uint64_t stride, size_t cap, uint64_t *idx, double *amp)
+{
+	CAP.on = 1;
+	CAP.stride = stride;
+	CAP.cap = cap;
+	CAP.got = 0;
+	CAP.idx = idx;
+	CAP.amp = amp;
+	return 0;
+}
+
+size_t refh_captured(void)
+{
+	return CAP.got;
+}
+
+static void capture(const struct qreg *reg)
+{
+	if (!CAP.on)
+		return;
+	CAP.on = 0;
+	CAP.got = 0;
+	for (uint64_t i = 0; i < reg->namp && CAP.got < CAP.cap;
+		i += CAP.stride ? CAP.stride : 1) {
+		const _Complex double z = reg->amp[i];
+		if (!CAP.stride && z == 0)
+			continue;
+		CAP.idx[CAP.got] = i;
+		CAP.amp[2 * CAP.got] = creal(z);
+		CAP.amp[2 * CAP.got + 1] = cimag(z);
+		CAP.got++;
+	}
+}
+
 /* amp: 2*2^nqb doubles, in/out.  Applies the n rotations with one
  * qreg_paulirot call per 1024-term batch, as the batch cache would. */
 int refh_paulirot(uint32_t nqb, double *amp, const uint64_t *flip,
@@ -143,6 +193,7 @@ int refh_trott(int order2, uint32_t nqb, const void *terms, size_t nterms,
 		}
 		rc = trott2_simul(&t2);
 		store_vals(&t2.ct.vals, out_z);
+		capture(&t2.ct.reg);
 		trott2_free(&t2);
 	} else {
 		struct trott tt;
@@ -165,6 +216,7 @@ int refh_trott(int order2, uint32_t nqb, const void *terms, size_t nterms,
 		}
 		rc = trott_simul(&tt);
 		store_vals(&tt.ct.vals, out_z);
+		capture(&tt.ct.reg);
 		trott_free(&tt);
 	}
 	return rc;
@@ -191,6 +243,7 @@ int refh_qdrift(uint32_t nqb, const void *terms, size_t nterms,
 		return -1;
 	const int rc = qdrift_simul(&qd);
 	store_vals(&qd.ct.vals, out_z);
+	capture(&qd.ct.reg);
 	qdrift_free(&qd);
 	return rc;
 }
@@ -217,6 +270,7 @@ int refh_cmpsit(uint32_t nqb, const void *terms, size_t nterms,
 		return -1;
 	const int rc = cmpsit_simul(&cp);
 	store_vals(&cp.ct.vals, out_z);
+	capture(&cp.ct.reg);
 	cmpsit_free(&cp);
 	return rc;
 }

@@ -460,6 +460,16 @@ def _run_driver(kind: str, nqb: int, terms: Terms, dets, **kw):
         st = _ffi.Stats()
         L.qreg_get_stats(C.byref(obj.ct.reg), C.byref(st))
         stats = {k: getattr(st, k) for k, _ in _ffi.Stats._fields_}
+        if kw.get("state_idx") is not None:
+            # selected amplitudes of the register after the run
+            idx = np.ascontiguousarray(kw["state_idx"], dtype=np.uint64)
+            amps = np.zeros(len(idx), dtype=np.complex128)
+            if len(idx) and L.qreg_getamps(
+                    C.byref(obj.ct.reg),
+                    idx.ctypes.data_as(C.POINTER(C.c_uint64)),
+                    amps.ctypes.data_as(C.POINTER(C.c_double)), len(idx)):
+                raise RuntimeError("qreg_getamps failed")
+            stats["amps"] = amps
         if kw.get("with_state"):
             # the register after the run (small registers)
             stats["state"] = np.empty(1 << nqb, dtype=np.complex128)
