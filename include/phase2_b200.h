@@ -60,14 +60,30 @@ int qreg_precision(const struct qreg *reg);
 int phase2_set_fusion(int max_span, int max_rots);
 int qreg_set_fusion(struct qreg *reg, int max_span, int max_rots);
 
-/* Launch choice of the pass kernel for one precision and span M (0..5):
- * variant 0 loads each thread's cosets straight into registers, variant 1
- * prefetches the next coset into shared memory with cp.async while the
- * current one is computed; per_sm caps resident blocks per SM in the grid
- * (0 = default).  Process-wide; the autotuner (phase2_b200/autotune.py)
- * sets these from its measurements.  0 or -1. */
+/* Launch choice of the pass kernel for one precision and span M (0..5).
+ * FP64: variant 0 loads each thread's cosets straight into registers,
+ * variant 1 prefetches the next coset into shared memory with cp.async
+ * while the current one is computed.  FP32 (FP64-arithmetic form only;
+ * the FP32-arithmetic form has one kernel): variant 0 loads directly,
+ * variant 1 stages each warp's next cosets in shared memory with bulk
+ * copies (cp.async.bulk), variant 2 with cp.async; passes that do not
+ * qualify for staging (a pivot below qubit 5, registers of fewer than
+ * M + 5 qubits or more than 31) load directly.  per_sm caps resident
+ * blocks per SM in the grid (0 = default).  Process-wide; the autotuner
+ * (phase2_b200/autotune.py) sets these from its measurements.  0 or
+ * -1. */
 int phase2_tune_set(int prec, int span, int variant, int per_sm);
 int phase2_tune_get(int prec, int span, int *variant, int *per_sm);
+
+/* Apply a launch table file (lines "gpu <name>" and "launch <prec> <span>
+ * <variant> <per_sm>", '#' comments; written by phase2_b200/autotune.py)
+ * if its GPU name equals `gpu` (NULL: the current CUDA device's name).
+ * Returns the entries applied, 0 for a table of another GPU, -1 for a
+ * missing or malformed file (nothing applied).  world_init applies the
+ * table shipped beside the library, tuning_b200.tab (or the file named by
+ * PHASE2_TUNING; PHASE2_TUNING=off skips it), before the PHASE2_*
+ * settings from the environment. */
+int phase2_load_tuning(const char *path, const char *gpu);
 
 /* ---- term order --------------------------------------------------------- */
 
@@ -138,7 +154,13 @@ int phase2_set_sweep_kernel(int on);
  * AUTO (default: device for qualifying registers of at most
  * PHASE2_DEVICE_SAMPLING_AUTO_QB qubits, where samples run concurrently;
  * wider registers keep the host loop, whose passes already fill the GPU).
- * Also PHASE2_DEVICE_SAMPLING=off|on|auto.  Returns -1 on a bad mode.
+ * Step writers: under AUTO a driver with a step writer attached keeps the
+ * host loop, which calls the writer as each sample completes (a writer
+ * that flushes per step stays crash-consistent and can report progress);
+ * under ON the writer is called for every sample, in sample order, after
+ * the device has run them all.  Either way it sees the same (index,
+ * overlap) sequence.  Also PHASE2_DEVICE_SAMPLING=off|on|auto.  Returns -1
+ * on a bad mode.
  */
 enum phase2_device_sampling {
 	PHASE2_DEVICE_SAMPLING_OFF = 0,

@@ -146,6 +146,15 @@ class Complex(C.Structure):
     _fields_ = [("re", C.c_double), ("im", C.c_double)]
 
 
+# struct phase2_step_writer (include/phase2/step_writer.h): the callback
+# receives the step's overlap as a _Complex double, passed as two doubles
+STEP_WRITE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_size_t, Complex)
+
+
+class StepWriter(C.Structure):
+    _fields_ = [("ctx", C.c_void_p), ("write", STEP_WRITE_FN)]
+
+
 class RotIn(C.Structure):
     _fields_ = [("flip", C.c_uint64), ("phase", C.c_uint64),
                 ("phi", C.c_double)]
@@ -321,6 +330,7 @@ _SIGS = {
     "qdrift_simul_batch": (C.c_int, [_P(C.c_void_p), C.c_size_t]),
     "cmpsit_simul_batch": (C.c_int, [_P(C.c_void_p), C.c_size_t]),
     "phase2_tune_set": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int]),
+    "phase2_load_tuning": (C.c_int, [C.c_char_p, C.c_char_p]),
     "phase2_tune_get": (C.c_int, [C.c_int, C.c_int, _P(C.c_int),
                                   _P(C.c_int)]),
     "phase2_version": (C.c_char_p, []),

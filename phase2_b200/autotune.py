@@ -7,10 +7,19 @@ on probe rotations whose flip masks span exactly M dimensions, then keeps
 the fastest.  It then compares fusion caps
 (max_span 4 vs 5) on a stream of qDRIFT-like draws, by rotations per second.
 
-Results are written as JSON (``save``) and applied to the running library
-with ``apply`` (phase2_tune_set / phase2_set_fusion).  ``python -m
-phase2_b200.autotune --nqb 28 --out phase2_b200/tuning_b200.json`` runs a
-sweep on the current GPU.
+FP32 passes: the grid density is tuned on the FP32-arithmetic kernel
+(one variant), then, at that density, the FP64-arithmetic form's variants
+(0 direct loads, 1 bulk-copy staging, 2 cp.async staging) are compared;
+the entry keeps both choices (the variant only steers the FP64-arithmetic
+form).
+
+Results are written as JSON (the full report) and as the flat launch table
+the library applies at world_init when the GPU name matches
+(``tuning_b200.tab`` beside libphase2.so, ``write_table``; C loader
+phase2_load_tuning).  ``apply`` loads a table into the running library
+(phase2_tune_set / phase2_set_fusion).  ``python -m phase2_b200.autotune
+--nqb 28 --out phase2_b200/tuning_b200.json`` runs a sweep on the current
+GPU and writes both files.
 """
 
 from __future__ import annotations
@@ -26,10 +35,14 @@ import numpy as np
 from . import PREC_FP32, PREC_FP64, Register, lib, world_ensure
 
 DEFAULT_FILE = Path(__file__).resolve().parent / "tuning_b200.json"
+TABLE_FILE = Path(__file__).resolve().parent / "tuning_b200.tab"
 PRECS = {"fp64": PREC_FP64, "fp32": PREC_FP32}
 # per precision: variant -> per_sm candidates
 GRIDS = {"fp64": {0: [0, 4, 8, 32], 1: [0, 1]},
          "fp32": {0: [0, 8, 16, 32]}}
+# FP32 variants of the FP64-arithmetic form, compared at the tuned density
+FP32_F64_VARIANTS = (0, 1, 2)
+FORM_LIFTED, FORM_LIFTED_F32 = 1, 2
 
 
 def _probe_rotations(nqb: int, M: int, groups: int, seed: int):
@@ -90,7 +103,33 @@ def sweep_launch(nqb: int, groups: int = 12, reps: int = 2) -> dict:
                                       "per_sm": best[1],
                                       "us_per_pass": best[2],
                                       "gbs": best[3], "trials": trials}
+                if prec == PREC_FP32 and M >= 3:
+                    out[pname][str(M)].update(_fp64_arith_variant(
+                        reg, M, best[1], flip, phase, phi, nqb, reps))
     return out
+
+
+def _fp64_arith_variant(reg, M, per_sm, flip, phase, phi, nqb, reps):
+    """The FP64-arithmetic form's kernel variant at the tuned density."""
+    L = lib()
+    form = L.phase2_get_fp32_form()
+    L.phase2_set_fp32_form(FORM_LIFTED)
+    trials, best = [], None
+    try:
+        for variant in FP32_F64_VARIANTS:
+            L.phase2_tune_set(PREC_FP32, M, variant, per_sm)
+            _time_passes(reg, flip[:M + 1], phase[:M + 1], phi[:M + 1])
+            ms = min(_time_passes(reg, flip, phase, phi)[0]
+                     for _ in range(reps))
+            gbs = 2 * (1 << nqb) * 8 / (ms * 1e-3) / 1e9
+            trials.append([variant, per_sm, ms * 1e3, gbs])
+            if best is None or ms * 1e3 < best[2]:
+                best = trials[-1]
+    finally:
+        L.phase2_set_fp32_form(form)
+    L.phase2_tune_set(PREC_FP32, M, best[0], per_sm)
+    return {"variant": best[0], "f64arith_us_per_pass": best[2],
+            "f64arith_gbs": best[3], "f64arith_trials": trials}
 
 
 def sweep_fusion(nqb: int, depth: int = 1024) -> dict:
@@ -160,6 +199,20 @@ def apply(table: dict | str | Path | None = None, prec: int | None = None):
     return table
 
 
+def write_table(table: dict, path: str | Path = TABLE_FILE) -> None:
+    """The flat launch table the library loads at world_init (C loader
+    phase2_load_tuning): the GPU name and one line per precision and
+    span."""
+    lines = ["# phase2 launch table, written by phase2_b200.autotune "
+             f"({table.get('nqb', '?')} qubits)",
+             f"gpu {table['gpu']}"]
+    for pname, per_m in table.get("launch", {}).items():
+        for M, e in sorted(per_m.items(), key=lambda kv: int(kv[0])):
+            lines.append(f"launch {PRECS[pname]} {int(M)} "
+                         f"{int(e['variant'])} {int(e['per_sm'])}")
+    Path(path).write_text("\n".join(lines) + "\n")
+
+
 def probe(nqb: int, pname: str, M: int, variant: int, per_sm: int,
           groups: int) -> dict:
     """Time `groups` passes of span M with a fixed launch choice (for
@@ -193,6 +246,7 @@ def main() -> None:
         return
     res = run(args.nqb)
     Path(args.out).write_text(json.dumps(res, indent=1))
+    write_table(res, Path(args.out).with_suffix(".tab"))
     for pname in PRECS:
         for M, e in res["launch"][pname].items():
             print(f"{pname} M={M}: variant={e['variant']} "

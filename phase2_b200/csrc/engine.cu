@@ -490,6 +490,19 @@ extern "C" int p2d_device_init(int dev, int *count)
 	return 0;
 }
 
+extern "C" int p2d_device_name(char *buf, size_t n)
+{
+	int dev = 0;
+	cudaDeviceProp prop;
+	if (!buf || n == 0 || cudaGetDevice(&dev) != cudaSuccess ||
+		cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
+		cudaGetLastError();
+		return -1;
+	}
+	snprintf(buf, n, "%s", prop.name);
+	return 0;
+}
+
 static int io_reserve(struct p2_dev *d, size_t n)
 {
 	if (n <= d->io_cap)

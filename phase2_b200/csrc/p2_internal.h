@@ -48,6 +48,13 @@ struct p2_dev;
  * number of visible devices when non-NULL. */
 int p2d_device_init(int dev, int *count);
 
+/* Name of the current CUDA device (as cudaDeviceProp.name); 0 or -1. */
+int p2d_device_name(char *buf, size_t n);
+
+/* tuning.c: apply the launch table shipped beside the library (or named
+ * by PHASE2_TUNING; "off" skips it) when its GPU name matches. */
+void p2_tuning_at_init(void);
+
 /* Register state of 2^nqb amplitudes at precision prec (enum phase2_prec),
  * with its own non-blocking stream.  NULL on failure (logged). */
 struct p2_dev *p2d_create(uint32_t nqb, int prec);

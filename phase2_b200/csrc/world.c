@@ -41,6 +41,9 @@ int world_init(int *argc, char ***argv, uint64_t seed)
 		log_error("world_init: CUDA device %d unavailable", dev);
 		return WORLD.stat = WORLD_ERR;
 	}
+	/* the shipped launch table first, so that settings from the
+	 * environment override it */
+	p2_tuning_at_init();
 	p2_settings_from_env();
 
 	WORLD.size = 1;
