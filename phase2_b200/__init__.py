@@ -446,7 +446,19 @@ def _run_driver(kind: str, nqb: int, terms: Terms, dets, **kw):
                              kw["depth"], kw["angle_det"], kw["angle_rand"],
                              kw["seed"])
     init = getattr(L, f"{kind}_init")
-    if init(C.byref(obj), C.byref(dt), hm, sp_kind, sp_ptr, None) != 0:
+    sw = None
+    if kw.get("writer") is not None:
+        # per-step output: writer(step_index, overlap) for every step or
+        # sample, as the driver produces it (the callback must outlive the
+        # run, hence kept here)
+        py_writer = kw["writer"]
+
+        def _write(_ctx, i, z):
+            py_writer(int(i), complex(z.re, z.im))
+            return 0
+        sw = _ffi.StepWriter(None, _ffi.STEP_WRITE_FN(_write))
+    if init(C.byref(obj), C.byref(dt), hm, sp_kind, sp_ptr,
+            C.cast(C.pointer(sw), C.c_void_p) if sw else None) != 0:
         raise RuntimeError(f"{kind}_init failed")
     try:
         if kw.get("fusion") is not None:

@@ -219,12 +219,18 @@ static int persistent_reg_ok(const struct qreg *reg)
  * current mode: those the persistent kernel runs (FP64, or FP32 in the
  * FP32-arithmetic form; at most 31 qubits) with a multi-determinant trial
  * state; AUTO also caps the width. */
-static int device_sampling_ok(const struct circ *ct)
+/* Whether a sampled driver runs on the device.  In AUTO mode a run with a
+ * step writer keeps the host loop, so the writer sees each sample as soon
+ * as it completes (a writer that flushes per step stays crash-consistent);
+ * ON runs such a run on the device too and calls the writer for every
+ * sample, in order, after the launch. */
+static int device_sampling_ok(const struct circ *ct,
+	const struct phase2_step_writer *sw)
 {
 	const struct p2_qreg *b = ct->reg.backend;
 	if (p2_cfg.device_sampling == PHASE2_DEVICE_SAMPLING_OFF ||
 		(p2_cfg.device_sampling == PHASE2_DEVICE_SAMPLING_AUTO &&
-			ct->reg.qb_lo > PHASE2_DEVICE_SAMPLING_AUTO_QB))
+			(ct->reg.qb_lo > PHASE2_DEVICE_SAMPLING_AUTO_QB || sw)))
 		return 0;
 	return b && b->rec == NULL && persistent_reg_ok(&ct->reg) &&
 		ct->stprep_kind == STPREP_MULTIDET && ct->md.len > 0;
@@ -363,7 +369,7 @@ static int qdrift_simul_device(struct qdrift *qd)
 
 static int qdrift_device_ok(const struct qdrift *qd)
 {
-	return device_sampling_ok(&qd->ct) && qd->ranct.cdf.len > 0 &&
+	return device_sampling_ok(&qd->ct, qd->sw) && qd->ranct.cdf.len > 0 &&
 		qd->ranct.hm_ran.len > 0 &&
 		qd->ranct.hm_ran.len < (UINT64_C(1) << 31);
 }
@@ -549,7 +555,7 @@ static int cmpsit_device_ok(const struct cmpsit *cp)
 {
 	const uint64_t T = 2 * (uint64_t)cp->dt.steps *
 		((uint64_t)cp->dt.length + cp->ranct.depth);
-	return device_sampling_ok(&cp->ct) && cp->dt.steps > 0 &&
+	return device_sampling_ok(&cp->ct, cp->sw) && cp->dt.steps > 0 &&
 		cp->dt.steps < (UINT64_C(1) << 30) &&
 		cp->ranct.depth < (UINT64_C(1) << 31) &&
 		cp->dt.length < (UINT64_C(1) << 31) &&
