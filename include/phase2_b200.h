@@ -170,6 +170,22 @@ enum phase2_device_sampling {
 #define PHASE2_DEVICE_SAMPLING_AUTO_QB 25
 int phase2_set_device_sampling(int mode);
 
+/* Check of the persistent kernel's bounded wait: runs it on a program
+ * that can never progress (its only tile taken, never completed), so
+ * every warp gives up after idle_limit idle rounds (about a microsecond
+ * each) and reports it, without touching any state.  1: the launch ended
+ * with the wait reported, 0: it ended without, -1: CUDA error.  No
+ * counterpart in the reference (its waits are MPI's). */
+int phase2_batch_wait_check(unsigned int idle_limit);
+
+/* Finish time of every instance of the last persistent batch launch, in
+ * ms after the launch's first warp started (device global timer), in the
+ * order the instances were given: copies min(n, count) values to out and
+ * returns the count (0 before any persistent launch).  Shows the tail of
+ * uneven batches: the spread between the first and the last instance to
+ * finish. */
+size_t phase2_batch_finish_ms(double *out, size_t n);
+
 /*
  * Run n independent, already initialised problems of one kind together.
  * Persistent mode (above): one launch for all instances and all their

@@ -531,12 +531,16 @@ def batch(kind: str, problems: list[dict], with_stats: bool = False):
             *[C.cast(C.pointer(o), C.c_void_p) for o in objs])
         if getattr(L, f"{kind}_simul_batch")(arr, len(objs)) != 0:
             raise RuntimeError(f"{kind}_simul_batch failed")
+        # per-instance finish times of the persistent launch (if it ran)
+        fin = (C.c_double * max(1, len(objs)))()
+        nfin = L.phase2_batch_finish_ms(fin, len(objs))
         vals = [_values(o.ct.vals) for o in objs]
         stats = []
-        for o in objs:
+        for k, o in enumerate(objs):
             st = _ffi.Stats()
             L.qreg_get_stats(C.byref(o.ct.reg), C.byref(st))
             stats.append({k: getattr(st, k) for k, _ in _ffi.Stats._fields_})
+            stats[-1]["finish_ms"] = fin[k] if nfin == len(objs) else None
     finally:
         for o in objs:
             getattr(L, f"{kind}_free")(C.byref(o))

@@ -331,6 +331,8 @@ _SIGS = {
     "cmpsit_simul_batch": (C.c_int, [_P(C.c_void_p), C.c_size_t]),
     "phase2_tune_set": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int]),
     "phase2_load_tuning": (C.c_int, [C.c_char_p, C.c_char_p]),
+    "phase2_batch_finish_ms": (C.c_size_t, [_P(C.c_double), C.c_size_t]),
+    "phase2_batch_wait_check": (C.c_int, [C.c_uint]),
     "phase2_tune_get": (C.c_int, [C.c_int, C.c_int, _P(C.c_int),
                                   _P(C.c_int)]),
     "phase2_version": (C.c_char_p, []),

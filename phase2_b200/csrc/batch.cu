@@ -19,21 +19,21 @@
 
 #include "p2_kernels.cuh"
 
-/* The cosets of one pass tile: thread k takes representatives
- * tile * cpt * P2_TPB + j * P2_TPB + k, j < cpt (coalesced per j). */
+/* The cosets of one pass tile of a warp: lane k takes representatives
+ * tile * cpt * 32 + j * 32 + k, j < cpt (coalesced per j). */
 template <int M>
 __device__ __forceinline__ void p2_batch_pass_tile(float2 *st,
 	const struct phase2_pass &p, uint32_t tile, uint64_t nrep, uint32_t cpt,
-	const struct p2_lift32_rec *srec)
+	const struct p2_lift32_rec *srec, uint32_t lane)
 {
 	uint32_t pb[M > 0 ? M : 1];
 #pragma unroll
 	for (int k = 0; k < M; ++k)
 		pb[k] = (uint32_t)p.basis[k];
 	const uint32_t negm = p.scale < 0 ? 0x80000000u : 0u;
-	const uint64_t t0 = (uint64_t)tile * cpt * P2_TPB + threadIdx.x;
+	const uint64_t t0 = (uint64_t)tile * cpt * 32 + lane;
 	for (uint32_t j = 0; j < cpt; ++j) {
-		const uint64_t t = t0 + (uint64_t)j * P2_TPB;
+		const uint64_t t = t0 + (uint64_t)j * 32;
 		if (t < nrep)
 			p2_lift32_coset<M, uint32_t, true>(st,
 				p2_rep_t<M, uint32_t>((uint32_t)t, p), pb, srec,
@@ -46,15 +46,15 @@ __device__ __forceinline__ void p2_batch_pass_tile(float2 *st,
 template <int M>
 __device__ __forceinline__ void p2_batch_pass_tile64(double2 *st,
 	const struct phase2_pass &p, uint32_t tile, uint64_t nrep, uint32_t cpt,
-	const struct phase2_rot_rec *srec)
+	const struct phase2_rot_rec *srec, uint32_t lane)
 {
 	uint64_t pb[M > 0 ? M : 1];
 #pragma unroll
 	for (int k = 0; k < M; ++k)
 		pb[k] = p.basis[k];
-	const uint64_t t0 = (uint64_t)tile * cpt * P2_TPB + threadIdx.x;
+	const uint64_t t0 = (uint64_t)tile * cpt * 32 + lane;
 	for (uint32_t j = 0; j < cpt; ++j) {
-		const uint64_t t = t0 + (uint64_t)j * P2_TPB;
+		const uint64_t t = t0 + (uint64_t)j * 32;
 		if (t >= nrep)
 			continue;
 		const uint64_t x = p2_rep<M>(t, p);
@@ -93,6 +93,64 @@ template <> struct p2_brec<double2> {
 	}
 };
 
+/* Span dispatch of a pass tile (FP32 or FP64 state). */
+template <typename ST, typename RT>
+__device__ __forceinline__ void p2_batch_pass(ST *st,
+	const struct phase2_pass &p, uint32_t tile, uint64_t nrep, uint32_t cpt,
+	const RT *srec, uint32_t lane)
+{
+	if constexpr (sizeof(ST) == 16) {
+		switch (p.span) {
+		case 0:
+			p2_batch_pass_tile64<0>(st, p, tile, nrep, cpt, srec, lane);
+			break;
+		case 1:
+			p2_batch_pass_tile64<1>(st, p, tile, nrep, cpt, srec, lane);
+			break;
+		case 2:
+			p2_batch_pass_tile64<2>(st, p, tile, nrep, cpt, srec, lane);
+			break;
+		case 3:
+			p2_batch_pass_tile64<3>(st, p, tile, nrep, cpt, srec, lane);
+			break;
+		case 4:
+			p2_batch_pass_tile64<4>(st, p, tile, nrep, cpt, srec, lane);
+			break;
+		default:
+			p2_batch_pass_tile64<5>(st, p, tile, nrep, cpt, srec, lane);
+			break;
+		}
+	} else {
+		switch (p.span) {
+		case 0:
+			p2_batch_pass_tile<0>(st, p, tile, nrep, cpt, srec, lane);
+			break;
+		case 1:
+			p2_batch_pass_tile<1>(st, p, tile, nrep, cpt, srec, lane);
+			break;
+		case 2:
+			p2_batch_pass_tile<2>(st, p, tile, nrep, cpt, srec, lane);
+			break;
+		case 3:
+			p2_batch_pass_tile<3>(st, p, tile, nrep, cpt, srec, lane);
+			break;
+		case 4:
+			p2_batch_pass_tile<4>(st, p, tile, nrep, cpt, srec, lane);
+			break;
+		default:
+			p2_batch_pass_tile<5>(st, p, tile, nrep, cpt, srec, lane);
+			break;
+		}
+	}
+}
+
+__device__ __forceinline__ unsigned long long p2_globaltimer()
+{
+	unsigned long long t;
+	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+	return t;
+}
+
 template <typename ST>
 __global__ void __launch_bounds__(P2_TPB, sizeof(ST) == 8 ? 5 : 2)
 	k_batch(const struct p2_binst *__restrict__ inst, uint32_t ninst,
@@ -107,17 +165,28 @@ __global__ void __launch_bounds__(P2_TPB, sizeof(ST) == 8 ? 5 : 2)
 {
 	constexpr bool F64 = sizeof(ST) == 16;
 	typedef typename p2_brec<ST>::type RT;
-	__shared__ RT srec[P2_MAX_ROTS_PER_PASS];
-	__shared__ uint32_t s_inst, s_seq, s_tile;
-	__shared__ int s_what; /* 0 nothing claimable yet, 1 work, 2 exit */
-	/* pass whose records srec holds (block-uniform), none at first */
-	uint32_t held = 0xffffffffu;
-	uint32_t cursor = blockIdx.x % ninst;
+	/* each warp keeps the records of the pass it last ran */
+	__shared__ RT srec_all[P2_BATCH_WARPS][P2_MAX_ROTS_PER_PASS];
+	const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+	RT *const srec = srec_all[wid];
+	const uint32_t gw = blockIdx.x * P2_BATCH_WARPS + wid;
+	if (lane == 0) {
+		/* start of the launch: the earliest warp's timer (status[2..3]
+		 * holds its complement, so that zero-initialised memory works
+		 * with atomicMax) */
+		atomicMax((unsigned long long *)(status + 2),
+			~p2_globaltimer());
+	}
+	uint32_t held = 0xffffffffu; /* pass whose records srec holds */
+	uint32_t cursor = gw % ninst;
 	unsigned int idle = 0;
 	unsigned long long seen = 0; /* tickets at the last idle round */
 	for (;;) {
-		if (threadIdx.x == 0) {
-			int what = 2;
+		/* lane 0 claims a tile: what = 0 nothing claimable yet, 1 work,
+		 * 2 exit */
+		int what = 2;
+		uint32_t ci = 0, cseq = 0, ctile = 0;
+		if (lane == 0) {
 			unsigned long long sig = 0;
 			for (uint32_t k = 0; k < ninst; ++k) {
 				const uint32_t i = cursor + k < ninst
@@ -141,9 +210,9 @@ __global__ void __launch_bounds__(P2_TPB, sizeof(ST) == 8 ? 5 : 2)
 				const uint32_t tile = (uint32_t)got;
 				if (seq < nops && tile < ops[off + seq].ntiles) {
 					__threadfence();
-					s_inst = i;
-					s_seq = seq;
-					s_tile = tile;
+					ci = i;
+					cseq = seq;
+					ctile = tile;
 					cursor = i;
 					what = 1;
 					break;
@@ -163,131 +232,137 @@ __global__ void __launch_bounds__(P2_TPB, sizeof(ST) == 8 ? 5 : 2)
 			} else if (what == 1) {
 				idle = 0;
 			}
-			s_what = what;
 		}
-		__syncthreads();
-		const int what = s_what;
+		what = __shfl_sync(0xffffffffu, what, 0);
 		if (what == 2)
 			return;
-		if (what == 1) {
-			const uint32_t i = s_inst, seq = s_seq, tile = s_tile;
-			ST *const st = (ST *)inst[i].state;
-			const uint64_t namp = inst[i].namp;
-			const struct p2_op op = ops[inst[i].op_off + seq];
-			if (op.kind == P2_OP_PASS) {
-				const struct phase2_pass p = passes[op.a];
-				/* consecutive tiles of one pass (a Trotter step
-				 * replays the same passes) keep their records */
-				if (held != op.a) {
-					for (uint32_t r = threadIdx.x; r < p.nrot;
-						r += blockDim.x)
-						srec[r] = p2_brec<ST>::of(
-							recs[p.rot_off + r]);
-					held = op.a;
-					__syncthreads();
-				}
-				const uint64_t nrep = namp >> p.span;
-				if constexpr (F64) {
-					switch (p.span) {
-					case 0:
-						p2_batch_pass_tile64<0>(st, p, tile,
-							nrep, op.b, srec);
-						break;
-					case 1:
-						p2_batch_pass_tile64<1>(st, p, tile,
-							nrep, op.b, srec);
-						break;
-					case 2:
-						p2_batch_pass_tile64<2>(st, p, tile,
-							nrep, op.b, srec);
-						break;
-					case 3:
-						p2_batch_pass_tile64<3>(st, p, tile,
-							nrep, op.b, srec);
-						break;
-					case 4:
-						p2_batch_pass_tile64<4>(st, p, tile,
-							nrep, op.b, srec);
-						break;
-					default:
-						p2_batch_pass_tile64<5>(st, p, tile,
-							nrep, op.b, srec);
-						break;
-					}
-				} else {
-					switch (p.span) {
-					case 0:
-						p2_batch_pass_tile<0>(st, p, tile,
-							nrep, op.b, srec);
-						break;
-					case 1:
-						p2_batch_pass_tile<1>(st, p, tile,
-							nrep, op.b, srec);
-						break;
-					case 2:
-						p2_batch_pass_tile<2>(st, p, tile,
-							nrep, op.b, srec);
-						break;
-					case 3:
-						p2_batch_pass_tile<3>(st, p, tile,
-							nrep, op.b, srec);
-						break;
-					case 4:
-						p2_batch_pass_tile<4>(st, p, tile,
-							nrep, op.b, srec);
-						break;
-					default:
-						p2_batch_pass_tile<5>(st, p, tile,
-							nrep, op.b, srec);
-						break;
-					}
-				}
-			} else if (op.kind == P2_OP_ZERO) {
-				const uint64_t base =
-					(uint64_t)tile * P2_BATCH_ZERO_TILE;
-				ST zero;
-				zero.x = 0;
-				zero.y = 0;
-				for (uint32_t k = threadIdx.x;
-					k < P2_BATCH_ZERO_TILE; k += blockDim.x)
-					if (base + k < namp)
-						__stcg(st + base + k, zero);
-			} else if (op.kind == P2_OP_WRITE) {
-				/* in order: later writes win */
-				if (threadIdx.x == 0)
-					for (uint32_t e = op.a; e < op.a + op.b; ++e) {
-						ST v;
-						if constexpr (F64) {
-							v.x = wval[2 * e];
-							v.y = wval[2 * e + 1];
-						} else {
-							v.x = (float)wval[2 * e];
-							v.y = (float)wval[2 * e + 1];
-						}
-						__stcg(st + widx[e], v);
-					}
-			} else {
-				for (uint32_t d = threadIdx.x; d < op.b;
-					d += blockDim.x) {
-					const ST v = __ldcg(st + gidx[op.a + d]);
-					gout[op.a + d] = make_double2(v.x, v.y);
-				}
+		if (what == 0)
+			continue;
+		const uint32_t i = __shfl_sync(0xffffffffu, ci, 0);
+		const uint32_t seq = __shfl_sync(0xffffffffu, cseq, 0);
+		const uint32_t tile = __shfl_sync(0xffffffffu, ctile, 0);
+		ST *const st = (ST *)inst[i].state;
+		const uint64_t namp = inst[i].namp;
+		const struct p2_op op = ops[inst[i].op_off + seq];
+		if (op.kind == P2_OP_PASS) {
+			const struct phase2_pass p = passes[op.a];
+			/* consecutive tiles of one pass (a Trotter step replays
+			 * the same passes) keep their records */
+			if (held != op.a) {
+				__syncwarp();
+				for (uint32_t r = lane; r < p.nrot; r += 32)
+					srec[r] = p2_brec<ST>::of(recs[p.rot_off + r]);
+				held = op.a;
+				__syncwarp();
 			}
-			__threadfence();
-			__syncthreads();
-			if (threadIdx.x == 0) {
-				const unsigned int d =
-					atomicAdd(&ctl[i].done, 1u) + 1u;
-				if (d == op.ntiles) {
-					atomicExch(&ctl[i].done, 0u);
-					__threadfence();
-					atomicExch(&ctl[i].ticket,
-						(unsigned long long)(seq + 1) << 32);
+			p2_batch_pass<ST, RT>(st, p, tile, namp >> p.span, op.b,
+				srec, lane);
+		} else if (op.kind == P2_OP_ZERO) {
+			const uint64_t base = (uint64_t)tile * P2_BATCH_ZERO_TILE;
+			ST zero;
+			zero.x = 0;
+			zero.y = 0;
+			for (uint32_t k = lane; k < P2_BATCH_ZERO_TILE; k += 32)
+				if (base + k < namp)
+					__stcg(st + base + k, zero);
+		} else if (op.kind == P2_OP_WRITE) {
+			/* in order: later writes win */
+			if (lane == 0)
+				for (uint32_t e = op.a; e < op.a + op.b; ++e) {
+					ST v;
+					if constexpr (F64) {
+						v.x = wval[2 * e];
+						v.y = wval[2 * e + 1];
+					} else {
+						v.x = (float)wval[2 * e];
+						v.y = (float)wval[2 * e + 1];
+					}
+					__stcg(st + widx[e], v);
 				}
+		} else {
+			for (uint32_t d = lane; d < op.b; d += 32) {
+				const ST v = __ldcg(st + gidx[op.a + d]);
+				gout[op.a + d] = make_double2(v.x, v.y);
 			}
 		}
-		__syncthreads();
+		__threadfence();
+		__syncwarp();
+		if (lane == 0) {
+			const unsigned int d = atomicAdd(&ctl[i].done, 1u) + 1u;
+			if (d == op.ntiles) {
+				atomicExch(&ctl[i].done, 0u);
+				if (seq + 1 == inst[i].nops)
+					ctl[i].end_ns = p2_globaltimer();
+				__threadfence();
+				atomicExch(&ctl[i].ticket,
+					(unsigned long long)(seq + 1) << 32);
+			}
+		}
 	}
+}
+
+/* ---- bounded-wait check -------------------------------------------------- */
+
+/*
+ * The persistent kernel on a program that can never make progress: one
+ * instance whose only op has one tile, with the ticket preset past that
+ * tile (taken) and no completion ever counted.  Every warp then finds
+ * nothing to claim while no ticket moves, so each gives up after
+ * idle_limit rounds, raises status and returns; no state memory is
+ * touched.  Returns 1 when the launch ended that way, 0 when it ended
+ * without raising status, -1 on a CUDA error.
+ */
+extern "C" int phase2_batch_wait_check(unsigned int idle_limit)
+{
+	struct p2_binst hinst;
+	struct p2_op hop;
+	struct p2_bctl hctl;
+	memset(&hinst, 0, sizeof hinst);
+	memset(&hop, 0, sizeof hop);
+	memset(&hctl, 0, sizeof hctl);
+	hinst.namp = 256;
+	hinst.op_off = 0;
+	hinst.nops = 1;
+	hop.kind = P2_OP_ZERO;
+	hop.ntiles = 1;
+	hctl.ticket = 1; /* op 0, tile 1: the op's only tile is taken */
+	unsigned char *buf = NULL;
+	const size_t o_state = 0, o_inst = 256, o_op = 512, o_ctl = 768,
+		     o_status = 1024, total = 1280;
+	cudaError_t e = cudaMalloc((void **)&buf, total);
+	if (e == cudaSuccess) {
+		hinst.state = buf + o_state;
+		e = cudaMemset(buf, 0, total);
+	}
+	if (e == cudaSuccess)
+		e = cudaMemcpy(buf + o_inst, &hinst, sizeof hinst,
+			cudaMemcpyHostToDevice);
+	if (e == cudaSuccess)
+		e = cudaMemcpy(buf + o_op, &hop, sizeof hop,
+			cudaMemcpyHostToDevice);
+	if (e == cudaSuccess)
+		e = cudaMemcpy(buf + o_ctl, &hctl, sizeof hctl,
+			cudaMemcpyHostToDevice);
+	unsigned int status = 0;
+	if (e == cudaSuccess) {
+		k_batch<float2><<<2, P2_TPB>>>(
+			(const struct p2_binst *)(buf + o_inst), 1,
+			(const struct p2_op *)(buf + o_op), NULL, NULL, NULL,
+			NULL, NULL, NULL, (struct p2_bctl *)(buf + o_ctl),
+			(unsigned int *)(buf + o_status), idle_limit);
+		e = cudaGetLastError();
+	}
+	if (e == cudaSuccess)
+		e = cudaDeviceSynchronize();
+	if (e == cudaSuccess)
+		e = cudaMemcpy(&status, buf + o_status, sizeof status,
+			cudaMemcpyDeviceToHost);
+	cudaFree(buf);
+	if (e != cudaSuccess) {
+		log_error("batch wait check: %s", cudaGetErrorString(e));
+		return -1;
+	}
+	return status ? 1 : 0;
 }
 
 /* ---- batched persistent execution --------------------------------------- */
@@ -302,6 +377,69 @@ extern "C" int p2d_batch_ok(const struct p2_dev *d)
 static size_t p2_align256(size_t v)
 {
 	return (v + 255) & ~(size_t)255;
+}
+
+/* Finish time of every program of the last persistent launch, in ms after
+ * the launch's first warp started (phase2_batch_finish_ms). */
+static double *last_finish;
+static size_t last_n;
+
+static cudaError_t finish_times(const unsigned char *d_ctl,
+	const unsigned char *d_status, size_t n)
+{
+	struct p2_bctl *c = (struct p2_bctl *)malloc(n * sizeof *c);
+	double *f = (double *)realloc(last_finish, n * sizeof *f);
+	if (!c || !f) {
+		free(c);
+		if (f)
+			last_finish = f;
+		return cudaErrorMemoryAllocation;
+	}
+	last_finish = f;
+	unsigned long long start = 0;
+	cudaError_t e = cudaMemcpy(c, d_ctl, n * sizeof *c,
+		cudaMemcpyDeviceToHost);
+	if (e == cudaSuccess)
+		e = cudaMemcpy(&start, d_status + 8, sizeof start,
+			cudaMemcpyDeviceToHost);
+	start = ~start;
+	for (size_t i = 0; i < n && e == cudaSuccess; i++)
+		f[i] = c[i].end_ns >= start ? (double)(c[i].end_ns - start) / 1e6
+					    : 0.0;
+	last_n = e == cudaSuccess ? n : 0;
+	free(c);
+	return e;
+}
+
+extern "C" void p2_batch_finish_reset(void)
+{
+	last_n = 0;
+}
+
+extern "C" int p2_batch_finish_map(const size_t *who, size_t m, size_t n)
+{
+	if (last_n != m)
+		return -1;
+	double *f = (double *)malloc((n ? n : 1) * sizeof *f);
+	if (!f)
+		return -1;
+	for (size_t i = 0; i < n; i++)
+		f[i] = -1.0;
+	for (size_t j = 0; j < m; j++)
+		if (who[j] < n)
+			f[who[j]] = last_finish[j];
+	free(last_finish);
+	last_finish = f;
+	last_n = n;
+	return 0;
+}
+
+extern "C" size_t phase2_batch_finish_ms(double *out, size_t n)
+{
+	const size_t k = n < last_n ? n : last_n;
+	if (out && k)
+		memcpy(out, last_finish, k * sizeof *out);
+	return last_n;
 }
 
 /* k_batch for FP32 or FP64 registers: its kernel function (occupancy
@@ -490,6 +628,8 @@ extern "C" int p2d_batch_run(struct p2_dev *const *devs,
 	if (e == cudaSuccess && ng)
 		e = cudaMemcpy(gout, dbuf + o_gout, ng * sizeof(double2),
 			cudaMemcpyDeviceToHost);
+	if (e == cudaSuccess)
+		e = finish_times(dbuf + o_ctl, dbuf + o_status, n);
 	float ms = 0.0f;
 	if (e == cudaSuccess)
 		e = cudaEventElapsedTime(&ms, d0->t0, d0->t1);

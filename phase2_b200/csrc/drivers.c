@@ -774,6 +774,7 @@ static int run_batch_persistent(struct batch_item *items, size_t n)
 			items[who[j]].failed = 1;
 		goto out;
 	}
+	(void)p2_batch_finish_map(who, m, n);
 	if (getenv("PHASE2_BATCH_TIMING"))
 		log_info("batch: %zu programs, record %.3f s, launch+copy %.3f s"
 			 " (kernel %.3f s)",
@@ -874,6 +875,7 @@ static int run_batch_streams(struct batch_item *items, size_t n)
 		struct batch_item *items = calloc(n, sizeof *items);           \
 		if (!items)                                                    \
 			return -1;                                             \
+		p2_batch_finish_reset();                                       \
 		for (size_t i = 0; i < n; i++) {                               \
 			items[i].obj = objs[i];                                \
 			items[i].ct = &objs[i]->ct;                            \

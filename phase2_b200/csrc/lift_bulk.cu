@@ -273,8 +273,8 @@ __device__ __forceinline__ void p2_cp16(uint32_t dst, const void *src)
 		: "memory");
 }
 
-template <int M>
-__global__ void __launch_bounds__(P2_LB_TPB, p2_lb_blocks(M))
+template <int M, int MINB>
+__global__ void __launch_bounds__(P2_LB_TPB, MINB)
 	k_pass_lift_pf(float2 *__restrict__ st, uint32_t nwc,
 		struct phase2_pass p,
 		const struct phase2_rot_rec *__restrict__ recs)
@@ -396,26 +396,26 @@ static unsigned lb_grid(const struct p2_dev *d, int per_sm_occ,
 	return (unsigned)grid;
 }
 
-template <int M>
+template <int M, int MINB>
 static int pf_launch_t(struct p2_dev *d, const struct phase2_pass *p,
 	const struct phase2_rot_rec *recs, unsigned per_sm_cap)
 {
 	static struct p2_lb_cfg cfg;
 	const unsigned smem = p2_lb_smem(M);
 	if (!cfg.ready) {
-		CUDA_OK(cudaFuncSetAttribute(k_pass_lift_pf<M>,
+		CUDA_OK(cudaFuncSetAttribute(k_pass_lift_pf<M, MINB>,
 				cudaFuncAttributeMaxDynamicSharedMemorySize,
 				(int)smem),
 			"staged pass shared memory");
 		int n = 0;
 		CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n,
-				k_pass_lift_pf<M>, P2_LB_TPB, smem),
+				k_pass_lift_pf<M, MINB>, P2_LB_TPB, smem),
 			"staged pass occupancy");
 		cfg.per_sm = n > 0 ? n : 1;
 		cfg.ready = 1;
 	}
 	const uint32_t nwc = (uint32_t)((d->namp >> M) >> 5);
-	k_pass_lift_pf<M><<<lb_grid(d, cfg.per_sm, per_sm_cap, nwc),
+	k_pass_lift_pf<M, MINB><<<lb_grid(d, cfg.per_sm, per_sm_cap, nwc),
 		P2_LB_TPB, smem, d->stream>>>((float2 *)d->state, nwc, *p,
 		recs);
 	return 1;
@@ -468,12 +468,17 @@ extern "C" int p2_lift_staged_launch(struct p2_dev *d,
 			return lb_launch_t<5>(d, p, recs, per_sm_cap);
 		}
 	}
+	/* a cap of two blocks per SM selects the build with the whole
+	 * register file of those blocks (up to 255 registers a thread) */
 	switch (p->span) {
 	case 3:
-		return pf_launch_t<3>(d, p, recs, per_sm_cap);
+		return pf_launch_t<3, p2_lb_blocks(3)>(d, p, recs, per_sm_cap);
 	case 4:
-		return pf_launch_t<4>(d, p, recs, per_sm_cap);
+		return pf_launch_t<4, p2_lb_blocks(4)>(d, p, recs, per_sm_cap);
 	default:
-		return pf_launch_t<5>(d, p, recs, per_sm_cap);
+		return per_sm_cap == 2
+			? pf_launch_t<5, 2>(d, p, recs, per_sm_cap)
+			: pf_launch_t<5, p2_lb_blocks(5)>(d, p, recs,
+				  per_sm_cap);
 	}
 }

@@ -124,7 +124,9 @@ struct p2_bctl;
 #define P2_BATCH_IDLE_LIMIT 2000000u
 
 /* batch.cu: the persistent kernel for FP32 or FP64 registers (its
- * function, for occupancy queries, and its launch). */
+ * function, for occupancy queries, and its launch).  status points to 16
+ * zeroed bytes: status[0] is raised when a wait gives up, status[2..3]
+ * receive the complement of the launch's start time (global timer). */
 const void *p2_batch_kernel(bool f64);
 void p2_batch_launch(bool f64, unsigned grid, cudaStream_t stream,
 	const struct p2_binst *inst, uint32_t ninst, const struct p2_op *ops,

@@ -181,6 +181,13 @@ void p2d_set_sweep_kernel(int on);
  * persistent launch; gout receives every program's gathered amplitudes
  * (FP64 re, im) in program order.  *kernel_ms (if non-NULL) gets the
  * launch's device time.  0 or -1. */
+/* batch.cu: per-instance finish times of the last persistent launch
+ * (phase2_batch_finish_ms): cleared at the start of a batched driver call,
+ * and re-indexed from launched programs to instances (who[j] = instance
+ * of program j; instances not launched get -1). */
+void p2_batch_finish_reset(void);
+int p2_batch_finish_map(const size_t *who, size_t m, size_t n);
+
 int p2d_batch_run(struct p2_dev *const *devs,
 	const struct p2_prog *const *progs, size_t n, double *gout,
 	double *kernel_ms);

@@ -584,33 +584,37 @@ __device__ __forceinline__ void p2_lift32_coset(float2 *__restrict__ st, IT x,
 
 /*
  * Many registers' recorded programs (p2_internal.h) in one launch.  Every
- * op of a program is cut into tiles (a pass: 128 cosets, one per thread;
- * a zero: 4096 amplitudes; a write or gather: one tile); op k+1 of a
- * program starts only when every tile of op k is done, programs are
- * independent.  Each program has a ticket, (op << 32) | next tile: a block
- * claims a tile with one atomicAdd, and the block that completes the last
- * tile of an op publishes the next op by resetting the ticket.  Blocks
- * look for work across programs starting from the last one they served,
- * so small programs interleave and the GPU stays busy without a launch per
- * pass.  Waiting is bounded: a block that finds nothing to claim while no
- * ticket moves for idle_limit consecutive rounds (about a microsecond
- * each; a ticket moves whenever any tile is claimed or any op is
- * published) raises status and returns, so a scheduling fault ends the
+ * op of a program is cut into tiles (a pass: 32 lanes times a few cosets
+ * each; a zero: 16384 amplitudes; a write or gather: one tile); op k+1 of
+ * a program starts only when every tile of op k is done, programs are
+ * independent.  Each program has a ticket, (op << 32) | next tile.  Every
+ * warp schedules itself: its lane 0 claims a tile with one atomicAdd and
+ * broadcasts it, the warp runs it, and the warp that completes the last
+ * tile of an op publishes the next op by resetting the ticket -- no block
+ * barrier anywhere, so a warp never waits for its block's other warps.
+ * Warps look for work across programs starting from the last one they
+ * served, so small programs interleave and the GPU stays busy without a
+ * launch per pass.  Waiting is bounded: a warp that finds nothing to claim
+ * while no ticket moves for idle_limit consecutive rounds (about a
+ * microsecond each; a ticket moves whenever any tile is claimed or any op
+ * is published) raises status and returns, so a scheduling fault ends the
  * launch instead of hanging it, while long single-program runs, where most
- * blocks wait on one op at a time, keep going.
+ * warps wait on one op at a time, keep going.
  *
- * Ordering: a tile's stores are made visible (each thread fences, then the
- * block barrier) before its completion count; the finisher fences before
- * publishing the next op; a claimer fences after its claim.  State loads
+ * Ordering: a tile's stores are made visible (each lane fences, then the
+ * warp synchronises) before its completion count; the finisher fences
+ * before publishing the next op; a claimer fences after its claim, and
+ * the other lanes read the claim only through the broadcast.  State loads
  * and stores go through L2 only (ld/st .cg), since L1 is not coherent
  * across SMs.
  */
-/* Cosets per thread in a pass tile: 4 for passes of at least
+/* Cosets per lane in a pass tile: 4 for passes of at least
  * P2_BATCH_BIG_PASS representatives, 1 below (more tiles for small
  * registers, whose passes are otherwise too few tiles to spread). */
 #define P2_BATCH_COSETS 4
 #define P2_BATCH_BIG_PASS (UINT64_C(1) << 16)
 #define P2_BATCH_ZERO_TILE (P2_TPB * 128)
+#define P2_BATCH_WARPS (P2_TPB / 32)
 
 struct p2_binst {
 	void *state; /* float2 (FP32) or double2 (FP64) amplitudes */
@@ -626,7 +630,7 @@ __host__ __device__ __forceinline__ uint32_t p2_op_tiles(uint32_t kind,
 	if (kind == P2_OP_PASS) {
 		const uint64_t nrep = namp >> span;
 		*b = nrep >= P2_BATCH_BIG_PASS ? P2_BATCH_COSETS : 1;
-		const uint64_t per = (uint64_t)*b * P2_TPB;
+		const uint64_t per = (uint64_t)*b * 32;
 		return (uint32_t)((nrep + per - 1) / per);
 	}
 	if (kind == P2_OP_ZERO)
@@ -639,6 +643,7 @@ struct p2_bctl {
 	unsigned long long ticket;
 	unsigned int done;
 	unsigned int pad;
+	unsigned long long end_ns; /* global timer when the program finished */
 };
 
 #endif /* P2_KERNELS_CUH */

@@ -341,7 +341,7 @@ extern "C" int p2d_sampled_device(struct p2_dev *d,
 		sz[SOFF] = G * sizeof(uint32_t);
 		sz[REGS] = R * (sizeof(struct p2_binst) +
 				       sizeof(struct p2_bctl)) +
-			sizeof(unsigned int) + (R - 1) * d->namp * d->elem;
+			4 * sizeof(unsigned int) + (R - 1) * d->namp * d->elem;
 		total = 0;
 		for (int i = 0; i < NBUF; i++) {
 			off[i] = total;
@@ -490,7 +490,7 @@ extern "C" int p2d_sampled_device(struct p2_dev *d,
 			e = cudaMemsetAsync(ctl, 0, nreg * sizeof *ctl,
 				d->stream);
 		if (e == cudaSuccess)
-			e = cudaMemsetAsync(status, 0, sizeof(unsigned int),
+			e = cudaMemsetAsync(status, 0, 4 * sizeof(unsigned int),
 				d->stream);
 		if (e == cudaSuccess)
 			p2_batch_launch(f64, grid, d->stream, inst, nreg,
