@@ -187,8 +187,35 @@ def _ffi_stats(p2, obj):
     return {k: getattr(st, k) for k, _ in _ffi.Stats._fields_}
 
 
-def _traffic_per_launch():
-    p = ROOT / "profiles" / "k_pass_lift32_traffic.json"
+# what the headline FP32 form computes, for the line's "storage" key
+STORAGE = {
+    2: ("complex64 state; each pair rotated by three shears in FP32 FMAs "
+        "whose coefficients s and t = tan(phi/2) are computed in FP64 and "
+        "rounded to FP32 (planner); norms and overlaps in FP64"),
+    1: ("complex64 state; each pass widens its amplitudes to FP64, applies "
+        "all its rotations in FP64 arithmetic with the FP64 coefficients "
+        "(s and t = tan(phi/2) from FP64 cos/sin), and rounds to FP32 once "
+        "at the store; norms and overlaps in FP64"),
+}
+FORM_NAME = {1: "f64 arithmetic (PHASE2_FORM_LIFTED)",
+             2: "f32 arithmetic (PHASE2_FORM_LIFTED_F32)"}
+
+
+def _headline_kernel(p2, form: int) -> str:
+    """The pass kernel that carries the headline's span-5 passes."""
+    if form == p2.FORM_LIFTED_F32:
+        return "k_pass_lift32<M,uint32_t>"
+    v, per = C.c_int(), C.c_int()
+    p2.lib().phase2_tune_get(p2.PREC_FP32, 5, C.byref(v), C.byref(per))
+    return {0: "k_pass_lift<M,uint32_t>", 1: "k_pass_lift_bulk<M>",
+            2: "k_pass_lift_pf<M,3>", 3: "k_pass_lift_pf<M,2>"}[v.value]
+
+
+def _traffic_per_launch(kernel: str):
+    """ncu DRAM bytes of one 30-qubit launch of the kernel (profiles/,
+    scaled from a 26-qubit capture), or None without a capture."""
+    name = kernel.split("<")[0]
+    p = ROOT / "profiles" / f"{name}_traffic.json"
     if p.is_file():
         try:
             return json.loads(p.read_text()).get("bytes_per_launch_30q_fp32")
@@ -221,38 +248,54 @@ def _reference_gpu(nqb: int, nrot: int = 16, reps: int = 3):
                      f"{nrot} rotations at {nqb} qubits")}
 
 
-def _cpu_baseline(nrot: int = 8, reps: int = 2, max_qb: int = 25) -> dict:
-    """Reference CPU qreg_paulirot on R processes x one 2^(30-log2 R) slab.
+# CPU baseline: the reference's own qdrift driver on the headline
+# workload, as R ranks of one job on the host cores
+CPU_DEPTH = 4    # draws per timed sample (of the workload's 4096)
+CPU_REPS = 3     # min of K, the reference's convention (bench/bench.h)
 
-    R is the largest power of two <= the host's cores (at most 128); each
-    process holds one rank's share of the 30-qubit state (capped at
-    2^max_qb amplitudes to bound the sample to tens of seconds)."""
-    exe = ROOT / "oracle" / "_ref" / "ref_bench"
-    if not exe.is_file():
-        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
-                "sample": "oracle/_ref/ref_bench not built"}
+
+def _cpu_ranks() -> int:
     cores = os.cpu_count() or 1
-    R = 1 << int(math.log2(max(1, min(cores, 128))))
-    qb = min(max(16, 30 - int(math.log2(R))), max_qb)
-    procs = [subprocess.Popen([str(exe), str(qb), str(nrot), str(reps)],
-                              stdout=subprocess.PIPE,
-                              stderr=subprocess.DEVNULL, text=True)
-             for _ in range(R)]
-    rates = []
-    for p in procs:
-        out, _ = p.communicate(timeout=600)
-        try:
-            rates.append(float(out.split()[-1]))
-        except (IndexError, ValueError):
-            pass
-    total = sum(rates)
-    return {"value": total, "unit": UNIT, "cores": len(rates),
-            "kind": "reference",
-            "sample": (f"{len(rates)} processes x reference qreg_paulirot "
-                       f"(CPU backend, 1 rank each) on a {qb}-qubit slab, "
-                       f"{nrot} JW-like rotations, min of {reps}; each process "
-                       f"is one rank's share of the 30-qubit state; the "
-                       f"partner exchange is omitted (upper bound)")}
+    return 1 << int(math.log2(max(1, min(cores, 256))))
+
+
+def _cpu_reference(cfg: dict, depth: int, reps: int, warmup: int,
+                   ranks: int | None = None) -> dict:
+    """The reference's qdrift_simul (phase2/circ/qdrift.c, CPU backend,
+    built from its sources with its release optimisation) on the
+    headline's Hamiltonian, determinant, step size and seed, as R MPI ranks
+    of one job on this host's cores (oracle/_ref/ref_mpi over the
+    shared-memory MPI stand-in), each holding its 2^(n - log2 R)
+    amplitudes as the reference distributes them; one sample per run,
+    truncated to `depth` of its draws (prepst, draws, rotations with their
+    slab exchanges, overlap), min over `reps` runs after `warmup`."""
+    import tempfile
+
+    from oracle import REF_MPI, run_ref_mpi, write_ref_input
+    nqb = cfg["nqb"]
+    R = ranks or _cpu_ranks()
+    base = {"unit": UNIT, "cores": R, "kind": "reference"}
+    if not REF_MPI.is_file():
+        return dict(base, value=None, sample=(
+            "oracle/_ref/ref_mpi not built (reference sources absent at "
+            "build time)"))
+    t, d = cfg["terms"], cfg["dets"]
+    with tempfile.TemporaryDirectory() as tmp:
+        path = Path(tmp) / "qdrift.in"
+        write_ref_input(path, "qdrift", nqb, t.flip, t.phase, t.cf, d.idx,
+                        d.cf, depth, cfg["step_size"], cfg["seed"])
+        r = run_ref_mpi(R, path, reps, warmup=warmup, timeout=3600)
+    return dict(base, value=r["rot_amp_s"], seconds_per_sample=r["seconds"],
+                rotations_per_sample=r["rotations"], sample=(
+                    f"reference qdrift_simul, CPU backend (-O3, AVX2/FMA), "
+                    f"as {R} MPI ranks of one job on {R} host cores "
+                    f"(shared-memory MPI stand-in, "
+                    f"{'mailbox' if r['mailbox'] else 'single-copy'} slab "
+                    f"exchange), on the {nqb}-qubit headline workload "
+                    f"({len(t.cf)} JW terms, same determinant, step size "
+                    f"and seed): one sample truncated to {depth} of its "
+                    f"{cfg['depth']} draws (prepst, draws, rotations, "
+                    f"overlap), min of {reps} runs after {warmup} warm-up"))
 
 
 def gpu_arm(args) -> None:
@@ -273,9 +316,11 @@ def gpu_arm(args) -> None:
     if args.lift_kernel:
         # FP64-arithmetic passes of span 3-5: direct loads, or the next
         # cosets staged by bulk copies or by cp.async
-        v = {"direct": 0, "bulk": 1, "staged": 2}[args.lift_kernel]
+        v = {"direct": 0, "bulk": 1, "staged": 2,
+             "staged2": 3}[args.lift_kernel]
         for span in (3, 4, 5):
             p2.lib().phase2_tune_set(p2.PREC_FP32, span, v, 32)
+    head_form = p2.get_fp32_form()
     cfg = workloads.qdrift30(nqb=args.nqb, depth=args.depth)
     nqb, depth = cfg["nqb"], cfg["depth"]
     namp = 1 << nqb
@@ -310,6 +355,8 @@ def gpu_arm(args) -> None:
             ("fp64_plain", p2.PREC_FP64, (1, 1), form0),
             ("fp64_fused", p2.PREC_FP64, (5, 0), form0),
             ("fp32_plain", p2.PREC_FP32, (1, 1), form0),
+            ("fp32_fused_f32arith", p2.PREC_FP32, (5, 0),
+             p2.FORM_LIFTED_F32),
             ("fp32_fused_f64arith", p2.PREC_FP32, (5, 0), p2.FORM_LIFTED)):
         if args.quick and name != "fp64_plain":
             continue
@@ -334,6 +381,14 @@ def gpu_arm(args) -> None:
         ref_gpu = _reference_gpu(nqb)
         if ref_gpu:
             arms["reference_gpu_fp64"] = ref_gpu
+    ratios = {}
+    if arms.get("fp64_fused"):
+        for name in ("fp32_fused_f32arith", "fp32_fused_f64arith"):
+            if arms.get(name):
+                ratios[f"{name}_vs_fp64_fused"] = (
+                    arms[name]["value"] / arms["fp64_fused"]["value"])
+    if arms.get("fp64_plain"):
+        ratios["headline_vs_fp64_plain"] = value / arms["fp64_plain"]["value"]
 
     peaks = _peaks()
     passes_per_step = st["passes"] / args.steps
@@ -345,11 +400,14 @@ def gpu_arm(args) -> None:
     achieved = bytes_per_launch / (launch_ms / 1e3) / 1e9
     hbm_gbs_step = trips_per_step * bytes_per_launch / (
         dev_ms / args.steps / 1e3) / 1e9
-    cpu = _cpu_baseline() if (rank == 0 and ws == 1 and not args.quick) \
-        else None
+    kernel = _headline_kernel(p2, head_form)
+    solo = ws == 1 and rank == 0 and not args.quick
+    cpu = _cpu_reference(cfg, CPU_DEPTH, CPU_REPS, 1) if solo else None
     extra = {}
-    if rank == 0 and not args.quick:
-        extra["fp32_error"] = {}
+    if solo:
+        t_studies = time.perf_counter()
+        extra["fp32_error"] = {"headline_samples": qdrift_error_study(
+            cfg, seed + 11, samples=4)}
         for fname, form in (("f32_arith", p2.FORM_LIFTED_F32),
                             ("f64_arith", p2.FORM_LIFTED)):
             p2.set_fp32_form(form)
@@ -358,9 +416,16 @@ def gpu_arm(args) -> None:
             finally:
                 p2.set_fp32_form(form0)
         studies = args.studies.split(",") if args.studies else []
-        for name in ("batched", "trott26", "cmpsit33", "sampling", "sweeps",
-                     "sharded"):
+        for name in STUDY_ORDER:
             if name not in studies:
+                continue
+            left = args.study_budget - (time.perf_counter() - t_studies)
+            need = STUDY_SECONDS.get(name, 60)
+            if left < need:
+                extra[name] = {"skipped": (
+                    f"study budget: {left:.0f} s left of "
+                    f"{args.study_budget:.0f} s, the study takes about "
+                    f"{need:.0f} s (--study-budget)")}
                 continue
             # a study that fails is reported in its slot; the bench line
             # itself still prints
@@ -368,6 +433,7 @@ def gpu_arm(args) -> None:
                 extra[name] = globals()[f"{name}_study"]()
             except Exception as e:  # noqa: BLE001
                 extra[name] = {"error": f"{type(e).__name__}: {e}"}
+        extra["study_seconds"] = time.perf_counter() - t_studies
     if rank != 0:
         return
     clocks = clk.summary()
@@ -376,14 +442,14 @@ def gpu_arm(args) -> None:
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "storage": ("complex64 state; rotations in FP32 FMAs (lifted "
-                    "form); angles, cos/sin, norms and overlaps in FP64"),
+        "storage": STORAGE[head_form],
         "data": "synthetic (seeded JW-like Hamiltonian, no dataset)",
         "config": {
             "workload": (f"qdrift {nqb} qubits, {len(cfg['terms'])} JW "
                          f"terms, {depth} draws per sample, FP32 state, "
                          f"fused passes"),
             "nqb": nqb, "terms": len(cfg["terms"]), "depth": depth,
+            "fp32_form": FORM_NAME[head_form],
             "step": "one qDRIFT sample: prepst + rotations + overlap",
             "l2": f"inputs larger than L2 ({namp * 8 / 2**30:.0f} GiB state)",
             "parallelism": f"replicas x{ws} (independent samples)"},
@@ -394,10 +460,10 @@ def gpu_arm(args) -> None:
                      "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"],
                      "peak_source": peaks["source"],
-                     "kernel": "k_pass_lift32<M,uint32_t>",
+                     "kernel": kernel,
                      "bytes_per_launch": bytes_per_launch,
                      "launch_ms": launch_ms,
-                     "traffic": _traffic_per_launch()},
+                     "traffic": _traffic_per_launch(kernel)},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": UNIT,
                 "h2d_bytes_per_step": st["h2d_bytes"] / args.steps,
@@ -405,12 +471,50 @@ def gpu_arm(args) -> None:
         "gpu_launches": st["launches"],
         "clocks": clocks,
         "comparison": arms,
-        "fp32_fused_vs_fp64_plain": (value / arms["fp64_plain"]["value"]
-                                     if arms.get("fp64_plain") else None),
+        "ratios": ratios,
         "overlaps": [[z.real, z.imag] for z in zs[:2]],
         **extra,
     }
     print(json.dumps(line), flush=True)
+
+
+def qdrift_error_study(cfg: dict, seed: int, samples: int = 4) -> dict:
+    """FP32 error on the headline workload itself: `samples` qDRIFT samples
+    of the 30-qubit configuration run in FP64 and in each FP32 form from
+    the same seed (the same draws), the error of every sample's overlap
+    against the FP64 one (the FP64 path is bit-identical to the reference,
+    tests/test_wide_parity_gpu.py)."""
+    import numpy as np
+
+    import phase2_b200 as p2
+    t, d = cfg["terms"], cfg["dets"]
+    form0 = p2.get_fp32_form()
+    zs, secs = {}, {}
+    try:
+        for name, prec, form in (("fp64", p2.PREC_FP64, form0),
+                                 ("f32_arith", p2.PREC_FP32,
+                                  p2.FORM_LIFTED_F32),
+                                 ("f64_arith", p2.PREC_FP32,
+                                  p2.FORM_LIFTED)):
+            p2.set_precision(prec)
+            p2.set_fp32_form(form)
+            t0 = time.perf_counter()
+            zs[name] = p2.qdrift(cfg["nqb"], t, d, samples, cfg["depth"],
+                                 cfg["step_size"], seed)
+            secs[name] = time.perf_counter() - t0
+    finally:
+        p2.set_fp32_form(form0)
+        p2.set_precision(p2.PREC_FP64)
+    out = {"workload": (f"qdrift {cfg['nqb']} qubits, {len(t.cf)} JW terms, "
+                        f"{samples} samples x {cfg['depth']} draws, FP32 vs "
+                        "FP64 on the same draws"),
+           "overlaps_fp64": [[z.real, z.imag] for z in zs["fp64"]],
+           "seconds": secs}
+    for name in ("f32_arith", "f64_arith"):
+        err = np.abs(zs[name] - zs["fp64"])
+        out[name] = {"abs_err_per_sample": [float(e) for e in err],
+                     "max_abs_err": float(err.max())}
+    return out
 
 
 def fp32_error_study(nqb: int = 20, nterms: int = 300, steps: int = 1000,
@@ -444,13 +548,14 @@ def fp32_error_study(nqb: int = 20, nterms: int = 300, steps: int = 1000,
             "seconds": time.perf_counter() - t0}
 
 
-def trott26_study(steps: int = 2) -> dict:
+def trott26_study(steps: int = 256) -> dict:
     """Second-order Trotter at 26 qubits (20,000 JW terms in flip-mask
     order -- phase2_set_term_order(FLIP), not the reference's lexicographic
     sort -- 16 determinants of weight 13, delta 0.05), FP64 and FP32 states
-    side by side on the same inputs, `steps` of its 256 steps (bounded
-    run): device rot.amp/s of each (CUDA events around the pass launches)
-    and the FP32 overlap error against the FP64 run."""
+    (the process's FP32 form) side by side on the same inputs, `steps` of
+    its 256 steps: device rot.amp/s of each (CUDA events around the pass
+    launches) and the FP32 overlap error against the FP64 run after every
+    step (the FP64 path is bit-identical to the reference)."""
     import numpy as np
 
     import phase2_b200 as p2
@@ -478,8 +583,13 @@ def trott26_study(steps: int = 2) -> dict:
                      "rotations_per_pass": rot / max(1, st["passes"]),
                      "pass_seconds": st["pass_ms"] / 1e3,
                      "hbm_gbs": st["bytes"] / (st["pass_ms"] / 1e3) / 1e9}
+    out["fp32_form"] = FORM_NAME.get(p2.get_fp32_form())
     out["fp32_vs_fp64"] = out["fp32"]["value"] / out["fp64"]["value"]
-    out["fp32_max_abs_err"] = float(np.max(np.abs(zs["fp32"] - zs["fp64"])))
+    err = np.abs(zs["fp32"] - zs["fp64"])
+    out["fp32_max_abs_err"] = float(np.max(err))
+    out["fp32_abs_err_per_step"] = [float(f"{e:.3g}") for e in err]
+    out["final_overlap_fp64"] = [float(zs["fp64"][-1].real),
+                                 float(zs["fp64"][-1].imag)]
     return out
 
 
@@ -738,45 +848,56 @@ def batch8fp64_study() -> dict:
     return batch8_study(prec=0)
 
 
-def batched_study(ninst: int = 64, step_cap: int = 4, seed: int = 0xBA7C4):
+def batched_study(ninst: int = 64, work_cap: float = 2.0e14,
+                  seed: int = 0xBA7C4):
     """Independent trott problems of uneven size run together: qubits
-    U{18..24}, JW terms log-uniform in [1e3, 5e4], steps U{16..512} capped
-    at step_cap for a bounded run, FP32 state, one determinant each.
-    Aggregate rot.amp/s over the batch (wall clock around the batch call,
-    recording/planning and result download included), once in one
-    persistent launch and once on per-instance streams; HBM GB/s counts
-    2 * 2^n * 8 bytes per pass, and l2_fit_byte_share is the part of
-    those bytes that belongs to instances whose state fits in L2 (n <= 23),
-    which the L2 can serve instead of HBM."""
+    U{18..24}, JW terms log-uniform in [1e3, 5e4], steps U{16..512}, FP32
+    state, one determinant each.  The drawn configuration totals about
+    9e14 rot.amp; to bound the run, every instance's step count is scaled
+    by the same factor so that the total is at most work_cap (at least 16
+    steps each), which keeps the unevenness between instances.  Aggregate
+    rot.amp/s over the batch (wall clock around the batch call,
+    recording/planning and result download included), in one persistent
+    launch and on per-instance streams; HBM GB/s counts 2 * 2^n * 8 bytes
+    per pass, l2_fit_byte_share is the part of those bytes that belongs to
+    instances whose state fits in L2 (n <= 23), which the L2 can serve
+    instead of HBM, and hbm_gbs_kernel_non_l2 counts only the others.  The
+    persistent launch also reports when each instance finished (device
+    timer): the tail is the time between the median and the last
+    finish."""
     import numpy as np
 
     import phase2_b200 as p2
     from phase2_b200 import workloads
     rng = np.random.Generator(np.random.PCG64(seed))
-    probs, work = [], 0
-    for k in range(ninst):
+    shape = []
+    for _ in range(ninst):
         n = int(rng.integers(18, 25))
         nt = int(round(10 ** rng.uniform(3, np.log10(5e4))))
-        steps = min(int(rng.integers(16, 513)), step_cap)
+        steps = int(rng.integers(16, 513))
+        shape.append((n, nt, steps))
+    drawn = sum(st * nt * (1 << n) for n, nt, st in shape)
+    scale = min(1.0, work_cap / drawn)
+    probs, work = [], 0
+    for k, (n, nt, steps) in enumerate(shape):
+        run = max(16, int(round(steps * scale)))
         t = workloads.jw_terms(n, nt, seed=seed + k)
         d = workloads.hamming_dets(n, 1, n // 2, seed=seed + 1000 + k)
-        probs.append(dict(nqb=n, terms=t, dets=d, steps=steps, delta=0.05))
-        work += steps * nt * (1 << n)
+        probs.append(dict(nqb=n, terms=t, dets=d, steps=run, delta=0.05))
+        work += run * nt * (1 << n)
     out = {"workload": (f"{ninst} trott instances, 18-24 qubits, 1e3-5e4 "
-                        f"JW terms, {step_cap} steps each, FP32 state"),
-           "rot_amp": work, "unit": UNIT}
+                        "JW terms, steps drawn U{16..512} and scaled by "
+                        f"{scale:.3f} (at least 16) to cap the batch at "
+                        f"{work_cap:.1e} rot.amp, FP32 state"),
+           "rot_amp": work, "rot_amp_drawn": drawn, "step_scale": scale,
+           "steps_run": [p["steps"] for p in probs], "unit": UNIT}
     p2.set_precision(p2.PREC_FP32)
     order = p2.lib().phase2_get_term_order()
     try:
-        # the reference's lexicographic term order in both modes, then the
-        # flip-mask order (a different, equally valid product order that
-        # fuses more rotations per pass) in the persistent mode
-        for mode, persistent, ordr in (
-                ("persistent", True, 0), ("streams", False, 0),
-                ("persistent_flip_order", True, 2)):
-            p2.set_term_order(ordr)
+        for mode, persistent in (("persistent", True), ("streams", False)):
+            p2.set_term_order(0)
             p2.set_batch_persistent(persistent)
-            p2.batch("trott", probs[:2])  # warm the kernels
+            p2.batch("trott", [dict(pr, steps=1) for pr in probs[:2]])
             t0 = time.perf_counter()
             _, stats = p2.batch("trott", probs, with_stats=True)
             wall = time.perf_counter() - t0
@@ -786,7 +907,7 @@ def batched_study(ninst: int = 64, step_cap: int = 4, seed: int = 0xBA7C4):
             # (n <= 23: 64 MiB); their passes can be served from L2
             l2 = sum(s["bytes"] for s, pr in zip(stats, probs)
                      if (1 << pr["nqb"]) * 8 <= 126 * 10 ** 6)
-            out[mode] = {
+            row = {
                 "seconds": wall, "value": work / wall,
                 "hbm_gbs_wall": hbm / wall / 1e9,
                 "kernel_seconds": kms / 1e3 if persistent else None,
@@ -794,9 +915,17 @@ def batched_study(ninst: int = 64, step_cap: int = 4, seed: int = 0xBA7C4):
                                    if persistent and kms else None),
                 "launches": int(sum(s["launches"] for s in stats)),
                 "passes": int(sum(s["passes"] for s in stats)),
-                "graph_replays": int(sum(s["graph_replays"]
-                                         for s in stats)),
                 "l2_fit_byte_share": l2 / hbm if hbm else None}
+            if persistent and kms:
+                row["hbm_gbs_kernel_non_l2"] = (hbm - l2) / (kms / 1e3) / 1e9
+                fin = sorted(s["finish_ms"] for s in stats
+                             if s.get("finish_ms") is not None)
+                if fin:
+                    row["finish_ms"] = {
+                        "first": fin[0], "median": fin[len(fin) // 2],
+                        "last": fin[-1],
+                        "tail_after_median": fin[-1] - fin[len(fin) // 2]}
+            out[mode] = row
     finally:
         p2.set_batch_persistent(True)
         p2.set_term_order(order)
@@ -805,38 +934,57 @@ def batched_study(ninst: int = 64, step_cap: int = 4, seed: int = 0xBA7C4):
     return out
 
 
+# studies appended to the N=1 line, in this order, with their approximate
+# B200 durations (for the study budget)
+STUDY_ORDER = ("trott26", "batched", "cmpsit33", "sharded", "sampling",
+               "sweeps")
+STUDY_SECONDS = {"trott26": 480, "batched": 200, "cmpsit33": 300,
+                 "sharded": 60, "sampling": 30, "sweeps": 60}
+
+
 # ---- the reference arm -------------------------------------------------
 
 
 def reference_arm(args) -> None:
+    """The reference's own CPU implementation of the path on the host
+    cores: its qdrift driver on the headline workload (same Hamiltonian,
+    determinant, step size, seed) as R MPI ranks of one job, each step one
+    sample truncated to CPU_DEPTH draws (the GPU arm's cpu_baseline is the
+    same measurement); value = rot.amp/s of the fastest of the --steps
+    samples after --warmup (the reference's min-of-K convention).  Under
+    torchrun only rank 0 runs it."""
     ws, rank, _ = _dist()
     if rank != 0:
         return
-    exe = ROOT / "oracle" / "_ref" / "ref_bench"
-    if not exe.is_file():
+    from phase2_b200 import workloads
+    from oracle import REF_MPI
+    if not REF_MPI.is_file():
         print(json.dumps({"impl": "reference", "unavailable":
-                          "oracle/_ref/ref_bench was not built (reference "
+                          "oracle/_ref/ref_mpi was not built (reference "
                           "sources absent at build time)"}), flush=True)
         return
-    for _ in range(args.warmup):
-        _cpu_baseline(nrot=1, reps=1)
-    vals = []
+    cfg = workloads.qdrift30(nqb=args.nqb, depth=args.depth)
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        vals.append(_cpu_baseline(nrot=4, reps=1))
+    cb = _cpu_reference(cfg, CPU_DEPTH, args.steps, args.warmup)
     elapsed = time.perf_counter() - t0
-    v = statistics.median(x["value"] for x in vals)
-    cb = dict(vals[0], value=v)
+    v = cb["value"]
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
         "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * elapsed / max(1, args.steps),
+        "ms_per_step": 1e3 * cb["seconds_per_sample"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic",
-        "config": {"workload": (f"qdrift {args.nqb} qubits rotation sweep "
-                                "(reference CPU qreg_paulirot)"),
-                   "nqb": args.nqb},
+        "dtype": "f64", "data": "synthetic (seeded JW-like Hamiltonian, no "
+                                "dataset)",
+        "config": {"workload": (f"qdrift {cfg['nqb']} qubits, "
+                                f"{len(cfg['terms'])} JW terms, "
+                                f"{CPU_DEPTH} of {cfg['depth']} draws per "
+                                "sample (bounded CPU sample), FP64 state"),
+                   "nqb": cfg["nqb"], "terms": len(cfg["terms"]),
+                   "depth": CPU_DEPTH,
+                   "step": "one qDRIFT sample: prepst + rotations + overlap",
+                   "parallelism": f"{cb['cores']} MPI ranks on host cores"},
         "cpu_baseline": cb,
+        "wall_seconds": elapsed,
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -857,16 +1005,21 @@ def main() -> None:
                          "FMAs) or f64 (FP64 arithmetic, one rounding to "
                          "FP32 per pass); default: the library's")
     ap.add_argument("--lift-kernel", default=None,
-                    choices=["direct", "bulk", "staged"],
+                    choices=["direct", "bulk", "staged", "staged2"],
                     help="kernel of FP64-arithmetic FP32 passes: direct "
                          "loads, or the next cosets staged by bulk copies "
-                         "or by cp.async")
+                         "or by cp.async (staged2: two blocks per SM with "
+                         "the whole register file)")
     ap.add_argument("--quick", action="store_true",
                     help="skip the CPU baseline and secondary arms")
-    ap.add_argument("--studies", default="batched,trott26,sharded",
-                    help="comma list of studies to append: batched, "
-                         "trott26, sharded, cmpsit33 (takes minutes), "
-                         "sampling, sweeps")
+    ap.add_argument("--studies", default="trott26,batched,cmpsit33,sharded",
+                    help="comma list of studies to append (run at N=1, in "
+                         "the order trott26, batched, cmpsit33, sharded, "
+                         "sampling, sweeps, each only while the study "
+                         "budget lasts)")
+    ap.add_argument("--study-budget", type=float, default=720.0,
+                    help="seconds of studies at most (a study that would "
+                         "not fit the remainder is skipped and reported)")
     ap.add_argument("--only-study", default=None,
                     help="run just this study (batched, trott26, cmpsit33, "
                          "batch8, batch8fp64, sampling, sweeps, sharded) "

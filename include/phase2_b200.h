@@ -66,7 +66,8 @@ int qreg_set_fusion(struct qreg *reg, int max_span, int max_rots);
  * while the current one is computed.  FP32 (FP64-arithmetic form only;
  * the FP32-arithmetic form has one kernel): variant 0 loads directly,
  * variant 1 stages each warp's next cosets in shared memory with bulk
- * copies (cp.async.bulk), variant 2 with cp.async; passes that do not
+ * copies (cp.async.bulk), variant 2 with cp.async, variant 3 as 2 in a
+ * build for two blocks per SM (more registers a thread); passes that do not
  * qualify for staging (a pivot below qubit 5, registers of fewer than
  * M + 5 qubits or more than 31) load directly.  per_sm caps resident
  * blocks per SM in the grid (0 = default).  Process-wide; the autotuner

@@ -9,7 +9,8 @@ the fastest.  It then compares fusion caps
 
 FP32 passes: the grid density is tuned on the FP32-arithmetic kernel
 (one variant), then, at that density, the FP64-arithmetic form's variants
-(0 direct loads, 1 bulk-copy staging, 2 cp.async staging) are compared;
+(0 direct loads, 1 bulk-copy staging, 2 cp.async staging, 3 the same in
+a build for two blocks per SM) are compared;
 the entry keeps both choices (the variant only steers the FP64-arithmetic
 form).
 
@@ -41,7 +42,7 @@ PRECS = {"fp64": PREC_FP64, "fp32": PREC_FP32}
 GRIDS = {"fp64": {0: [0, 4, 8, 32], 1: [0, 1]},
          "fp32": {0: [0, 8, 16, 32]}}
 # FP32 variants of the FP64-arithmetic form, compared at the tuned density
-FP32_F64_VARIANTS = (0, 1, 2)
+FP32_F64_VARIANTS = (0, 1, 2, 3)
 FORM_LIFTED, FORM_LIFTED_F32 = 1, 2
 
 

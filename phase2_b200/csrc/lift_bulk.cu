@@ -468,16 +468,17 @@ extern "C" int p2_lift_staged_launch(struct p2_dev *d,
 			return lb_launch_t<5>(d, p, recs, per_sm_cap);
 		}
 	}
-	/* a cap of two blocks per SM selects the build with the whole
-	 * register file of those blocks (up to 255 registers a thread) */
+	/* variant 3: at span 5 the build for two blocks per SM, with the
+	 * whole register file of those blocks (up to 255 registers a
+	 * thread) */
 	switch (p->span) {
 	case 3:
 		return pf_launch_t<3, p2_lb_blocks(3)>(d, p, recs, per_sm_cap);
 	case 4:
 		return pf_launch_t<4, p2_lb_blocks(4)>(d, p, recs, per_sm_cap);
 	default:
-		return per_sm_cap == 2
-			? pf_launch_t<5, 2>(d, p, recs, per_sm_cap)
+		return variant == 3
+			? pf_launch_t<5, 2>(d, p, recs, 0)
 			: pf_launch_t<5, p2_lb_blocks(5)>(d, p, recs,
 				  per_sm_cap);
 	}

@@ -95,7 +95,8 @@ def test_random_rotations_bit_exact(n, fusion, oracle_lib):
 
 
 @pytest.mark.parametrize("v64,v32,per_sm", [(0, 0, 0), (1, 1, 0), (0, 2, 0),
-                                             (0, 0, 4), (1, 2, 2)])
+                                             (0, 0, 4), (1, 2, 2),
+                                             (0, 3, 0)])
 @pytest.mark.parametrize("n", [5, 11, 17])
 def test_launch_variants(v64, v32, per_sm, n, fp32_form, oracle_lib):
     """The direct-load and shared-memory-prefetch FP64 kernels give the
@@ -112,7 +113,7 @@ def test_launch_variants(v64, v32, per_sm, n, fp32_form, oracle_lib):
             saved.append((prec, m, v.value, s.value))
             assert L.phase2_tune_set(prec, m, variant, per_sm) == 0
     assert L.phase2_tune_set(0, 5, 2, 0) == -1
-    assert L.phase2_tune_set(1, 5, 3, 0) == -1
+    assert L.phase2_tune_set(1, 5, 4, 0) == -1
     try:
         rng = np.random.Generator(np.random.PCG64(300 + n))
         amp = _rand_state(rng, n)
