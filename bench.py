@@ -1,14 +1,23 @@
 """Benchmark of the phase2 state-vector hot path on B200.
 
 Metric: Pauli-rotation x amplitudes per second (and HBM GB/s) at 30 qubits,
-FP32 state ("FP32-batched": fused passes, rotations as three FP32 shears
-per pair; angles, cos/sin and overlaps in FP64) against the plain FP64 path
-(one rotation per pass), on the qDRIFT workload: 30 qubits, 100,000
-Jordan-Wigner-like terms (seeded synthetic, phase2_b200.workloads), 4096
-draws per sample, step_size 1e-3.  The line also carries comparison arms
-(FP64 plain/fused, FP32 plain, FP32 with FP64 arithmetic, and the
-reference's own CUDA kernel built from its sources), the FP32 error study
-and the batched study.
+FP32 state ("FP32-batched": fused passes) against the FP64 path, on the
+qDRIFT workload: 30 qubits, 100,000 Jordan-Wigner-like terms (seeded
+synthetic, phase2_b200.workloads), 4096 draws per sample, step_size 1e-3.
+The headline runs the library's FP32 form (--fp32-form; the line's
+``fp32_form`` and ``storage`` say what it computes).  The line also
+carries comparison arms on the same draws -- FP64 one rotation per pass
+("plain"), FP64 fused, FP32 one rotation per pass, and both FP32 forms
+fused (FP32 arithmetic with FP32 coefficients; FP64 arithmetic with FP64
+coefficients and one rounding per pass) -- with each FP32 form's ratio
+to the fused FP64 path (like for like) and the headline's ratio to the
+plain FP64 path, the reference's own CUDA kernel built from its sources,
+the FP32 error of both forms on the headline samples and on a 1000-step
+Trotter run, and, at N=1, studies within a time budget (--studies,
+--study-budget): the 26-qubit second-order Trotter configuration over
+all 256 steps with the FP32 error after every step, the batched
+configuration (64 uneven instances in one persistent launch, with finish
+times), the 33-qubit composite configuration and sharded registers.
 
 A step is one qDRIFT sample through the library's C-ABI driver
 (qdrift_simul): state prep, 4096 rotations, overlap.  ``value`` is timed
@@ -21,8 +30,10 @@ Multi-GPU (torchrun): each rank runs independent qDRIFT samples of its own
 seed on its own GPU (replicas, weak scaling); no data-path collective.
 Timing is the max over ranks.
 
-``--impl reference`` times the reference's own CPU path (oracle/_ref,
-qreg_paulirot compiled from the reference sources) on the host cores.
+``cpu_baseline`` and ``--impl reference`` time the reference's own CPU
+path: its qdrift driver (oracle/_ref/ref_mpi, built from the reference
+sources) on the same workload as R MPI ranks of one job on the host cores,
+each step a sample truncated to a few draws (the metric is a rate).
 """
 
 from __future__ import annotations
@@ -248,6 +259,15 @@ def _reference_gpu(nqb: int, nrot: int = 16, reps: int = 3):
                      f"{nrot} rotations at {nqb} qubits")}
 
 
+def _config(cfg: dict) -> dict:
+    """The workload both arms report (the same dict in each line)."""
+    return {"workload": (f"qdrift {cfg['nqb']} qubits, {len(cfg['terms'])} "
+                         f"JW terms, {cfg['depth']} draws per sample"),
+            "nqb": cfg["nqb"], "terms": len(cfg["terms"]),
+            "depth": cfg["depth"],
+            "step": "one qDRIFT sample: prepst + rotations + overlap"}
+
+
 # CPU baseline: the reference's own qdrift driver on the headline
 # workload, as R ranks of one job on the host cores
 CPU_DEPTH = 4    # draws per timed sample (of the workload's 4096)
@@ -444,15 +464,10 @@ def gpu_arm(args) -> None:
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "storage": STORAGE[head_form],
         "data": "synthetic (seeded JW-like Hamiltonian, no dataset)",
-        "config": {
-            "workload": (f"qdrift {nqb} qubits, {len(cfg['terms'])} JW "
-                         f"terms, {depth} draws per sample, FP32 state, "
-                         f"fused passes"),
-            "nqb": nqb, "terms": len(cfg["terms"]), "depth": depth,
-            "fp32_form": FORM_NAME[head_form],
-            "step": "one qDRIFT sample: prepst + rotations + overlap",
-            "l2": f"inputs larger than L2 ({namp * 8 / 2**30:.0f} GiB state)",
-            "parallelism": f"replicas x{ws} (independent samples)"},
+        "config": _config(cfg),
+        "fp32_form": FORM_NAME[head_form],
+        "l2": f"inputs larger than L2 ({namp * 8 / 2**30:.0f} GiB state)",
+        "parallelism": f"replicas x{ws} (independent samples)",
         "hbm_gbs": hbm_gbs_step,
         "passes_per_step": passes_per_step,
         "rotations_per_pass": depth / passes_per_step,
@@ -655,7 +670,9 @@ def sweeps_study(nqb: int = 26) -> dict:
     t, d = cfg["terms"], cfg["dets"]
     rows = []
     old = p2.get_sweep()
+    form = p2.get_fp32_form()
     p2.set_precision(p2.PREC_FP32)
+    p2.set_fp32_form(p2.FORM_LIFTED_F32)  # the form sweeps run in
     p2.set_device_sampling(p2.DEVICE_SAMPLING_OFF)
     try:
         for shape in ((0, 5), (13, 5), (13, 4), (12, 4), (14, 5)):
@@ -677,8 +694,10 @@ def sweeps_study(nqb: int = 26) -> dict:
         p2.set_sweep_kernel(True)
         p2.set_device_sampling(p2.DEVICE_SAMPLING_AUTO)
         p2.set_precision(p2.PREC_FP64)
+        p2.set_fp32_form(form)
     return {"workload": (f"qdrift {nqb} qubits, 100000 JW terms, 2 samples "
-                         f"x {cfg['depth']} draws, FP32"), "unit": UNIT,
+                         f"x {cfg['depth']} draws, FP32 (FP32 arithmetic)"),
+            "unit": UNIT,
             "rows": rows}
 
 
@@ -975,14 +994,11 @@ def reference_arm(args) -> None:
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded JW-like Hamiltonian, no "
                                 "dataset)",
-        "config": {"workload": (f"qdrift {cfg['nqb']} qubits, "
-                                f"{len(cfg['terms'])} JW terms, "
-                                f"{CPU_DEPTH} of {cfg['depth']} draws per "
-                                "sample (bounded CPU sample), FP64 state"),
-                   "nqb": cfg["nqb"], "terms": len(cfg["terms"]),
-                   "depth": CPU_DEPTH,
-                   "step": "one qDRIFT sample: prepst + rotations + overlap",
-                   "parallelism": f"{cb['cores']} MPI ranks on host cores"},
+        "config": _config(cfg),
+        "sample": (f"each step is the workload's qDRIFT sample truncated "
+                   f"to {CPU_DEPTH} of its {cfg['depth']} draws (a bounded "
+                   "CPU sample; the metric is a rate)"),
+        "parallelism": f"{cb['cores']} MPI ranks on host cores",
         "cpu_baseline": cb,
         "wall_seconds": elapsed,
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,

@@ -38,9 +38,11 @@ int phase2_get_precision(void);
 
 /* Arithmetic of FP32 passes (enum phase2_form below), both rotating each
  * amplitude pair by three in-place shears:
- *   PHASE2_FORM_LIFTED_F32 (default) FP32 FMAs on FP32 coefficients;
- *   PHASE2_FORM_LIFTED      FP64 arithmetic, one rounding to FP32 per pass.
- * Also PHASE2_FP32_FORM=lifted_f32|lifted at world_init.  Applies to
+ *   PHASE2_FORM_LIFTED (default)  coefficients from FP64 cos/sin, FP64
+ *                                 arithmetic, one rounding to FP32 per pass;
+ *   PHASE2_FORM_LIFTED_F32        FP32 FMAs on coefficients rounded to FP32
+ *                                 (faster; one rounding per shear).
+ * Also PHASE2_FP32_FORM=lifted|lifted_f32 at world_init.  Applies to
  * rotations planned afterwards.  0 or -1. */
 int phase2_set_fp32_form(int form);
 int phase2_get_fp32_form(void);
@@ -108,12 +110,13 @@ void circ_hamil_sort_flip(struct circ_hamil *hm);
 
 /*
  * Batched drivers run in one of two ways.  Persistent (default, when every
- * instance is a register of at most 31 qubits of one precision: FP64, or
- * FP32 with the FP32 form PHASE2_FORM_LIFTED_F32): each instance's steps
+ * instance is a register of at most 31 qubits of one precision, FP32 in
+ * either FP32 form or FP64): each instance's steps
  * are recorded as a program and all programs run in ONE persistent kernel
- * launch that schedules (instance, op, tile) work over all SMs; FP64
- * instances keep the pass kernels' exact arithmetic (bit-identical to the
- * reference).  Otherwise, or after phase2_set_batch_persistent(0):
+ * launch that schedules (instance, op, tile) work over all SMs; every
+ * instance keeps the pass kernels' arithmetic (FP64: exact, bit-identical
+ * to the reference; FP32: that of its form), so results equal the
+ * per-instance stream mode's bit for bit.  Otherwise, or after phase2_set_batch_persistent(0):
  * per-instance streams as described below.
  */
 int phase2_set_batch_persistent(int on);
@@ -141,7 +144,7 @@ int phase2_set_sweep_kernel(int on);
 /*
  * qdrift_simul and cmpsit_simul with device sampling: when the register
  * runs in the persistent kernel (at most 31 qubits; FP64, or FP32 in
- * PHASE2_FORM_LIFTED_F32) and the trial state is a MULTIDET, the samples'
+ * either form) and the trial state is a MULTIDET, the samples'
  * term draws (CDF inversion of the host generator's
  * uniforms), their pass plans and their passes all run on the GPU: one
  * planning kernel per round of samples (a block per sample) writes the

@@ -66,8 +66,9 @@ def set_precision(prec: int) -> None:
 
 
 def set_fp32_form(form: int) -> None:
-    """Arithmetic of FP32 passes: FORM_LIFTED_F32 (default, FP32 FMAs) or
-    FORM_LIFTED (FP64 arithmetic, one rounding to FP32 per pass)."""
+    """Arithmetic of FP32 passes: FORM_LIFTED (default: coefficients from
+    FP64 cos/sin, FP64 arithmetic, one rounding to FP32 per pass) or
+    FORM_LIFTED_F32 (FP32 FMAs on FP32 coefficients)."""
     if lib().phase2_set_fp32_form(form) != 0:
         raise ValueError(f"bad FP32 form {form}")
 
@@ -77,8 +78,8 @@ def get_fp32_form() -> int:
 
 
 def set_batch_persistent(on: bool) -> None:
-    """Batched drivers: one persistent launch for all instances (default,
-    FP32 registers in the FP32-arithmetic form) or per-instance streams."""
+    """Batched drivers: one persistent launch for all instances (default)
+    or per-instance streams."""
     lib().phase2_set_batch_persistent(1 if on else 0)
 
 

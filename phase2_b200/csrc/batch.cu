@@ -41,6 +41,60 @@ __device__ __forceinline__ void p2_batch_pass_tile(float2 *st,
 	}
 }
 
+/* The same for an FP32 register in the FP64-arithmetic form: each coset
+ * widened to FP64, the run applied by p2_rot_lift (the arithmetic of
+ * k_pass_lift and k_pass_lift_pf, the same bits), one rounding to FP32 at
+ * the store (negated when the pass scale is -1). */
+template <int M>
+__device__ __forceinline__ void p2_batch_pass_tile_x(float2 *st,
+	const struct phase2_pass &p, uint32_t tile, uint64_t nrep, uint32_t cpt,
+	const struct p2_lift_rec *srec, uint32_t lane)
+{
+	uint32_t pb[M > 0 ? M : 1];
+#pragma unroll
+	for (int k = 0; k < M; ++k)
+		pb[k] = (uint32_t)p.basis[k];
+	const bool neg = p.scale < 0;
+	const uint64_t t0 = (uint64_t)tile * cpt * 32 + lane;
+	for (uint32_t j = 0; j < cpt; ++j) {
+		const uint64_t t = t0 + (uint64_t)j * 32;
+		if (t >= nrep)
+			continue;
+		const uint32_t x = p2_rep_t<M, uint32_t>((uint32_t)t, p);
+		double re[1 << M], im[1 << M];
+#pragma unroll
+		for (int u = 0; u < (1 << M); ++u) {
+			uint32_t off = 0;
+#pragma unroll
+			for (int k = 0; k < M; ++k)
+				if (u >> k & 1)
+					off ^= pb[k];
+			const float2 v = __ldcg(st + (x ^ off));
+			re[u] = (double)v.x;
+			im[u] = (double)v.y;
+		}
+		for (uint32_t r = 0; r < p.nrot; ++r) {
+			const struct p2_lift_rec q = srec[r];
+			const uint32_t sm =
+				q.sm ^ (0u - p2_parity(x & (uint32_t)q.z));
+			p2_apply_lift<M>(q.key, re, im, q.t, q.s, sm);
+		}
+		const uint32_t xs = p2_opaque(x);
+#pragma unroll
+		for (int u = 0; u < (1 << M); ++u) {
+			uint32_t off = 0;
+#pragma unroll
+			for (int k = 0; k < M; ++k)
+				if (u >> k & 1)
+					off ^= pb[k];
+			const double a = neg ? -re[u] : re[u];
+			const double b = neg ? -im[u] : im[u];
+			__stcg(st + (xs ^ off), make_float2(__double2float_rn(a),
+							 __double2float_rn(b)));
+		}
+	}
+}
+
 /* The same for an FP64 register: the exact per-coset arithmetic of
  * k_pass (p2_apply_run), loads and stores at L2 only. */
 template <int M>
@@ -77,15 +131,28 @@ __device__ __forceinline__ void p2_batch_pass_tile64(double2 *st,
 /* Records as a batch kernel of state type ST holds them in shared
  * memory: repacked lifted records (FP32) or the records themselves
  * (FP64). */
-template <typename ST> struct p2_brec;
-template <> struct p2_brec<float2> {
+template <typename ST, bool X> struct p2_brec;
+template <> struct p2_brec<float2, false> {
 	typedef struct p2_lift32_rec type;
 	static __device__ __forceinline__ type of(const phase2_rot_rec &r)
 	{
 		return p2_lift32_of(r);
 	}
 };
-template <> struct p2_brec<double2> {
+template <> struct p2_brec<float2, true> {
+	typedef struct p2_lift_rec type;
+	static __device__ __forceinline__ type of(const phase2_rot_rec &r)
+	{
+		struct p2_lift_rec o;
+		o.t = r.c;
+		o.s = r.s;
+		o.z = r.z;
+		o.sm = r.smask;
+		o.key = ((uint32_t)r.U << 1) | r.odd;
+		return o;
+	}
+};
+template <> struct p2_brec<double2, false> {
 	typedef struct phase2_rot_rec type;
 	static __device__ __forceinline__ type of(const phase2_rot_rec &r)
 	{
@@ -93,13 +160,34 @@ template <> struct p2_brec<double2> {
 	}
 };
 
-/* Span dispatch of a pass tile (FP32 or FP64 state). */
-template <typename ST, typename RT>
+/* Span dispatch of a pass tile (FP32 state in either form, or FP64). */
+template <typename ST, bool X, typename RT>
 __device__ __forceinline__ void p2_batch_pass(ST *st,
 	const struct phase2_pass &p, uint32_t tile, uint64_t nrep, uint32_t cpt,
 	const RT *srec, uint32_t lane)
 {
-	if constexpr (sizeof(ST) == 16) {
+	if constexpr (X) {
+		switch (p.span) {
+		case 0:
+			p2_batch_pass_tile_x<0>(st, p, tile, nrep, cpt, srec, lane);
+			break;
+		case 1:
+			p2_batch_pass_tile_x<1>(st, p, tile, nrep, cpt, srec, lane);
+			break;
+		case 2:
+			p2_batch_pass_tile_x<2>(st, p, tile, nrep, cpt, srec, lane);
+			break;
+		case 3:
+			p2_batch_pass_tile_x<3>(st, p, tile, nrep, cpt, srec, lane);
+			break;
+		case 4:
+			p2_batch_pass_tile_x<4>(st, p, tile, nrep, cpt, srec, lane);
+			break;
+		default:
+			p2_batch_pass_tile_x<5>(st, p, tile, nrep, cpt, srec, lane);
+			break;
+		}
+	} else if constexpr (sizeof(ST) == 16) {
 		switch (p.span) {
 		case 0:
 			p2_batch_pass_tile64<0>(st, p, tile, nrep, cpt, srec, lane);
@@ -151,8 +239,16 @@ __device__ __forceinline__ unsigned long long p2_globaltimer()
 	return t;
 }
 
-template <typename ST>
-__global__ void __launch_bounds__(P2_TPB, sizeof(ST) == 8 ? 5 : 2)
+/* Resident blocks per SM of a k_batch instance: FP32 arithmetic 5, FP32
+ * state with FP64 arithmetic 3 (32 complex doubles a thread), FP64 2. */
+__host__ __device__ constexpr int p2_batch_blocks(bool f64, bool x)
+{
+	return f64 ? 2 : (x ? 3 : 5);
+}
+
+template <typename ST, bool X>
+__global__ void __launch_bounds__(P2_TPB,
+	p2_batch_blocks(sizeof(ST) == 16, X))
 	k_batch(const struct p2_binst *__restrict__ inst, uint32_t ninst,
 		const struct p2_op *__restrict__ ops,
 		const struct phase2_pass *__restrict__ passes,
@@ -164,7 +260,7 @@ __global__ void __launch_bounds__(P2_TPB, sizeof(ST) == 8 ? 5 : 2)
 		unsigned int idle_limit)
 {
 	constexpr bool F64 = sizeof(ST) == 16;
-	typedef typename p2_brec<ST>::type RT;
+	typedef typename p2_brec<ST, X>::type RT;
 	/* each warp keeps the records of the pass it last ran */
 	__shared__ RT srec_all[P2_BATCH_WARPS][P2_MAX_ROTS_PER_PASS];
 	const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
@@ -251,12 +347,13 @@ __global__ void __launch_bounds__(P2_TPB, sizeof(ST) == 8 ? 5 : 2)
 			if (held != op.a) {
 				__syncwarp();
 				for (uint32_t r = lane; r < p.nrot; r += 32)
-					srec[r] = p2_brec<ST>::of(recs[p.rot_off + r]);
+					srec[r] = p2_brec<ST, X>::of(
+						recs[p.rot_off + r]);
 				held = op.a;
 				__syncwarp();
 			}
-			p2_batch_pass<ST, RT>(st, p, tile, namp >> p.span, op.b,
-				srec, lane);
+			p2_batch_pass<ST, X, RT>(st, p, tile, namp >> p.span,
+				op.b, srec, lane);
 		} else if (op.kind == P2_OP_ZERO) {
 			const uint64_t base = (uint64_t)tile * P2_BATCH_ZERO_TILE;
 			ST zero;
@@ -345,7 +442,7 @@ extern "C" int phase2_batch_wait_check(unsigned int idle_limit)
 			cudaMemcpyHostToDevice);
 	unsigned int status = 0;
 	if (e == cudaSuccess) {
-		k_batch<float2><<<2, P2_TPB>>>(
+		k_batch<float2, false><<<2, P2_TPB>>>(
 			(const struct p2_binst *)(buf + o_inst), 1,
 			(const struct p2_op *)(buf + o_op), NULL, NULL, NULL,
 			NULL, NULL, NULL, (struct p2_bctl *)(buf + o_ctl),
@@ -444,26 +541,38 @@ extern "C" size_t phase2_batch_finish_ms(double *out, size_t n)
 
 /* k_batch for FP32 or FP64 registers: its kernel function (occupancy
  * queries) and its launch. */
-const void *p2_batch_kernel(bool f64)
+int p2_batch_kind(int prec, int form)
 {
-	return f64 ? (const void *)k_batch<double2>
-		   : (const void *)k_batch<float2>;
+	if (prec == PHASE2_PREC_FP64)
+		return P2_BK_F64;
+	return form == PHASE2_FORM_LIFTED ? P2_BK_F32X : P2_BK_F32;
 }
 
-void p2_batch_launch(bool f64, unsigned grid, cudaStream_t stream,
+const void *p2_batch_kernel(int kind)
+{
+	return kind == P2_BK_F64 ? (const void *)k_batch<double2, false>
+		: kind == P2_BK_F32X ? (const void *)k_batch<float2, true>
+				      : (const void *)k_batch<float2, false>;
+}
+
+void p2_batch_launch(int kind, unsigned grid, cudaStream_t stream,
 	const struct p2_binst *inst, uint32_t ninst, const struct p2_op *ops,
 	const struct phase2_pass *passes, const struct phase2_rot_rec *recs,
 	const uint64_t *widx, const double *wval, const uint64_t *gidx,
 	double2 *gout, struct p2_bctl *ctl, unsigned int *status)
 {
-	if (f64)
-		k_batch<double2><<<grid, P2_TPB, 0, stream>>>(inst, ninst, ops,
-			passes, recs, widx, wval, gidx, gout, ctl, status,
-			P2_BATCH_IDLE_LIMIT);
+	if (kind == P2_BK_F64)
+		k_batch<double2, false><<<grid, P2_TPB, 0, stream>>>(inst,
+			ninst, ops, passes, recs, widx, wval, gidx, gout, ctl,
+			status, P2_BATCH_IDLE_LIMIT);
+	else if (kind == P2_BK_F32X)
+		k_batch<float2, true><<<grid, P2_TPB, 0, stream>>>(inst,
+			ninst, ops, passes, recs, widx, wval, gidx, gout, ctl,
+			status, P2_BATCH_IDLE_LIMIT);
 	else
-		k_batch<float2><<<grid, P2_TPB, 0, stream>>>(inst, ninst, ops,
-			passes, recs, widx, wval, gidx, gout, ctl, status,
-			P2_BATCH_IDLE_LIMIT);
+		k_batch<float2, false><<<grid, P2_TPB, 0, stream>>>(inst,
+			ninst, ops, passes, recs, widx, wval, gidx, gout, ctl,
+			status, P2_BATCH_IDLE_LIMIT);
 }
 
 /* Host seconds (PHASE2_BATCH_TIMING breakdown). */
@@ -594,11 +703,20 @@ extern "C" int p2d_batch_run(struct p2_dev *const *devs,
 	const double tb3 = p2_now();
 	if (e == cudaSuccess)
 		e = cudaMemsetAsync(dbuf + o_ctl, 0, total - o_ctl, d0->stream);
-	const bool f64 = d0->prec == PHASE2_PREC_FP64;
+	/* the kernel instance for the precision and the form the programs'
+	 * passes were planned in (one process-wide FP32 form) */
+	int form = d0->prec == PHASE2_PREC_FP64 ? PHASE2_FORM_EXACT
+						: PHASE2_FORM_LIFTED_F32;
+	for (size_t i = 0; i < n && d0->prec != PHASE2_PREC_FP64; i++)
+		if (progs[i]->npass) {
+			form = progs[i]->passes[0].form;
+			break;
+		}
+	const int kind = p2_batch_kind(d0->prec, form);
 	int per_sm = 0;
 	if (e == cudaSuccess)
 		e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm,
-			p2_batch_kernel(f64), P2_TPB, 0);
+			p2_batch_kernel(kind), P2_TPB, 0);
 	if (e != cudaSuccess) {
 		p2_scratch_free(dbuf, d0->stream);
 		log_error("batch: setup: %s", cudaGetErrorString(e));
@@ -607,7 +725,7 @@ extern "C" int p2d_batch_run(struct p2_dev *const *devs,
 	const unsigned grid =
 		(unsigned)d0->sm_count * (unsigned)(per_sm > 0 ? per_sm : 1);
 	cudaEventRecord(d0->t0, d0->stream);
-	p2_batch_launch(f64, grid, d0->stream,
+	p2_batch_launch(kind, grid, d0->stream,
 		(const struct p2_binst *)(dbuf + o_inst), (uint32_t)n,
 		(const struct p2_op *)(dbuf + o_ops),
 		(const struct phase2_pass *)(dbuf + o_pass),

@@ -204,21 +204,18 @@ static void qdrift_draw(struct qdrift *qd)
 	}
 }
 
-/* A register the persistent kernel runs: FP64 (exact form), or FP32 in
- * the FP32-arithmetic form; at most 31 qubits. */
+/* A register the persistent kernel runs: FP64 (exact form) or FP32
+ * (either FP32 form); at most 31 qubits. */
 static int persistent_reg_ok(const struct qreg *reg)
 {
 	const struct p2_qreg *b = reg->backend;
-	return b && p2d_batch_ok(b->dev) &&
-		(b->prec == PHASE2_PREC_FP64 ||
-			p2_form_for(PHASE2_PREC_FP32) ==
-				PHASE2_FORM_LIFTED_F32);
+	return b && p2d_batch_ok(b->dev);
 }
 
 /* Registers that device sampling (p2d_sampled_device) takes under the
- * current mode: those the persistent kernel runs (FP64, or FP32 in the
- * FP32-arithmetic form; at most 31 qubits) with a multi-determinant trial
- * state; AUTO also caps the width. */
+ * current mode: those the persistent kernel runs (FP64, or FP32 in either
+ * form; at most 31 qubits) with a multi-determinant trial state; AUTO
+ * also caps the width. */
 /* Whether a sampled driver runs on the device.  In AUTO mode a run with a
  * step writer keeps the host loop, so the writer sees each sample as soon
  * as it completes (a writer that flushes per step stays crash-consistent);
@@ -658,8 +655,8 @@ static void batch_launch(struct batch_item *it)
 }
 
 /*
- * One persistent launch for the whole batch (FP32 registers in the
- * FP32-arithmetic form): each instance's work is recorded as a program
+ * One persistent launch for the whole batch: each instance's work is
+ * recorded as a program
  * (its enqueue calls, then a gather of its determinant amplitudes per
  * output), all programs run in p2d_batch_run, and every output is then
  * formed on the host from its gathered amplitudes with circ_measure's

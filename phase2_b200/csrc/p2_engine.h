@@ -123,12 +123,16 @@ struct p2_bctl;
  * up. */
 #define P2_BATCH_IDLE_LIMIT 2000000u
 
-/* batch.cu: the persistent kernel for FP32 or FP64 registers (its
- * function, for occupancy queries, and its launch).  status points to 16
+/* batch.cu: the persistent kernel for FP32 registers (FP32 arithmetic,
+ * P2_BK_F32, or FP64 arithmetic, P2_BK_F32X) or FP64 registers
+ * (P2_BK_F64): the instance for a precision and FP32 form, its function
+ * (occupancy queries) and its launch.  status points to 16
  * zeroed bytes: status[0] is raised when a wait gives up, status[2..3]
  * receive the complement of the launch's start time (global timer). */
-const void *p2_batch_kernel(bool f64);
-void p2_batch_launch(bool f64, unsigned grid, cudaStream_t stream,
+enum { P2_BK_F32 = 0, P2_BK_F32X = 1, P2_BK_F64 = 2 };
+int p2_batch_kind(int prec, int form);
+const void *p2_batch_kernel(int kind);
+void p2_batch_launch(int kind, unsigned grid, cudaStream_t stream,
 	const struct p2_binst *inst, uint32_t ninst, const struct p2_op *ops,
 	const struct phase2_pass *passes, const struct phase2_rot_rec *recs,
 	const uint64_t *widx, const double *wval, const uint64_t *gidx,

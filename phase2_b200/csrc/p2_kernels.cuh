@@ -270,50 +270,107 @@ __device__ __forceinline__ void p2_prefetch(double2 *stage, const double2 *st,
  * gives the same bits as flipping the partner's sign around the shears.
  * U = 0 (the string is diagonal on the coset, and then odd = 1) is the
  * phase c + i sigma s, applied to (re, im) by the same three shears.
+ *
+ * The three shears of a pair depend on each other, so the pairs are taken
+ * P2_LIFT_GROUP at a time, shear by shear: each shear of a group is
+ * 2 * P2_LIFT_GROUP independent FMAs, enough to cover the FP64 FMA latency
+ * (pairs are independent, so the order gives the same bits).
  */
+#ifndef P2_LIFT_GROUP
+#define P2_LIFT_GROUP 2
+#endif
+#ifndef P2_LIFT32_GROUP
+#define P2_LIFT32_GROUP 1
+#endif
+
 template <int M, int U, int ODD>
 __device__ __forceinline__ void p2_rot_lift(double (&re)[1 << M],
 	double (&im)[1 << M], double t, double s, uint32_t sm)
 {
 	if constexpr (U == 0) {
+		constexpr int S = 1 << M;
+		constexpr int G = S < P2_LIFT_GROUP ? S : P2_LIFT_GROUP;
 #pragma unroll
-		for (int u = 0; u < (1 << M); ++u) {
-			const uint32_t g = p2_bitmask(sm, u);
+		for (int g = 0; g < S; g += G) {
+			double st[G], ss[G];
+#pragma unroll
+			for (int j = 0; j < G; ++j) {
+				const uint32_t b = p2_bitmask(sm, g + j);
+				st[j] = p2_sgn(t, b);
+				ss[j] = p2_sgn(s, b);
+			}
 			if constexpr (ODD) {
-				const double st = p2_sgn(t, g), ss = p2_sgn(s, g);
-				re[u] = fma(-st, im[u], re[u]);
-				im[u] = fma(ss, re[u], im[u]);
-				re[u] = fma(-st, im[u], re[u]);
+#pragma unroll
+				for (int j = 0; j < G; ++j)
+					re[g + j] = fma(-st[j], im[g + j], re[g + j]);
+#pragma unroll
+				for (int j = 0; j < G; ++j)
+					im[g + j] = fma(ss[j], re[g + j], im[g + j]);
+#pragma unroll
+				for (int j = 0; j < G; ++j)
+					re[g + j] = fma(-st[j], im[g + j], re[g + j]);
 			} else {
 				/* (c +- s) y with c = 1 - t s; a Hermitian string
 				 * that is diagonal on the coset never has it */
-				const double k = p2_sgn(s, g) + fma(-t, s, 1.0);
-				re[u] *= k;
-				im[u] *= k;
+#pragma unroll
+				for (int j = 0; j < G; ++j) {
+					const double k = ss[j] + fma(-t, s, 1.0);
+					re[g + j] *= k;
+					im[g + j] *= k;
+				}
 			}
 		}
 	} else {
 		constexpr int H = p2_hibit(U);
+		constexpr int NP = 1 << (M - 1);
+		constexpr int G = NP < P2_LIFT_GROUP ? NP : P2_LIFT_GROUP;
 #pragma unroll
-		for (int k = 0; k < (1 << (M - 1)); ++k) {
-			const int u = p2_ins0(k, H);
-			const int w = u ^ U;
-			const uint32_t g = p2_bitmask(sm, u);
-			const double st = p2_sgn(t, g), ss = p2_sgn(s, g);
+		for (int g = 0; g < NP; g += G) {
+			double st[G], ss[G];
+#pragma unroll
+			for (int j = 0; j < G; ++j) {
+				const uint32_t b = p2_bitmask(sm, p2_ins0(g + j, H));
+				st[j] = p2_sgn(t, b);
+				ss[j] = p2_sgn(s, b);
+			}
 			if constexpr (ODD) {
-				re[u] = fma(-st, im[w], re[u]);
-				im[u] = fma(st, re[w], im[u]);
-				re[w] = fma(-ss, im[u], re[w]);
-				im[w] = fma(ss, re[u], im[w]);
-				re[u] = fma(-st, im[w], re[u]);
-				im[u] = fma(st, re[w], im[u]);
+#pragma unroll
+				for (int j = 0; j < G; ++j) {
+					const int u = p2_ins0(g + j, H), w = u ^ U;
+					re[u] = fma(-st[j], im[w], re[u]);
+					im[u] = fma(st[j], re[w], im[u]);
+				}
+#pragma unroll
+				for (int j = 0; j < G; ++j) {
+					const int u = p2_ins0(g + j, H), w = u ^ U;
+					re[w] = fma(-ss[j], im[u], re[w]);
+					im[w] = fma(ss[j], re[u], im[w]);
+				}
+#pragma unroll
+				for (int j = 0; j < G; ++j) {
+					const int u = p2_ins0(g + j, H), w = u ^ U;
+					re[u] = fma(-st[j], im[w], re[u]);
+					im[u] = fma(st[j], re[w], im[u]);
+				}
 			} else {
-				re[u] = fma(st, re[w], re[u]);
-				im[u] = fma(st, im[w], im[u]);
-				re[w] = fma(-ss, re[u], re[w]);
-				im[w] = fma(-ss, im[u], im[w]);
-				re[u] = fma(st, re[w], re[u]);
-				im[u] = fma(st, im[w], im[u]);
+#pragma unroll
+				for (int j = 0; j < G; ++j) {
+					const int u = p2_ins0(g + j, H), w = u ^ U;
+					re[u] = fma(st[j], re[w], re[u]);
+					im[u] = fma(st[j], im[w], im[u]);
+				}
+#pragma unroll
+				for (int j = 0; j < G; ++j) {
+					const int u = p2_ins0(g + j, H), w = u ^ U;
+					re[w] = fma(-ss[j], re[u], re[w]);
+					im[w] = fma(-ss[j], im[u], im[w]);
+				}
+#pragma unroll
+				for (int j = 0; j < G; ++j) {
+					const int u = p2_ins0(g + j, H), w = u ^ U;
+					re[u] = fma(st[j], re[w], re[u]);
+					im[u] = fma(st[j], im[w], im[u]);
+				}
 			}
 		}
 	}
@@ -438,35 +495,70 @@ __device__ __forceinline__ void p2_rot_lift32(float (&re)[1 << M],
 			}
 		}
 	} else {
+		/* pairs P2_LIFT32_GROUP at a time, shear by shear (as in
+		 * p2_rot_lift: independent pairs, the same bits) */
 		constexpr int H = p2_hibit(U);
+		constexpr int NP = 1 << (M - 1);
+		constexpr int G = NP < P2_LIFT32_GROUP ? NP : P2_LIFT32_GROUP;
 #pragma unroll
-		for (int k = 0; k < (1 << (M - 1)); ++k) {
-			const int u = p2_ins0(k, H);
-			const int w = u ^ U;
-			const uint32_t g = p2_bitmask(sm, u);
-			const float st = p2_fsgn(t, g), ss = p2_fsgn(s, g);
+		for (int g0 = 0; g0 < NP; g0 += G) {
+			float st[G], ss[G];
+#pragma unroll
+			for (int j = 0; j < G; ++j) {
+				const uint32_t b = p2_bitmask(sm, p2_ins0(g0 + j, H));
+				st[j] = p2_fsgn(t, b);
+				ss[j] = p2_fsgn(s, b);
+			}
 			if constexpr (ODD) {
-				re[u] = fmaf(-st, im[w], re[u]);
-				im[u] = fmaf(st, re[w], im[u]);
-				re[w] = fmaf(-ss, im[u], re[w]);
-				im[w] = fmaf(ss, re[u], im[w]);
-				re[u] = fmaf(-st, im[w], re[u]);
-				im[u] = fmaf(st, re[w], im[u]);
+#pragma unroll
+				for (int j = 0; j < G; ++j) {
+					const int u = p2_ins0(g0 + j, H), w = u ^ U;
+					re[u] = fmaf(-st[j], im[w], re[u]);
+					im[u] = fmaf(st[j], re[w], im[u]);
+				}
+#pragma unroll
+				for (int j = 0; j < G; ++j) {
+					const int u = p2_ins0(g0 + j, H), w = u ^ U;
+					re[w] = fmaf(-ss[j], im[u], re[w]);
+					im[w] = fmaf(ss[j], re[u], im[w]);
+				}
+#pragma unroll
+				for (int j = 0; j < G; ++j) {
+					const int u = p2_ins0(g0 + j, H), w = u ^ U;
+					re[u] = fmaf(-st[j], im[w], re[u]);
+					im[u] = fmaf(st[j], re[w], im[u]);
+				}
 			} else {
 				/* the same three shears as six fmaf, two lanes
 				 * per packed FMA (round-to-nearest per lane: the
 				 * same bits) */
-				const float2 a = make_float2(st, st);
-				const float2 b = make_float2(-ss, -ss);
-				float2 yu = make_float2(re[u], im[u]);
-				float2 yw = make_float2(re[w], im[w]);
-				yu = __ffma2_rn(a, yw, yu);
-				yw = __ffma2_rn(b, yu, yw);
-				yu = __ffma2_rn(a, yw, yu);
-				re[u] = yu.x;
-				im[u] = yu.y;
-				re[w] = yw.x;
-				im[w] = yw.y;
+				float2 yu[G], yw[G];
+#pragma unroll
+				for (int j = 0; j < G; ++j) {
+					const int u = p2_ins0(g0 + j, H), w = u ^ U;
+					yu[j] = make_float2(re[u], im[u]);
+					yw[j] = make_float2(re[w], im[w]);
+				}
+#pragma unroll
+				for (int j = 0; j < G; ++j)
+					yu[j] = __ffma2_rn(make_float2(st[j], st[j]),
+						yw[j], yu[j]);
+#pragma unroll
+				for (int j = 0; j < G; ++j)
+					yw[j] = __ffma2_rn(make_float2(-ss[j], -ss[j]),
+						yu[j], yw[j]);
+#pragma unroll
+				for (int j = 0; j < G; ++j)
+					yu[j] = __ffma2_rn(make_float2(st[j], st[j]),
+						yw[j], yu[j]);
+#pragma unroll
+				for (int j = 0; j < G; ++j) {
+					const int u = p2_ins0(g0 + j, H), w = u ^ U;
+					re[u] = yu[j].x;
+					im[u] = yu[j].y;
+					re[w] = yw[j].x;
+					im[w] = yw[j].y;
+				}
 			}
 		}
 	}

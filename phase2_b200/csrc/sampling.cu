@@ -407,11 +407,11 @@ extern "C" int p2d_sampled_device(struct p2_dev *d,
 				R * sizeof(struct p2_binst),
 				cudaMemcpyHostToDevice, d->stream);
 	}
-	const bool f64 = d->prec == PHASE2_PREC_FP64;
+	const int kind = p2_batch_kind(d->prec, job->form);
 	int per_sm = 0;
 	if (e == cudaSuccess)
 		e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm,
-			p2_batch_kernel(f64), P2_TPB, 0);
+			p2_batch_kernel(kind), P2_TPB, 0);
 	if (e == cudaSuccess)
 		e = cudaFuncSetAttribute(k_smp_plan,
 			cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -493,7 +493,7 @@ extern "C" int p2d_sampled_device(struct p2_dev *d,
 			e = cudaMemsetAsync(status, 0, 4 * sizeof(unsigned int),
 				d->stream);
 		if (e == cudaSuccess)
-			p2_batch_launch(f64, grid, d->stream, inst, nreg,
+			p2_batch_launch(kind, grid, d->stream, inst, nreg,
 				(const struct p2_op *)(b + off[PROG]),
 				(const struct phase2_pass *)(b + off[PASS]),
 				(const struct phase2_rot_rec *)(b + off[REC]),

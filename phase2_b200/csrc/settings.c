@@ -17,7 +17,7 @@ struct p2_settings p2_cfg = {
 	.max_span = PHASE2_MAX_SPAN,
 	.max_rots = 0,
 	.order = PHASE2_ORDER_LEX,
-	.fp32_form = PHASE2_FORM_LIFTED_F32,
+	.fp32_form = PHASE2_FORM_LIFTED,
 	.batch_persistent = 1,
 	.device_sampling = PHASE2_DEVICE_SAMPLING_AUTO,
 };

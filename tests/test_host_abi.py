@@ -305,10 +305,11 @@ def _rank(vectors):
 
 @pytest.mark.parametrize("tile,low", [(13, 5), (12, 4), (11, 3)])
 def test_planner_sweep_grouping(tile, low, oracle_lib):
-    """FP32 plans of registers of tile + 3 qubits or more group passes into
-    sweeps: every sweep's bases, modulo the low qubits, span at most
-    tile - low dimensions; the plan still applies every rotation in order
-    (emulated execution matches the oracle)."""
+    """FP32 plans (FP32-arithmetic form, the one sweeps run in) of
+    registers of tile + 3 qubits or more group passes into sweeps: every
+    sweep's bases, modulo the low qubits, span at most tile - low
+    dimensions; the plan still applies every rotation in order (emulated
+    execution matches the oracle)."""
     n = 17
     rng = np.random.Generator(np.random.PCG64(tile * 7 + low))
     jw = workloads.jw_terms(n, 3000, seed=tile)
@@ -316,6 +317,8 @@ def test_planner_sweep_grouping(tile, low, oracle_lib):
     flip, phase = jw.flip[pick], jw.phase[pick]
     phi = rng.uniform(-np.pi, np.pi, len(pick))
     old = p2.get_sweep()
+    form = p2.get_fp32_form()
+    p2.set_fp32_form(p2.FORM_LIFTED_F32)
     p2.set_sweep(tile, low)
     try:
         passes, recs = plan(n, flip, phase, phi, 5, 0, prec=1)
@@ -323,6 +326,7 @@ def test_planner_sweep_grouping(tile, low, oracle_lib):
         plain, _ = plan(n, flip, phase, phi, 5, 0, prec=1)
     finally:
         p2.set_sweep(*old)
+        p2.set_fp32_form(form)
     assert passes[0]["sweep"] == 1
     assert sum(p["sweep"] for p in plain) == 1
     heads = [i for i, p in enumerate(passes) if p["sweep"]] + [len(passes)]

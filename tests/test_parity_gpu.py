@@ -226,6 +226,15 @@ def test_stats_count_passes():
     assert st["sweeps"] == st["passes"]
 
 
+@pytest.fixture
+def f32_arith():
+    """The FP32-arithmetic form, the one sweeps run in."""
+    old = p2.get_fp32_form()
+    p2.set_fp32_form(p2.FORM_LIFTED_F32)
+    yield
+    p2.set_fp32_form(old)
+
+
 def _fp32_run(n, amp, flip, phase, phi, shape, kernel=True):
     """FP32 register through the pass executor under a sweep shape, the
     planned sweeps run as one kernel each or one kernel per pass."""
@@ -248,7 +257,7 @@ def _fp32_run(n, amp, flip, phase, phi, shape, kernel=True):
 @pytest.mark.parametrize("tile,low", [(13, 5), (12, 4), (14, 6), (13, 4),
                                       (11, 3), (14, 5)])
 @pytest.mark.parametrize("n", [17, 20])
-def test_sweeps_bit_identical(tile, low, n, oracle_lib):
+def test_sweeps_bit_identical(tile, low, n, oracle_lib, f32_arith):
     """A plan's sweeps run as one kernel each (shared-memory tiles, one
     state round trip per sweep) give the same bits as one kernel per pass
     of the same plan, for every tile shape; and fewer round trips."""
@@ -273,7 +282,7 @@ def test_sweeps_bit_identical(tile, low, n, oracle_lib):
 
 
 @pytest.mark.parametrize("span,rots", [(5, 0), (3, 0), (2, 7), (1, 1)])
-def test_sweeps_fusion_settings_and_random_strings(span, rots):
+def test_sweeps_fusion_settings_and_random_strings(span, rots, f32_arith):
     """Sweep kernels under every fusion setting, with diagonal strings and
     random (wide) flip masks: bit-identical to one kernel per pass."""
     n = 18
@@ -302,7 +311,7 @@ def test_sweeps_fusion_settings_and_random_strings(span, rots):
     assert np.array_equal(outs[0], outs[1])
 
 
-def test_sweeps_drivers_and_graphs(oracle_lib):
+def test_sweeps_drivers_and_graphs(oracle_lib, f32_arith):
     """Trotter steps replayed from CUDA graphs and qDRIFT samples (host and
     device sampling) with sweep kernels: the same overlaps as one kernel
     per pass of the same plans; within FP32 tolerance of the oracle."""
@@ -534,11 +543,11 @@ def _uneven_problems():
 
 
 @pytest.mark.parametrize("kind", ["trott", "trott2", "qdrift", "cmpsit"])
-def test_persistent_batch(kind, oracle_lib):
-    """FP32 batches in one persistent launch: bit-identical to the same
-    batch run on per-instance streams (same plans, same per-coset
-    arithmetic), within the FP32 tolerance of the FP64 oracle, and one
-    kernel launch for the whole batch."""
+def test_persistent_batch(kind, fp32_form, oracle_lib):
+    """FP32 batches in one persistent launch (both FP32 forms): bit-identical
+    to the same batch run on per-instance streams (same plans, same
+    per-coset arithmetic), within the FP32 tolerance of the FP64 oracle,
+    and one kernel launch for the whole batch."""
     probs = _uneven_problems()
     if kind == "cmpsit":
         probs = [dict(p, samples=2, steps=2, depth=12) for p in probs]
@@ -732,6 +741,34 @@ def test_cmpsit_device_sampling(nqb, nterms, ndet, samples, steps, length,
             assert np.array_equal(dev, want)
         else:
             assert np.max(np.abs(dev - want)) < FP32_TOL
+
+
+@pytest.mark.parametrize("kind", ["qdrift", "cmpsit"])
+def test_device_sampling_fp64_arith(kind, oracle_lib):
+    """Device sampling of an FP32 register in the FP64-arithmetic form
+    (the persistent kernel's FP64-arithmetic instance): the host loop's
+    overlaps and final register bit for bit, within the FP32 tolerance of
+    the oracle."""
+    old = p2.get_fp32_form()
+    p2.set_fp32_form(p2.FORM_LIFTED)
+    try:
+        t = workloads.jw_terms(11, 400, seed=0xF64A)
+        d = workloads.hamming_dets(11, 3, 5, seed=0xF64B)
+        if kind == "qdrift":
+            args = (5, 300, 0.02, 0x5EE1)
+            host, dev, _ = _qdrift_both_ways(11, t, d, *args)
+            want = oracle_lib.qdrift(11, t.flip, t.phase, t.cf, d.idx,
+                                     d.cf, *args)
+        else:
+            args = (3, 2, 40, 120, 0.05, 0.004, 0xC0DF)
+            host, dev, _ = _cmpsit_both_ways(11, t, d, *args,
+                                             prec=p2.PREC_FP32)
+            want = oracle_lib.cmpsit(11, t.flip, t.phase, t.cf, d.idx,
+                                     d.cf, *args)
+    finally:
+        p2.set_fp32_form(old)
+    assert np.array_equal(dev, host)
+    assert np.max(np.abs(dev - want)) < FP32_TOL
 
 
 def test_device_sampling_h2o(golden):
