@@ -834,14 +834,18 @@ def cmpsit33_study(steps: int = 1) -> dict:
     return out
 
 
-def batch8_study(prec: int = 1) -> dict:
+def batch8_study(prec: int = 1, form: int | None = None) -> dict:
     """A small, L2-resident persistent batch (8 trott instances of 18-20
-    qubits, 2,000 JW terms, 2 steps, FP32), run twice: the case the
-    persistent kernel's profile summary captures (its second launch)."""
+    qubits, 2,000 JW terms, 2 steps, FP32 in the process's form unless
+    `form` is given), run twice: the case the persistent kernel's profile
+    summaries capture (its second launch)."""
     import numpy as np
 
     import phase2_b200 as p2
     from phase2_b200 import workloads
+    form0 = p2.get_fp32_form()
+    if form is not None:
+        p2.set_fp32_form(form)
     g = np.random.Generator(np.random.PCG64(5))
     probs = []
     for k in range(8):
@@ -857,8 +861,16 @@ def batch8_study(prec: int = 1) -> dict:
             _, st = p2.batch("trott", probs, with_stats=True)
     finally:
         p2.set_precision(p2.PREC_FP64)
+        p2.set_fp32_form(form0)
     return {"passes": int(sum(s["passes"] for s in st)),
             "kernel_ms": float(sum(s["pass_ms"] for s in st))}
+
+
+def batch8f32_study() -> dict:
+    """batch8 in the FP32-arithmetic form (the persistent kernel's FP32
+    instance), for its profile summary."""
+    import phase2_b200 as p2
+    return batch8_study(prec=1, form=p2.FORM_LIFTED_F32)
 
 
 def batch8fp64_study() -> dict:
@@ -867,7 +879,7 @@ def batch8fp64_study() -> dict:
     return batch8_study(prec=0)
 
 
-def batched_study(ninst: int = 64, work_cap: float = 2.0e14,
+def batched_study(ninst: int = 64, work_cap: float = 1.5e14,
                   seed: int = 0xBA7C4):
     """Independent trott problems of uneven size run together: qubits
     U{18..24}, JW terms log-uniform in [1e3, 5e4], steps U{16..512}, FP32
@@ -955,10 +967,10 @@ def batched_study(ninst: int = 64, work_cap: float = 2.0e14,
 
 # studies appended to the N=1 line, in this order, with their approximate
 # B200 durations (for the study budget)
-STUDY_ORDER = ("trott26", "batched", "cmpsit33", "sharded", "sampling",
+STUDY_ORDER = ("batched", "cmpsit33", "trott26", "sharded", "sampling",
                "sweeps")
-STUDY_SECONDS = {"trott26": 480, "batched": 200, "cmpsit33": 300,
-                 "sharded": 60, "sampling": 30, "sweeps": 60}
+STUDY_SECONDS = {"trott26": 600, "batched": 180, "cmpsit33": 300,
+                 "sharded": 70, "sampling": 30, "sweeps": 60}
 
 
 # ---- the reference arm -------------------------------------------------
@@ -1028,17 +1040,18 @@ def main() -> None:
                          "the whole register file)")
     ap.add_argument("--quick", action="store_true",
                     help="skip the CPU baseline and secondary arms")
-    ap.add_argument("--studies", default="trott26,batched,cmpsit33,sharded",
+    ap.add_argument("--studies", default="batched,cmpsit33,trott26,sharded",
                     help="comma list of studies to append (run at N=1, in "
-                         "the order trott26, batched, cmpsit33, sharded, "
+                         "the order batched, cmpsit33, trott26, sharded, "
                          "sampling, sweeps, each only while the study "
                          "budget lasts)")
-    ap.add_argument("--study-budget", type=float, default=720.0,
+    ap.add_argument("--study-budget", type=float, default=1100.0,
                     help="seconds of studies at most (a study that would "
                          "not fit the remainder is skipped and reported)")
     ap.add_argument("--only-study", default=None,
                     help="run just this study (batched, trott26, cmpsit33, "
-                         "batch8, batch8fp64, sampling, sweeps, sharded) "
+                         "batch8, batch8f32, batch8fp64, sampling, sweeps, "
+                         "sharded) "
                          "and print its JSON; --nqb, when given, sets the "
                          "sweeps or sharded study's width")
     args = ap.parse_args()

@@ -50,6 +50,10 @@ __device__ __forceinline__ double p2_sgn(double v, uint32_t mask)
 		__double2loint(v));
 }
 
+#ifndef P2_ROT_GROUP
+#define P2_ROT_GROUP 1
+#endif
+
 /*
  * One rotation on the 2^M slots of a coset (FP64 state, exact rounding).
  * The sign of slot u is bit u of sm (the thread's parity already folded
@@ -77,33 +81,46 @@ __device__ __forceinline__ void p2_rot(double (&re)[1 << M],
 			im[u] = p2_cxt(c, im[u], ti);
 		}
 	} else {
+		/* pairs P2_ROT_GROUP at a time, step by step (independent
+		 * pairs: the same bits, more independent FP64 operations in
+		 * flight where the pass is compute-bound) */
 		constexpr int H = p2_hibit(U);
+		constexpr int NP = 1 << (M - 1);
+		constexpr int G = NP < P2_ROT_GROUP ? NP : P2_ROT_GROUP;
 #pragma unroll
-		for (int k = 0; k < (1 << (M - 1)); ++k) {
-			const int u = p2_ins0(k, H);
-			const int w = u ^ U;
-			const double su = p2_sgn(s, p2_bitmask(sm, u));
-			const double sw = p2_sgn(s, p2_bitmask(sm, w));
-			double tur, tui, twr, twi;
-			if constexpr (ODD) {
-				tur = p2_mul(-su, im[w]);
-				tui = p2_mul(su, re[w]);
-				twr = p2_mul(-sw, im[u]);
-				twi = p2_mul(sw, re[u]);
-			} else {
-				tur = p2_mul(su, re[w]);
-				tui = p2_mul(su, im[w]);
-				twr = p2_mul(sw, re[u]);
-				twi = p2_mul(sw, im[u]);
+		for (int g0 = 0; g0 < NP; g0 += G) {
+			double tur[G], tui[G], twr[G], twi[G];
+#pragma unroll
+			for (int j = 0; j < G; ++j) {
+				const int u = p2_ins0(g0 + j, H);
+				const int w = u ^ U;
+				const double su = p2_sgn(s, p2_bitmask(sm, u));
+				const double sw = p2_sgn(s, p2_bitmask(sm, w));
+				if constexpr (ODD) {
+					tur[j] = p2_mul(-su, im[w]);
+					tui[j] = p2_mul(su, re[w]);
+					twr[j] = p2_mul(-sw, im[u]);
+					twi[j] = p2_mul(sw, re[u]);
+				} else {
+					tur[j] = p2_mul(su, re[w]);
+					tui[j] = p2_mul(su, im[w]);
+					twr[j] = p2_mul(sw, re[u]);
+					twi[j] = p2_mul(sw, im[u]);
+				}
 			}
-			const double nur = p2_cxt(c, re[u], tur);
-			const double nui = p2_cxt(c, im[u], tui);
-			const double nwr = p2_cxt(c, re[w], twr);
-			const double nwi = p2_cxt(c, im[w], twi);
-			re[u] = nur;
-			im[u] = nui;
-			re[w] = nwr;
-			im[w] = nwi;
+#pragma unroll
+			for (int j = 0; j < G; ++j) {
+				const int u = p2_ins0(g0 + j, H);
+				const int w = u ^ U;
+				const double nur = p2_cxt(c, re[u], tur[j]);
+				const double nui = p2_cxt(c, im[u], tui[j]);
+				const double nwr = p2_cxt(c, re[w], twr[j]);
+				const double nwi = p2_cxt(c, im[w], twi[j]);
+				re[u] = nur;
+				im[u] = nui;
+				re[w] = nwr;
+				im[w] = nwi;
+			}
 		}
 	}
 }
@@ -280,7 +297,7 @@ __device__ __forceinline__ void p2_prefetch(double2 *stage, const double2 *st,
 #define P2_LIFT_GROUP 2
 #endif
 #ifndef P2_LIFT32_GROUP
-#define P2_LIFT32_GROUP 1
+#define P2_LIFT32_GROUP 4
 #endif
 
 template <int M, int U, int ODD>
