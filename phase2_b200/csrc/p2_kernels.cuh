@@ -693,8 +693,8 @@ __device__ __forceinline__ void p2_lift32_coset(float2 *__restrict__ st, IT x,
 
 /*
  * Many registers' recorded programs (p2_internal.h) in one launch.  Every
- * op of a program is cut into tiles (a pass: 32 lanes times a few cosets
- * each; a zero: 16384 amplitudes; a write or gather: one tile); op k+1 of
+ * op of a program is cut into tiles (a pass: 32 lanes times 4 or 16
+ * cosets each; a zero: 16384 amplitudes; a write or gather: one tile); op k+1 of
  * a program starts only when every tile of op k is done, programs are
  * independent.  Each program has a ticket, (op << 32) | next tile.  Every
  * warp schedules itself: its lane 0 claims a tile with one atomicAdd and
@@ -717,10 +717,13 @@ __device__ __forceinline__ void p2_lift32_coset(float2 *__restrict__ st, IT x,
  * and stores go through L2 only (ld/st .cg), since L1 is not coherent
  * across SMs.
  */
-/* Cosets per lane in a pass tile: 4 for passes of at least
- * P2_BATCH_BIG_PASS representatives, 1 below (more tiles for small
- * registers, whose passes are otherwise too few tiles to spread). */
-#define P2_BATCH_COSETS 4
+/* Cosets per lane in a pass tile: 16 (512 cosets a warp) for passes of
+ * at least P2_BATCH_BIG_PASS representatives, 4 (128 cosets) below (more
+ * tiles for small registers, whose passes are otherwise too few tiles to
+ * spread).  A tile is one claim and one completion count: smaller tiles
+ * measured slower on small batches (4x the claims and fences). */
+#define P2_BATCH_COSETS 16
+#define P2_BATCH_SMALL_COSETS 4
 #define P2_BATCH_BIG_PASS (UINT64_C(1) << 16)
 #define P2_BATCH_ZERO_TILE (P2_TPB * 128)
 #define P2_BATCH_WARPS (P2_TPB / 32)
@@ -738,7 +741,8 @@ __host__ __device__ __forceinline__ uint32_t p2_op_tiles(uint32_t kind,
 {
 	if (kind == P2_OP_PASS) {
 		const uint64_t nrep = namp >> span;
-		*b = nrep >= P2_BATCH_BIG_PASS ? P2_BATCH_COSETS : 1;
+		*b = nrep >= P2_BATCH_BIG_PASS ? P2_BATCH_COSETS
+					       : P2_BATCH_SMALL_COSETS;
 		const uint64_t per = (uint64_t)*b * 32;
 		return (uint32_t)((nrep + per - 1) / per);
 	}
