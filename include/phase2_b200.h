@@ -122,6 +122,15 @@ void circ_hamil_sort_flip(struct circ_hamil *hm);
 int phase2_set_batch_persistent(int on);
 
 /*
+ * Run length of the persistent launch (also device sampling's): an op is
+ * cut into tiles of 1024 amplitudes, and a warp claims runs of tiles, what
+ * is left of the op divided by (resident warps x per_warp), 1 to 16 tiles.
+ * Larger per_warp: shorter runs (more claims, finer balance).  Default 2;
+ * 1..64, else -1.  Results do not depend on it.
+ */
+int phase2_set_batch_runs(unsigned int per_warp);
+
+/*
  * Sweeps (FP32 registers in PHASE2_FORM_LIFTED_F32, tile + 3 to 31
  * qubits): the planner also closes passes at sweep boundaries, a sweep
  * being a run of passes whose bases, modulo the low `low_qubits` qubits,

@@ -83,6 +83,14 @@ def set_batch_persistent(on: bool) -> None:
     lib().phase2_set_batch_persistent(1 if on else 0)
 
 
+def set_batch_runs(per_warp: int) -> None:
+    """Persistent launch run length: a warp claims what is left of an op
+    over (resident warps x per_warp) tiles of 1024 amplitudes, 1 to 16
+    (default 2; 1..64)."""
+    if lib().phase2_set_batch_runs(per_warp) != 0:
+        raise ValueError(f"batch runs per warp {per_warp} not in 1..64")
+
+
 def set_sweep(tile_qubits: int, low_qubits: int = 5) -> None:
     """FP32 sweeps: plans group passes that fit a tile of 2^tile_qubits
     amplitudes (low_qubits of them the lowest qubits), and each group runs

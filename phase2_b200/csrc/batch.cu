@@ -19,11 +19,11 @@
 
 #include "p2_kernels.cuh"
 
-/* The cosets of one pass tile of a warp: lane k takes representatives
- * tile * cpt * 32 + j * 32 + k, j < cpt (coalesced per j). */
+/* The cosets of a warp's run of pass tiles: lane k takes representatives
+ * r0 + j * 32 + k, j < cpt (coalesced per j). */
 template <int M>
 __device__ __forceinline__ void p2_batch_pass_tile(float2 *st,
-	const struct phase2_pass &p, uint32_t tile, uint64_t nrep, uint32_t cpt,
+	const struct phase2_pass &p, uint64_t r0, uint64_t nrep, uint32_t cpt,
 	const struct p2_lift32_rec *srec, uint32_t lane)
 {
 	uint32_t pb[M > 0 ? M : 1];
@@ -31,7 +31,7 @@ __device__ __forceinline__ void p2_batch_pass_tile(float2 *st,
 	for (int k = 0; k < M; ++k)
 		pb[k] = (uint32_t)p.basis[k];
 	const uint32_t negm = p.scale < 0 ? 0x80000000u : 0u;
-	const uint64_t t0 = (uint64_t)tile * cpt * 32 + lane;
+	const uint64_t t0 = r0 + lane;
 	for (uint32_t j = 0; j < cpt; ++j) {
 		const uint64_t t = t0 + (uint64_t)j * 32;
 		if (t < nrep)
@@ -47,7 +47,7 @@ __device__ __forceinline__ void p2_batch_pass_tile(float2 *st,
  * the store (negated when the pass scale is -1). */
 template <int M>
 __device__ __forceinline__ void p2_batch_pass_tile_x(float2 *st,
-	const struct phase2_pass &p, uint32_t tile, uint64_t nrep, uint32_t cpt,
+	const struct phase2_pass &p, uint64_t r0, uint64_t nrep, uint32_t cpt,
 	const struct p2_lift_rec *srec, uint32_t lane)
 {
 	uint32_t pb[M > 0 ? M : 1];
@@ -55,7 +55,7 @@ __device__ __forceinline__ void p2_batch_pass_tile_x(float2 *st,
 	for (int k = 0; k < M; ++k)
 		pb[k] = (uint32_t)p.basis[k];
 	const bool neg = p.scale < 0;
-	const uint64_t t0 = (uint64_t)tile * cpt * 32 + lane;
+	const uint64_t t0 = r0 + lane;
 	for (uint32_t j = 0; j < cpt; ++j) {
 		const uint64_t t = t0 + (uint64_t)j * 32;
 		if (t >= nrep)
@@ -99,14 +99,14 @@ __device__ __forceinline__ void p2_batch_pass_tile_x(float2 *st,
  * k_pass (p2_apply_run), loads and stores at L2 only. */
 template <int M>
 __device__ __forceinline__ void p2_batch_pass_tile64(double2 *st,
-	const struct phase2_pass &p, uint32_t tile, uint64_t nrep, uint32_t cpt,
+	const struct phase2_pass &p, uint64_t r0, uint64_t nrep, uint32_t cpt,
 	const struct phase2_rot_rec *srec, uint32_t lane)
 {
 	uint64_t pb[M > 0 ? M : 1];
 #pragma unroll
 	for (int k = 0; k < M; ++k)
 		pb[k] = p.basis[k];
-	const uint64_t t0 = (uint64_t)tile * cpt * 32 + lane;
+	const uint64_t t0 = r0 + lane;
 	for (uint32_t j = 0; j < cpt; ++j) {
 		const uint64_t t = t0 + (uint64_t)j * 32;
 		if (t >= nrep)
@@ -163,70 +163,70 @@ template <> struct p2_brec<double2, false> {
 /* Span dispatch of a pass tile (FP32 state in either form, or FP64). */
 template <typename ST, bool X, typename RT>
 __device__ __forceinline__ void p2_batch_pass(ST *st,
-	const struct phase2_pass &p, uint32_t tile, uint64_t nrep, uint32_t cpt,
+	const struct phase2_pass &p, uint64_t r0, uint64_t nrep, uint32_t cpt,
 	const RT *srec, uint32_t lane)
 {
 	if constexpr (X) {
 		switch (p.span) {
 		case 0:
-			p2_batch_pass_tile_x<0>(st, p, tile, nrep, cpt, srec, lane);
+			p2_batch_pass_tile_x<0>(st, p, r0, nrep, cpt, srec, lane);
 			break;
 		case 1:
-			p2_batch_pass_tile_x<1>(st, p, tile, nrep, cpt, srec, lane);
+			p2_batch_pass_tile_x<1>(st, p, r0, nrep, cpt, srec, lane);
 			break;
 		case 2:
-			p2_batch_pass_tile_x<2>(st, p, tile, nrep, cpt, srec, lane);
+			p2_batch_pass_tile_x<2>(st, p, r0, nrep, cpt, srec, lane);
 			break;
 		case 3:
-			p2_batch_pass_tile_x<3>(st, p, tile, nrep, cpt, srec, lane);
+			p2_batch_pass_tile_x<3>(st, p, r0, nrep, cpt, srec, lane);
 			break;
 		case 4:
-			p2_batch_pass_tile_x<4>(st, p, tile, nrep, cpt, srec, lane);
+			p2_batch_pass_tile_x<4>(st, p, r0, nrep, cpt, srec, lane);
 			break;
 		default:
-			p2_batch_pass_tile_x<5>(st, p, tile, nrep, cpt, srec, lane);
+			p2_batch_pass_tile_x<5>(st, p, r0, nrep, cpt, srec, lane);
 			break;
 		}
 	} else if constexpr (sizeof(ST) == 16) {
 		switch (p.span) {
 		case 0:
-			p2_batch_pass_tile64<0>(st, p, tile, nrep, cpt, srec, lane);
+			p2_batch_pass_tile64<0>(st, p, r0, nrep, cpt, srec, lane);
 			break;
 		case 1:
-			p2_batch_pass_tile64<1>(st, p, tile, nrep, cpt, srec, lane);
+			p2_batch_pass_tile64<1>(st, p, r0, nrep, cpt, srec, lane);
 			break;
 		case 2:
-			p2_batch_pass_tile64<2>(st, p, tile, nrep, cpt, srec, lane);
+			p2_batch_pass_tile64<2>(st, p, r0, nrep, cpt, srec, lane);
 			break;
 		case 3:
-			p2_batch_pass_tile64<3>(st, p, tile, nrep, cpt, srec, lane);
+			p2_batch_pass_tile64<3>(st, p, r0, nrep, cpt, srec, lane);
 			break;
 		case 4:
-			p2_batch_pass_tile64<4>(st, p, tile, nrep, cpt, srec, lane);
+			p2_batch_pass_tile64<4>(st, p, r0, nrep, cpt, srec, lane);
 			break;
 		default:
-			p2_batch_pass_tile64<5>(st, p, tile, nrep, cpt, srec, lane);
+			p2_batch_pass_tile64<5>(st, p, r0, nrep, cpt, srec, lane);
 			break;
 		}
 	} else {
 		switch (p.span) {
 		case 0:
-			p2_batch_pass_tile<0>(st, p, tile, nrep, cpt, srec, lane);
+			p2_batch_pass_tile<0>(st, p, r0, nrep, cpt, srec, lane);
 			break;
 		case 1:
-			p2_batch_pass_tile<1>(st, p, tile, nrep, cpt, srec, lane);
+			p2_batch_pass_tile<1>(st, p, r0, nrep, cpt, srec, lane);
 			break;
 		case 2:
-			p2_batch_pass_tile<2>(st, p, tile, nrep, cpt, srec, lane);
+			p2_batch_pass_tile<2>(st, p, r0, nrep, cpt, srec, lane);
 			break;
 		case 3:
-			p2_batch_pass_tile<3>(st, p, tile, nrep, cpt, srec, lane);
+			p2_batch_pass_tile<3>(st, p, r0, nrep, cpt, srec, lane);
 			break;
 		case 4:
-			p2_batch_pass_tile<4>(st, p, tile, nrep, cpt, srec, lane);
+			p2_batch_pass_tile<4>(st, p, r0, nrep, cpt, srec, lane);
 			break;
 		default:
-			p2_batch_pass_tile<5>(st, p, tile, nrep, cpt, srec, lane);
+			p2_batch_pass_tile<5>(st, p, r0, nrep, cpt, srec, lane);
 			break;
 		}
 	}
@@ -246,6 +246,14 @@ __host__ __device__ constexpr int p2_batch_blocks(bool f64, bool x)
 	return f64 ? 2 : (x ? 3 : 5);
 }
 
+/* Hash of a program's ticket for the idle check (any move changes it). */
+__device__ __forceinline__ unsigned int p2_tk_hash(unsigned long long tk,
+	uint32_t i)
+{
+	return ((unsigned int)tk ^ (unsigned int)(tk >> 32) * 0x9e3779b9u) *
+		(2u * i + 1u);
+}
+
 template <typename ST, bool X>
 __global__ void __launch_bounds__(P2_TPB,
 	p2_batch_blocks(sizeof(ST) == 16, X))
@@ -257,14 +265,17 @@ __global__ void __launch_bounds__(P2_TPB,
 		const double *__restrict__ wval,
 		const uint64_t *__restrict__ gidx, double2 *__restrict__ gout,
 		struct p2_bctl *ctl, unsigned int *status,
+		const double *__restrict__ cum, unsigned int per_warp,
 		unsigned int idle_limit)
 {
 	constexpr bool F64 = sizeof(ST) == 16;
+	constexpr unsigned FULL = 0xffffffffu;
 	typedef typename p2_brec<ST, X>::type RT;
 	/* each warp keeps the records of the pass it last ran */
 	__shared__ RT srec_all[P2_BATCH_WARPS][P2_MAX_ROTS_PER_PASS];
 	const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
 	RT *const srec = srec_all[wid];
+	const uint32_t nwarps = gridDim.x * P2_BATCH_WARPS;
 	const uint32_t gw = blockIdx.x * P2_BATCH_WARPS + wid;
 	if (lane == 0) {
 		/* start of the launch: the earliest warp's timer (status[2..3]
@@ -273,70 +284,118 @@ __global__ void __launch_bounds__(P2_TPB,
 		atomicMax((unsigned long long *)(status + 2),
 			~p2_globaltimer());
 	}
+	/* home program: warps are spread over the programs in proportion to
+	 * their work (cum: running totals), so a large program gets many
+	 * warps that look at it first; without cum, round robin */
+	uint32_t home = gw % ninst;
+	if (cum) {
+		const double at = ((double)gw + 0.5) / (double)nwarps *
+			cum[ninst - 1];
+		uint32_t lo = 0, hi = ninst - 1;
+		while (lo < hi) {
+			const uint32_t mid = (lo + hi) >> 1;
+			if (cum[mid] > at)
+				hi = mid;
+			else
+				lo = mid + 1;
+		}
+		home = lo;
+	}
 	uint32_t held = 0xffffffffu; /* pass whose records srec holds */
-	uint32_t cursor = gw % ninst;
 	unsigned int idle = 0;
-	unsigned long long seen = 0; /* tickets at the last idle round */
+	unsigned int nap = 32; /* ns slept by the next idle round */
+	unsigned int seen = 0; /* ticket hash at the last idle round */
 	for (;;) {
-		/* lane 0 claims a tile: what = 0 nothing claimable yet, 1 work,
-		 * 2 exit */
+		/* look at 32 programs at a time (one lane each, from home on)
+		 * and claim a run of tiles from the first that has some:
+		 * what = 0 nothing claimable yet, 1 work, 2 exit */
 		int what = 2;
-		uint32_t ci = 0, cseq = 0, ctile = 0;
-		if (lane == 0) {
-			unsigned long long sig = 0;
-			for (uint32_t k = 0; k < ninst; ++k) {
-				const uint32_t i = cursor + k < ninst
-					? cursor + k
-					: cursor + k - ninst;
-				const uint32_t nops = inst[i].nops;
-				const unsigned long long tk =
-					*(volatile unsigned long long *)&ctl[i]
-						 .ticket;
-				sig += tk * (2ull * i + 1ull);
-				if ((uint32_t)(tk >> 32) >= nops)
-					continue; /* program finished */
-				what = 0;
-				const uint32_t off = inst[i].op_off;
-				if ((uint32_t)tk >=
-					ops[off + (uint32_t)(tk >> 32)].ntiles)
-					continue; /* all tiles taken */
-				const unsigned long long got =
-					atomicAdd(&ctl[i].ticket, 1ull);
-				const uint32_t seq = (uint32_t)(got >> 32);
-				const uint32_t tile = (uint32_t)got;
-				if (seq < nops && tile < ops[off + seq].ntiles) {
-					__threadfence();
-					ci = i;
-					cseq = seq;
-					ctile = tile;
-					cursor = i;
+		uint32_t ci = 0, cseq = 0, cfirst = 0, cend = 0;
+		unsigned int sig = 0;
+		for (uint32_t base = 0; base < ninst && what != 1; base += 32) {
+			const uint32_t k = base + lane;
+			uint32_t i = 0, seq = 0, nt = 0, off = 0, nops = 0;
+			unsigned long long tk = 0;
+			bool avail = false;
+			if (k < ninst) {
+				i = home + k < ninst ? home + k : home + k - ninst;
+				tk = *(volatile unsigned long long *)&ctl[i].ticket;
+				sig += p2_tk_hash(tk, i);
+				seq = (uint32_t)(tk >> 32);
+				nops = inst[i].nops;
+				off = inst[i].op_off;
+				if (seq < nops) {
+					what = 0;
+					nt = ops[off + seq].ntiles;
+					avail = (uint32_t)tk < nt;
+				}
+			}
+			unsigned int m = __ballot_sync(FULL, avail);
+			while (m) {
+				const int src = __ffs(m) - 1;
+				m &= m - 1;
+				int ok = 0;
+				if (lane == (uint32_t)src) {
+					/* guided run: the warp's share of what is
+					 * left of the op, cut into per_warp runs,
+					 * 1 to P2_BATCH_RUN tiles */
+					const uint32_t rem = nt - (uint32_t)tk;
+					uint32_t n = rem / (nwarps * per_warp);
+					n = n < 1 ? 1 : n > P2_BATCH_RUN ? P2_BATCH_RUN : n;
+					const unsigned long long got =
+						atomicAdd(&ctl[i].ticket,
+							(unsigned long long)n);
+					const uint32_t gs = (uint32_t)(got >> 32);
+					const uint32_t first = (uint32_t)got;
+					if (gs < nops) {
+						const uint32_t gnt = gs == seq
+							? nt : ops[off + gs].ntiles;
+						if (first < gnt) {
+							__threadfence();
+							ok = 1;
+							ci = i;
+							cseq = gs;
+							cfirst = first;
+							cend = first + n < gnt
+								? first + n : gnt;
+						}
+					}
+				}
+				const int who = __ballot_sync(FULL, ok);
+				if (who) {
+					const int w = __ffs(who) - 1;
+					ci = __shfl_sync(FULL, ci, w);
+					cseq = __shfl_sync(FULL, cseq, w);
+					cfirst = __shfl_sync(FULL, cfirst, w);
+					cend = __shfl_sync(FULL, cend, w);
 					what = 1;
 					break;
 				}
 			}
-			if (what == 0) {
-				if (sig != seen) {
-					seen = sig;
-					idle = 0;
-				}
-				if (++idle > idle_limit) {
-					atomicOr(status, 1u);
-					what = 2;
-				} else {
-					__nanosleep(1000);
-				}
-			} else if (what == 1) {
-				idle = 0;
-			}
+			if (what != 1)
+				what = __any_sync(FULL, what == 0) ? 0 : 2;
 		}
-		what = __shfl_sync(0xffffffffu, what, 0);
 		if (what == 2)
 			return;
-		if (what == 0)
+		if (what == 0) {
+			sig = __reduce_add_sync(FULL, sig);
+			if (sig != seen) {
+				seen = sig;
+				idle = 0;
+			}
+			if (++idle > idle_limit) {
+				if (lane == 0)
+					atomicOr(status, 1u);
+				return;
+			}
+			__nanosleep(nap);
+			if (nap < 1024)
+				nap <<= 1;
 			continue;
-		const uint32_t i = __shfl_sync(0xffffffffu, ci, 0);
-		const uint32_t seq = __shfl_sync(0xffffffffu, cseq, 0);
-		const uint32_t tile = __shfl_sync(0xffffffffu, ctile, 0);
+		}
+		idle = 0;
+		nap = 32;
+		const uint32_t i = ci, seq = cseq;
 		ST *const st = (ST *)inst[i].state;
 		const uint64_t namp = inst[i].namp;
 		const struct p2_op op = ops[inst[i].op_off + seq];
@@ -352,16 +411,18 @@ __global__ void __launch_bounds__(P2_TPB,
 				held = op.a;
 				__syncwarp();
 			}
-			p2_batch_pass<ST, X, RT>(st, p, tile, namp >> p.span,
-				op.b, srec, lane);
+			p2_batch_pass<ST, X, RT>(st, p,
+				(uint64_t)cfirst * op.b * 32, namp >> p.span,
+				(cend - cfirst) * op.b, srec, lane);
 		} else if (op.kind == P2_OP_ZERO) {
-			const uint64_t base = (uint64_t)tile * P2_BATCH_ZERO_TILE;
+			const uint64_t lo = (uint64_t)cfirst * P2_BATCH_ZERO_TILE;
+			uint64_t hi = (uint64_t)cend * P2_BATCH_ZERO_TILE;
+			hi = hi < namp ? hi : namp;
 			ST zero;
 			zero.x = 0;
 			zero.y = 0;
-			for (uint32_t k = lane; k < P2_BATCH_ZERO_TILE; k += 32)
-				if (base + k < namp)
-					__stcg(st + base + k, zero);
+			for (uint64_t k = lo + lane; k < hi; k += 32)
+				__stcg(st + k, zero);
 		} else if (op.kind == P2_OP_WRITE) {
 			/* in order: later writes win */
 			if (lane == 0)
@@ -385,7 +446,8 @@ __global__ void __launch_bounds__(P2_TPB,
 		__threadfence();
 		__syncwarp();
 		if (lane == 0) {
-			const unsigned int d = atomicAdd(&ctl[i].done, 1u) + 1u;
+			const unsigned int cnt = cend - cfirst;
+			const unsigned int d = atomicAdd(&ctl[i].done, cnt) + cnt;
 			if (d == op.ntiles) {
 				atomicExch(&ctl[i].done, 0u);
 				if (seq + 1 == inst[i].nops)
@@ -446,7 +508,7 @@ extern "C" int phase2_batch_wait_check(unsigned int idle_limit)
 			(const struct p2_binst *)(buf + o_inst), 1,
 			(const struct p2_op *)(buf + o_op), NULL, NULL, NULL,
 			NULL, NULL, NULL, (struct p2_bctl *)(buf + o_ctl),
-			(unsigned int *)(buf + o_status), idle_limit);
+			(unsigned int *)(buf + o_status), NULL, 2, idle_limit);
 		e = cudaGetLastError();
 	}
 	if (e == cudaSuccess)
@@ -539,6 +601,17 @@ extern "C" size_t phase2_batch_finish_ms(double *out, size_t n)
 	return last_n;
 }
 
+/* Runs a warp's share of an op is cut into (phase2_set_batch_runs). */
+static unsigned int g_batch_runs = 2;
+
+extern "C" int phase2_set_batch_runs(unsigned int per_warp)
+{
+	if (per_warp < 1 || per_warp > 64)
+		return -1;
+	g_batch_runs = per_warp;
+	return 0;
+}
+
 /* k_batch for FP32 or FP64 registers: its kernel function (occupancy
  * queries) and its launch. */
 int p2_batch_kind(int prec, int form)
@@ -559,20 +632,21 @@ void p2_batch_launch(int kind, unsigned grid, cudaStream_t stream,
 	const struct p2_binst *inst, uint32_t ninst, const struct p2_op *ops,
 	const struct phase2_pass *passes, const struct phase2_rot_rec *recs,
 	const uint64_t *widx, const double *wval, const uint64_t *gidx,
-	double2 *gout, struct p2_bctl *ctl, unsigned int *status)
+	double2 *gout, struct p2_bctl *ctl, unsigned int *status,
+	const double *cum)
 {
 	if (kind == P2_BK_F64)
 		k_batch<double2, false><<<grid, P2_TPB, 0, stream>>>(inst,
 			ninst, ops, passes, recs, widx, wval, gidx, gout, ctl,
-			status, P2_BATCH_IDLE_LIMIT);
+			status, cum, g_batch_runs, P2_BATCH_IDLE_LIMIT);
 	else if (kind == P2_BK_F32X)
 		k_batch<float2, true><<<grid, P2_TPB, 0, stream>>>(inst,
 			ninst, ops, passes, recs, widx, wval, gidx, gout, ctl,
-			status, P2_BATCH_IDLE_LIMIT);
+			status, cum, g_batch_runs, P2_BATCH_IDLE_LIMIT);
 	else
 		k_batch<float2, false><<<grid, P2_TPB, 0, stream>>>(inst,
 			ninst, ops, passes, recs, widx, wval, gidx, gout, ctl,
-			status, P2_BATCH_IDLE_LIMIT);
+			status, cum, g_batch_runs, P2_BATCH_IDLE_LIMIT);
 }
 
 /* Host seconds (PHASE2_BATCH_TIMING breakdown). */
@@ -617,16 +691,42 @@ extern "C" int p2d_batch_run(struct p2_dev *const *devs,
 		p2_align256(o_rec + nrec * sizeof(struct phase2_rot_rec));
 	const size_t o_wval = p2_align256(o_widx + nw * sizeof(uint64_t));
 	const size_t o_gidx = p2_align256(o_wval + 2 * nw * sizeof(double));
-	const size_t up = p2_align256(o_gidx + ng * sizeof(uint64_t));
+	const size_t o_cum = p2_align256(o_gidx + ng * sizeof(uint64_t));
+	const size_t up = p2_align256(o_cum + n * sizeof(double));
 	const size_t o_gout = up;
 	const size_t o_ctl = p2_align256(o_gout + ng * sizeof(double2));
 	const size_t o_status = p2_align256(o_ctl + n * sizeof(struct p2_bctl));
 	const size_t total = o_status + 256;
 
+	/* the kernel instance for the precision and the form the programs'
+	 * passes were planned in (one process-wide FP32 form), and its
+	 * resident blocks */
+	struct p2_dev *d0 = devs[0];
+	int form = d0->prec == PHASE2_PREC_FP64 ? PHASE2_FORM_EXACT
+						: PHASE2_FORM_LIFTED_F32;
+	for (size_t i = 0; i < n && d0->prec != PHASE2_PREC_FP64; i++)
+		if (progs[i]->npass) {
+			form = progs[i]->passes[0].form;
+			break;
+		}
+	const int kind = p2_batch_kind(d0->prec, form);
+	int per_sm = 0;
+	cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm,
+		p2_batch_kernel(kind), P2_TPB, 0);
+	if (e != cudaSuccess) {
+		log_error("batch: setup: %s", cudaGetErrorString(e));
+		return -1;
+	}
+	unsigned grid =
+		(unsigned)d0->sm_count * (unsigned)(per_sm > 0 ? per_sm : 1);
+
 	const double tb0 = p2_now();
 	unsigned char *h = (unsigned char *)malloc(up);
 	if (!h)
 		return -1;
+	/* warps that can ever find work at once: the largest op of every
+	 * program (more would only poll) */
+	uint64_t busiest = 0;
 	struct p2_binst *hi = (struct p2_binst *)(h + o_inst);
 	struct p2_op *ho = (struct p2_op *)(h + o_ops);
 	struct phase2_pass *hp = (struct phase2_pass *)(h + o_pass);
@@ -634,6 +734,10 @@ extern "C" int p2d_batch_run(struct p2_dev *const *devs,
 	uint64_t *hwi = (uint64_t *)(h + o_widx);
 	double *hwv = (double *)(h + o_wval);
 	uint64_t *hgi = (uint64_t *)(h + o_gidx);
+	/* running totals of the programs' work (amplitudes times rotations
+	 * plus two per pass for its loads and stores): home programs */
+	double *hcum = (double *)(h + o_cum);
+	double work = 0;
 	size_t bo = 0, bp = 0, br = 0, bw = 0, bg = 0;
 	for (size_t i = 0; i < n; i++) {
 		const struct p2_prog *pg = progs[i];
@@ -646,6 +750,7 @@ extern "C" int p2d_batch_run(struct p2_dev *const *devs,
 			hp[bp + k] = pg->passes[k];
 			hp[bp + k].rot_off += (uint32_t)br;
 		}
+		uint32_t most = 1;
 		for (size_t k = 0; k < pg->nops; k++) {
 			struct p2_op op = pg->ops[k];
 			switch (op.kind) {
@@ -653,10 +758,12 @@ extern "C" int p2d_batch_run(struct p2_dev *const *devs,
 				op.a += (uint32_t)bp;
 				op.ntiles = p2_op_tiles(P2_OP_PASS, d->namp,
 					hp[op.a].span, &op.b);
+				work += (double)d->namp * (hp[op.a].nrot + 2.0);
 				break;
 			case P2_OP_ZERO:
 				op.ntiles = p2_op_tiles(P2_OP_ZERO, d->namp, 0,
 					&op.b);
+				work += (double)d->namp;
 				break;
 			case P2_OP_WRITE:
 				op.a += (uint32_t)bw;
@@ -668,7 +775,12 @@ extern "C" int p2d_batch_run(struct p2_dev *const *devs,
 				break;
 			}
 			ho[bo + k] = op;
+			if (op.ntiles > most)
+				most = op.ntiles;
 		}
+		busiest += most;
+		work += 1.0; /* every program at least one unit */
+		hcum[i] = work;
 		if (pg->nrec)
 			memcpy(hr + br, pg->recs, pg->nrec * sizeof *hr);
 		if (pg->nw) {
@@ -685,9 +797,10 @@ extern "C" int p2d_batch_run(struct p2_dev *const *devs,
 		bg += pg->ng;
 	}
 
-	struct p2_dev *d0 = devs[0];
+	const uint64_t want = (busiest + P2_BATCH_WARPS - 1) / P2_BATCH_WARPS;
+	if (want < grid)
+		grid = (unsigned)want;
 	unsigned char *dbuf = NULL;
-	cudaError_t e = cudaSuccess;
 	const double tb1 = p2_now();
 	for (size_t i = 0; i < n && e == cudaSuccess; i++)
 		e = cudaStreamSynchronize(devs[i]->stream);
@@ -703,27 +816,11 @@ extern "C" int p2d_batch_run(struct p2_dev *const *devs,
 	const double tb3 = p2_now();
 	if (e == cudaSuccess)
 		e = cudaMemsetAsync(dbuf + o_ctl, 0, total - o_ctl, d0->stream);
-	/* the kernel instance for the precision and the form the programs'
-	 * passes were planned in (one process-wide FP32 form) */
-	int form = d0->prec == PHASE2_PREC_FP64 ? PHASE2_FORM_EXACT
-						: PHASE2_FORM_LIFTED_F32;
-	for (size_t i = 0; i < n && d0->prec != PHASE2_PREC_FP64; i++)
-		if (progs[i]->npass) {
-			form = progs[i]->passes[0].form;
-			break;
-		}
-	const int kind = p2_batch_kind(d0->prec, form);
-	int per_sm = 0;
-	if (e == cudaSuccess)
-		e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm,
-			p2_batch_kernel(kind), P2_TPB, 0);
 	if (e != cudaSuccess) {
 		p2_scratch_free(dbuf, d0->stream);
 		log_error("batch: setup: %s", cudaGetErrorString(e));
 		return -1;
 	}
-	const unsigned grid =
-		(unsigned)d0->sm_count * (unsigned)(per_sm > 0 ? per_sm : 1);
 	cudaEventRecord(d0->t0, d0->stream);
 	p2_batch_launch(kind, grid, d0->stream,
 		(const struct p2_binst *)(dbuf + o_inst), (uint32_t)n,
@@ -734,7 +831,8 @@ extern "C" int p2d_batch_run(struct p2_dev *const *devs,
 		(const double *)(dbuf + o_wval),
 		(const uint64_t *)(dbuf + o_gidx), (double2 *)(dbuf + o_gout),
 		(struct p2_bctl *)(dbuf + o_ctl),
-		(unsigned int *)(dbuf + o_status));
+		(unsigned int *)(dbuf + o_status),
+		(const double *)(dbuf + o_cum));
 	e = cudaGetLastError();
 	cudaEventRecord(d0->t1, d0->stream);
 	unsigned int status = 0;

@@ -362,18 +362,11 @@ __global__ void __launch_bounds__(P2_LB_TPB, MINB)
 			im[u] = (double)v.y;
 		}
 		const uint32_t x = p2_rep_t<M, uint32_t>(c << 5, p) | lane;
-		/* the next record and its sign word are read before the current
-		 * rotation is dispatched, so their latency overlaps its work */
-		struct p2_lift_rec q = srec[0];
-		uint32_t sm = q.sm ^ (0u - p2_parity(x & (uint32_t)q.z));
 		for (uint32_t r = 0; r < nrot; ++r) {
-			const struct p2_lift_rec qn =
-				srec[r + 1 < nrot ? r + 1 : r];
-			const uint32_t smn =
-				qn.sm ^ (0u - p2_parity(x & (uint32_t)qn.z));
+			const struct p2_lift_rec q = srec[r];
+			const uint32_t sm =
+				q.sm ^ (0u - p2_parity(x & (uint32_t)q.z));
 			p2_apply_lift<M>(q.key, re, im, q.t, q.s, sm);
-			q = qn;
-			sm = smn;
 		}
 		if (neg)
 			p2_lb_store<M, true>(st, x, pb, re, im);

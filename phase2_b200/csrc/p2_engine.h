@@ -128,7 +128,9 @@ struct p2_bctl;
  * (P2_BK_F64): the instance for a precision and FP32 form, its function
  * (occupancy queries) and its launch.  status points to 16
  * zeroed bytes: status[0] is raised when a wait gives up, status[2..3]
- * receive the complement of the launch's start time (global timer). */
+ * receive the complement of the launch's start time (global timer).  cum
+ * (device, one double per program, or NULL for round robin): running
+ * totals of the programs' work, which spread the warps' home programs. */
 enum { P2_BK_F32 = 0, P2_BK_F32X = 1, P2_BK_F64 = 2 };
 int p2_batch_kind(int prec, int form);
 const void *p2_batch_kernel(int kind);
@@ -136,7 +138,8 @@ void p2_batch_launch(int kind, unsigned grid, cudaStream_t stream,
 	const struct p2_binst *inst, uint32_t ninst, const struct p2_op *ops,
 	const struct phase2_pass *passes, const struct phase2_rot_rec *recs,
 	const uint64_t *widx, const double *wval, const uint64_t *gidx,
-	double2 *gout, struct p2_bctl *ctl, unsigned int *status);
+	double2 *gout, struct p2_bctl *ctl, unsigned int *status,
+	const double *cum);
 
 /* lift_bulk.cu: one FP32 pass of the FP64-arithmetic form on a kernel
  * whose next cosets are staged in shared memory, by bulk copies (variant

@@ -693,20 +693,27 @@ __device__ __forceinline__ void p2_lift32_coset(float2 *__restrict__ st, IT x,
 
 /*
  * Many registers' recorded programs (p2_internal.h) in one launch.  Every
- * op of a program is cut into tiles (a pass: 32 lanes times 4 or 16
- * cosets each; a zero: 16384 amplitudes; a write or gather: one tile); op k+1 of
- * a program starts only when every tile of op k is done, programs are
- * independent.  Each program has a ticket, (op << 32) | next tile.  Every
- * warp schedules itself: its lane 0 claims a tile with one atomicAdd and
- * broadcasts it, the warp runs it, and the warp that completes the last
- * tile of an op publishes the next op by resetting the ticket -- no block
- * barrier anywhere, so a warp never waits for its block's other warps.
- * Warps look for work across programs starting from the last one they
- * served, so small programs interleave and the GPU stays busy without a
- * launch per pass.  Waiting is bounded: a warp that finds nothing to claim
- * while no ticket moves for idle_limit consecutive rounds (about a
- * microsecond each; a ticket moves whenever any tile is claimed or any op
- * is published) raises status and returns, so a scheduling fault ends the
+ * op of a program is cut into tiles (a pass: 1024 amplitudes, 32 lanes
+ * times 2^(5 - span) cosets; a zero: 16384 amplitudes; a write or gather:
+ * one tile); op k+1 of a program starts only when every tile of op k is
+ * done, programs are independent.  Each program has a ticket, (op << 32) |
+ * next tile, on a line of its own.  Every warp schedules itself, with no
+ * block barrier anywhere: its 32 lanes read 32 programs' tickets at once
+ * (one memory round trip), the first program with tiles left, in order
+ * from the warp's home program, is claimed with one atomicAdd of a run of
+ * tiles, the warp runs them, and the warp that completes the last tile of
+ * an op publishes the next op by resetting the ticket.  Runs are guided:
+ * what is left of the op over (warps x per_warp), 1 to P2_BATCH_RUN tiles,
+ * so a large op is claimed in long runs while every warp can take part,
+ * and its last tiles in single ones.  Home programs spread the warps over
+ * the programs in proportion to their work, so a long program is not
+ * starved by many short ones and its chain of ops does not run alone at
+ * the end.  A warp that finds nothing to claim sleeps between looks, 32 ns
+ * at first, doubling to about a microsecond, until it claims again.
+ * Waiting is bounded: a warp that finds nothing to claim while no ticket
+ * moves for idle_limit consecutive rounds (at most about a microsecond
+ * each; a ticket moves whenever any tile is claimed or any op is
+ * published) raises status and returns, so a scheduling fault ends the
  * launch instead of hanging it, while long single-program runs, where most
  * warps wait on one op at a time, keep going.
  *
@@ -717,14 +724,10 @@ __device__ __forceinline__ void p2_lift32_coset(float2 *__restrict__ st, IT x,
  * and stores go through L2 only (ld/st .cg), since L1 is not coherent
  * across SMs.
  */
-/* Cosets per lane in a pass tile: 16 (512 cosets a warp) for passes of
- * at least P2_BATCH_BIG_PASS representatives, 4 (128 cosets) below (more
- * tiles for small registers, whose passes are otherwise too few tiles to
- * spread).  A tile is one claim and one completion count: smaller tiles
- * measured slower on small batches (4x the claims and fences). */
-#define P2_BATCH_COSETS 16
-#define P2_BATCH_SMALL_COSETS 4
-#define P2_BATCH_BIG_PASS (UINT64_C(1) << 16)
+/* A pass tile is 32 amplitudes a lane: 32 lanes times 2^(5 - span) cosets
+ * (a warp's 1024 amplitudes, whatever the span); a warp claims runs of 1
+ * to P2_BATCH_RUN tiles. */
+#define P2_BATCH_RUN 16
 #define P2_BATCH_ZERO_TILE (P2_TPB * 128)
 #define P2_BATCH_WARPS (P2_TPB / 32)
 
@@ -735,14 +738,13 @@ struct p2_binst {
 };
 
 /* Work tiles of an op on a register of namp amplitudes; for a pass of
- * span `span` also the cosets per thread of a tile (*b). */
+ * span `span` also the cosets per lane of a tile (*b). */
 __host__ __device__ __forceinline__ uint32_t p2_op_tiles(uint32_t kind,
 	uint64_t namp, uint32_t span, uint32_t *b)
 {
 	if (kind == P2_OP_PASS) {
 		const uint64_t nrep = namp >> span;
-		*b = nrep >= P2_BATCH_BIG_PASS ? P2_BATCH_COSETS
-					       : P2_BATCH_SMALL_COSETS;
+		*b = 1u << (span < 5 ? 5 - span : 0);
 		const uint64_t per = (uint64_t)*b * 32;
 		return (uint32_t)((nrep + per - 1) / per);
 	}
@@ -752,11 +754,15 @@ __host__ __device__ __forceinline__ uint32_t p2_op_tiles(uint32_t kind,
 	return 1;
 }
 
+/* A program's scheduling state, one 128-byte line each: every warp polls
+ * the tickets and counts completions with atomics, so two programs never
+ * share a line (nor an L2 slice's queue for it). */
 struct p2_bctl {
 	unsigned long long ticket;
 	unsigned int done;
 	unsigned int pad;
 	unsigned long long end_ns; /* global timer when the program finished */
+	unsigned long long line[13];
 };
 
 #endif /* P2_KERNELS_CUH */

@@ -416,16 +416,16 @@ extern "C" int p2d_sampled_device(struct p2_dev *d,
 		e = cudaFuncSetAttribute(k_smp_plan,
 			cudaFuncAttributeMaxDynamicSharedMemorySize,
 			(int)P2_SMP_PLAN_SMEM);
-	/* no op has more tiles than a span-0 pass or a zero (more blocks
+	/* no op has more tiles than a span-0 pass or a zero (more warps
 	 * would only poll) */
+	unsigned grid =
+		(unsigned)d->sm_count * (unsigned)(per_sm > 0 ? per_sm : 1);
 	uint32_t cpt = 0;
 	uint64_t most = p2_op_tiles(P2_OP_PASS, d->namp, 0, &cpt);
 	const uint32_t zt = p2_op_tiles(P2_OP_ZERO, d->namp, 0, &cpt);
 	if (zt > most)
 		most = zt;
-	most *= R;
-	unsigned grid =
-		(unsigned)d->sm_count * (unsigned)(per_sm > 0 ? per_sm : 1);
+	most = (most * R + P2_BATCH_WARPS - 1) / P2_BATCH_WARPS;
 	if (most < grid)
 		grid = (unsigned)most;
 	uint32_t *npc = (uint32_t *)(b + off[NPC]);
@@ -500,7 +500,7 @@ extern "C" int p2d_sampled_device(struct p2_dev *d,
 				(const uint64_t *)(b + off[WIDX]),
 				(const double *)(b + off[WVAL]),
 				(const uint64_t *)(b + off[GIDX]),
-				(double2 *)(b + off[GOUT]), ctl, status);
+				(double2 *)(b + off[GOUT]), ctl, status, NULL);
 		if (e == cudaSuccess)
 			e = cudaGetLastError();
 		if (timing)

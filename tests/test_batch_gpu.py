@@ -58,3 +58,46 @@ def test_finish_times(prec):
     fin = [s["finish_ms"] for s in stats]
     assert all(f is not None and f > 0 for f in fin), fin
     assert fin[2] > max(fin[0], fin[1]), fin
+
+
+@pytest.mark.parametrize("runs", [1, 64])
+def test_run_lengths(runs, oracle_lib):
+    """Every run length gives the oracle's bits (FP64): the tiles a warp
+    claims at a time change only the schedule.  Out-of-range values are
+    refused."""
+    with pytest.raises(ValueError):
+        p2.set_batch_runs(0)
+    probs = []
+    for k, n in enumerate((16, 9, 14)):
+        t = workloads.jw_terms(n, 60 + 20 * k, seed=0xB30 + k)
+        d = workloads.hamming_dets(n, 2, n // 2, seed=0xB40 + k)
+        probs.append(dict(nqb=n, terms=t, dets=d, steps=3, delta=0.07))
+    p2.set_batch_runs(runs)
+    try:
+        zs = p2.batch("trott", probs)
+    finally:
+        p2.set_batch_runs(2)
+    for p, z in zip(probs, zs):
+        t, d = p["terms"], p["dets"]
+        want = oracle_lib.trott(p["nqb"], t.flip, t.phase, t.cf, d.idx, d.cf,
+                                3, 0.07)
+        assert np.array_equal(z, want)
+
+
+def test_many_programs(oracle_lib):
+    """More programs than a warp has lanes (the scan looks at 32 tickets
+    at a time), of uneven sizes: every result is the oracle's (FP64)."""
+    probs = []
+    for k in range(45):
+        n = 5 + k % 8
+        t = workloads.jw_terms(n, 12 + k, seed=0xB50 + k)
+        d = workloads.hamming_dets(n, 1, n // 2, seed=0xB90 + k)
+        probs.append(dict(nqb=n, terms=t, dets=d, steps=1 + k % 4,
+                          delta=0.11))
+    zs, stats = p2.batch("trott2", probs, with_stats=True)
+    assert sum(s["launches"] for s in stats) == 1
+    for p, z in zip(probs, zs):
+        t, d = p["terms"], p["dets"]
+        want = oracle_lib.trott(p["nqb"], t.flip, t.phase, t.cf, d.idx, d.cf,
+                                p["steps"], 0.11, order2=True)
+        assert np.array_equal(z, want)
