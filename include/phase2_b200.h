@@ -124,7 +124,8 @@ int phase2_set_batch_persistent(int on);
 /*
  * Run length of the persistent launch (also device sampling's): an op is
  * cut into tiles of 1024 amplitudes, and a warp claims runs of tiles, what
- * is left of the op divided by (resident warps x per_warp), 1 to 16 tiles.
+ * is left of the op times the programs running, divided by (resident
+ * warps x per_warp), 1 to 16 tiles.
  * Larger per_warp: shorter runs (more claims, finer balance).  Default 2;
  * 1..64, else -1.  Results do not depend on it.
  */

@@ -85,8 +85,8 @@ def set_batch_persistent(on: bool) -> None:
 
 def set_batch_runs(per_warp: int) -> None:
     """Persistent launch run length: a warp claims what is left of an op
-    over (resident warps x per_warp) tiles of 1024 amplitudes, 1 to 16
-    (default 2; 1..64)."""
+    times the programs running, over (resident warps x per_warp), tiles of
+    1024 amplitudes, 1 to 16 (default 2; 1..64)."""
     if lib().phase2_set_batch_runs(per_warp) != 0:
         raise ValueError(f"batch runs per warp {per_warp} not in 1..64")
 

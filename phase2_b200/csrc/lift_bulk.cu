@@ -266,13 +266,6 @@ __global__ void __launch_bounds__(P2_LB_TPB, p2_lb_blocks(M))
  * lanes read pieces other lanes copied.  No waits of the kernel's own: the
  * copies complete by themselves.
  */
-__device__ __forceinline__ void p2_cp16(uint32_t dst, const void *src)
-{
-	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst),
-		"l"(src)
-		: "memory");
-}
-
 template <int M, int MINB>
 __global__ void __launch_bounds__(P2_LB_TPB, MINB)
 	k_pass_lift_pf(float2 *__restrict__ st, uint32_t nwc,

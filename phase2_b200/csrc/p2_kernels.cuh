@@ -236,6 +236,14 @@ __device__ __forceinline__ void p2_cp_async(double2 *smem, const double2 *g)
 		: "memory");
 }
 
+/* Asynchronous global -> shared copy of 16 bytes to a shared address. */
+__device__ __forceinline__ void p2_cp16(uint32_t dst, const void *src)
+{
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst),
+		"l"(src)
+		: "memory");
+}
+
 __device__ __forceinline__ void p2_cp_commit()
 {
 	asm volatile("cp.async.commit_group;\n" ::: "memory");
@@ -703,9 +711,10 @@ __device__ __forceinline__ void p2_lift32_coset(float2 *__restrict__ st, IT x,
  * from the warp's home program, is claimed with one atomicAdd of a run of
  * tiles, the warp runs them, and the warp that completes the last tile of
  * an op publishes the next op by resetting the ticket.  Runs are guided:
- * what is left of the op over (warps x per_warp), 1 to P2_BATCH_RUN tiles,
- * so a large op is claimed in long runs while every warp can take part,
- * and its last tiles in single ones.  Home programs spread the warps over
+ * what is left of the op times the programs seen running, over (warps x
+ * per_warp), 1 to P2_BATCH_RUN tiles, so an op is claimed in long runs
+ * while every warp that can reach it still gets some, and its last tiles
+ * in single ones.  Home programs spread the warps over
  * the programs in proportion to their work, so a long program is not
  * starved by many short ones and its chain of ops does not run alone at
  * the end.  A warp that finds nothing to claim sleeps between looks, 32 ns
