@@ -504,10 +504,12 @@ __global__ void __launch_bounds__(P2_TPB,
 			}
 			bool staged = false;
 			if constexpr (X) {
-				/* whole span-5 tiles with every pivot at bit 5
-				 * or above: staged */
+				/* runs of two or more whole span-5 tiles with
+				 * every pivot at bit 5 or above: staged (a
+				 * single tile has nothing to overlap its copy
+				 * with, and loads directly) */
 				staged = p.span == 5 && p.piv[0] >= 5 &&
-					namp >= 1024;
+					namp >= 1024 && cend - cfirst >= 2;
 				if (staged)
 					p2_batch_pass_staged_x((float2 *)st, p,
 						cfirst, cend, srec, lane,
