@@ -130,6 +130,7 @@ int phase2_set_batch_persistent(int on);
  * 1..64, else -1.  Results do not depend on it.
  */
 int phase2_set_batch_runs(unsigned int per_warp);
+unsigned int phase2_get_batch_runs(void);
 
 /*
  * Sweeps (FP32 registers in PHASE2_FORM_LIFTED_F32, tile + 3 to 31

@@ -302,6 +302,7 @@ _SIGS = {
     "phase2_set_fp32_form": (C.c_int, [C.c_int]),
     "phase2_set_batch_persistent": (C.c_int, [C.c_int]),
     "phase2_set_batch_runs": (C.c_int, [C.c_uint]),
+    "phase2_get_batch_runs": (C.c_uint, []),
     "phase2_set_device_sampling": (C.c_int, [C.c_int]),
     "phase2_set_sweep": (C.c_int, [C.c_int, C.c_int]),
     "phase2_get_sweep": (None, [C.POINTER(C.c_int), C.POINTER(C.c_int)]),

@@ -1,4 +1,5 @@
-"""Autotuner for the pass kernel launch table and the fusion cap.
+"""Autotuner for the pass kernel launch table, the fusion cap and the
+persistent batch kernel's run length.
 
 For each state precision and span M (amplitudes per thread = 2^M) it times
 passes of the kernel variants (FP64: direct loads / shared-memory prefetch;
@@ -13,6 +14,11 @@ FP32 passes: the grid density is tuned on the FP32-arithmetic kernel
 a build for two blocks per SM) are compared;
 the entry keeps both choices (the variant only steers the FP64-arithmetic
 form).
+
+Last, the persistent batch kernel's run length (phase2_set_batch_runs:
+runs per warp's share of an op, 1, 2, 4 or 8) is timed on a batch of 16
+small trott instances (18-21 qubits, FP32 in the current form) and the
+fastest kept.
 
 Results are written as JSON (the full report) and as the flat launch table
 the library applies at world_init when the GPU name matches
@@ -157,11 +163,50 @@ def sweep_fusion(nqb: int, depth: int = 1024) -> dict:
     return out
 
 
+BATCH_RUNS = (1, 2, 4, 8)
+
+
+def sweep_batch_runs(ninst: int = 16, reps: int = 2) -> dict:
+    """Kernel milliseconds of one persistent launch per run length, on
+    `ninst` trott instances of 18-21 qubits (2,000 JW terms, 2 steps,
+    FP32 state in the current form); the best of `reps` launches each."""
+    from . import batch, set_batch_runs, set_precision, workloads
+    g = np.random.Generator(np.random.PCG64(21))
+    probs = []
+    for k in range(ninst):
+        n = int(g.integers(18, 22))
+        probs.append(dict(nqb=n, terms=workloads.jw_terms(n, 2000,
+                                                          seed=300 + k),
+                          dets=workloads.hamming_dets(n, 1, n // 2,
+                                                      seed=400 + k),
+                          steps=2, delta=0.05))
+    before = lib().phase2_get_batch_runs()
+    out: dict = {"workload": f"{ninst} trott instances, 18-21 qubits, "
+                 "2000 JW terms, 2 steps, FP32", "kernel_ms": {}}
+    set_precision(PREC_FP32)
+    try:
+        for runs in BATCH_RUNS:
+            set_batch_runs(runs)
+            best = None
+            for _ in range(reps + 1):  # the first launch warms up
+                _, st = batch("trott", probs, with_stats=True)
+                ms = float(sum(s["pass_ms"] for s in st))
+                best = ms if best is None or ms < best else best
+            out["kernel_ms"][str(runs)] = best
+    finally:
+        set_batch_runs(before)
+        set_precision(PREC_FP64)
+    out["best"] = int(min(out["kernel_ms"], key=lambda r:
+                          out["kernel_ms"][r]))
+    return out
+
+
 def run(nqb: int) -> dict:
     world_ensure()
     t0 = time.time()
     launch = sweep_launch(nqb)
     fusion = sweep_fusion(nqb)
+    runs = sweep_batch_runs()
     best_span = {p: int(max(v, key=lambda s: v[s]["rot_amp_per_s"]))
                  for p, v in fusion.items()}
     import subprocess
@@ -172,7 +217,8 @@ def run(nqb: int) -> dict:
     except (OSError, IndexError):
         gpu = "unknown"
     return {"gpu": gpu, "nqb": nqb, "seconds": time.time() - t0,
-            "launch": launch, "fusion": fusion, "max_span": best_span}
+            "launch": launch, "fusion": fusion, "max_span": best_span,
+            "batch_runs": runs}
 
 
 def apply(table: dict | str | Path | None = None, prec: int | None = None):
@@ -192,6 +238,8 @@ def apply(table: dict | str | Path | None = None, prec: int | None = None):
         for M, e in per_m.items():
             L.phase2_tune_set(pr, int(M), int(e["variant"]),
                               int(e["per_sm"]))
+    if "batch_runs" in table:
+        L.phase2_set_batch_runs(int(table["batch_runs"]["best"]))
     if prec is not None:
         pname = "fp32" if prec == PREC_FP32 else "fp64"
         span = table.get("max_span", {}).get(pname)
@@ -211,6 +259,8 @@ def write_table(table: dict, path: str | Path = TABLE_FILE) -> None:
         for M, e in sorted(per_m.items(), key=lambda kv: int(kv[0])):
             lines.append(f"launch {PRECS[pname]} {int(M)} "
                          f"{int(e['variant'])} {int(e['per_sm'])}")
+    if "batch_runs" in table:
+        lines.append(f"batch_runs {int(table['batch_runs']['best'])}")
     Path(path).write_text("\n".join(lines) + "\n")
 
 
@@ -254,6 +304,7 @@ def main() -> None:
                   f"per_sm={e['per_sm']} {e['us_per_pass']:.1f} us/pass "
                   f"{e['gbs']:.0f} GB/s")
         print(pname, "fusion", json.dumps(res["fusion"][pname]))
+    print("batch_runs", json.dumps(res["batch_runs"]))
     print("max_span", res["max_span"], f"({res['seconds']:.0f} s)")
 
 

@@ -719,6 +719,11 @@ extern "C" int phase2_set_batch_runs(unsigned int per_warp)
 	return 0;
 }
 
+extern "C" unsigned int phase2_get_batch_runs(void)
+{
+	return g_batch_runs;
+}
+
 /* k_batch for FP32 or FP64 registers: its kernel function (occupancy
  * queries) and its launch. */
 int p2_batch_kind(int prec, int form)

@@ -6,6 +6,7 @@
  * File format, one entry per line ('#' starts a comment line):
  *   gpu <device name as the CUDA runtime reports it>
  *   launch <prec 0|1> <span 0..5> <variant> <per_sm>
+ *   batch_runs <1..64>     (phase2_set_batch_runs: persistent run length)
  * A table applies only to a device of the same name: launch choices that
  * were measured on one GPU are not carried to another.
  */
@@ -62,8 +63,18 @@ int phase2_load_tuning(const char *path, const char *gpu)
 			match = strcmp(p + 4, gpu) == 0;
 			continue;
 		}
-		int prec, span, variant, per_sm;
+		int prec, span, variant, per_sm, runs;
 		char tail;
+		if (strncmp(p, "batch_runs ", 11) == 0) {
+			if (sscanf(p, "batch_runs %d %c", &runs, &tail) != 1 ||
+				runs < 1 || runs > 64) {
+				log_error("launch table %s: bad line \"%s\"", path,
+					p);
+				bad = 1;
+				break;
+			}
+			continue;
+		}
 		if (sscanf(p, "launch %d %d %d %d %c", &prec, &span, &variant,
 			    &per_sm, &tail) != 4 ||
 			prec < 0 || prec > 1 || span < 0 ||
@@ -88,10 +99,15 @@ int phase2_load_tuning(const char *path, const char *gpu)
 	rewind(f);
 	int applied = 0;
 	while (fgets(line, sizeof line, f)) {
-		int prec, span, variant, per_sm;
+		int prec, span, variant, per_sm, runs;
 		char *p = line;
 		while (*p == ' ' || *p == '\t')
 			p++;
+		if (sscanf(p, "batch_runs %d", &runs) == 1) {
+			phase2_set_batch_runs((unsigned int)runs);
+			applied++;
+			continue;
+		}
 		if (sscanf(p, "launch %d %d %d %d", &prec, &span, &variant,
 			    &per_sm) == 4) {
 			if (phase2_tune_set(prec, span, variant, per_sm) < 0) {

@@ -33,10 +33,12 @@ def _table():
 @pytest.fixture(autouse=True)
 def _restore():
     saved = _table()
+    runs = lib().phase2_get_batch_runs()
     yield
     L = lib()
     for (prec, m), (v, s) in saved.items():
         L.phase2_tune_set(prec, m, v, s)
+    L.phase2_set_batch_runs(runs)
 
 
 def test_load_matching_gpu(tmp_path):
@@ -48,6 +50,23 @@ def test_load_matching_gpu(tmp_path):
     assert t[(0, 3)] == (1, 8)
     assert t[(1, 5)] == (2, 3)
     assert t[(1, 4)] == (0, 16)
+
+
+def test_batch_runs_line(tmp_path):
+    """`batch_runs n` sets the persistent kernel's run length (1..64);
+    a value out of range rejects the file."""
+    path = tmp_path / "r.tab"
+    path.write_text("gpu TEST GPU\nlaunch 0 3 1 8\nbatch_runs 4\n")
+    assert lib().phase2_load_tuning(str(path).encode(), b"TEST GPU") == 2
+    assert lib().phase2_get_batch_runs() == 4
+    for body in ("gpu TEST GPU\nbatch_runs 0\n",
+                 "gpu TEST GPU\nbatch_runs 65\n",
+                 "gpu TEST GPU\nbatch_runs 2 3\n"):
+        bad = tmp_path / "b.tab"
+        bad.write_text(body)
+        assert lib().phase2_load_tuning(str(bad).encode(), b"TEST GPU") \
+            == -1, body
+        assert lib().phase2_get_batch_runs() == 4, body
 
 
 def test_other_gpu_and_bad_files_change_nothing(tmp_path):
@@ -75,7 +94,9 @@ def test_shipped_table_matches_its_report():
     tab = PKG / "tuning_b200.tab"
     n = lib().phase2_load_tuning(str(tab).encode(), report["gpu"].encode())
     entries = sum(len(v) for v in report["launch"].values())
-    assert n == entries
+    assert n == entries + ("batch_runs" in report)
+    if "batch_runs" in report:
+        assert lib().phase2_get_batch_runs() == report["batch_runs"]["best"]
     t = _table()
     for pname, per_m in report["launch"].items():
         prec = autotune.PRECS[pname]
@@ -87,10 +108,12 @@ def test_write_table_roundtrip(tmp_path):
     report = {"gpu": "TEST GPU", "nqb": 20, "launch": {
         "fp64": {"5": {"variant": 1, "per_sm": 0}},
         "fp32": {"3": {"variant": 2, "per_sm": 3},
-                 "5": {"variant": 0, "per_sm": 32}}}}
+                 "5": {"variant": 0, "per_sm": 32}}},
+        "batch_runs": {"kernel_ms": {"1": 2.0, "8": 1.0}, "best": 8}}
     path = tmp_path / "w.tab"
     autotune.write_table(report, path)
-    assert lib().phase2_load_tuning(str(path).encode(), b"TEST GPU") == 3
+    assert lib().phase2_load_tuning(str(path).encode(), b"TEST GPU") == 4
+    assert lib().phase2_get_batch_runs() == 8
     t = _table()
     assert t[(0, 5)] == (1, 0)
     assert t[(1, 3)] == (2, 3)
