@@ -95,91 +95,6 @@ __device__ __forceinline__ void p2_batch_pass_tile_x(float2 *st,
 	}
 }
 
-/* Bytes of a warp's stage in the FP64-arithmetic instance: the 32 slot
- * blocks of 256 bytes of one span-5 tile. */
-#define P2_BATCH_STAGE 8192u
-
-/* A run of span-5 tiles [first, end) of an FP32 register in the
- * FP64-arithmetic form, each tile's 32 slot blocks staged in the warp's
- * shared memory by cp.async while the warp rotates the tile before it.
- * With every pivot at bit 5 or above, slot u of tile c is one aligned
- * block of 32 amplitudes, (x0 ^ off(u)) & ~31, lane l taking element
- * l ^ (off(u) & 31); lane l copies 16-byte piece l % 16 of slot blocks
- * 2j + l / 16, j < 16.  Same arithmetic, and bits, as p2_batch_pass_tile_x. */
-__device__ __forceinline__ void p2_batch_pass_staged_x(float2 *st,
-	const struct phase2_pass &p, uint32_t first, uint32_t end,
-	const struct p2_lift_rec *srec, uint32_t lane, float2 *stage)
-{
-	constexpr int M = 5, S = 1 << M;
-	uint32_t pb[M], ob[M];
-#pragma unroll
-	for (int k = 0; k < M; ++k) {
-		pb[k] = (uint32_t)p.basis[k];
-		ob[k] = pb[k] & 31u;
-	}
-	/* slot bit 0 of this lane's blocks */
-	const uint32_t hb = (lane >> 4) ? pb[0] : 0u;
-	const char *const src0 = (const char *)st + (lane & 15u) * 16u;
-	const uint32_t sdst =
-		(uint32_t)__cvta_generic_to_shared(stage) + lane * 16u;
-	const bool neg = p.scale < 0;
-	auto issue = [&](uint32_t c) {
-		const uint32_t xb = p2_rep_t<M, uint32_t>(c << 5, p) ^ hb;
-#pragma unroll
-		for (int j = 0; j < S / 2; ++j) {
-			uint32_t o = 0;
-#pragma unroll
-			for (int k = 1; k < M; ++k)
-				if (j >> (k - 1) & 1)
-					o ^= pb[k];
-			p2_cp16(sdst + (uint32_t)j * 512u,
-				src0 + (size_t)((xb ^ o) & ~31u) * 8u);
-		}
-		p2_cp_commit();
-	};
-	issue(first);
-	for (uint32_t c = first; c < end; ++c) {
-		p2_cp_wait<0>();
-		__syncwarp();
-		double re[S], im[S];
-#pragma unroll
-		for (int u = 0; u < S; ++u) {
-			uint32_t ou = 0;
-#pragma unroll
-			for (int b = 0; b < M; ++b)
-				if (u >> b & 1)
-					ou ^= ob[b];
-			const float2 v = stage[u * 32 + (lane ^ ou)];
-			re[u] = (double)v.x;
-			im[u] = (double)v.y;
-		}
-		/* every lane has read the stage before it is refilled */
-		__syncwarp();
-		if (c + 1 < end)
-			issue(c + 1);
-		const uint32_t x = p2_rep_t<M, uint32_t>(c << 5, p) | lane;
-		for (uint32_t r = 0; r < p.nrot; ++r) {
-			const struct p2_lift_rec q = srec[r];
-			const uint32_t sm =
-				q.sm ^ (0u - p2_parity(x & (uint32_t)q.z));
-			p2_apply_lift<M>(q.key, re, im, q.t, q.s, sm);
-		}
-		const uint32_t xs = p2_opaque(x);
-#pragma unroll
-		for (int u = 0; u < S; ++u) {
-			uint32_t off = 0;
-#pragma unroll
-			for (int k = 0; k < M; ++k)
-				if (u >> k & 1)
-					off ^= pb[k];
-			const double a = neg ? -re[u] : re[u];
-			const double b = neg ? -im[u] : im[u];
-			__stcg(st + (xs ^ off), make_float2(__double2float_rn(a),
-							 __double2float_rn(b)));
-		}
-	}
-}
-
 /* The same for an FP64 register: the exact per-coset arithmetic of
  * k_pass (p2_apply_run), loads and stores at L2 only. */
 template <int M>
@@ -358,8 +273,6 @@ __global__ void __launch_bounds__(P2_TPB,
 	typedef typename p2_brec<ST, X>::type RT;
 	/* each warp keeps the records of the pass it last ran */
 	__shared__ RT srec_all[P2_BATCH_WARPS][P2_MAX_ROTS_PER_PASS];
-	/* FP64-arithmetic instance: each warp's stage (dynamic, 16-aligned) */
-	extern __shared__ __align__(16) unsigned char p2_bstage[];
 	const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
 	RT *const srec = srec_all[wid];
 	const uint32_t nwarps = gridDim.x * P2_BATCH_WARPS;
@@ -502,25 +415,9 @@ __global__ void __launch_bounds__(P2_TPB,
 				held = op.a;
 				__syncwarp();
 			}
-			bool staged = false;
-			if constexpr (X) {
-				/* runs of two or more whole span-5 tiles with
-				 * every pivot at bit 5 or above: staged (a
-				 * single tile has nothing to overlap its copy
-				 * with, and loads directly) */
-				staged = p.span == 5 && p.piv[0] >= 5 &&
-					namp >= 1024 && cend - cfirst >= 2;
-				if (staged)
-					p2_batch_pass_staged_x((float2 *)st, p,
-						cfirst, cend, srec, lane,
-						(float2 *)(p2_bstage +
-							wid * P2_BATCH_STAGE));
-			}
-			if (!staged)
-				p2_batch_pass<ST, X, RT>(st, p,
-					(uint64_t)cfirst * op.b * 32,
-					namp >> p.span,
-					(cend - cfirst) * op.b, srec, lane);
+			p2_batch_pass<ST, X, RT>(st, p,
+				(uint64_t)cfirst * op.b * 32, namp >> p.span,
+				(cend - cfirst) * op.b, srec, lane);
 		} else if (op.kind == P2_OP_ZERO) {
 			const uint64_t lo = (uint64_t)cfirst * P2_BATCH_ZERO_TILE;
 			uint64_t hi = (uint64_t)cend * P2_BATCH_ZERO_TILE;
@@ -740,22 +637,6 @@ const void *p2_batch_kernel(int kind)
 				      : (const void *)k_batch<float2, false>;
 }
 
-/* Dynamic shared memory of an instance's launch (the FP64-arithmetic
- * instance's stages), its limit raised on first use. */
-size_t p2_batch_smem(int kind)
-{
-	if (kind != P2_BK_F32X)
-		return 0;
-	static int raised;
-	const size_t bytes = (size_t)P2_BATCH_WARPS * P2_BATCH_STAGE;
-	if (!raised) {
-		cudaFuncSetAttribute(k_batch<float2, true>,
-			cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-		raised = 1;
-	}
-	return bytes;
-}
-
 void p2_batch_launch(int kind, unsigned grid, cudaStream_t stream,
 	const struct p2_binst *inst, uint32_t ninst, const struct p2_op *ops,
 	const struct phase2_pass *passes, const struct phase2_rot_rec *recs,
@@ -768,8 +649,7 @@ void p2_batch_launch(int kind, unsigned grid, cudaStream_t stream,
 			ninst, ops, passes, recs, widx, wval, gidx, gout, ctl,
 			status, cum, g_batch_runs, P2_BATCH_IDLE_LIMIT);
 	else if (kind == P2_BK_F32X)
-		k_batch<float2, true><<<grid, P2_TPB, p2_batch_smem(kind),
-			stream>>>(inst,
+		k_batch<float2, true><<<grid, P2_TPB, 0, stream>>>(inst,
 			ninst, ops, passes, recs, widx, wval, gidx, gout, ctl,
 			status, cum, g_batch_runs, P2_BATCH_IDLE_LIMIT);
 	else
@@ -841,7 +721,7 @@ extern "C" int p2d_batch_run(struct p2_dev *const *devs,
 	const int kind = p2_batch_kind(d0->prec, form);
 	int per_sm = 0;
 	cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm,
-		p2_batch_kernel(kind), P2_TPB, p2_batch_smem(kind));
+		p2_batch_kernel(kind), P2_TPB, 0);
 	if (e != cudaSuccess) {
 		log_error("batch: setup: %s", cudaGetErrorString(e));
 		return -1;

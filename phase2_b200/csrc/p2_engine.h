@@ -134,7 +134,6 @@ struct p2_bctl;
 enum { P2_BK_F32 = 0, P2_BK_F32X = 1, P2_BK_F64 = 2 };
 int p2_batch_kind(int prec, int form);
 const void *p2_batch_kernel(int kind);
-size_t p2_batch_smem(int kind); /* dynamic shared memory of its launch */
 void p2_batch_launch(int kind, unsigned grid, cudaStream_t stream,
 	const struct p2_binst *inst, uint32_t ninst, const struct p2_op *ops,
 	const struct phase2_pass *passes, const struct phase2_rot_rec *recs,

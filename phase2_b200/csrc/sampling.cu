@@ -411,7 +411,7 @@ extern "C" int p2d_sampled_device(struct p2_dev *d,
 	int per_sm = 0;
 	if (e == cudaSuccess)
 		e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm,
-			p2_batch_kernel(kind), P2_TPB, p2_batch_smem(kind));
+			p2_batch_kernel(kind), P2_TPB, 0);
 	if (e == cudaSuccess)
 		e = cudaFuncSetAttribute(k_smp_plan,
 			cudaFuncAttributeMaxDynamicSharedMemorySize,
