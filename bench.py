@@ -563,28 +563,31 @@ def fp32_error_study(nqb: int = 20, nterms: int = 300, steps: int = 1000,
             "seconds": time.perf_counter() - t0}
 
 
-def trott26_study(steps: int = 256) -> dict:
+def trott26_study(steps: int = 256, term_order: int = 2) -> dict:
     """Second-order Trotter at 26 qubits (20,000 JW terms in flip-mask
     order -- phase2_set_term_order(FLIP), not the reference's lexicographic
-    sort -- 16 determinants of weight 13, delta 0.05), FP64 and FP32 states
-    (the process's FP32 form) side by side on the same inputs, `steps` of
-    its 256 steps: device rot.amp/s of each (CUDA events around the pass
-    launches) and the FP32 overlap error against the FP64 run after every
-    step (the FP64 path is bit-identical to the reference)."""
+    sort, unless `term_order` says otherwise -- 16 determinants of weight
+    13, delta 0.05), FP64 and FP32 states (the process's FP32 form) side by
+    side on the same inputs, `steps` of its 256 steps: device rot.amp/s of
+    each (CUDA events around the pass launches) and the FP32 overlap error
+    against the FP64 run after every step (the FP64 path is bit-identical
+    to the reference)."""
     import numpy as np
 
     import phase2_b200 as p2
     from phase2_b200 import workloads
     cfg = workloads.strang26(steps=steps)
     t, d = cfg["terms"], cfg["dets"]
-    out = {"workload": ("trott2 26 qubits, 20000 JW terms in flip-mask "
+    oname = {0: "the reference's lexicographic", 1: "given",
+             2: "flip-mask"}[term_order]
+    out = {"workload": (f"trott2 26 qubits, 20000 JW terms in {oname} "
                         f"order, 16 determinants, delta 0.05, {steps} of "
                         "256 steps"), "unit": UNIT}
     zs = {}
     order = p2.lib().phase2_get_term_order()
     for name, prec in (("fp64", p2.PREC_FP64), ("fp32", p2.PREC_FP32)):
         p2.set_precision(prec)
-        p2.set_term_order(2)  # PHASE2_ORDER_FLIP
+        p2.set_term_order(term_order)
         try:
             z, st = p2.trott2(26, t, d, steps, cfg["delta"], timing=True,
                               with_stats=True)
@@ -606,6 +609,13 @@ def trott26_study(steps: int = 256) -> dict:
     out["final_overlap_fp64"] = [float(zs["fp64"][-1].real),
                                  float(zs["fp64"][-1].imag)]
     return out
+
+
+def trott26lex_study(steps: int = 2) -> dict:
+    """Config 2 in the reference's own term order (lexicographic, the
+    drivers' default), 2 of its 256 steps: fewer rotations per pass than
+    the flip-mask order (the pass kernels' memory-bound end)."""
+    return trott26_study(steps=steps, term_order=0)
 
 
 def sampling_study() -> dict:
@@ -1050,7 +1060,8 @@ def main() -> None:
                          "not fit the remainder is skipped and reported)")
     ap.add_argument("--only-study", default=None,
                     help="run just this study (batched, trott26, cmpsit33, "
-                         "batch8, batch8f32, batch8fp64, sampling, sweeps, "
+                         "batch8, batch8f32, batch8fp64, trott26lex, "
+                         "sampling, sweeps, "
                          "sharded) "
                          "and print its JSON; --nqb, when given, sets the "
                          "sweeps or sharded study's width")
