@@ -1055,7 +1055,7 @@ def main() -> None:
                          "the order batched, cmpsit33, trott26, sharded, "
                          "sampling, sweeps, each only while the study "
                          "budget lasts)")
-    ap.add_argument("--study-budget", type=float, default=1100.0,
+    ap.add_argument("--study-budget", type=float, default=1200.0,
                     help="seconds of studies at most (a study that would "
                          "not fit the remainder is skipped and reported)")
     ap.add_argument("--only-study", default=None,
