@@ -1071,6 +1071,9 @@ def main() -> None:
 
         import phase2_b200 as p2
         p2.world_ensure()
+        if args.fp32_form:
+            p2.set_fp32_form({"f32": p2.FORM_LIFTED_F32,
+                              "f64": p2.FORM_LIFTED}[args.fp32_form])
         fn = globals()[f"{args.only_study}_study"]
         kw = {}
         if "nqb" in inspect.signature(fn).parameters and \
