@@ -931,7 +931,8 @@ def batched_study(ninst: int = 64, work_cap: float = 1.5e14,
                         f"{scale:.3f} (at least 16) to cap the batch at "
                         f"{work_cap:.1e} rot.amp, FP32 state"),
            "rot_amp": work, "rot_amp_drawn": drawn, "step_scale": scale,
-           "steps_run": [p["steps"] for p in probs], "unit": UNIT}
+           "steps_run": [p["steps"] for p in probs], "unit": UNIT,
+           "fp32_form": FORM_NAME.get(p2.get_fp32_form())}
     p2.set_precision(p2.PREC_FP32)
     order = p2.lib().phase2_get_term_order()
     try:
