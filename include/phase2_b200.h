@@ -182,7 +182,7 @@ enum phase2_device_sampling {
 	PHASE2_DEVICE_SAMPLING_ON = 1,
 	PHASE2_DEVICE_SAMPLING_AUTO = 2,
 };
-#define PHASE2_DEVICE_SAMPLING_AUTO_QB 25
+#define PHASE2_DEVICE_SAMPLING_AUTO_QB 21
 int phase2_set_device_sampling(int mode);
 
 /* Check of the persistent kernel's bounded wait: runs it on a program

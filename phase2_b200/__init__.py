@@ -116,10 +116,10 @@ DEVICE_SAMPLING_OFF, DEVICE_SAMPLING_ON, DEVICE_SAMPLING_AUTO = 0, 1, 2
 
 
 def set_device_sampling(mode) -> None:
-    """qdrift on FP32 registers: draw, plan and run the samples on the GPU
-    (same results as the host loop, bit for bit).  True/False force it on
-    or off; DEVICE_SAMPLING_AUTO (default) uses it for registers of at most
-    25 qubits."""
+    """qdrift and cmpsit: draw, plan and run the samples on the GPU (same
+    results as the host loop, bit for bit).  True/False force it on or
+    off; DEVICE_SAMPLING_AUTO (default) uses it for registers of at most
+    21 qubits."""
     mode = {True: 1, False: 0}.get(mode, mode)
     if lib().phase2_set_device_sampling(int(mode)) != 0:
         raise ValueError(f"bad device sampling mode {mode}")
