@@ -241,6 +241,24 @@ _SIGS = {
                                 C.c_uint64, C.c_uint64, C.c_void_p]),
     "qreg_slab_swap": (C.c_int, [_P(Qreg), _P(Qreg), C.c_uint32,
                                  C.c_uint32, C.c_uint32]),
+    "phase2_sharded_new": (C.c_void_p, [C.c_uint32, C.c_uint32,
+                                        _P(C.c_uint32), C.c_uint32, C.c_int,
+                                        C.c_void_p, C.c_uint64]),
+    "phase2_sharded_free": (None, [C.c_void_p]),
+    "phase2_sharded_paulirot": (C.c_int, [C.c_void_p, _P(C.c_uint64),
+                                          _P(C.c_uint64), _P(C.c_double),
+                                          C.c_size_t]),
+    "phase2_sharded_prepst": (C.c_int, [C.c_void_p, _P(C.c_uint64),
+                                        _P(C.c_double), C.c_size_t]),
+    "phase2_sharded_getamps": (C.c_int, [C.c_void_p, _P(C.c_uint64),
+                                         _P(C.c_double), C.c_size_t]),
+    "phase2_sharded_measure": (C.c_int, [C.c_void_p, _P(C.c_uint64),
+                                         _P(C.c_double), C.c_size_t,
+                                         _P(C.c_double)]),
+    "phase2_sharded_norm2": (C.c_int, [C.c_void_p, _P(C.c_double)]),
+    "phase2_sharded_layout": (C.c_int, [C.c_void_p, _P(C.c_uint32)]),
+    "phase2_sharded_counters": (None, [C.c_void_p, _P(C.c_uint64),
+                                       _P(C.c_uint64)]),
     "qreg_inner_dense": (C.c_int, [_P(Qreg), _P(C.c_double),
                                    _P(C.c_double)]),
     "qreg_get_stats": (C.c_int, [_P(Qreg), _P(Stats)]),
@@ -281,6 +299,16 @@ _SIGS = {
     "cmpsit_ranct_init": (C.c_int, [_P(CmpsitRanct), _P(CircHamil),
                                     _P(CmpsitData)]),
     "cmpsit_ranct_free": (None, [_P(CmpsitRanct)]),
+    "phase2_sharded_trott": (C.c_int, [C.c_void_p, _P(CircHamil),
+                                       _P(CircMuldet), C.c_size_t,
+                                       C.c_double, C.c_int, _P(C.c_double)]),
+    "phase2_sharded_qdrift": (C.c_int, [C.c_void_p, _P(CircHamil),
+                                        _P(CircMuldet), C.c_size_t,
+                                        C.c_size_t, C.c_double, C.c_uint64,
+                                        _P(C.c_double)]),
+    "phase2_sharded_cmpsit": (C.c_int, [C.c_void_p, _P(CircHamil),
+                                        _P(CircMuldet), _P(CmpsitData),
+                                        _P(C.c_double)]),
     "prob_cdf_init": (C.c_int, [_P(ProbCdf), C.c_size_t]),
     "prob_cdf_free": (None, [_P(ProbCdf)]),
     "prob_cdf_from_array_strided": (C.c_int, [_P(ProbCdf), _P(C.c_double),

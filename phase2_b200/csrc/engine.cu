@@ -1360,6 +1360,25 @@ extern "C" int p2d_inner_dense(struct p2_dev *d, const double *trial,
 	return rc;
 }
 
+/* Device memory for a caller of the host layer (exchange buffers of
+ * sharded registers), on the current device; NULL on failure. */
+extern "C" void *p2d_buffer_alloc(size_t bytes)
+{
+	void *p = NULL;
+	if (cudaMalloc(&p, bytes) != cudaSuccess) {
+		cudaGetLastError();
+		log_error("device buffer of %zu bytes: allocation failed", bytes);
+		return NULL;
+	}
+	return p;
+}
+
+extern "C" void p2d_buffer_free(void *p)
+{
+	if (p)
+		cudaFree(p);
+}
+
 extern "C" int p2d_sync(struct p2_dev *d)
 {
 	CUDA_OK(cudaStreamSynchronize(d->stream), "stream sync");

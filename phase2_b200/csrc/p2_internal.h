@@ -88,6 +88,10 @@ int p2d_slab_swap(struct p2_dev *a, struct p2_dev *b, uint32_t bit,
 /* Wait for the stream; -1 if any CUDA error is pending. */
 int p2d_sync(struct p2_dev *d);
 
+/* Device memory on the current device (cudaMalloc / cudaFree). */
+void *p2d_buffer_alloc(size_t bytes);
+void p2d_buffer_free(void *p);
+
 void p2d_stats(const struct p2_dev *d, struct phase2_stats *st);
 void p2d_stats_reset(struct p2_dev *d);
 void p2d_set_timing(struct p2_dev *d, int on);
