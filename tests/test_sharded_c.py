@@ -47,3 +47,25 @@ def test_runs(tmp_path):
                        timeout=600)
     assert r.returncode == 0 and r.stdout.strip().endswith("ok"), \
         r.stdout + r.stderr
+
+
+NCCL_SRC = ROOT / "tests" / "c" / "sharded_nccl.c"
+
+
+def test_nccl_program_builds(tmp_path):
+    """The NCCL-transport program (tests/c/sharded_nccl.c) compiles and
+    links against include/, the library and NCCL.  It runs one process per
+    GPU and needs two or more GPUs (NCCL ranks must not share one), so
+    only its build is checked here."""
+    if not Path("/usr/include/nccl.h").is_file():
+        pytest.skip("NCCL headers are not available")
+    if shutil.which("gcc") is None or not (CUDA / "include").is_dir():
+        pytest.skip("gcc or the CUDA headers are not available")
+    exe = tmp_path / "sharded_nccl"
+    cmd = ["gcc", "-std=gnu11", "-O2", "-Wall", "-Wextra", "-Werror",
+           f"-I{ROOT / 'include'}", f"-I{CUDA / 'include'}", str(NCCL_SRC),
+           f"-L{LIB}", "-lphase2", f"-L{CUDA / 'lib64'}", "-lcudart",
+           "-lnccl", f"-Wl,-rpath,{LIB}", f"-Wl,-rpath,{CUDA / 'lib64'}",
+           "-o", str(exe)]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
