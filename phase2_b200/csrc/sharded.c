@@ -350,16 +350,32 @@ int phase2_sharded_getamps(struct phase2_sharded *s, const uint64_t *idx,
 	if (!s || (n && (!idx || !out)))
 		return -1;
 	const uint64_t lomask = (UINT64_C(1) << s->nloc) - 1;
-	for (size_t i = 0; i < n; i++) {
+	/* one read per rank held: its indices gathered, then scattered back */
+	uint64_t *loc = malloc((n ? n : 1) * sizeof *loc);
+	size_t *at = malloc((n ? n : 1) * sizeof *at);
+	_Complex double *val = malloc((n ? n : 1) * sizeof *val);
+	int rc = loc && at && val ? 0 : -1;
+	for (size_t i = 0; i < n; i++)
 		out[i] = 0;
-		const uint64_t p = phys_mask(s, idx[i]);
-		const int j = s->held[p >> s->nloc];
-		if (j < 0)
-			continue;
-		const uint64_t loc = p & lomask;
-		if (qreg_getamps(&s->slab[j], &loc, &out[i], 1) != 0)
-			return -1;
+	for (uint32_t j = 0; j < s->nranks && rc == 0; j++) {
+		size_t m = 0;
+		for (size_t i = 0; i < n; i++) {
+			const uint64_t p = phys_mask(s, idx[i]);
+			if ((p >> s->nloc) != s->ranks[j])
+				continue;
+			loc[m] = p & lomask;
+			at[m++] = i;
+		}
+		if (m && qreg_getamps(&s->slab[j], loc, val, m) != 0)
+			rc = -1;
+		for (size_t k = 0; k < m && rc == 0; k++)
+			out[at[k]] = val[k];
 	}
+	free(loc);
+	free(at);
+	free(val);
+	if (rc != 0)
+		return -1;
 	if (s->nranks < s->world &&
 		s->io.sum(s->io.ctx, (double *)out, 2 * n) != 0) {
 		log_error("sharded register: sum over ranks failed");
