@@ -711,6 +711,50 @@ def sweeps_study(nqb: int = 26) -> dict:
             "rows": rows}
 
 
+def _sharded_c_timing(nqb, world, dets, samples):
+    """The same samples on the C sharded layer (include/phase2_sharded.h,
+    every rank held, in-place swaps): mean wall seconds per sample after
+    the first, and swaps per sample."""
+    import numpy as np
+    import torch
+
+    import phase2_b200 as p2
+    torch.cuda.empty_cache()
+    L = p2.lib()
+    ranks = (C.c_uint32 * world)(*range(world))
+    h = L.phase2_sharded_new(nqb, world, ranks, world, p2.PREC_FP32, None, 0)
+    if not h:
+        raise RuntimeError("phase2_sharded_new failed")
+    u64 = C.POINTER(C.c_uint64)
+    f64 = C.POINTER(C.c_double)
+    idx = np.ascontiguousarray(dets.idx, dtype=np.uint64)
+    cf = np.ascontiguousarray(dets.cf, dtype=np.complex128)
+    sec = []
+    sw0 = C.c_uint64()
+    sw1 = C.c_uint64()
+    try:
+        L.phase2_sharded_counters(h, C.byref(sw0), None)
+        for f, ph, phi in samples:
+            f = np.ascontiguousarray(f, dtype=np.uint64)
+            ph = np.ascontiguousarray(ph, dtype=np.uint64)
+            phi = np.ascontiguousarray(phi, dtype=np.float64)
+            L.phase2_sharded_prepst(h, idx.ctypes.data_as(u64),
+                                    cf.ctypes.data_as(f64), len(idx))
+            L.phase2_sharded_synchronize(h)
+            t0 = time.perf_counter()
+            if L.phase2_sharded_paulirot(h, f.ctypes.data_as(u64),
+                                         ph.ctypes.data_as(u64),
+                                         phi.ctypes.data_as(f64), len(phi)):
+                raise RuntimeError("phase2_sharded_paulirot failed")
+            L.phase2_sharded_synchronize(h)
+            sec.append(time.perf_counter() - t0)
+        L.phase2_sharded_counters(h, C.byref(sw1), None)
+    finally:
+        L.phase2_sharded_free(h)
+    return (float(np.mean(sec[1:])),
+            (sw1.value - sw0.value) / len(samples))
+
+
 def sharded_study(nqb: int = 30, worlds=(2, 4, 8)) -> dict:
     """A register split by its high qubits over 2, 4, 8 ranks held by this
     process on one GPU (phase2_b200.sharded: qubit swaps through
@@ -722,7 +766,8 @@ def sharded_study(nqb: int = 30, worlds=(2, 4, 8)) -> dict:
     place, qreg_slab_swap), the bandwidth of one in-place swap (4 x 8 B
     per half amplitude) and of the half-slab gather that exchanges between
     processes use (2 x 8 B per amplitude), from CUDA events on the
-    register's stream."""
+    register's stream; and the same samples on the C layer
+    (include/phase2_sharded.h, `c_layer`)."""
     import numpy as np
     import torch
 
@@ -796,13 +841,17 @@ def sharded_study(nqb: int = 30, worlds=(2, 4, 8)) -> dict:
                 ev[1].synchronize()
                 swap_gbs = (4 * 8 * nhalf /
                             (ev[0].elapsed_time(ev[1]) * 1e-3) / 1e9)
+            csec, cswaps = _sharded_c_timing(nqb, world, d, samples)
             rows.append({
                 "world": world, "local_qubits": reg.nlocal,
                 "sec_per_sample": float(np.mean(sec)),
                 "value": cfg["depth"] * (1 << nqb) / float(np.mean(sec)),
                 "swaps_per_sample": swaps, "in_place": reg.in_place,
                 "swap_gbs": swap_gbs,
-                "gather_gbs": gbs, "gather_amplitudes": cnt})
+                "gather_gbs": gbs, "gather_amplitudes": cnt,
+                "c_layer": {"sec_per_sample": csec,
+                            "value": cfg["depth"] * (1 << nqb) / csec,
+                            "swaps_per_sample": cswaps}})
         res["sharded"] = rows
     finally:
         p2.set_device_sampling(p2.DEVICE_SAMPLING_AUTO)

@@ -96,6 +96,10 @@ int phase2_sharded_measure(struct phase2_sharded *s, const uint64_t *idx,
 /* sum |a_i|^2: each rank's device reduction, added in rank order. */
 int phase2_sharded_norm2(struct phase2_sharded *s, double *out);
 
+/* Run every queued rotation of the ranks held and wait for the device;
+ * -1 if a CUDA error is pending. */
+int phase2_sharded_synchronize(struct phase2_sharded *s);
+
 /* pos[q]: the physical position of global qubit q (nqb entries). */
 int phase2_sharded_layout(const struct phase2_sharded *s, uint32_t *pos);
 

@@ -256,6 +256,7 @@ _SIGS = {
                                          _P(C.c_double), C.c_size_t,
                                          _P(C.c_double)]),
     "phase2_sharded_norm2": (C.c_int, [C.c_void_p, _P(C.c_double)]),
+    "phase2_sharded_synchronize": (C.c_int, [C.c_void_p]),
     "phase2_sharded_layout": (C.c_int, [C.c_void_p, _P(C.c_uint32)]),
     "phase2_sharded_counters": (None, [C.c_void_p, _P(C.c_uint64),
                                        _P(C.c_uint64)]),

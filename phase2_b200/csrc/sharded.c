@@ -141,6 +141,17 @@ struct phase2_sharded *phase2_sharded_new(uint32_t nqb, uint32_t world,
 	return s;
 }
 
+int phase2_sharded_synchronize(struct phase2_sharded *s)
+{
+	if (!s)
+		return -1;
+	int rc = 0;
+	for (uint32_t k = 0; k < s->nranks; k++)
+		if (qreg_synchronize(&s->slab[k]) != 0)
+			rc = -1;
+	return rc;
+}
+
 int phase2_sharded_layout(const struct phase2_sharded *s, uint32_t *pos)
 {
 	if (!s || !pos)
