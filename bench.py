@@ -938,6 +938,38 @@ def batch8fp64_study() -> dict:
     return batch8_study(prec=0)
 
 
+def batch4big_study() -> dict:
+    """A small persistent batch of HBM-sized registers: 4 trott instances
+    of 23-24 qubits (512 MiB of FP32 states in all, above L2), 2,000 JW
+    terms, 1 step, FP32 in the process's form, run twice: the case the
+    persistent kernel's profile summary for config-4-sized registers
+    captures (its second launch).  Algorithmic bytes: 2 * 2^n * 8 per
+    pass, summed."""
+    import numpy as np
+
+    import phase2_b200 as p2
+    from phase2_b200 import workloads
+    probs = []
+    for k, n in enumerate((24, 23, 24, 23)):
+        probs.append(dict(nqb=n, terms=workloads.jw_terms(n, 2000,
+                                                          seed=500 + k),
+                          dets=workloads.hamming_dets(n, 1, n // 2,
+                                                      seed=600 + k),
+                          steps=1, delta=0.05))
+    p2.set_precision(p2.PREC_FP32)
+    try:
+        for _ in range(2):
+            _, st = p2.batch("trott", probs, with_stats=True)
+    finally:
+        p2.set_precision(p2.PREC_FP64)
+    ms = float(sum(s["pass_ms"] for s in st))
+    nbytes = int(sum(s["bytes"] for s in st))
+    return {"passes": int(sum(s["passes"] for s in st)), "kernel_ms": ms,
+            "algorithmic_bytes": nbytes,
+            "hbm_gbs_kernel": nbytes / (ms * 1e-3) / 1e9,
+            "fp32_form": FORM_NAME.get(p2.get_fp32_form())}
+
+
 def batched_study(ninst: int = 64, work_cap: float = 1.5e14,
                   seed: int = 0xBA7C4):
     """Independent trott problems of uneven size run together: qubits
@@ -1110,7 +1142,8 @@ def main() -> None:
                          "not fit the remainder is skipped and reported)")
     ap.add_argument("--only-study", default=None,
                     help="run just this study (batched, trott26, cmpsit33, "
-                         "batch8, batch8f32, batch8fp64, trott26lex, "
+                         "batch8, batch8f32, batch8fp64, batch4big, "
+                         "trott26lex, "
                          "sampling, sweeps, "
                          "sharded) "
                          "and print its JSON; --nqb, when given, sets the "
