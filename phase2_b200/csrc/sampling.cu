@@ -337,7 +337,7 @@ extern "C" int p2d_sampled_device(struct p2_dev *d,
 		sz[PASS] = GT * sizeof(struct phase2_pass);
 		sz[REC] = GT * sizeof(struct phase2_rot_rec);
 		sz[PROG] = (G * T + 3 * G) * sizeof(struct p2_op);
-		sz[NPC] = sz[POFF] = (G * C ? G * C : 1) * sizeof(uint32_t);
+		sz[NPC] = sz[POFF] = (G * C != 0 ? G * C : 1) * sizeof(uint32_t);
 		sz[SOFF] = G * sizeof(uint32_t);
 		sz[REGS] = R * (sizeof(struct p2_binst) +
 				       sizeof(struct p2_bctl)) +
