@@ -466,7 +466,7 @@ def gpu_arm(args) -> None:
         "data": "synthetic (seeded JW-like Hamiltonian, no dataset)",
         "config": _config(cfg),
         "fp32_form": FORM_NAME[head_form],
-        "l2": f"inputs larger than L2 ({namp * 8 / 2**30:.0f} GiB state)",
+        "l2": f"inputs larger than L2 ({namp * 8 / 2**30:.1f} GiB state)",
         "parallelism": f"replicas x{ws} (independent samples)",
         "hbm_gbs": hbm_gbs_step,
         "passes_per_step": passes_per_step,
