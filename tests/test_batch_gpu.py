@@ -101,3 +101,26 @@ def test_many_programs(oracle_lib):
         want = oracle_lib.trott(p["nqb"], t.flip, t.phase, t.cf, d.idx, d.cf,
                                 p["steps"], 0.11, order2=True)
         assert np.array_equal(z, want)
+
+
+def test_hundreds_of_tiny_programs(oracle_lib):
+    """Hundreds of programs of 4-9 qubits (registers smaller than one
+    1024-amplitude tile; the look over tickets spans ten rounds of 32):
+    every result is the oracle's (FP64), and every program has a finish
+    time."""
+    probs = []
+    for k in range(300):
+        n = 4 + k % 6
+        t = workloads.jw_terms(n, 6 + k % 9, seed=0xC00 + k)
+        d = workloads.hamming_dets(n, 1, max(1, n // 2), seed=0xE00 + k)
+        probs.append(dict(nqb=n, terms=t, dets=d, steps=1 + k % 3,
+                          delta=0.13))
+    zs, stats = p2.batch("trott", probs, with_stats=True)
+    assert sum(s["launches"] for s in stats) == 1
+    assert all(s["finish_ms"] is not None and s["finish_ms"] >= 0
+               for s in stats)
+    for p, z in zip(probs, zs):
+        t, d = p["terms"], p["dets"]
+        want = oracle_lib.trott(p["nqb"], t.flip, t.phase, t.cf, d.idx, d.cf,
+                                p["steps"], 0.13)
+        assert np.array_equal(z, want)
