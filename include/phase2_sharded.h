@@ -48,7 +48,11 @@ extern "C" {
  *   receive `bytes` from it into device memory `recv` (both buffers the
  *   library's, on this process's GPU); `rank` is the sending rank of this
  *   process.  Both ranks of the pair make the matching call.  Finished when
- *   it returns; 0 or -1.
+ *   it returns; 0 or -1.  A process makes a swap's exchanges in increasing
+ *   order of its ranks (whatever order `ranks` listed them in), which is
+ *   increasing order of the pairs on every process: a blocking pairwise
+ *   transport cannot deadlock.  After a failed exchange the register's
+ *   state is undefined until the next prepst.
  * sum: element-wise sum of n doubles (host memory) over the processes, in
  *   place, the same result on every process (each process passes the sum
  *   over the ranks it holds).  0 or -1.

@@ -117,9 +117,18 @@ struct phase2_sharded *phase2_sharded_new(uint32_t nqb, uint32_t world,
 			phase2_sharded_free(s);
 			return NULL;
 		}
-		s->held[ranks[k]] = (int)k;
-		s->ranks[k] = ranks[k];
+		s->held[ranks[k]] = 0;
 	}
+	/* Ranks held in increasing order, whatever the caller's order: a swap
+	 * of rank bit b then runs its exchanges in increasing order of the
+	 * pair (r with bit b cleared) on every process, one total order, so a
+	 * blocking pairwise transport cannot deadlock. */
+	uint32_t nh = 0;
+	for (uint32_t r = 0; r < world; r++)
+		if (s->held[r] >= 0) {
+			s->held[r] = (int)nh;
+			s->ranks[nh++] = r;
+		}
 	for (uint32_t k = 0; k < nranks; k++) {
 		if (qreg_init_prec(&s->slab[k], s->nloc, prec) != 0) {
 			s->nranks = k;
@@ -176,7 +185,8 @@ void phase2_sharded_counters(const struct phase2_sharded *s,
  * Trade the qubits at high position h and local position l: rank r swaps
  * the half of its slab whose bit l differs from its rank bit b = h - L
  * (val = 1 - bit b of r) with the partner r ^ 2^b.  Held pairs trade in
- * place; others through the transport, chunk by chunk.
+ * place; others through the transport, chunk by chunk, in increasing rank
+ * order (s->ranks is sorted).
  */
 static int swap_positions(struct phase2_sharded *s, uint32_t h, uint32_t l)
 {
@@ -398,7 +408,7 @@ int phase2_sharded_getamps(struct phase2_sharded *s, const uint64_t *idx,
 int phase2_sharded_measure(struct phase2_sharded *s, const uint64_t *idx,
 	const _Complex double *cf, size_t ndet, _Complex double *z)
 {
-	if (!z)
+	if (!z || (ndet && !cf))
 		return -1;
 	_Complex double *a = malloc((ndet ? ndet : 1) * sizeof *a);
 	if (!a || phase2_sharded_getamps(s, idx, a, ndet) != 0) {

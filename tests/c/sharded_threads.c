@@ -11,9 +11,11 @@
  * GPUs would call ncclSend/ncclRecv); sum adds the holders' partial
  * vectors.  Both holders must report the overlaps of the single holder
  * bit for bit (FP64): Trotter (first and second order) and qDRIFT, for
- * world 2 (one rank each) and world 4 (ranks {0,1} and {2,3}: swaps of
- * rank bit 0 stay inside a holder, swaps of bit 1 go through the
- * transport), with small exchange chunks.  Exit 0 and "ok" on success.
+ * world 2 (one rank each), world 4 (ranks {1,0} and {2,3}: swaps of rank
+ * bit 0 stay inside a holder, swaps of bit 1 go through the transport)
+ * and world 8 (ranks {6,4,2,0} and {1,3,5,7}: swaps of bit 0 make four
+ * exchanges per holder, which must pair up in the same order), with small
+ * exchange chunks.  Exit 0 and "ok" on success.
  */
 #include <complex.h>
 #include <pthread.h>
@@ -112,7 +114,7 @@ static int make_problem(void)
 }
 
 struct job {
-	uint32_t world, ranks[4], nranks;
+	uint32_t world, ranks[8], nranks;
 	int use_io;
 	_Complex double out[3][STEPS > SAMPLES ? STEPS : SAMPLES];
 	int rc;
@@ -142,7 +144,10 @@ static int same(const _Complex double *a, const _Complex double *b, size_t n)
 	return memcmp(a, b, n * sizeof *a) == 0;
 }
 
-static int check_world(uint32_t world)
+/* Holder t holds the upper or lower half of the ranks (interleave 0) or
+ * the odd or even ranks (interleave 1); holder 0 lists its ranks in
+ * decreasing order, holder 1 in increasing order. */
+static int check_world(uint32_t world, int interleave)
 {
 	struct job all = { .world = world, .nranks = world };
 	for (uint32_t r = 0; r < world; r++)
@@ -158,8 +163,11 @@ static int check_world(uint32_t world)
 		part[t].world = world;
 		part[t].nranks = world / 2;
 		part[t].use_io = 1;
-		for (uint32_t r = 0; r < world / 2; r++)
-			part[t].ranks[r] = (uint32_t)t * (world / 2) + r;
+		for (uint32_t r = 0; r < world / 2; r++) {
+			const uint32_t i = t == 0 ? world / 2 - 1 - r : r;
+			part[t].ranks[r] = interleave ? 2 * i + (uint32_t)t
+						      : (uint32_t)t * (world / 2) + i;
+		}
 	}
 	pthread_t th[2];
 	for (int t = 0; t < 2; t++)
@@ -168,15 +176,16 @@ static int check_world(uint32_t world)
 		pthread_join(th[t], NULL);
 	for (int t = 0; t < 2; t++) {
 		if (part[t].rc != 0) {
-			fprintf(stderr, "world %u: holder %d failed\n", world, t);
+			fprintf(stderr, "world %u/%d: holder %d failed\n", world,
+				interleave, t);
 			return -1;
 		}
 		if (!same(part[t].out[0], all.out[0], STEPS) ||
 			!same(part[t].out[1], all.out[1], STEPS) ||
 			!same(part[t].out[2], all.out[2], SAMPLES)) {
-			fprintf(stderr, "world %u: holder %d differs: %.17g%+.17gi"
-					" vs %.17g%+.17gi\n",
-				world, t, creal(part[t].out[0][0]),
+			fprintf(stderr, "world %u/%d: holder %d differs: "
+					"%.17g%+.17gi vs %.17g%+.17gi\n",
+				world, interleave, t, creal(part[t].out[0][0]),
 				cimag(part[t].out[0][0]), creal(all.out[0][0]),
 				cimag(all.out[0][0]));
 			return -1;
@@ -194,7 +203,8 @@ int main(void)
 	pthread_barrier_init(&M.bar, NULL, 2);
 	pthread_mutex_init(&M.mu, NULL);
 	int rc = 1;
-	if (make_problem() == 0 && check_world(2) == 0 && check_world(4) == 0) {
+	if (make_problem() == 0 && check_world(2, 0) == 0 &&
+		check_world(4, 0) == 0 && check_world(8, 1) == 0) {
 		printf("ok\n");
 		rc = 0;
 	}
