@@ -7,13 +7,14 @@ synthetic, phase2_b200.workloads), 4096 draws per sample, step_size 1e-3.
 The headline runs the library's FP32 form (--fp32-form; the line's
 ``fp32_form`` and ``storage`` say what it computes).  The line also
 carries comparison arms on the same draws -- FP64 one rotation per pass
-("plain"), FP64 fused, FP32 one rotation per pass, and both FP32 forms
-fused (FP32 arithmetic with FP32 coefficients; FP64 arithmetic with FP64
-coefficients and one rounding per pass) -- with each FP32 form's ratio
-to the fused FP64 path (like for like) and the headline's ratio to the
-plain FP64 path, the reference's own CUDA kernel built from its sources,
-the FP32 error of both forms on the headline samples and on a 1000-step
-Trotter run, and, at N=1, studies within a time budget (--studies,
+("plain"), FP64 fused, FP32 one rotation per pass, and the three FP32
+forms fused (FP32 arithmetic with FP32 coefficients; FP64 arithmetic with
+FP64 coefficients and one rounding per pass; FP32 arithmetic with FP64 on
+the cosets that hold an amplitude >= 2^-10) -- with each FP32 form's
+ratio to the fused FP64 path (like for like) and the headline's ratio to
+the plain FP64 path, the reference's own CUDA kernel built from its
+sources, the FP32 error of every form on the headline samples and on a
+1000-step Trotter run, and, at N=1, studies within a time budget (--studies,
 --study-budget): the 26-qubit second-order Trotter configuration over
 all 256 steps with the FP32 error after every step, the batched
 configuration (64 uneven instances in one persistent launch, with finish
@@ -207,15 +208,23 @@ STORAGE = {
         "all its rotations in FP64 arithmetic with the FP64 coefficients "
         "(s and t = tan(phi/2) from FP64 cos/sin), and rounds to FP32 once "
         "at the store; norms and overlaps in FP64"),
+    3: ("complex64 state; cosets whose amplitudes are all below 2^-10 in "
+        "magnitude rotated as form 2 (FP32 FMAs, coefficients rounded to "
+        "FP32), cosets holding a larger amplitude rotated in FP64 "
+        "arithmetic by their warp and rounded to FP32 once per pass; norms "
+        "and overlaps in FP64"),
 }
 FORM_NAME = {1: "f64 arithmetic (PHASE2_FORM_LIFTED)",
-             2: "f32 arithmetic (PHASE2_FORM_LIFTED_F32)"}
+             2: "f32 arithmetic (PHASE2_FORM_LIFTED_F32)",
+             3: "f32 arithmetic, f64 on heavy cosets (PHASE2_FORM_LIFTED_MIXED)"}
 
 
 def _headline_kernel(p2, form: int) -> str:
     """The pass kernel that carries the headline's span-5 passes."""
     if form == p2.FORM_LIFTED_F32:
         return "k_pass_lift32<M,uint32_t>"
+    if form == p2.FORM_LIFTED_MIXED:
+        return "k_pass_lift32h<M,uint32_t>"
     v, per = C.c_int(), C.c_int()
     p2.lib().phase2_tune_get(p2.PREC_FP32, 5, C.byref(v), C.byref(per))
     return {0: "k_pass_lift<M,uint32_t>", 1: "k_pass_lift_bulk<M>",
@@ -332,7 +341,8 @@ def gpu_arm(args) -> None:
     p2.world_ensure()
     if args.fp32_form:
         p2.set_fp32_form({"f32": p2.FORM_LIFTED_F32,
-                          "f64": p2.FORM_LIFTED}[args.fp32_form])
+                          "f64": p2.FORM_LIFTED,
+                          "mixed": p2.FORM_LIFTED_MIXED}[args.fp32_form])
     if args.lift_kernel:
         # FP64-arithmetic passes of span 3-5: direct loads, or the next
         # cosets staged by bulk copies or by cp.async
@@ -377,7 +387,9 @@ def gpu_arm(args) -> None:
             ("fp32_plain", p2.PREC_FP32, (1, 1), form0),
             ("fp32_fused_f32arith", p2.PREC_FP32, (5, 0),
              p2.FORM_LIFTED_F32),
-            ("fp32_fused_f64arith", p2.PREC_FP32, (5, 0), p2.FORM_LIFTED)):
+            ("fp32_fused_f64arith", p2.PREC_FP32, (5, 0), p2.FORM_LIFTED),
+            ("fp32_fused_mixed", p2.PREC_FP32, (5, 0),
+             p2.FORM_LIFTED_MIXED)):
         if args.quick and name != "fp64_plain":
             continue
         p2.set_fp32_form(form)
@@ -403,7 +415,8 @@ def gpu_arm(args) -> None:
             arms["reference_gpu_fp64"] = ref_gpu
     ratios = {}
     if arms.get("fp64_fused"):
-        for name in ("fp32_fused_f32arith", "fp32_fused_f64arith"):
+        for name in ("fp32_fused_f32arith", "fp32_fused_f64arith",
+                     "fp32_fused_mixed"):
             if arms.get(name):
                 ratios[f"{name}_vs_fp64_fused"] = (
                     arms[name]["value"] / arms["fp64_fused"]["value"])
@@ -429,7 +442,8 @@ def gpu_arm(args) -> None:
         extra["fp32_error"] = {"headline_samples": qdrift_error_study(
             cfg, seed + 11, samples=4)}
         for fname, form in (("f32_arith", p2.FORM_LIFTED_F32),
-                            ("f64_arith", p2.FORM_LIFTED)):
+                            ("f64_arith", p2.FORM_LIFTED),
+                            ("mixed", p2.FORM_LIFTED_MIXED)):
             p2.set_fp32_form(form)
             try:
                 extra["fp32_error"][fname] = fp32_error_study()
@@ -510,7 +524,9 @@ def qdrift_error_study(cfg: dict, seed: int, samples: int = 4) -> dict:
                                  ("f32_arith", p2.PREC_FP32,
                                   p2.FORM_LIFTED_F32),
                                  ("f64_arith", p2.PREC_FP32,
-                                  p2.FORM_LIFTED)):
+                                  p2.FORM_LIFTED),
+                                 ("mixed", p2.PREC_FP32,
+                                  p2.FORM_LIFTED_MIXED)):
             p2.set_precision(prec)
             p2.set_fp32_form(form)
             t0 = time.perf_counter()
@@ -525,7 +541,7 @@ def qdrift_error_study(cfg: dict, seed: int, samples: int = 4) -> dict:
                         "FP64 on the same draws"),
            "overlaps_fp64": [[z.real, z.imag] for z in zs["fp64"]],
            "seconds": secs}
-    for name in ("f32_arith", "f64_arith"):
+    for name in ("f32_arith", "f64_arith", "mixed"):
         err = np.abs(zs[name] - zs["fp64"])
         out[name] = {"abs_err_per_sample": [float(e) for e in err],
                      "max_abs_err": float(err.max())}
@@ -1120,10 +1136,13 @@ def main() -> None:
     ap.add_argument("--nqb", type=int, default=30)
     ap.add_argument("--depth", type=int, default=4096)
     ap.add_argument("--cmp-depth", type=int, default=512)
-    ap.add_argument("--fp32-form", default=None, choices=["f32", "f64"],
+    ap.add_argument("--fp32-form", default=None,
+                    choices=["f32", "f64", "mixed"],
                     help="arithmetic of FP32 passes for the run: f32 (FP32 "
-                         "FMAs) or f64 (FP64 arithmetic, one rounding to "
-                         "FP32 per pass); default: the library's")
+                         "FMAs), f64 (FP64 arithmetic, one rounding to "
+                         "FP32 per pass) or mixed (FP32 FMAs, FP64 on "
+                         "cosets holding an amplitude >= 2^-10); default: "
+                         "the library's")
     ap.add_argument("--lift-kernel", default=None,
                     choices=["direct", "bulk", "staged", "staged2"],
                     help="kernel of FP64-arithmetic FP32 passes: direct "
@@ -1156,7 +1175,8 @@ def main() -> None:
         p2.world_ensure()
         if args.fp32_form:
             p2.set_fp32_form({"f32": p2.FORM_LIFTED_F32,
-                              "f64": p2.FORM_LIFTED}[args.fp32_form])
+                              "f64": p2.FORM_LIFTED,
+                              "mixed": p2.FORM_LIFTED_MIXED}[args.fp32_form])
         fn = globals()[f"{args.only_study}_study"]
         kw = {}
         if "nqb" in inspect.signature(fn).parameters and \

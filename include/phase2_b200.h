@@ -36,13 +36,25 @@ enum phase2_prec {
 int phase2_set_precision(int prec);
 int phase2_get_precision(void);
 
-/* Arithmetic of FP32 passes (enum phase2_form below), both rotating each
+/* Arithmetic of FP32 passes (enum phase2_form below), all rotating each
  * amplitude pair by three in-place shears:
- *   PHASE2_FORM_LIFTED (default)  coefficients from FP64 cos/sin, FP64
+ *   PHASE2_FORM_LIFTED            coefficients from FP64 cos/sin, FP64
  *                                 arithmetic, one rounding to FP32 per pass;
  *   PHASE2_FORM_LIFTED_F32        FP32 FMAs on coefficients rounded to FP32
- *                                 (faster; one rounding per shear).
- * Also PHASE2_FP32_FORM=lifted|lifted_f32 at world_init.  Applies to
+ *                                 (faster; one rounding per shear);
+ *   PHASE2_FORM_LIFTED_MIXED      (default) per coset of a pass: FP32
+ *                                 arithmetic as LIFTED_F32, except cosets
+ *                                 holding an amplitude of magnitude
+ *                                 >= 2^-10 (re or im) when the pass starts,
+ *                                 which take FP64 arithmetic and one
+ *                                 rounding per pass.
+ * An FP32 shear absorbs increments below half an ulp of the amplitude it
+ * updates, so LIFTED_F32 loses the small updates of large amplitudes; the
+ * mixed form keeps FP64 arithmetic for those.  Registers of fewer than 24
+ * qubits (whose spread states have many such amplitudes), the persistent
+ * batch kernel and device sampling run mixed-form programs with FP64
+ * arithmetic on every coset; sweeps are off in this form.
+ * Also PHASE2_FP32_FORM=lifted|lifted_f32|mixed at world_init.  Applies to
  * rotations planned afterwards.  0 or -1. */
 int phase2_set_fp32_form(int form);
 int phase2_get_fp32_form(void);
@@ -409,6 +421,9 @@ enum phase2_form {
 				     * arithmetic */
 	PHASE2_FORM_LIFTED_F32 = 2, /* FP32 state, records of form 1 with FP32
 				     * s, FP32 arithmetic */
+	PHASE2_FORM_LIFTED_MIXED = 3, /* records as LIFTED_F32; FP32
+				       * arithmetic, FP64 on cosets with an
+				       * amplitude >= 2^-10 */
 };
 
 /* Rotation record in slot coordinates: the partner of slot u is u ^ U; the
@@ -422,8 +437,9 @@ enum phase2_form {
  *     q_u = (+-1)(odd ? i : 1), q_w = -conj(q_u), t = (1 - cos phi) / s
  *     held in `c`; a rotation with cos(phi) < 0 is stored as
  *     exp(i(phi -+ pi)P) and the pass negates every amplitude once per such
- *     rotation (`scale` = +-1).  For PHASE2_FORM_LIFTED_F32 passes s is an
- *     FP32 value and t is taken against it. */
+ *     rotation (`scale` = +-1).  For PHASE2_FORM_LIFTED_F32 and
+ *     PHASE2_FORM_LIFTED_MIXED passes s is an FP32 value and t is taken
+ *     against it. */
 struct phase2_rot_rec {
 	uint64_t z;
 	double c, s;
@@ -436,7 +452,7 @@ struct phase2_rot_rec {
 };
 
 /* Plan n rotations for an nqb-qubit register of precision prec (FP64:
- * exact form; FP32: the process's FP32 form, lifted by default).  Writes at most n passes and n records;
+ * exact form; FP32: the process's FP32 form, mixed by default).  Writes at most n passes and n records;
  * returns the number of passes, or -1. */
 long phase2_plan(uint32_t nqb, const struct phase2_rot_in *rots, size_t n,
 	int max_span, int max_rots, int prec, struct phase2_pass *passes,

@@ -26,7 +26,7 @@ __all__ = ["run", "world_ensure", "Register", "Terms", "Dets", "trott",
 
 PREC_FP64 = _ffi.PREC_FP64
 PREC_FP32 = _ffi.PREC_FP32
-FORM_EXACT, FORM_LIFTED, FORM_LIFTED_F32 = 0, 1, 2
+FORM_EXACT, FORM_LIFTED, FORM_LIFTED_F32, FORM_LIFTED_MIXED = 0, 1, 2, 3
 _WORLD_SEED = 0x2B200C0DE5EED001
 
 
@@ -66,9 +66,12 @@ def set_precision(prec: int) -> None:
 
 
 def set_fp32_form(form: int) -> None:
-    """Arithmetic of FP32 passes: FORM_LIFTED (default: coefficients from
-    FP64 cos/sin, FP64 arithmetic, one rounding to FP32 per pass) or
-    FORM_LIFTED_F32 (FP32 FMAs on FP32 coefficients)."""
+    """Arithmetic of FP32 passes: FORM_LIFTED_MIXED (default: FP32 FMAs,
+    except cosets holding an amplitude >= 2^-10, which take FP64
+    arithmetic and one rounding per pass; registers below 24 qubits FP64
+    arithmetic throughout), FORM_LIFTED (coefficients from FP64 cos/sin,
+    FP64 arithmetic, one rounding to FP32 per pass) or FORM_LIFTED_F32
+    (FP32 FMAs on FP32 coefficients)."""
     if lib().phase2_set_fp32_form(form) != 0:
         raise ValueError(f"bad FP32 form {form}")
 

@@ -622,12 +622,14 @@ extern "C" unsigned int phase2_get_batch_runs(void)
 }
 
 /* k_batch for FP32 or FP64 registers: its kernel function (occupancy
- * queries) and its launch. */
+ * queries) and its launch.  Mixed-form programs run on the FP64-arithmetic
+ * instance (every coset in FP64; their records are the FP32 form's). */
 int p2_batch_kind(int prec, int form)
 {
 	if (prec == PHASE2_PREC_FP64)
 		return P2_BK_F64;
-	return form == PHASE2_FORM_LIFTED ? P2_BK_F32X : P2_BK_F32;
+	return form == PHASE2_FORM_LIFTED || form == PHASE2_FORM_LIFTED_MIXED
+		? P2_BK_F32X : P2_BK_F32;
 }
 
 const void *p2_batch_kernel(int kind)

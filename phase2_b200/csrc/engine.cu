@@ -260,6 +260,187 @@ __global__ void __launch_bounds__(P2_TPB, p2_lift32_blocks(M))
 			pb, srec, nrot, negm);
 }
 
+/* ---- mixed form: FP32 arithmetic, FP64 on heavy cosets ------------------ */
+
+/* A coset is heavy when one of its amplitudes has |re| or |im| >= this at
+ * the start of the pass.  Below it, the absolute error of an FP32 shear
+ * (half an ulp) is at most 2^-35. */
+#define P2_HEAVY_MIN 0x1p-10f
+
+/* Registers below this many qubits run mixed-form passes on the FP64-
+ * arithmetic kernels: a spread state of n qubits has components of
+ * standard deviation 2^-(n+1)/2, which reach P2_HEAVY_MIN often below 24
+ * qubits (at 22, a quarter of the cosets), and a heavy coset costs its
+ * warp a serial FP64 run; at 24 the threshold is 5.7 deviations away. */
+#define P2_MIXED_MIN_QB 24
+
+/*
+ * The run of rotations on one coset held in shared memory as FP64 (hv: 2^M
+ * slots), by the whole warp: lane j rotates pair j (slot u with a zero at
+ * the top bit of U, and u ^ U) by the three shears of p2_rot_lift32 in FP64
+ * FMAs, or slot j when the string is diagonal on the coset (U = 0).  t is
+ * the record's FP64 t and s its FP32 s (exact in FP64); x is the coset's
+ * representative (the signs).  Every lane of the warp calls it.
+ */
+template <int M, typename IT>
+__device__ __forceinline__ void p2_heavy_run(double2 *hv, IT x,
+	const struct p2_lift32_rec *srec, const double *tt, uint32_t nrot,
+	uint32_t lane)
+{
+	for (uint32_t r = 0; r < nrot; ++r) {
+		const struct p2_lift32_rec q = srec[r];
+		const uint32_t sm = q.sm ^ (0u - p2_parity(x & (IT)q.z));
+		const uint32_t U = q.key >> 1, odd = q.key & 1u;
+		const double t = tt[r], s = (double)q.s;
+		if (U == 0) {
+			if (lane < (1u << M)) {
+				const uint32_t b = p2_bitmask(sm, (int)lane);
+				const double st = p2_sgn(t, b), ss = p2_sgn(s, b);
+				double2 y = hv[lane];
+				if (odd) {
+					y.x = fma(-st, y.y, y.x);
+					y.y = fma(ss, y.x, y.y);
+					y.x = fma(-st, y.y, y.x);
+				} else {
+					const double k = ss + fma(-t, s, 1.0);
+					y.x *= k;
+					y.y *= k;
+				}
+				hv[lane] = y;
+			}
+		} else if (M > 0 && U < (1u << M) &&
+			lane < (1u << (M > 0 ? M - 1 : 0))) {
+			const uint32_t h = 31u - (uint32_t)__clz(U);
+			const uint32_t u = ((lane >> h) << (h + 1)) |
+				(lane & ((1u << h) - 1u));
+			const uint32_t w = u ^ U;
+			const uint32_t b = p2_bitmask(sm, (int)u);
+			const double st = p2_sgn(t, b), ss = p2_sgn(s, b);
+			double2 yu = hv[u], yw = hv[w];
+			if (odd) {
+				yu.x = fma(-st, yw.y, yu.x);
+				yu.y = fma(st, yw.x, yu.y);
+				yw.x = fma(-ss, yu.y, yw.x);
+				yw.y = fma(ss, yu.x, yw.y);
+				yu.x = fma(-st, yw.y, yu.x);
+				yu.y = fma(st, yw.x, yu.y);
+			} else {
+				yu.x = fma(st, yw.x, yu.x);
+				yu.y = fma(st, yw.y, yu.y);
+				yw.x = fma(-ss, yu.x, yw.x);
+				yw.y = fma(-ss, yu.y, yw.y);
+				yu.x = fma(st, yw.x, yu.x);
+				yu.y = fma(st, yw.y, yu.y);
+			}
+			hv[u] = yu;
+			hv[w] = yw;
+		}
+		__syncwarp();
+	}
+}
+
+/*
+ * One FP32 pass in the mixed form.  Each thread loads its coset into FP32
+ * registers (as k_pass_lift32); a thread whose coset holds an amplitude of
+ * magnitude >= P2_HEAVY_MIN hands it to its warp, which rotates it in FP64
+ * in shared memory (p2_heavy_run) and rounds once; the other threads apply
+ * the run with FP32 FMAs, the same bits as k_pass_lift32.  The warps walk
+ * the cosets 32 at a time, so every lane is present for the heavy runs.
+ */
+template <int M, typename IT>
+__global__ void __launch_bounds__(P2_TPB, p2_lift32_blocks(M))
+	k_pass_lift32h(float2 *__restrict__ st, uint64_t nrep,
+		struct phase2_pass p,
+		const struct phase2_rot_rec *__restrict__ recs)
+{
+	constexpr int S = 1 << M;
+	constexpr unsigned FULL = 0xffffffffu;
+	__shared__ struct p2_lift32_rec srec[P2_MAX_ROTS_PER_PASS];
+	__shared__ double tt[P2_MAX_ROTS_PER_PASS];
+	__shared__ double2 hv_all[P2_TPB / 32][S];
+	for (uint32_t r = threadIdx.x; r < p.nrot; r += blockDim.x) {
+		srec[r] = p2_lift32_of(recs[p.rot_off + r]);
+		tt[r] = recs[p.rot_off + r].c;
+	}
+	__syncthreads();
+	IT pb[M > 0 ? M : 1];
+#pragma unroll
+	for (int k = 0; k < M; ++k)
+		pb[k] = (IT)p.basis[k];
+	const uint32_t negm = p.scale < 0 ? 0x80000000u : 0u;
+	const uint32_t nrot = p.nrot;
+	const uint32_t lane = threadIdx.x & 31u;
+	double2 *const hv = hv_all[threadIdx.x >> 5];
+
+	const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+	for (uint64_t t0 = (uint64_t)blockIdx.x * blockDim.x +
+			(threadIdx.x & ~31u);
+		t0 < nrep; t0 += stride) {
+		const uint64_t t = t0 + lane;
+		const bool active = t < nrep;
+		const IT x = p2_rep_t<M, IT>((IT)t, p);
+		float re[S], im[S];
+		float mx = 0.f;
+#pragma unroll
+		for (int u = 0; u < S; ++u) {
+			IT off = 0;
+#pragma unroll
+			for (int k = 0; k < M; ++k)
+				if (u >> k & 1)
+					off ^= pb[k];
+			const float2 v = active ? st[x ^ off]
+						: make_float2(0.f, 0.f);
+			re[u] = v.x;
+			im[u] = v.y;
+			mx = fmaxf(mx, fmaxf(fabsf(v.x), fabsf(v.y)));
+		}
+		const bool heavy = active && mx >= P2_HEAVY_MIN;
+		unsigned hm = __ballot_sync(FULL, heavy);
+		while (hm) {
+			const int src = __ffs(hm) - 1;
+			hm &= hm - 1;
+			const IT hx = __shfl_sync(FULL, x, src);
+			if (lane == (uint32_t)src) {
+#pragma unroll
+				for (int u = 0; u < S; ++u)
+					hv[u] = make_double2((double)re[u],
+						(double)im[u]);
+			}
+			__syncwarp();
+			p2_heavy_run<M, IT>(hv, hx, srec, tt, nrot, lane);
+			if (lane == (uint32_t)src) {
+#pragma unroll
+				for (int u = 0; u < S; ++u) {
+					re[u] = __double2float_rn(hv[u].x);
+					im[u] = __double2float_rn(hv[u].y);
+				}
+			}
+			__syncwarp();
+		}
+		if (active && !heavy) {
+			for (uint32_t r = 0; r < nrot; ++r) {
+				const struct p2_lift32_rec q = srec[r];
+				const uint32_t sm =
+					q.sm ^ (0u - p2_parity(x & (IT)q.z));
+				p2_apply_lift32<M>(q, re, im, sm);
+			}
+		}
+		if (active) {
+			const IT xs = p2_opaque(x);
+#pragma unroll
+			for (int u = 0; u < S; ++u) {
+				IT off = 0;
+#pragma unroll
+				for (int k = 0; k < M; ++k)
+					if (u >> k & 1)
+						off ^= pb[k];
+				st[xs ^ off] = make_float2(p2_fsgn(re[u], negm),
+					p2_fsgn(im[u], negm));
+			}
+		}
+	}
+}
+
 /* ---- small kernels ------------------------------------------------------ */
 
 template <typename ST>
@@ -936,7 +1117,18 @@ static int launch_lift_t(struct p2_dev *d, const struct phase2_pass &p,
 		else
 			k_pass_lift32<M, uint64_t>
 				<<<grid, P2_TPB, 0, d->stream>>>(sv, nrep, p, recs);
-	} else if (p.form == PHASE2_FORM_LIFTED) {
+	} else if (p.form == PHASE2_FORM_LIFTED_MIXED &&
+		d->nqb >= P2_MIXED_MIN_QB) {
+		if (narrow)
+			k_pass_lift32h<M, uint32_t>
+				<<<grid, P2_TPB, 0, d->stream>>>(sv, nrep, p, recs);
+		else
+			k_pass_lift32h<M, uint64_t>
+				<<<grid, P2_TPB, 0, d->stream>>>(sv, nrep, p, recs);
+	} else if (p.form == PHASE2_FORM_LIFTED ||
+		p.form == PHASE2_FORM_LIFTED_MIXED) {
+		/* mixed-form passes of smaller registers: FP64 arithmetic on
+		 * every coset (their records are the FP32 form's) */
 		/* variants 1 and 2: the next cosets staged in shared memory by
 		 * bulk copies or cp.async (lift_bulk.cu), where the pass
 		 * qualifies */

@@ -445,7 +445,9 @@ extern "C" int p2_lift_staged_launch(struct p2_dev *d,
 	int variant, unsigned per_sm_cap)
 {
 	/* whole warp-cosets of 32-bit indices, every pivot at bit 5 or above */
-	if (d->prec != PHASE2_PREC_FP32 || p->form != PHASE2_FORM_LIFTED ||
+	if (d->prec != PHASE2_PREC_FP32 ||
+		(p->form != PHASE2_FORM_LIFTED &&
+			p->form != PHASE2_FORM_LIFTED_MIXED) ||
 		d->nqb > 31 || p->span < 3 || p->span > 5 ||
 		d->nqb < p->span + 5 || p->piv[0] < 5)
 		return 0;

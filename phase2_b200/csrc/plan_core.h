@@ -211,7 +211,8 @@ P2_HD int p2_rec_fill(const struct phase2_pass *pass, uint64_t flip,
 	rec->s = s;
 	const int form = pass->form;
 	int neg = 0;
-	if (form == PHASE2_FORM_LIFTED || form == PHASE2_FORM_LIFTED_F32) {
+	if (form == PHASE2_FORM_LIFTED || form == PHASE2_FORM_LIFTED_F32 ||
+		form == PHASE2_FORM_LIFTED_MIXED) {
 		/* Three shears per pair (no temporaries, no pass-wide factor):
 		 * t = tan(phi/2) = s / (1 + c), computed with c >= 0 so it
 		 * stays in [-1, 1]; for c < 0 the rotation is
@@ -222,7 +223,8 @@ P2_HD int p2_rec_fill(const struct phase2_pass *pass, uint64_t flip,
 			neg = 1;
 		}
 		rec->form = 1;
-		if (form == PHASE2_FORM_LIFTED_F32) {
+		if (form == PHASE2_FORM_LIFTED_F32 ||
+			form == PHASE2_FORM_LIFTED_MIXED) {
 			lift_f32(c, s, &rec->c, &rec->s);
 		} else {
 			rec->c = s / (1.0 + c);

@@ -17,7 +17,7 @@ struct p2_settings p2_cfg = {
 	.max_span = PHASE2_MAX_SPAN,
 	.max_rots = 0,
 	.order = PHASE2_ORDER_LEX,
-	.fp32_form = PHASE2_FORM_LIFTED,
+	.fp32_form = PHASE2_FORM_LIFTED_MIXED,
 	.batch_persistent = 1,
 	.device_sampling = PHASE2_DEVICE_SAMPLING_AUTO,
 };
@@ -39,6 +39,8 @@ void p2_settings_from_env(void)
 			p2_cfg.fp32_form = PHASE2_FORM_LIFTED;
 		else if (!strcmp(f, "lifted_f32"))
 			p2_cfg.fp32_form = PHASE2_FORM_LIFTED_F32;
+		else if (!strcmp(f, "mixed"))
+			p2_cfg.fp32_form = PHASE2_FORM_LIFTED_MIXED;
 		else
 			log_warn("PHASE2_FP32_FORM=%s not understood", f);
 	}
@@ -57,7 +59,8 @@ void p2_settings_from_env(void)
 
 int phase2_set_fp32_form(int form)
 {
-	if (form != PHASE2_FORM_LIFTED && form != PHASE2_FORM_LIFTED_F32)
+	if (form != PHASE2_FORM_LIFTED && form != PHASE2_FORM_LIFTED_F32 &&
+		form != PHASE2_FORM_LIFTED_MIXED)
 		return -1;
 	p2_cfg.fp32_form = form;
 	return 0;

@@ -250,8 +250,25 @@ def test_planner_emulation_bit_exact(n, span, max_rots, oracle_lib):
     assert np.array_equal(got, want)
 
 
+def test_fp32_form_setting():
+    """The three FP32 forms are accepted, anything else refused."""
+    old = p2.get_fp32_form()
+    try:
+        for form in (p2.FORM_LIFTED, p2.FORM_LIFTED_F32,
+                     p2.FORM_LIFTED_MIXED):
+            p2.set_fp32_form(form)
+            assert p2.get_fp32_form() == form
+        for bad in (p2.FORM_EXACT, 4, -1):
+            with pytest.raises(ValueError):
+                p2.set_fp32_form(bad)
+        assert p2.get_fp32_form() == p2.FORM_LIFTED_MIXED
+    finally:
+        p2.set_fp32_form(old)
+
+
 @pytest.mark.parametrize("n", [2, 6, 11])
-@pytest.mark.parametrize("form", [p2.FORM_LIFTED, p2.FORM_LIFTED_F32])
+@pytest.mark.parametrize("form", [p2.FORM_LIFTED, p2.FORM_LIFTED_F32,
+                                  p2.FORM_LIFTED_MIXED])
 def test_planner_fp32_forms(n, form, oracle_lib):
     """FP32 plans (lifted shears with a pass-wide sign) reproduce the
     oracle when executed in FP64: to FP64 rounding with FP64 coefficients,

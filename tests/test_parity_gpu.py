@@ -46,8 +46,9 @@ def _rand_rots(rng, n, k, diag_frac=0.2):
     return t.flip, t.phase, rng.uniform(-math.pi, math.pi, k)
 
 
-@pytest.fixture(params=[p2.FORM_LIFTED_F32, p2.FORM_LIFTED],
-                ids=["f32arith", "f64arith"])
+@pytest.fixture(params=[p2.FORM_LIFTED_F32, p2.FORM_LIFTED,
+                        p2.FORM_LIFTED_MIXED],
+                ids=["f32arith", "f64arith", "mixed"])
 def fp32_form(request):
     """Run an FP32 test under each FP32 arithmetic form."""
     old = p2.get_fp32_form()

@@ -58,7 +58,8 @@ def _run(prec, form, fn, *args, **kw):
 
 CASES = [("fp64", p2.PREC_FP64, p2.FORM_LIFTED_F32),
          ("fp32_f32arith", p2.PREC_FP32, p2.FORM_LIFTED_F32),
-         ("fp32_f64arith", p2.PREC_FP32, p2.FORM_LIFTED)]
+         ("fp32_f64arith", p2.PREC_FP32, p2.FORM_LIFTED),
+         ("fp32_mixed", p2.PREC_FP32, p2.FORM_LIFTED_MIXED)]
 
 
 @pytest.mark.parametrize("name,prec,form", CASES, ids=[c[0] for c in CASES])
