@@ -299,6 +299,29 @@ def test_planner_fp32_forms(n, form, oracle_lib):
     assert np.max(np.abs(got - want)) < tol * np.max(np.abs(want))
 
 
+@pytest.mark.parametrize("n", [6, 24])
+def test_mixed_plan_is_the_f32_plan(n):
+    """The mixed form's kernel rotates light cosets from the FP32 form's
+    records and heavy ones from the same records in FP64: its plan must be
+    the FP32-arithmetic form's, record for record, with only each pass's
+    form changed."""
+    rng = np.random.Generator(np.random.PCG64(700 + n))
+    flip, phase, phi = _rand_rotations(rng, n, 120)
+    old = p2.get_fp32_form()
+    try:
+        p2.set_fp32_form(p2.FORM_LIFTED_F32)
+        pf, rf = plan(n, flip, phase, phi, 5, 0, prec=1)
+        p2.set_fp32_form(p2.FORM_LIFTED_MIXED)
+        pm, rm = plan(n, flip, phase, phi, 5, 0, prec=1)
+    finally:
+        p2.set_fp32_form(old)
+    assert rm == rf
+    assert {p["form"] for p in pm} == {p2.FORM_LIFTED_MIXED}
+    for a, b in zip(pm, pf):
+        assert dict(a, form=0) == dict(b, form=0)
+    assert len(pm) == len(pf)
+
+
 def test_planner_fuses_jw_runs():
     t = workloads.jw_terms(20, 2000, seed=4)
     phi = np.full(len(t), 0.01)
